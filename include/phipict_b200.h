@@ -1,0 +1,211 @@
+/*
+ * phipict_b200 C ABI: the B200 (sm_100a) PISO/MHD step behind phiPICT's backend
+ * protocol. Every entry point takes plain pointers and sizes, launches on the given
+ * CUDA stream, never synchronises the device and returns 0 on success or a negative
+ * phb_status code. No torch type crosses this boundary.
+ *
+ * Each declaration names the phiPICT binding it replaces (csrc/phipict/bindings.cpp
+ * and the kernel it wraps). The Python mirror of the reference API lives in
+ * phipict_b200/_C.py; INTEGRATION.md shows the ctypes binding.
+ *
+ * Data layout (all device memory):
+ *   - cells of all instances are concatenated: instance i owns cells
+ *     [insts[i].cellOff, insts[i].cellOff + insts[i].ncells), blocks x-fastest inside;
+ *     a batch of B environments of one domain is B instances, so scalar fields are
+ *     [B][ncells] and vector fields [B][dims][ncells], as in phiPICT.
+ *   - matrices are stored as stencils: value[slot][cell], slot 0 the diagonal,
+ *     slot f+1 the neighbour across face f (-x,+x,-y,+y,-z,+z); prescribed faces hold 0.
+ *     CSR (phiPICT's CSRmatrix) is produced on demand by phb_csr_pattern/phb_csr_gather.
+ *   - cell metrics are SoA: metrics[k * metric_stride + m], k over {M (d*d), Minv (d*d), det}.
+ */
+#ifndef PHIPICT_B200_H
+#define PHIPICT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void *phb_stream; /* cudaStream_t */
+
+enum phb_status {
+	PHB_OK = 0,
+	PHB_ERR_ARG = -1,      /* invalid argument (null pointer, bad size or dtype) */
+	PHB_ERR_CUDA = -2,     /* a CUDA runtime call failed; see phb_last_error() */
+	PHB_ERR_RANGE = -3,    /* a size exceeds a documented maximum */
+	PHB_ERR_STATE = -4     /* an object was used before it was initialised */
+};
+
+enum phb_dtype { PHB_F32 = 0, PHB_F64 = 1 };
+
+/* record sizes (int32 words) */
+#define PHB_BREC 48   /* block record  */
+#define PHB_FREC 16   /* fixed-face record */
+#define PHB_IREC 8    /* instance record */
+#define PHB_TILE 256  /* cells per tile (one CTA of the per-cell kernels) */
+
+/* Domain descriptor: device pointers produced by Domain.PrepareSolve(). It plays the
+ * part of phiPICT's DomainGPU/BlockGPU atlas (domain/domain_structs_gpu.h:168-447). */
+typedef struct phb_domain {
+	int32_t dims;           /* 2 or 3 */
+	int32_t dtype;          /* phb_dtype of fields and metrics */
+	int32_t nblocks, ninst, ntiles, nfixed;
+	int64_t ncells;         /* cells of all instances */
+	int64_t metric_stride;  /* cells in the metric array */
+	int64_t face_metric_stride;
+	const int32_t *blocks;  /* [nblocks][PHB_BREC] */
+	const int32_t *tiles;   /* [ntiles][2] = (block, first local cell) */
+	const int32_t *fixed;   /* [nfixed][PHB_FREC] */
+	const int32_t *insts;   /* [ninst][PHB_IREC] */
+	const void *metrics;    /* [2d^2+1][metric_stride] */
+	const void *face_metrics; /* [2d^2+1][face_metric_stride] */
+	const void *fvel;       /* fixed-face velocities */
+	const void *fpot;       /* fixed-face potential values */
+	const void *fcw;        /* [nfixed] wall conductance ratio */
+	const int8_t *fmask;    /* fixed-face potential BC masks */
+	const double *dt;       /* [ninst] time step */
+	const double *nu;       /* [ninst] viscosity */
+} phb_domain;
+
+const char *phb_last_error(void);
+int phb_version(void);
+
+/* --- grid metrics ------------------------------------------------------------------
+ * Replaces CoordsToTransforms / CoordsToFaceTransforms (grid/grid_gen.cu:299-396,
+ * 398-496, bound through Block::setVertexCoordinates, domain/block.cpp:1005-1010).
+ * coords: [dims][vz][vy][vx] vertices of one block. cell_out: SoA metric slice of the
+ * block (stride metric_stride); face_out: SoA metrics of the cells of one face. */
+int phb_cell_metrics(int dims, int dtype, int nx, int ny, int nz, const void *coords,
+                     void *cell_out, int64_t stride, phb_stream stream);
+int phb_face_metrics(int dims, int dtype, int nx, int ny, int nz, const void *coords, int face,
+                     void *face_out, int64_t stride, phb_stream stream);
+
+/* --- assembly (one launch each, all instances) ------------------------------------- */
+/* SetupAdvectionMatrix (bindings.cpp:639, advection.cu:27-305 PISO_build_matrix).
+ * u: block velocity [inst][dims][cells]; C: stencil [2d+1][ncells]; Adiag [ncells].
+ * C_lo (optional, may be NULL): float32 copy of C for mixed-precision inner solves. */
+int phb_advection_matrix(const phb_domain *dom, const void *u, void *C, void *Adiag, float *C_lo, phb_stream stream);
+/* SetupAdvectionVelocity (bindings.cpp:645, advection.cu:800-954). src: velocity source,
+ * src_mode 0 none, 1 static per instance [inst][dims], 2 per cell [inst][dims][cells]. */
+int phb_advection_rhs(const phb_domain *dom, const void *u, const void *src, int src_mode, void *rhs, phb_stream stream);
+/* SetupPressureMatrix (pressure.cu:26-191). P: stencil [2d+1][ncells]. */
+int phb_pressure_matrix(const phb_domain *dom, const void *Adiag, void *P, float *P_lo, phb_stream stream);
+/* SetupPressureRHS (pressure.cu:350-521, then :756-801): HbyA [inst][dims][cells] and its
+ * flux divergence div [ncells]. ustar: current velocity iterate (velocityResult). */
+int phb_pressure_rhs(const phb_domain *dom, const void *C, const void *Adiag, const void *u, const void *ustar,
+                     const void *src, int src_mode, void *hbya, phb_stream stream);
+int phb_divergence(const phb_domain *dom, const void *field, void *div, phb_stream stream);
+/* CorrectVelocity version 1 (velocity_correction.cu:27-60): u = HbyA - grad(p)/A. */
+int phb_correct_velocity(const phb_domain *dom, const void *p, const void *hbya, const void *Adiag, void *u, phb_stream stream);
+/* SetupEpotMatrix (mhd/potential.cu:30-233). */
+int phb_epot_matrix(const phb_domain *dom, void *E, float *E_lo, phb_stream stream);
+/* ComputeEpotRHS (mhd/potential.cu:273-366) fused with u x e_b (simulation/mhd.py:276-355):
+ * writes uxb [inst][3][cells] and rhs [ncells]. e_b: [inst][3] (double). */
+/* ComputeEpotRHS of a given in-plane field [inst][dims][cells] (bindings.cpp:667-689). */
+int phb_epot_rhs(const phb_domain *dom, const void *field, void *rhs, phb_stream stream);
+int phb_uxb_epot_rhs(const phb_domain *dom, const void *u, const double *e_b, void *uxb, void *rhs, phb_stream stream);
+/* ComputeCurrentDensityFaceBased (mhd/potential.cu:718-916) fused with the Lorentz force
+ * of simulation/mhd.py:543-595: J [inst][3][cells]; src[inst][dims][cells] =
+ * N (J x e_b)[:dims] + (accumulate ? src : 0). stuart: [inst] (double). */
+int phb_current_lorentz(const phb_domain *dom, const void *phi, const void *uxb, const double *e_b,
+                        const double *stuart, void *J, void *src, int accumulate, phb_stream stream);
+
+/* --- vectors ------------------------------------------------------------------------ */
+/* Per-instance reductions use a caller-owned scratch of phb_scratch_doubles() doubles whose
+ * first word must be zero before the first call (each call leaves it zero again).
+ * subtract_env_mean / _subtract_env_mean (piso_simulation.py:68-89, mhd.py:112-121):
+ * x[inst][comps][cells] -= the mean of each instance's component. */
+int64_t phb_scratch_doubles(const phb_domain *dom, int comps);
+int phb_subtract_mean(const phb_domain *dom, void *x, int comps, double *scratch, phb_stream stream);
+/* RMS of each instance's slice of v over all comps (the right-hand-side scale ||b||/sqrt(n)
+ * of SolverTolerance, solvers/tolerance.py:116-140); out: [ninst] */
+int phb_rms(const phb_domain *dom, const void *v, int comps, double *scratch, double *out, phb_stream stream);
+
+/* --- CSR export (phiPICT CSRmatrix view of a stencil matrix) ----------------------- */
+/* Row pointers and columns of the shared pattern of instance 0's geometry, entries sorted
+ * by column as PISO_build_matrix writes them; perm[k] = slot*ncells + cell of entry k.
+ * row: [ncells+1] (filled on device), col/perm: [nnz]. */
+int phb_csr_row_sizes(const phb_domain *dom, int32_t *rowsize, phb_stream stream);
+int phb_csr_pattern(const phb_domain *dom, const int32_t *row, int32_t *col, int32_t *perm, phb_stream stream);
+int phb_csr_gather(int dtype, int64_t nnz, const int32_t *perm, const void *stencil, void *value, phb_stream stream);
+
+/* --- Krylov solvers (SolveLinear, solvers/linear_solve.cu:22-162 and the fused kernels
+ *     of solvers/krylov/krylov.cu:252-1186) ----------------------------------------- */
+/* Tolerance of a solve, in the units of the stop test ||r||_2/sqrt(n) < tol.
+ * mode 0: the constant atol for every system (phiPICT's plain float tolerance);
+ * mode 1: SolverTolerance.resolve (solvers/tolerance.py:180-257) per instance, from the
+ *         right-hand side b of the solve: tol = max(rtol*s, atol, floor_eps*s), s =
+ *         ||b_inst||_2/sqrt(n_inst*nrhs), and `fallback` when that is 0 (rtol or atol <= 0
+ *         means "not given");
+ * mode 2: per-system values from `values` [ninst*nrhs]. */
+typedef struct phb_tolerance {
+	int32_t mode;
+	int32_t pad;
+	double rtol, atol, floor_eps, fallback;
+	const double *values;
+} phb_tolerance;
+
+typedef struct phb_solve {
+	int32_t kind;         /* 0 CG, 1 BiCGStab */
+	int32_t vec_dtype;    /* phb_dtype of the Krylov vectors */
+	int32_t mat_dtype;    /* phb_dtype of the stencil matrix */
+	int32_t nrhs;         /* right-hand sides per instance sharing its matrix (1..3) */
+	int32_t maxit;
+	int32_t return_best;  /* CG only: keep the iterate with the lowest residual */
+	int32_t use_graph;    /* 1: conditional-WHILE CUDA graph; 0: host loop */
+	int32_t check_every;  /* host loop only: iterations between completion checks */
+	phb_tolerance tol;
+	const void *A;        /* stencil [2d+1][ncells] */
+	const void *b;        /* [inst][nrhs][cells] */
+	void *x;              /* in: initial guess, out: solution */
+	void *work;           /* >= phb_solve_work_bytes() bytes, 256-byte aligned */
+	void *state;          /* >= phb_solve_state_bytes() bytes */
+} phb_solve;
+
+/* per-system result, mirrors LinearSolverResultInfo (bindings.cpp:727-732) */
+typedef struct phb_solve_result {
+	double final_residual;
+	int32_t used_iterations;
+	int32_t converged;
+	int32_t finite;
+	int32_t status;       /* 1 converged, 2 non-finite, 3 max iterations, 4 rising */
+} phb_solve_result;
+
+int64_t phb_solve_work_bytes(const phb_domain *dom, int kind, int vec_dtype, int nrhs);
+int64_t phb_solve_state_bytes(const phb_domain *dom, int nrhs);
+int phb_solve_run(const phb_domain *dom, const phb_solve *s, phb_stream stream);
+/* copies the per-system results to host (synchronises the stream) */
+int phb_solve_results(const phb_domain *dom, const phb_solve *s, phb_solve_result *out, phb_stream stream);
+/* drops cached solver graphs (ReleaseKrylovWorkspaces, bindings.cpp:775) */
+int phb_release_graphs(void);
+
+/* Mixed precision: FP64 outer iterative refinement around FP32 inner Krylov solves.
+ * A64/A32: the system in float64 and its float32 copy; b/x float64. The outer loop stops
+ * when ||b - A64 x||/sqrt(n) < tol for every system or after max_outer sweeps; inner
+ * solves run to inner_rtol relative to their own right-hand side. */
+typedef struct phb_refine {
+	int32_t kind;         /* inner solver: 0 CG, 1 BiCGStab */
+	int32_t nrhs;
+	int32_t max_outer;
+	int32_t inner_maxit;
+	double inner_rtol;
+	phb_tolerance tol;    /* outer tolerance, on the float64 residual */
+	const double *A64;
+	const float *A32;
+	const double *b;
+	double *x;
+	void *work;           /* >= phb_refine_work_bytes() */
+	void *state;          /* >= phb_solve_state_bytes() */
+} phb_refine;
+int64_t phb_refine_work_bytes(const phb_domain *dom, int kind, int nrhs);
+/* out (optional): per-system outer results, as phb_refine_results (synchronises) */
+int phb_refine_run(const phb_domain *dom, const phb_refine *r, phb_solve_result *out, int *outer_used, phb_stream stream);
+/* per-system outer results of the last refinement (synchronises the stream) */
+int phb_refine_results(const phb_domain *dom, const phb_refine *r, phb_solve_result *out, int *outer_used, phb_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,238 @@
+"""Backend protocol of the PISO step: the functions phiPICT's simulation driver calls on
+its ``_C`` module (csrc/phipict/bindings.cpp:639-815), with the same names, arguments and
+in-place semantics, implemented on the phipict_b200 CUDA kernels.
+
+Every function launches on torch's current CUDA stream and returns without synchronising
+the device (phiPICT's launchers call ``cudaDeviceSynchronize()`` around every kernel,
+e.g. piso/advection.cu:1217,1225). Matrices live in stencil form on the domain
+(``domain._C_st`` etc.); ``domain.C``/``domain.P``/``domain.Epot`` are CSR views of them.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+
+import torch
+
+from . import _lib
+from .domain import CSRmatrix, Domain
+from .solvers import BICGSTAB, CG, LinearSolverResultInfo, solver_for
+
+NON_ORTHO_DIRECT_MATRIX = 1
+NON_ORTHO_DIRECT_RHS = 2
+NON_ORTHO_DIAGONAL_MATRIX = 4
+NON_ORTHO_DIAGONAL_RHS = 8
+NON_ORTHO_CENTER_MATRIX = 16
+
+
+def _check(domain: Domain) -> None:
+    if domain.getNumBlocks() == 0:
+        raise RuntimeError("Domain does not contain blocks.")
+    if not domain.IsInitialized():
+        raise RuntimeError("Domain is not initialized.")
+
+
+def _no_nonortho(flags) -> None:
+    if int(flags) != 0:
+        raise NotImplementedError("phipict_b200 assembles the orthogonal discretization (non-orthogonal flags must be 0)")
+
+
+def _S(domain: Domain) -> int:
+    return _lib.stream_ptr(domain.getDevice())
+
+
+def _lo(domain: Domain, which: str) -> torch.Tensor | None:
+    """The float32 shadow of a float64 stencil matrix (mixed precision), if enabled."""
+    if not getattr(domain, "_mixed", False):
+        return None
+    key = "_" + which + "_lo"
+    t = getattr(domain, key, None)
+    st = domain._stencil(which)
+    if t is None or t.shape != st.shape:
+        t = torch.empty(st.shape, dtype=torch.float32, device=st.device)
+        setattr(domain, key, t)
+    return t
+
+
+def _src(domain: Domain) -> tuple[int | None, int]:
+    return (domain._src.data_ptr() if domain._src is not None else None), domain._src_mode
+
+
+# --- momentum ---------------------------------------------------------------------------
+def SetupAdvectionMatrix(domain: Domain, timeStep, nonOrthoFlags=0, forPassiveScalar: bool = False,
+                         passiveScalarChannel: int = 0) -> None:
+    """Implicit Euler advection-diffusion matrix C and its diagonal A (advection.cu:27-305)."""
+    _check(domain)
+    _no_nonortho(nonOrthoFlags)
+    if forPassiveScalar:
+        raise NotImplementedError("passive scalar advection is not implemented by phipict_b200")
+    domain.setTimeStep(timeStep)
+    lo = _lo(domain, "C")
+    _lib.call("phb_advection_matrix", ct.byref(domain.desc()), domain._u_block.data_ptr(), domain._C_st.data_ptr(),
+              domain.A.data_ptr(), lo.data_ptr() if lo is not None else None, _S(domain))
+
+
+def SetupAdvectionVelocity(domain: Domain, timeStep, nonOrthoFlags=0, applyPressureGradient: bool = False) -> None:
+    """Momentum right-hand side into ``domain.velocityRHS`` (advection.cu:800-954)."""
+    _check(domain)
+    _no_nonortho(nonOrthoFlags)
+    if applyPressureGradient:
+        raise NotImplementedError("applyPressureGradient is not used by the PISO step")
+    domain.setTimeStep(timeStep)
+    src, mode = _src(domain)
+    _lib.call("phb_advection_rhs", ct.byref(domain.desc()), domain._u_block.data_ptr(), src, mode,
+              domain.velocityRHS.data_ptr(), _S(domain))
+
+
+# --- pressure ---------------------------------------------------------------------------
+def SetupPressureMatrix(domain: Domain, timeStep, nonOrthoMode=0, useFaceTransform: bool = False) -> None:
+    """Pressure Laplacian P = div(A^-1 grad) (pressure.cu:26-191)."""
+    _check(domain)
+    _no_nonortho(nonOrthoMode)
+    if useFaceTransform:
+        raise NotImplementedError("face transforms are not used by the orthogonal pressure matrix")
+    domain.setTimeStep(timeStep)
+    lo = _lo(domain, "P")
+    _lib.call("phb_pressure_matrix", ct.byref(domain.desc()), domain.A.data_ptr(), domain._P_st.data_ptr(),
+              lo.data_ptr() if lo is not None else None, _S(domain))
+
+
+def SetupPressureRHS(domain: Domain, timeStep, nonOrthoMode=0, useFaceTransform: bool = False,
+                     timeStepNorm: bool = False) -> None:
+    """HbyA into ``pressureRHS`` and its divergence into ``pressureRHSdiv``
+    (pressure.cu:350-521, :756-801)."""
+    _check(domain)
+    _no_nonortho(nonOrthoMode)
+    if useFaceTransform or timeStepNorm:
+        raise NotImplementedError("face transforms and time step normalisation are not implemented")
+    domain.setTimeStep(timeStep)
+    src, mode = _src(domain)
+    _lib.call("phb_pressure_rhs", ct.byref(domain.desc()), domain._C_st.data_ptr(), domain.A.data_ptr(),
+              domain._u_block.data_ptr(), domain.velocityResult.data_ptr(), src, mode, domain.pressureRHS.data_ptr(),
+              _S(domain))
+    SetupPressureRHSdiv(domain, timeStep, nonOrthoMode, useFaceTransform, timeStepNorm)
+
+
+def SetupPressureRHSdiv(domain: Domain, timeStep, nonOrthoMode=0, useFaceTransform: bool = False,
+                        timeStepNorm: bool = False) -> None:
+    _check(domain)
+    _lib.call("phb_divergence", ct.byref(domain.desc()), domain.pressureRHS.data_ptr(),
+              domain.pressureRHSdiv.data_ptr(), _S(domain))
+
+
+def SetupPressureCorrection(domain: Domain, timeStep, nonOrthoMode=0, useFaceTransform: bool = False,
+                            timeStepNorm: bool = False) -> None:
+    """Matrix, HbyA and divergence of one corrector (pressure.cu:882-927)."""
+    SetupPressureMatrix(domain, timeStep, nonOrthoMode, useFaceTransform)
+    SetupPressureRHS(domain, timeStep, nonOrthoMode, useFaceTransform, timeStepNorm)
+
+
+def CorrectVelocity(domain: Domain, timeStep, version: int = 0, timeStepNorm: bool = False) -> None:
+    """u = HbyA - grad(p)/A into ``velocityResult`` (velocity_correction.cu:27-60). The
+    pressure is read from the blocks, as in phiPICT (CopyPressureResultToBlocks first)."""
+    _check(domain)
+    if version not in (0, 1):
+        raise NotImplementedError("phipict_b200 implements the finite-difference corrector (version 1)")
+    if timeStepNorm:
+        raise NotImplementedError("time step normalisation is not implemented")
+    _lib.call("phb_correct_velocity", ct.byref(domain.desc()), domain._p_block.data_ptr(),
+              domain.pressureRHS.data_ptr(), domain.A.data_ptr(), domain.velocityResult.data_ptr(), _S(domain))
+
+
+# --- result copies (piso/result_copy.cu): one flat device copy each ----------------------
+def CopyVelocityResultToBlocks(domain: Domain) -> None:
+    domain._u_block.view(-1).copy_(domain.velocityResult)
+
+
+def CopyVelocityResultFromBlocks(domain: Domain) -> None:
+    domain.velocityResult.copy_(domain._u_block.view(-1))
+
+
+def CopyPressureResultToBlocks(domain: Domain) -> None:
+    domain._p_block.view(-1).copy_(domain.pressureResult)
+
+
+def CopyPressureResultFromBlocks(domain: Domain) -> None:
+    domain.pressureResult.copy_(domain._p_block.view(-1))
+
+
+def CopyEpotResultToBlocks(domain: Domain) -> None:
+    domain._epot_block.view(-1).copy_(domain.epotResult)
+
+
+def CopyEpotResultFromBlocks(domain: Domain) -> None:
+    domain.epotResult.copy_(domain._epot_block.view(-1))
+
+
+# --- MHD --------------------------------------------------------------------------------
+def SetupEpotMatrix(domain: Domain, nonOrthoFlags=0, useFaceTransform: bool = False) -> None:
+    domain.SetupEpotOnDomain(nonOrthoFlags, useFaceTransform)
+
+
+def ComputeEpotRHS(domain: Domain, vectorField: torch.Tensor) -> torch.Tensor:
+    """div(field) with the potential boundary fluxes (mhd/potential.cu:273-366)."""
+    _check(domain)
+    n = domain.getTotalSize() * domain.getSpatialDims() * domain.getBatchSize()
+    if vectorField.dim() != 1 or vectorField.numel() != n:
+        raise RuntimeError("vectorField size must be totalSize * spatialDims (* batch size).")
+    if vectorField.dtype != domain.getDtype() or vectorField.device != domain.getDevice():
+        raise RuntimeError("vectorField must match the domain dtype and device")
+    f = vectorField.contiguous()
+    out = torch.zeros(domain.getTotalSize() * domain.getBatchSize(), dtype=domain.getDtype(), device=domain.getDevice())
+    _lib.call("phb_epot_rhs", ct.byref(domain.desc()), f.data_ptr(), out.data_ptr(), _S(domain))
+    return out
+
+
+def ComputeCurrentDensityFaceBased(domain: Domain, epotField: torch.Tensor, uCrossBField: torch.Tensor) -> torch.Tensor:
+    """Face-based current density J, flat ``[B*3*cells]`` (mhd/potential.cu:718-977)."""
+    _check(domain)
+    d, B, N = domain.getSpatialDims(), domain.getBatchSize(), domain.getTotalSize()
+    if epotField.numel() != B * N:
+        raise RuntimeError("epotField size must equal domain totalSize (* batch size).")
+    if uCrossBField.numel() != B * N * 3:
+        if d == 3 and uCrossBField.numel() == B * N * d:
+            pass
+        else:
+            raise RuntimeError("uCrossBField must hold 3 components per cell")
+    J = torch.zeros(B * 3 * N, dtype=domain.getDtype(), device=domain.getDevice())
+    e_b = torch.zeros(B, 3, dtype=torch.float64, device=domain.getDevice())
+    _lib.call("phb_current_lorentz", ct.byref(domain.desc()), epotField.contiguous().data_ptr(),
+              uCrossBField.contiguous().data_ptr(), e_b.data_ptr(), None, J.data_ptr(), None, 0, _S(domain))
+    return J
+
+
+# --- linear solves ----------------------------------------------------------------------
+def SolveLinear(A: CSRmatrix, RHS: torch.Tensor, x: torch.Tensor, maxit, tol, conv=None, useBiCG: bool = False,
+                matrixRankDeficient: bool = False, residualResetSteps: int = 0, transposeA: bool = False,
+                printResidual: bool = False, returnBestResult: bool = False,
+                BiCGwithPreconditioner: bool = False) -> list[LinearSolverResultInfo]:
+    """Solve ``A x = RHS`` in place (solvers/linear_solve.cu:22-162). ``A`` must be one of
+    a domain's matrices (C, P or Epot); right-hand sides per instance = RHS size / rows."""
+    src = A.stencil_source() if isinstance(A, CSRmatrix) else None
+    if src is None:
+        raise NotImplementedError("phipict_b200 solves the stencil matrices of a Domain (C, P, Epot)")
+    if transposeA or BiCGwithPreconditioner or residualResetSteps:
+        raise NotImplementedError("transposed, preconditioned BiCGStab and residual resets are not implemented")
+    domain, which = src
+    st = domain._stencil(which)
+    B, N = domain.getBatchSize(), domain.getTotalSize()
+    nrhs = RHS.numel() // (B * N)
+    if nrhs * B * N != RHS.numel() or x.numel() != RHS.numel():
+        raise RuntimeError("RHS/x size must be a multiple of the matrix rows")
+    maxit = int(maxit.reshape(-1)[0]) if isinstance(maxit, torch.Tensor) else int(maxit)
+    if isinstance(tol, torch.Tensor) and tol.numel() > 1 and tol.numel() != B * nrhs:
+        raise RuntimeError("tolerance must have 1 or (batch * right-hand sides) entries")
+    solver = solver_for(domain, BICGSTAB if useBiCG else CG, domain.getDtype(), nrhs, tag="SolveLinear")
+    solver.solve(st, RHS.contiguous(), x, tol, maxit, return_best=returnBestResult)
+    return solver.results()
+
+
+def GetKrylovSettings() -> dict:
+    return {"enabled": True, "useGraphs": True}
+
+
+def SetKrylovSettings(*args, **kwargs) -> None:
+    pass
+
+
+def ReleaseKrylovWorkspaces() -> None:
+    _lib.call("phb_release_graphs")

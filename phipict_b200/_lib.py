@@ -1,0 +1,183 @@
+"""ctypes binding of the phipict_b200 CUDA library (``include/phipict_b200.h``).
+
+The library is built in-tree (``python -m phipict_b200.build``). Loading fails loudly
+when it is missing or when no CUDA device is visible: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+from pathlib import Path
+
+import torch
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libphipict_b200.so"
+
+PHB_F32, PHB_F64 = 0, 1
+BREC, FREC, IREC, TILE = 48, 16, 8, 256
+
+# every exported symbol of include/phipict_b200.h
+EXPORTS = (
+    "phb_last_error", "phb_version",
+    "phb_cell_metrics", "phb_face_metrics",
+    "phb_advection_matrix", "phb_advection_rhs", "phb_pressure_matrix", "phb_pressure_rhs",
+    "phb_divergence", "phb_correct_velocity", "phb_epot_matrix", "phb_epot_rhs", "phb_uxb_epot_rhs",
+    "phb_current_lorentz",
+    "phb_scratch_doubles", "phb_subtract_mean", "phb_rms",
+    "phb_csr_row_sizes", "phb_csr_pattern", "phb_csr_gather",
+    "phb_solve_work_bytes", "phb_solve_state_bytes", "phb_solve_run", "phb_solve_results",
+    "phb_release_graphs", "phb_refine_work_bytes", "phb_refine_run", "phb_refine_results",
+)
+
+
+class PhbDomain(ct.Structure):
+    _fields_ = [
+        ("dims", ct.c_int32), ("dtype", ct.c_int32),
+        ("nblocks", ct.c_int32), ("ninst", ct.c_int32), ("ntiles", ct.c_int32), ("nfixed", ct.c_int32),
+        ("ncells", ct.c_int64), ("metric_stride", ct.c_int64), ("face_metric_stride", ct.c_int64),
+        ("blocks", ct.c_void_p), ("tiles", ct.c_void_p), ("fixed", ct.c_void_p), ("insts", ct.c_void_p),
+        ("metrics", ct.c_void_p), ("face_metrics", ct.c_void_p),
+        ("fvel", ct.c_void_p), ("fpot", ct.c_void_p), ("fcw", ct.c_void_p), ("fmask", ct.c_void_p),
+        ("dt", ct.c_void_p), ("nu", ct.c_void_p),
+    ]
+
+
+class PhbTolerance(ct.Structure):
+    _fields_ = [
+        ("mode", ct.c_int32), ("pad", ct.c_int32),
+        ("rtol", ct.c_double), ("atol", ct.c_double), ("floor_eps", ct.c_double), ("fallback", ct.c_double),
+        ("values", ct.c_void_p),
+    ]
+
+
+class PhbSolve(ct.Structure):
+    _fields_ = [
+        ("kind", ct.c_int32), ("vec_dtype", ct.c_int32), ("mat_dtype", ct.c_int32), ("nrhs", ct.c_int32),
+        ("maxit", ct.c_int32), ("return_best", ct.c_int32), ("use_graph", ct.c_int32), ("check_every", ct.c_int32),
+        ("tol", PhbTolerance),
+        ("A", ct.c_void_p), ("b", ct.c_void_p), ("x", ct.c_void_p),
+        ("work", ct.c_void_p), ("state", ct.c_void_p),
+    ]
+
+
+class PhbSolveResult(ct.Structure):
+    _fields_ = [
+        ("final_residual", ct.c_double), ("used_iterations", ct.c_int32), ("converged", ct.c_int32),
+        ("finite", ct.c_int32), ("status", ct.c_int32),
+    ]
+
+
+class PhbRefine(ct.Structure):
+    _fields_ = [
+        ("kind", ct.c_int32), ("nrhs", ct.c_int32), ("max_outer", ct.c_int32), ("inner_maxit", ct.c_int32),
+        ("inner_rtol", ct.c_double),
+        ("tol", PhbTolerance),
+        ("A64", ct.c_void_p), ("A32", ct.c_void_p), ("b", ct.c_void_p), ("x", ct.c_void_p),
+        ("work", ct.c_void_p), ("state", ct.c_void_p),
+    ]
+
+
+_lib: ct.CDLL | None = None
+
+
+def load() -> ct.CDLL:
+    """Load the library (building it first if this is a source checkout without it)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        if os.environ.get("PHIPICT_B200_NO_BUILD"):
+            raise RuntimeError(f"phipict_b200 CUDA library missing: {LIB_PATH}")
+        from phipict_b200 import build as _build
+
+        _build.build()
+    lib = ct.CDLL(str(LIB_PATH))
+    P = ct.c_void_p
+    I = ct.c_int
+    I64 = ct.c_int64
+    DP = ct.POINTER(PhbDomain)
+    lib.phb_last_error.restype = ct.c_char_p
+    lib.phb_version.restype = I
+    sig = {
+        "phb_cell_metrics": [I, I, I, I, I, P, P, I64, P],
+        "phb_face_metrics": [I, I, I, I, I, P, I, P, I64, P],
+        "phb_advection_matrix": [DP, P, P, P, P, P],
+        "phb_advection_rhs": [DP, P, P, I, P, P],
+        "phb_pressure_matrix": [DP, P, P, P, P],
+        "phb_pressure_rhs": [DP, P, P, P, P, P, I, P, P],
+        "phb_divergence": [DP, P, P, P],
+        "phb_correct_velocity": [DP, P, P, P, P, P],
+        "phb_epot_matrix": [DP, P, P, P],
+        "phb_epot_rhs": [DP, P, P, P],
+        "phb_uxb_epot_rhs": [DP, P, P, P, P, P],
+        "phb_current_lorentz": [DP, P, P, P, P, P, P, I, P],
+        "phb_subtract_mean": [DP, P, I, P, P],
+        "phb_rms": [DP, P, I, P, P, P],
+        "phb_csr_row_sizes": [DP, P, P],
+        "phb_csr_pattern": [DP, P, P, P, P],
+        "phb_csr_gather": [I, I64, P, P, P, P],
+        "phb_solve_run": [DP, ct.POINTER(PhbSolve), P],
+        "phb_solve_results": [DP, ct.POINTER(PhbSolve), ct.POINTER(PhbSolveResult), P],
+        "phb_release_graphs": [],
+        "phb_refine_run": [DP, ct.POINTER(PhbRefine), ct.POINTER(PhbSolveResult), ct.POINTER(ct.c_int), P],
+        "phb_refine_results": [DP, ct.POINTER(PhbRefine), ct.POINTER(PhbSolveResult), ct.POINTER(ct.c_int), P],
+    }
+    for name, args in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = I
+    for name, args in {
+        "phb_scratch_doubles": [DP, I],
+        "phb_solve_work_bytes": [DP, I, I, I],
+        "phb_solve_state_bytes": [DP, I],
+        "phb_refine_work_bytes": [DP, I, I],
+    }.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = I64
+    _lib = lib
+    return lib
+
+
+class PhbError(RuntimeError):
+    pass
+
+
+def call(name: str, *args) -> int:
+    """Call an entry point and raise PhbError with the library's message on failure."""
+    lib = load()
+    rc = getattr(lib, name)(*args)
+    if rc != 0:
+        msg = lib.phb_last_error().decode(errors="replace")
+        raise PhbError(f"{name} failed ({rc}): {msg}")
+    return rc
+
+
+def stream_ptr(device: torch.device | None = None) -> int:
+    """The raw handle of torch's current CUDA stream."""
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def ptr(t: torch.Tensor | None) -> int | None:
+    if t is None:
+        return None
+    return t.data_ptr()
+
+
+def dtype_code(dtype: torch.dtype) -> int:
+    if dtype == torch.float64:
+        return PHB_F64
+    if dtype == torch.float32:
+        return PHB_F32
+    raise TypeError(f"unsupported dtype {dtype}; phipict_b200 computes in float32 or float64")
+
+
+def require_cuda(device: torch.device) -> None:
+    if device.type != "cuda":
+        raise RuntimeError(
+            "phipict_b200 runs on CUDA devices only (the product path has no CPU fallback); "
+            f"got device {device}"
+        )
+    if not torch.cuda.is_available():
+        raise RuntimeError("phipict_b200 needs a CUDA device, but torch.cuda.is_available() is False")

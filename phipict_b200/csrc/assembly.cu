@@ -1,0 +1,576 @@
+// Per-cell assembly kernels of the PISO/MHD step (orthogonal grids, CENTRAL advection).
+//
+// One thread per cell, one CTA per tile of one block (phb_device.cuh). Matrices are
+// written as stencils value[slot][cell] (slot 0 diagonal, slot f+1 face f), which keeps
+// every store coalesced and needs no column indices; the CSR view phiPICT exposes is a
+// gather over the same values (csr.cu). Metrics are SoA so that each of the 2d^2+1
+// metric loads of a warp is one coalesced transaction.
+//
+// The arithmetic of every kernel follows the reference kernel named in its comment
+// (paths relative to the phiPICT source tree).
+#include "phb_device.cuh"
+#include "phb_launch.cuh"
+
+namespace phb {
+
+// computeFluxesNDLoop (piso/device/discretization.cuh:758-838): contravariant face fluxes
+// of `field` (not multiplied by the face sign). Fixed faces take the boundary velocity.
+template <typename S, int D>
+__device__ __forceinline__ void faceFluxes(const Dom<S, D> &dom, const Cell &c, const S *__restrict__ field, S *fl) {
+#pragma unroll
+	for (int dim = 0; dim < D; ++dim) {
+		const S velC = contraAt<S, D>(dom, c.B, c.g, c.mi, dim, field);
+#pragma unroll
+		for (int up = 0; up < 2; ++up) {
+			const int f = dim * 2 + up;
+			if (atBound(c.B, f, c.p) && fType(c.B, f) == FT_FIXED) {
+				const int32_t *FR = dom.fix(fRec(c.B, f)[5]);
+				fl[f] = contraFixed<S, D>(dom, FR, faceCell(c.B, f, c.p), dim);
+			} else {
+				const Nbr n = neighbor<S, D>(dom, c, f);
+				S velN = contraAt<S, D>(dom, n.B, n.g, n.mi, n.comp, field);
+				if (n.flip) velN = -velN;
+				fl[f] = (velN + velC) * S(0.5);
+			}
+		}
+	}
+}
+
+// PISO_build_matrix (piso/advection.cu:27-305): implicit Euler advection-diffusion row
+// divided by the cell determinant; Adiag = its diagonal.
+template <typename S, int D>
+__global__ void __launch_bounds__(PHB_TILE) kAdvectionMatrix(Dom<S, D> dom, const S *__restrict__ u, S *__restrict__ C,
+		S *__restrict__ Adiag, float *__restrict__ Clo) {
+	__shared__ int32_t sB[PHB_BREC];
+	Cell c;
+	if (!loadCell<S, D>(dom, sB, c)) return;
+	const int inst = c.B[B_INST];
+	const S dt = S(dom.dt[inst]);
+	const S nu = S(dom.nu[inst]);
+	S fl[2 * D];
+	faceFluxes<S, D>(dom, c, u, fl);
+	const S det = detAt<S, D>(dom, c.mi);
+	S diag = det / dt;
+	S alphaP[D];
+#pragma unroll
+	for (int d = 0; d < D; ++d) alphaP[d] = alphaAt<S, D>(dom, c.mi, d);
+	S rv[2 * D + 1];
+#pragma unroll
+	for (int s = 0; s < 2 * D + 1; ++s) rv[s] = 0;
+#pragma unroll
+	for (int f = 0; f < 2 * D; ++f) {
+		const int dim = f >> 1;
+		const S faceSign = (f & 1) ? S(1) : S(-1);
+		if (!atBound(c.B, f, c.p) || fType(c.B, f) != FT_FIXED) {
+			const S half = S(0.5) * (faceSign * fl[f]);
+			diag += half;
+			rv[f + 1] += half;
+			const Nbr n = neighbor<S, D>(dom, c, f);
+			const S alphaN = alphaAt<S, D>(dom, n.mi, n.comp);
+			const S coeff = (alphaP[dim] * nu + alphaN * nu) * S(0.5);
+			diag += coeff;
+			rv[f + 1] -= coeff;
+		} else {
+			const int32_t *FR = dom.fix(fRec(c.B, f)[5]);
+			const S slip = FR[F_VELTYPE] == 0 ? S(0) : S(1);
+			diag += (S(1) - slip) * S(2) * nu * alphaP[dim];
+		}
+	}
+	rv[0] = diag;
+	const int64_t N = dom.ncells;
+#pragma unroll
+	for (int s = 0; s < 2 * D + 1; ++s) {
+		const S v = rv[s] / det;
+		C[s * N + c.g] = v;
+		if (Clo) Clo[s * N + c.g] = float(v);
+	}
+	Adiag[c.g] = rv[0] / det;
+}
+
+// boundary source of the momentum equation at fixed faces (advection.cu:834-866, the same
+// terms as pressure.cu:404-432): -u_b F_b + 2 nu alpha u_b (no-slip faces)
+template <typename S, int D>
+__device__ __forceinline__ S boundarySource(const Dom<S, D> &dom, const Cell &c, int dim, S nu) {
+	S r = 0;
+#pragma unroll
+	for (int f = 0; f < 2 * D; ++f) {
+		if (!atBound(c.B, f, c.p) || fType(c.B, f) != FT_FIXED) continue;
+		const S faceNormal = (f & 1) ? S(1) : S(-1);
+		const int32_t *FR = dom.fix(fRec(c.B, f)[5]);
+		const int fc = faceCell(c.B, f, c.p);
+		const S vel = fixedVel<S, D>(dom, FR, fc, dim);
+		const S alpha = alphaFixed<S, D>(dom, FR, fc, f >> 1);
+		const S flux = contraFixed<S, D>(dom, FR, fc, f >> 1) * faceNormal;
+		r -= vel * flux;
+		const S slip = FR[F_VELTYPE] == 0 ? S(0) : S(1);
+		r += vel * (S(1) - slip) * nu * S(2) * alpha;
+	}
+	return r;
+}
+template <typename S, int D>
+__device__ __forceinline__ S sourceAt(const Cell &c, const S *__restrict__ src, int mode, int dim) {
+	if (mode == 1) return src[c.B[B_INST] * D + dim];
+	if (mode == 2) return src[vidx<D>(c.B, c.g, dim)];
+	return S(0);
+}
+
+// kPISO_build_advection_RHS (advection.cu:800-954), CENTRAL scheme, no pressure gradient
+template <typename S, int D>
+__global__ void __launch_bounds__(PHB_TILE) kAdvectionRhs(Dom<S, D> dom, const S *__restrict__ u, const S *__restrict__ src,
+		int srcMode, S *__restrict__ rhs) {
+	__shared__ int32_t sB[PHB_BREC];
+	Cell c;
+	if (!loadCell<S, D>(dom, sB, c)) return;
+	const int inst = c.B[B_INST];
+	const S dt = S(dom.dt[inst]);
+	const S nu = S(dom.nu[inst]);
+	const S det = detAt<S, D>(dom, c.mi);
+#pragma unroll
+	for (int dim = 0; dim < D; ++dim) {
+		const int64_t o = vidx<D>(c.B, c.g, dim);
+		S r = det * u[o] / dt;
+		r += boundarySource<S, D>(dom, c, dim, nu);
+		r /= det;
+		r += sourceAt<S, D>(c, src, srcMode, dim);
+		rhs[o] = r;
+	}
+}
+
+// PISO_build_pressure_matrix (pressure.cu:26-191) with raP = 1/A, and
+// PISO_build_epot_matrix (mhd/potential.cu:30-233) with raP = 1 plus the Dirichlet ghost
+// diagonal and the thin-wall Robin correction.
+template <typename S, int D, bool EPOT>
+__global__ void __launch_bounds__(PHB_TILE) kLaplaceMatrix(Dom<S, D> dom, const S *__restrict__ Adiag, S *__restrict__ P,
+		float *__restrict__ Plo) {
+	__shared__ int32_t sB[PHB_BREC];
+	Cell c;
+	if (!loadCell<S, D>(dom, sB, c)) return;
+	S alphaP[D];
+#pragma unroll
+	for (int d = 0; d < D; ++d) alphaP[d] = alphaAt<S, D>(dom, c.mi, d);
+	const S raP = EPOT ? S(1) : S(1) / Adiag[c.g];
+	S rv[2 * D + 1];
+	bool has[2 * D + 1];
+#pragma unroll
+	for (int s = 0; s < 2 * D + 1; ++s) { rv[s] = 0; has[s] = false; }
+#pragma unroll
+	for (int f = 0; f < 2 * D; ++f) {
+		const int dim = f >> 1;
+		const bool ab = atBound(c.B, f, c.p);
+		if (!(ab && fType(c.B, f) == FT_FIXED)) {
+			const Nbr n = neighbor<S, D>(dom, c, f);
+			const S alphaN = alphaAt<S, D>(dom, n.mi, n.comp);
+			const S raN = EPOT ? S(1) : S(1) / Adiag[n.g];
+			const S coeff = S(0.5) * (alphaP[dim] * raP + alphaN * raN);
+			rv[0] -= coeff;
+			rv[f + 1] += coeff;
+			has[f + 1] = true;
+		} else if (EPOT) {
+			const int32_t *FR = dom.fix(fRec(c.B, f)[5]);
+			if (potBC(dom.fmask, FR, faceCell(c.B, f, c.p)) == PB_DIRICHLET) rv[0] -= alphaP[dim] * raP;
+		}
+	}
+	if (EPOT) {
+		// potential.cu:175-219: C_w * surface Laplacian along thin conducting walls
+#pragma unroll
+		for (int tw = 0; tw < 2 * D; ++tw) {
+			const int twDim = tw >> 1;
+			if (!atBound(c.B, tw, c.p) || fType(c.B, tw) != FT_FIXED) continue;
+			const int32_t *FR = dom.fix(fRec(c.B, tw)[5]);
+			if (potBC(dom.fmask, FR, faceCell(c.B, tw, c.p)) != PB_THIN_WALL) continue;
+			const S Cw = dom.fcw[fRec(c.B, tw)[5]];
+			S nP = 0;
+#pragma unroll
+			for (int j = 0; j < D; ++j) { const S v = dom.m(Tr<D>::MINV + twDim * D + j, c.mi); nP += v * v; }
+			const S MinvNP = sqrt(nP);
+#pragma unroll
+			for (int tDim = 0; tDim < D; ++tDim) {
+				if (tDim == twDim) continue;
+#pragma unroll
+				for (int side = 0; side < 2; ++side) {
+					const int tb = tDim * 2 + side;
+					if (!has[tb + 1]) continue;
+					int q[3] = {c.p[0], c.p[1], c.p[2]};
+					if (atBound(c.B, tb, c.p)) {
+						if (fType(c.B, tb) == FT_PERIODIC) q[tDim] = side ? 0 : c.B[B_NX + tDim] - 1;
+						else continue;
+					} else {
+						q[tDim] += side ? 1 : -1;
+					}
+					if (potBC(dom.fmask, FR, faceCell(c.B, tw, q)) != PB_THIN_WALL) continue;
+					const int64_t qm = c.B[B_METOFF] + flat(c.B, q);
+					const S alphaNt = alphaAt<S, D>(dom, qm, tDim);
+					S nN = 0;
+#pragma unroll
+					for (int j = 0; j < D; ++j) { const S v = dom.m(Tr<D>::MINV + twDim * D + j, qm); nN += v * v; }
+					const S MinvNN = sqrt(nN);
+					const S surf = Cw * S(0.5) * (alphaP[tDim] * MinvNP + alphaNt * MinvNN);
+					rv[0] -= surf;
+					rv[tb + 1] += surf;
+				}
+			}
+		}
+	}
+	const int64_t N = dom.ncells;
+#pragma unroll
+	for (int s = 0; s < 2 * D + 1; ++s) {
+		P[s * N + c.g] = rv[s];
+		if (Plo) Plo[s * N + c.g] = float(rv[s]);
+	}
+}
+
+// PISO_build_pressure_rhs (pressure.cu:350-521): HbyA = (u/dt - H(u*) + S)/A per component
+template <typename S, int D>
+__global__ void __launch_bounds__(PHB_TILE) kPressureRhs(Dom<S, D> dom, const S *__restrict__ C, const S *__restrict__ Adiag,
+		const S *__restrict__ u, const S *__restrict__ ustar, const S *__restrict__ src, int srcMode, S *__restrict__ hbya) {
+	__shared__ int32_t sB[PHB_BREC];
+	Cell c;
+	if (!loadCell<S, D>(dom, sB, c)) return;
+	const int inst = c.B[B_INST];
+	const S dt = S(dom.dt[inst]);
+	const S nu = S(dom.nu[inst]);
+	const S rDiag = S(1) / Adiag[c.g];
+	const S det = detAt<S, D>(dom, c.mi);
+	const int64_t N = dom.ncells;
+	int64_t nb[2 * D];
+	S cv[2 * D];
+#pragma unroll
+	for (int f = 0; f < 2 * D; ++f) {
+		nb[f] = neighborIndex<S, D>(dom, c, f);
+		cv[f] = C[(f + 1) * N + c.g];
+	}
+#pragma unroll
+	for (int dim = 0; dim < D; ++dim) {
+		const int64_t o = vidx<D>(c.B, c.g, dim);
+		const S velOld = u[o] / dt;
+		S H = 0;
+#pragma unroll
+		for (int f = 0; f < 2 * D; ++f)
+			if (nb[f] >= 0 && nb[f] != c.g) H += cv[f] * ustar[vidx<D>(c.B, nb[f], dim)];
+		S Ssum = boundarySource<S, D>(dom, c, dim, nu);
+		Ssum /= det;
+		Ssum += sourceAt<S, D>(c, src, srcMode, dim);
+		hbya[o] = rDiag * (velOld - H + Ssum);
+	}
+}
+
+// k_computePressureRHSdivergenceFromFlux (pressure.cu:756-801), no face transforms
+template <typename S, int D>
+__global__ void __launch_bounds__(PHB_TILE) kDivergence(Dom<S, D> dom, const S *__restrict__ field, S *__restrict__ div) {
+	__shared__ int32_t sB[PHB_BREC];
+	Cell c;
+	if (!loadCell<S, D>(dom, sB, c)) return;
+	S fl[2 * D];
+	faceFluxes<S, D>(dom, c, field, fl);
+	S dv = 0;
+#pragma unroll
+	for (int d = 0; d < D; ++d) dv += fl[d * 2 + 1] - fl[d * 2];
+	div[c.g] = dv;
+}
+
+// getPressureAtWithBounds for the +-1 neighbours (nonortho_laplace.cuh:302-381)
+template <typename S, int D>
+__device__ __forceinline__ S scalarAcross(const Dom<S, D> &dom, const Cell &c, int f, const S *__restrict__ p) {
+	if (atBound(c.B, f, c.p) && fType(c.B, f) == FT_FIXED) return p[c.g];
+	return p[neighbor<S, D>(dom, c, f).g];
+}
+
+// PISO_update_velocity, version 1 (velocity_correction.cu:27-60) with the finite
+// difference gradient of getPressureGradient (piso/device/velocity.cuh:347-378)
+template <typename S, int D>
+__global__ void __launch_bounds__(PHB_TILE) kCorrectVelocity(Dom<S, D> dom, const S *__restrict__ p, const S *__restrict__ hbya,
+		const S *__restrict__ Adiag, S *__restrict__ u) {
+	__shared__ int32_t sB[PHB_BREC];
+	Cell c;
+	if (!loadCell<S, D>(dom, sB, c)) return;
+	const S rDiag = S(1) / Adiag[c.g];
+	S gr[D];
+#pragma unroll
+	for (int dim = 0; dim < D; ++dim) {
+		S fac = 0.5;
+		const bool lowFixed = c.p[dim] == 0 && fType(c.B, dim * 2) == FT_FIXED;
+		const bool upFixed = c.p[dim] == c.B[B_NX + dim] - 1 && fType(c.B, dim * 2 + 1) == FT_FIXED;
+		if (lowFixed || upFixed) fac = 1;
+		const S valN = lowFixed ? p[c.g] : scalarAcross<S, D>(dom, c, dim * 2, p);
+		const S valP = upFixed ? p[c.g] : scalarAcross<S, D>(dom, c, dim * 2 + 1, p);
+		gr[dim] = (valP - valN) * fac;
+	}
+	S grad[D];
+#pragma unroll
+	for (int k = 0; k < D; ++k) grad[k] = 0;
+#pragma unroll
+	for (int r = 0; r < D; ++r)
+#pragma unroll
+		for (int k = 0; k < D; ++k) grad[k] += dom.m(Tr<D>::MINV + r * D + k, c.mi) * gr[r];
+#pragma unroll
+	for (int d = 0; d < D; ++d) {
+		const int64_t o = vidx<D>(c.B, c.g, d);
+		u[o] = -rDiag * grad[d] + hbya[o];
+	}
+}
+
+// u x e_b at a cell (simulation/mhd.py:276-355): 2D velocities are lifted to 3D
+template <typename S, int D>
+__device__ __forceinline__ void uCrossB(const int32_t *B, int64_t g, const S *__restrict__ u, const double *eb, S *out) {
+	const S u0 = u[vidx<D>(B, g, 0)], u1 = u[vidx<D>(B, g, 1)];
+	const S u2 = D > 2 ? u[vidx<D>(B, g, D > 2 ? 2 : 0)] : S(0);
+	const S e0 = S(eb[0]), e1 = S(eb[1]), e2 = S(eb[2]);
+	out[0] = u1 * e2 - u2 * e1;
+	out[1] = u2 * e0 - u0 * e2;
+	out[2] = u0 * e1 - u1 * e0;
+}
+template <typename S, int D>
+__device__ __forceinline__ S contraVec(const Dom<S, D> &dom, int64_t mi, int c, const S *v) {
+	S s = 0;
+#pragma unroll
+	for (int j = 0; j < D; ++j) s += dom.m(Tr<D>::MINV + c * D + j, mi) * v[j];
+	return dom.m(Tr<D>::DET, mi) * s;
+}
+// [inst][3][cells] index
+__device__ __forceinline__ int64_t vidx3(const int32_t *B, int64_t g, int k) { return g + 2 * (int64_t)B[B_INSTOFF] + (int64_t)k * B[B_INSTN]; }
+
+// u x e_b fused with k_computeEpotRHS (mhd/potential.cu:273-323) and its face fluxes
+// computeEpotFluxesNDLoop (discretization.cuh:856-912)
+template <typename S, int D>
+__global__ void __launch_bounds__(PHB_TILE) kUxbEpotRhs(Dom<S, D> dom, const S *__restrict__ u, const double *__restrict__ eb,
+		S *__restrict__ uxb, S *__restrict__ rhs) {
+	__shared__ int32_t sB[PHB_BREC];
+	Cell c;
+	if (!loadCell<S, D>(dom, sB, c)) return;
+	const double *e = eb + 3 * c.B[B_INST];
+	S x[3];
+	uCrossB<S, D>(c.B, c.g, u, e, x);
+#pragma unroll
+	for (int k = 0; k < 3; ++k) uxb[vidx3(c.B, c.g, k)] = x[k];
+	S fl[2 * D];
+#pragma unroll
+	for (int dim = 0; dim < D; ++dim) {
+		const S velC = contraVec<S, D>(dom, c.mi, dim, x);
+#pragma unroll
+		for (int up = 0; up < 2; ++up) {
+			const int f = dim * 2 + up;
+			if (atBound(c.B, f, c.p) && fType(c.B, f) == FT_FIXED) {
+				const int32_t *FR = dom.fix(fRec(c.B, f)[5]);
+				const int bc = potBC(dom.fmask, FR, faceCell(c.B, f, c.p));
+				fl[f] = (bc == PB_INSULATING || bc == PB_THIN_WALL) ? S(0) : velC;
+			} else {
+				const Nbr n = neighbor<S, D>(dom, c, f);
+				S xn[3];
+				uCrossB<S, D>(n.B, n.g, u, e, xn);
+				S velN = contraVec<S, D>(dom, n.mi, n.comp, xn);
+				if (n.flip) velN = -velN;
+				fl[f] = (velN + velC) * S(0.5);
+			}
+		}
+	}
+	S dv = 0;
+#pragma unroll
+	for (int d = 0; d < D; ++d) dv += fl[d * 2 + 1] - fl[d * 2];
+#pragma unroll
+	for (int f = 0; f < 2 * D; ++f) {
+		if (!atBound(c.B, f, c.p) || fType(c.B, f) != FT_FIXED) continue;
+		const int32_t *FR = dom.fix(fRec(c.B, f)[5]);
+		const int fc = faceCell(c.B, f, c.p);
+		if (potBC(dom.fmask, FR, fc) != PB_DIRICHLET) continue;
+		const S gv = potValue<S, D>(dom, FR, fc);
+		if (gv == S(0)) continue;
+		dv -= alphaAt<S, D>(dom, c.mi, f >> 1) * gv;
+	}
+	rhs[c.g] = dv;
+}
+
+// k_computeEpotRHS (mhd/potential.cu:273-323) of a given in-plane field [inst][dims][cells]
+template <typename S, int D>
+__global__ void __launch_bounds__(PHB_TILE) kEpotRhs(Dom<S, D> dom, const S *__restrict__ field, S *__restrict__ rhs) {
+	__shared__ int32_t sB[PHB_BREC];
+	Cell c;
+	if (!loadCell<S, D>(dom, sB, c)) return;
+	S fl[2 * D];
+#pragma unroll
+	for (int dim = 0; dim < D; ++dim) {
+		const S velC = contraAt<S, D>(dom, c.B, c.g, c.mi, dim, field);
+#pragma unroll
+		for (int up = 0; up < 2; ++up) {
+			const int f = dim * 2 + up;
+			if (atBound(c.B, f, c.p) && fType(c.B, f) == FT_FIXED) {
+				const int32_t *FR = dom.fix(fRec(c.B, f)[5]);
+				const int bc = potBC(dom.fmask, FR, faceCell(c.B, f, c.p));
+				fl[f] = (bc == PB_INSULATING || bc == PB_THIN_WALL) ? S(0) : velC;
+			} else {
+				const Nbr n = neighbor<S, D>(dom, c, f);
+				S velN = contraAt<S, D>(dom, n.B, n.g, n.mi, n.comp, field);
+				if (n.flip) velN = -velN;
+				fl[f] = (velN + velC) * S(0.5);
+			}
+		}
+	}
+	S dv = 0;
+#pragma unroll
+	for (int d = 0; d < D; ++d) dv += fl[d * 2 + 1] - fl[d * 2];
+#pragma unroll
+	for (int f = 0; f < 2 * D; ++f) {
+		if (!atBound(c.B, f, c.p) || fType(c.B, f) != FT_FIXED) continue;
+		const int32_t *FR = dom.fix(fRec(c.B, f)[5]);
+		const int fc = faceCell(c.B, f, c.p);
+		if (potBC(dom.fmask, FR, fc) != PB_DIRICHLET) continue;
+		const S gv = potValue<S, D>(dom, FR, fc);
+		if (gv == S(0)) continue;
+		dv -= alphaAt<S, D>(dom, c.mi, f >> 1) * gv;
+	}
+	rhs[c.g] = dv;
+}
+
+// computeCurrentDensityFaceBased (mhd/potential.cu:718-880) fused with the Lorentz force
+// F_L = N (J x e_b) of simulation/mhd.py:543-595 added to the velocity source
+template <typename S, int D>
+__global__ void __launch_bounds__(PHB_TILE) kCurrentLorentz(Dom<S, D> dom, const S *__restrict__ phi, const S *__restrict__ uxb,
+		const double *__restrict__ eb, const double *__restrict__ stuart, S *__restrict__ Jout, S *__restrict__ src, int accumulate) {
+	__shared__ int32_t sB[PHB_BREC];
+	Cell c;
+	if (!loadCell<S, D>(dom, sB, c)) return;
+	const int inst = c.B[B_INST];
+	const S phiP = phi[c.g];
+	S alphaP[D], cvelP[D];
+	S xP[D];
+#pragma unroll
+	for (int k = 0; k < D; ++k) xP[k] = uxb[vidx3(c.B, c.g, k)];
+#pragma unroll
+	for (int d = 0; d < D; ++d) { alphaP[d] = alphaAt<S, D>(dom, c.mi, d); cvelP[d] = contraVec<S, D>(dom, c.mi, d, xP); }
+	S jf[2 * D];
+#pragma unroll
+	for (int f = 0; f < 2 * D; ++f) {
+		const int dim = f >> 1;
+		const S faceSign = (f & 1) ? S(1) : S(-1);
+		const bool ab = atBound(c.B, f, c.p);
+		if (ab && fType(c.B, f) == FT_FIXED) {
+			const int32_t *FR = dom.fix(fRec(c.B, f)[5]);
+			const int fc = faceCell(c.B, f, c.p);
+			const int bc = potBC(dom.fmask, FR, fc);
+			if (bc == PB_INSULATING || bc == PB_THIN_WALL) jf[f] = 0;
+			else if (bc == PB_DIRICHLET) jf[f] = alphaP[dim] * faceSign * (phiP - potValue<S, D>(dom, FR, fc)) + cvelP[dim];
+			else jf[f] = cvelP[dim];
+			continue;
+		}
+		const Nbr n = neighbor<S, D>(dom, c, f);
+		const S phiN = phi[n.g];
+		const S alphaN = alphaAt<S, D>(dom, n.mi, n.comp);
+		S xN[D];
+#pragma unroll
+		for (int k = 0; k < D; ++k) xN[k] = uxb[vidx3(n.B, n.g, k)];
+		S cvelN = contraVec<S, D>(dom, n.mi, n.comp, xN);
+		if (n.flip) cvelN = -cvelN;
+		const S coeff = S(0.5) * (alphaP[dim] + alphaN);
+		const S chi = S(0.5) * (cvelP[dim] + cvelN);
+		jf[f] = -coeff * faceSign * (phiN - phiP) + chi;
+	}
+	S javg[D];
+#pragma unroll
+	for (int d = 0; d < D; ++d) javg[d] = S(0.5) * (jf[d * 2] + jf[d * 2 + 1]);
+	const S invDet = S(1) / detAt<S, D>(dom, c.mi);
+	S J[3] = {0, 0, 0};
+#pragma unroll
+	for (int r = 0; r < D; ++r) {
+		S s = 0;
+#pragma unroll
+		for (int k = 0; k < D; ++k) s += dom.m(r * D + k, c.mi) * javg[k];
+		J[r] = s * invDet;
+	}
+	if (D == 2) J[2] = uxb[vidx3(c.B, c.g, 2)];
+	if (Jout) {
+#pragma unroll
+		for (int k = 0; k < 3; ++k) Jout[vidx3(c.B, c.g, k)] = J[k];
+	}
+	if (src) {
+		const double *e = eb + 3 * inst;
+		const S N = S(stuart[inst]);
+		const S e0 = S(e[0]), e1 = S(e[1]), e2 = S(e[2]);
+		const S F[3] = {J[1] * e2 - J[2] * e1, J[2] * e0 - J[0] * e2, J[0] * e1 - J[1] * e0};
+#pragma unroll
+		for (int d = 0; d < D; ++d) {
+			const int64_t o = vidx<D>(c.B, c.g, d);
+			const S v = N * F[d];
+			src[o] = accumulate ? v + src[o] : v;
+		}
+	}
+}
+
+} // namespace phb
+
+using namespace phb;
+
+#define PHB_DISPATCH(DOM, ...)                                                                     \
+	do {                                                                                           \
+		if ((DOM)->dims == 2 && (DOM)->dtype == PHB_F64) { using S = double; constexpr int D = 2; __VA_ARGS__; } \
+		else if ((DOM)->dims == 3 && (DOM)->dtype == PHB_F64) { using S = double; constexpr int D = 3; __VA_ARGS__; } \
+		else if ((DOM)->dims == 2 && (DOM)->dtype == PHB_F32) { using S = float; constexpr int D = 2; __VA_ARGS__; } \
+		else if ((DOM)->dims == 3 && (DOM)->dtype == PHB_F32) { using S = float; constexpr int D = 3; __VA_ARGS__; } \
+		else return setError(PHB_ERR_ARG, "unsupported dims/dtype");                                \
+	} while (0)
+
+#define PHB_TILES(DOM) dim3((DOM)->ntiles), dim3(PHB_TILE), 0, (cudaStream_t)stream
+
+extern "C" int phb_advection_matrix(const phb_domain *dom, const void *u, void *C, void *Adiag, float *C_lo, phb_stream stream) {
+	if (!dom || !u || !C || !Adiag) return setError(PHB_ERR_ARG, "phb_advection_matrix: null argument");
+	if (dom->ntiles == 0) return PHB_OK;
+	PHB_DISPATCH(dom, kAdvectionMatrix<S, D><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)u, (S *)C, (S *)Adiag, C_lo));
+	return checkLaunch("kAdvectionMatrix");
+}
+extern "C" int phb_advection_rhs(const phb_domain *dom, const void *u, const void *src, int src_mode, void *rhs, phb_stream stream) {
+	if (!dom || !u || !rhs || (src_mode != 0 && !src) || src_mode < 0 || src_mode > 2) return setError(PHB_ERR_ARG, "phb_advection_rhs: bad argument");
+	if (dom->ntiles == 0) return PHB_OK;
+	PHB_DISPATCH(dom, kAdvectionRhs<S, D><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)u, (const S *)src, src_mode, (S *)rhs));
+	return checkLaunch("kAdvectionRhs");
+}
+extern "C" int phb_pressure_matrix(const phb_domain *dom, const void *Adiag, void *P, float *P_lo, phb_stream stream) {
+	if (!dom || !Adiag || !P) return setError(PHB_ERR_ARG, "phb_pressure_matrix: null argument");
+	if (dom->ntiles == 0) return PHB_OK;
+	PHB_DISPATCH(dom, (kLaplaceMatrix<S, D, false><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)Adiag, (S *)P, P_lo)));
+	return checkLaunch("kLaplaceMatrix");
+}
+extern "C" int phb_epot_matrix(const phb_domain *dom, void *E, float *E_lo, phb_stream stream) {
+	if (!dom || !E) return setError(PHB_ERR_ARG, "phb_epot_matrix: null argument");
+	if (dom->ntiles == 0) return PHB_OK;
+	PHB_DISPATCH(dom, (kLaplaceMatrix<S, D, true><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)nullptr, (S *)E, E_lo)));
+	return checkLaunch("kLaplaceMatrix(epot)");
+}
+extern "C" int phb_pressure_rhs(const phb_domain *dom, const void *C, const void *Adiag, const void *u, const void *ustar,
+		const void *src, int src_mode, void *hbya, phb_stream stream) {
+	if (!dom || !C || !Adiag || !u || !ustar || !hbya || (src_mode != 0 && !src) || src_mode < 0 || src_mode > 2)
+		return setError(PHB_ERR_ARG, "phb_pressure_rhs: bad argument");
+	if (dom->ntiles == 0) return PHB_OK;
+	PHB_DISPATCH(dom, kPressureRhs<S, D><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)C, (const S *)Adiag, (const S *)u,
+		(const S *)ustar, (const S *)src, src_mode, (S *)hbya));
+	return checkLaunch("kPressureRhs");
+}
+extern "C" int phb_divergence(const phb_domain *dom, const void *field, void *div, phb_stream stream) {
+	if (!dom || !field || !div) return setError(PHB_ERR_ARG, "phb_divergence: null argument");
+	if (dom->ntiles == 0) return PHB_OK;
+	PHB_DISPATCH(dom, kDivergence<S, D><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)field, (S *)div));
+	return checkLaunch("kDivergence");
+}
+extern "C" int phb_correct_velocity(const phb_domain *dom, const void *p, const void *hbya, const void *Adiag, void *u, phb_stream stream) {
+	if (!dom || !p || !hbya || !Adiag || !u) return setError(PHB_ERR_ARG, "phb_correct_velocity: null argument");
+	if (dom->ntiles == 0) return PHB_OK;
+	PHB_DISPATCH(dom, kCorrectVelocity<S, D><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)p, (const S *)hbya, (const S *)Adiag, (S *)u));
+	return checkLaunch("kCorrectVelocity");
+}
+extern "C" int phb_uxb_epot_rhs(const phb_domain *dom, const void *u, const double *e_b, void *uxb, void *rhs, phb_stream stream) {
+	if (!dom || !u || !e_b || !uxb || !rhs) return setError(PHB_ERR_ARG, "phb_uxb_epot_rhs: null argument");
+	if (dom->ntiles == 0) return PHB_OK;
+	PHB_DISPATCH(dom, kUxbEpotRhs<S, D><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)u, e_b, (S *)uxb, (S *)rhs));
+	return checkLaunch("kUxbEpotRhs");
+}
+extern "C" int phb_current_lorentz(const phb_domain *dom, const void *phi, const void *uxb, const double *e_b,
+		const double *stuart, void *J, void *src, int accumulate, phb_stream stream) {
+	if (!dom || !phi || !uxb || !e_b || (src && !stuart)) return setError(PHB_ERR_ARG, "phb_current_lorentz: null argument");
+	if (dom->ntiles == 0) return PHB_OK;
+	PHB_DISPATCH(dom, kCurrentLorentz<S, D><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)phi, (const S *)uxb, e_b, stuart,
+		(S *)J, (S *)src, accumulate));
+	return checkLaunch("kCurrentLorentz");
+}
+extern "C" int phb_epot_rhs(const phb_domain *dom, const void *field, void *rhs, phb_stream stream) {
+	if (!dom || !field || !rhs) return setError(PHB_ERR_ARG, "phb_epot_rhs: null argument");
+	if (dom->ntiles == 0) return PHB_OK;
+	PHB_DISPATCH(dom, kEpotRhs<S, D><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)field, (S *)rhs));
+	return checkLaunch("kEpotRhs");
+}

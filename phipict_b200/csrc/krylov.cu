@@ -1,0 +1,1013 @@
+// Fused, batched Krylov solvers on stencil matrices: CG and BiCGStab for many systems at
+// once (instances x right-hand sides), plus FP64 iterative refinement around FP32 inner
+// solves.
+//
+// Algorithm and stop rule follow phiPICT's fused solvers (solvers/krylov/krylov.cu):
+// classic CG in two fused phases per iteration (:428-568), van der Vorst BiCGStab with a
+// half-step convergence check (:599-824), the criterion ||r||_2/sqrt(n) < tol per system,
+// FP64 accumulation of every inner product and a deterministic fixed-order reduction in
+// the last CTA to finish (:157-202). The B200 design differs where the hardware rewards it:
+//   - the SpMV reads a stencil (2d+1 values per row, no column indices, neighbours by
+//     index arithmetic), one CTA per 256-cell tile of one block, so every CTA belongs to
+//     one instance and per-instance reductions are contiguous CTA ranges;
+//   - the search direction update is folded into the SpMV of the next phase (p is evaluated
+//     on the fly at the stencil points), which also removes BiCGStab's separate p kernel;
+//   - the iteration loop is a conditional WHILE node of a CUDA graph whose condition the
+//     last CTA sets, so a solve is one graph launch with no host round trip, and when the
+//     caller is capturing a stream (a whole PISO step as one graph) the loop is spliced
+//     into that capture instead.
+#include <map>
+#include <vector>
+#include <mutex>
+#include <string>
+#include <cstring>
+#include <cmath>
+#include <functional>
+#include "phb_device.cuh"
+#include "phb_launch.cuh"
+
+namespace phb {
+
+constexpr int NWARPS = PHB_TILE / 32;
+enum Done : int { RUNNING = 0, CONVERGED = 1, NONFINITE = 2, MAXIT = 3, RISING = 4 };
+constexpr int RISING_CUTOFF = 100;
+
+struct SysState {
+	double tol, rho, alpha, beta, omega, crit, best, last, halfCrit, innerTol;
+	int it, maxit, bestIt, rising, done, restart, saveBest, halfDone, usedIt, pad1;
+	int pad2[2];
+};
+static_assert(sizeof(SysState) == 128, "SysState layout");
+
+struct Control {
+	unsigned int counter;
+	int allDone;
+	int loops;
+	int maxLoops;
+	int pad[4];
+};
+static_assert(sizeof(Control) == 32, "Control layout");
+
+// device helpers -----------------------------------------------------------------------
+__device__ __forceinline__ double warpSum(double v) {
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	return v;
+}
+
+// Block-reduce NV values, write this CTA's partials, and return whether this CTA is the
+// last of the grid to finish (the ticket pattern of krylov.cu:157-182).
+template <int NV>
+__device__ __forceinline__ bool storePartials(double (&v)[NV], double *partial, unsigned int *counter) {
+	__shared__ double sm[NV][NWARPS];
+	__shared__ bool isLast;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+	for (int q = 0; q < NV; ++q) {
+		const double s = warpSum(v[q]);
+		if (lane == 0) sm[q][warp] = s;
+	}
+	__syncthreads();
+	if (threadIdx.x < NV) {
+		double s = 0;
+#pragma unroll
+		for (int w = 0; w < NWARPS; ++w) s += sm[threadIdx.x][w];
+		partial[(size_t)blockIdx.x * NV + threadIdx.x] = s;
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		__threadfence();
+		const unsigned int ticket = atomicAdd(counter, 1u);
+		isLast = ticket == gridDim.x - 1;
+	}
+	__syncthreads();
+	return isLast;
+}
+
+// In the last CTA: one warp per running system sums its instance's CTA partials in a fixed
+// order and lane 0 calls fn(state, inst, sums, instSum); then allDone is updated and the
+// ticket counter reset for the next kernel. With INSTQ >= 0 the warp also sums quantity
+// INSTQ over all K systems of the instance (instSum), e.g. the whole right-hand side norm.
+template <int K, int NQ, int INSTQ = -1, typename Fn>
+__device__ __forceinline__ void finalizeSystems(const int32_t *insts, int ninst, const double *partial, SysState *st, Control *ctrl, Fn fn) {
+	__shared__ int running;
+	if (threadIdx.x == 0) running = 0;
+	__threadfence();
+	__syncthreads();
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const int nsys = ninst * K;
+	for (int s = warp; s < nsys; s += NWARPS) {
+		const int inst = s / K, k = s - inst * K;
+		if (st[s].done == RUNNING) {
+			const int t0 = insts[inst * PHB_IREC + I_TILESTART], tc = insts[inst * PHB_IREC + I_TILECOUNT];
+			double acc[NQ];
+			double inst_acc = 0;
+#pragma unroll
+			for (int q = 0; q < NQ; ++q) acc[q] = 0;
+			for (int t = lane; t < tc; t += 32) {
+#pragma unroll
+				for (int q = 0; q < NQ; ++q) acc[q] += __ldcg(partial + ((size_t)(t0 + t) * K + k) * NQ + q);
+				if (INSTQ >= 0) {
+#pragma unroll
+					for (int kk = 0; kk < K; ++kk) inst_acc += __ldcg(partial + ((size_t)(t0 + t) * K + kk) * NQ + (INSTQ < 0 ? 0 : INSTQ));
+				}
+			}
+#pragma unroll
+			for (int q = 0; q < NQ; ++q) acc[q] = warpSum(acc[q]);
+			if (INSTQ >= 0) inst_acc = warpSum(inst_acc);
+			if (lane == 0) fn(st[s], inst, acc, inst_acc);
+			__syncwarp();
+		}
+		if (lane == 0 && st[s].done == RUNNING) atomicAdd(&running, 1);
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		ctrl->allDone = running == 0;
+		ctrl->counter = 0;
+	}
+}
+
+__device__ __forceinline__ bool fin(double v) { return isfinite(v); }
+__device__ __forceinline__ double normScale(const int32_t *insts, int inst) { return 1.0 / sqrt(double(insts[inst * PHB_IREC + I_NCELLS])); }
+
+template <int K>
+__device__ __forceinline__ int64_t vk(const int32_t *B, int64_t g, int k) {
+	return g + (int64_t)(K - 1) * B[B_INSTOFF] + (int64_t)k * B[B_INSTN];
+}
+
+template <int D>
+__device__ __forceinline__ void stencilNeighbors(const Dom<double, D> &dom, const Cell &c, int64_t *nb) {
+#pragma unroll
+	for (int f = 0; f < 2 * D; ++f) nb[f] = neighborIndex<double, D>(dom, c, f);
+}
+
+// y = A v at cell c, v(g, k) evaluated by `val` (also at the stencil neighbours).
+template <typename T, int D, int K, typename Val>
+__device__ __forceinline__ void applyA(const T *__restrict__ A, int64_t N, const Cell &c, const int64_t *nb, const bool *act, Val val, T *out) {
+	const T a0 = A[c.g];
+	T af[2 * D];
+#pragma unroll
+	for (int f = 0; f < 2 * D; ++f) af[f] = A[(f + 1) * N + c.g];
+#pragma unroll
+	for (int k = 0; k < K; ++k) {
+		if (!act[k]) { out[k] = 0; continue; }
+		T s = a0 * val(c.g, k);
+#pragma unroll
+		for (int f = 0; f < 2 * D; ++f)
+			if (nb[f] >= 0) s += af[f] * val(nb[f], k);
+		out[k] = s;
+	}
+}
+
+struct LoopCond {
+	cudaGraphConditionalHandle handle;
+	int active; // this kernel sets the loop condition
+};
+__device__ __forceinline__ void setLoop(const LoopCond lc, Control *ctrl) {
+	if (!lc.active) return;
+	const int loops = ++ctrl->loops; // one count per pass of the loop body
+	const bool cont = !ctrl->allDone && loops < ctrl->maxLoops;
+	cudaGraphSetConditional(lc.handle, cont ? 1u : 0u);
+}
+
+// kernels ------------------------------------------------------------------------------
+// SolverTolerance._resolve_scale (solvers/tolerance.py:241-257)
+__device__ __forceinline__ double resolveTol(const phb_tolerance &t, double scale) {
+	double tol = 0.0;
+	if (t.rtol > 0) tol = t.rtol * scale;
+	if (t.atol > 0) tol = fmax(tol, t.atol);
+	tol = fmax(tol, t.floor_eps * scale);
+	if (!(tol > 0.0)) tol = t.fallback;
+	return tol;
+}
+
+// Initial state of every system. fromInner: the tolerance was written into
+// SysState::innerTol by the refinement residual (mode ignored).
+__global__ void kInit(SysState *st, int nsys, phb_tolerance tol, int fromInner, int maxit, Control *ctrl, int maxLoops) {
+	for (int s = threadIdx.x; s < nsys; s += blockDim.x) {
+		double t;
+		if (fromInner) t = st[s].innerTol;
+		else if (tol.mode == 0) t = tol.atol;
+		else if (tol.mode == 2) t = tol.values[s];
+		else t = NAN; // resolved from the right-hand side by kResidual
+		SysState z;
+		memset(&z, 0, sizeof(z));
+		z.tol = t;
+		z.innerTol = t;
+		z.maxit = maxit;
+		z.best = INFINITY;
+		z.restart = 1;
+		z.bestIt = -1;
+		st[s] = z;
+	}
+	if (threadIdx.x == 0) { ctrl->counter = 0; ctrl->allDone = 0; ctrl->loops = 0; ctrl->maxLoops = maxLoops; }
+}
+
+// r = b - A x (and r0 = r for BiCGStab); rho = (r, r); the relative tolerance from (b, b);
+// initial convergence check (krylov.cu:292-366). The reference CG stops on an exactly zero
+// residual only, BiCGStab (and, here, every inner solve of the refinement: STOPSTART) on
+// crit < tol.
+template <typename T, int D, int K, bool BICG, bool STOPSTART>
+__global__ void __launch_bounds__(PHB_TILE) kResidual(Dom<double, D> dom, const T *__restrict__ A, const T *__restrict__ b,
+		const T *__restrict__ x, T *__restrict__ r, T *__restrict__ r0, SysState *st, double *partial, Control *ctrl, phb_tolerance tol) {
+	__shared__ int32_t sB[PHB_BREC];
+	Cell c;
+	const bool valid = loadCell<double, D>(dom, sB, c);
+	const int inst = sB[B_INST];
+	bool act[K];
+#pragma unroll
+	for (int k = 0; k < K; ++k) act[k] = st[inst * K + k].done == RUNNING;
+	double acc[2 * K];
+#pragma unroll
+	for (int k = 0; k < 2 * K; ++k) acc[k] = 0;
+	if (valid) {
+		int64_t nb[2 * D];
+		stencilNeighbors<D>(dom, c, nb);
+		T y[K];
+		applyA<T, D, K>(A, dom.ncells, c, nb, act, [&](int64_t g, int k) { return x[vk<K>(c.B, g, k)]; }, y);
+#pragma unroll
+		for (int k = 0; k < K; ++k) {
+			if (!act[k]) continue;
+			const int64_t o = vk<K>(c.B, c.g, k);
+			const T bi = b[o];
+			const T ri = bi - y[k];
+			r[o] = ri;
+			if (BICG) r0[o] = ri;
+			acc[2 * k] = double(ri) * double(ri);
+			acc[2 * k + 1] = double(bi) * double(bi);
+		}
+	}
+	if (storePartials<2 * K>(acc, partial, &ctrl->counter)) {
+		const bool relative = tol.mode == 1;
+		finalizeSystems<K, 2, 1>(dom.insts, dom.ninst, partial, st, ctrl, [&](SysState &s, int in, const double *red, double bb) {
+			const double ns = normScale(dom.insts, in);
+			// the rhs scale of the whole instance: all K right-hand sides together
+			if (relative) s.tol = resolveTol(tol, sqrt(bb / double(K)) * ns);
+			const double crit = sqrt(red[0]) * ns;
+			s.rho = red[0];
+			s.restart = 1;
+			s.crit = crit;
+			if (!fin(crit)) { s.done = NONFINITE; s.usedIt = 0; }
+			else if ((BICG || STOPSTART) ? crit < s.tol : crit == 0.0) { s.done = CONVERGED; s.usedIt = BICG ? -1 : 0; }
+		});
+	}
+}
+
+// CG phase 1 (kCgDirection, krylov.cu:428-498): p' = r + beta p (p' = r on restart,
+// evaluated at the stencil points), q = A p', (p', q); last CTA: alpha = rho / (p', q)
+template <typename T, int D, int K>
+__global__ void __launch_bounds__(PHB_TILE) kCgDirection(Dom<double, D> dom, const T *__restrict__ A, const T *__restrict__ r,
+		const T *__restrict__ pIn, T *__restrict__ pOut, T *__restrict__ q, SysState *st, double *partial, Control *ctrl) {
+	__shared__ int32_t sB[PHB_BREC];
+	Cell c;
+	const bool valid = loadCell<double, D>(dom, sB, c);
+	const int inst = sB[B_INST];
+	bool act[K], rs[K];
+	T beta[K];
+#pragma unroll
+	for (int k = 0; k < K; ++k) {
+		const SysState &s = st[inst * K + k];
+		act[k] = s.done == RUNNING;
+		rs[k] = s.restart;
+		beta[k] = T(s.beta);
+	}
+	double acc[K];
+#pragma unroll
+	for (int k = 0; k < K; ++k) acc[k] = 0;
+	if (valid) {
+		int64_t nb[2 * D];
+		stencilNeighbors<D>(dom, c, nb);
+		auto pv = [&](int64_t g, int k) {
+			const int64_t o = vk<K>(c.B, g, k);
+			return rs[k] ? r[o] : r[o] + beta[k] * pIn[o];
+		};
+		T y[K];
+		applyA<T, D, K>(A, dom.ncells, c, nb, act, pv, y);
+#pragma unroll
+		for (int k = 0; k < K; ++k) {
+			if (!act[k]) continue;
+			const int64_t o = vk<K>(c.B, c.g, k);
+			const T pi = pv(c.g, k);
+			pOut[o] = pi;
+			q[o] = y[k];
+			acc[k] = double(pi) * double(y[k]);
+		}
+	}
+	if (storePartials<K>(acc, partial, &ctrl->counter)) {
+		finalizeSystems<K, 1>(dom.insts, dom.ninst, partial, st, ctrl, [&](SysState &s, int, const double *red, double) {
+			const double alpha = s.rho / red[0];
+			s.restart = 0;
+			if (!fin(alpha)) { s.done = NONFINITE; s.usedIt = s.it; }
+			else s.alpha = alpha;
+		});
+	}
+}
+
+// CG phase 2 (kCgUpdate, krylov.cu:502-568): x += alpha p, r -= alpha q, (r, r); last CTA:
+// convergence, beta = (r, r)_new / (r, r)_old, optional best-iterate tracking.
+template <typename T, int D, int K>
+__global__ void __launch_bounds__(PHB_TILE) kCgUpdate(Dom<double, D> dom, T *__restrict__ r, const T *__restrict__ p,
+		const T *__restrict__ q, T *__restrict__ x, T *__restrict__ xbest, SysState *st, double *partial, Control *ctrl,
+		int returnBest, LoopCond lc) {
+	__shared__ int32_t sB[PHB_BREC];
+	Cell c;
+	const bool valid = loadCell<double, D>(dom, sB, c);
+	const int inst = sB[B_INST];
+	double acc[K];
+#pragma unroll
+	for (int k = 0; k < K; ++k) acc[k] = 0;
+	if (valid) {
+#pragma unroll
+		for (int k = 0; k < K; ++k) {
+			const SysState &s = st[inst * K + k];
+			if (s.done != RUNNING) continue;
+			const T alpha = T(s.alpha);
+			const int64_t o = vk<K>(c.B, c.g, k);
+			const T xi = x[o];
+			if (s.saveBest && xbest) xbest[o] = xi;
+			x[o] = xi + alpha * p[o];
+			const T ri = r[o] - alpha * q[o];
+			r[o] = ri;
+			acc[k] = double(ri) * double(ri);
+		}
+	}
+	if (storePartials<K>(acc, partial, &ctrl->counter)) {
+		finalizeSystems<K, 1>(dom.insts, dom.ninst, partial, st, ctrl, [&](SysState &s, int in, const double *red, double) {
+			const double crit = sqrt(red[0]) * normScale(dom.insts, in);
+			++s.it;
+			s.crit = crit;
+			s.saveBest = 0;
+			s.usedIt = s.it - 1;
+			if (!fin(crit)) { s.done = NONFINITE; return; }
+			if (returnBest) {
+				if (crit < s.best) { s.best = crit; s.bestIt = s.it - 1; s.saveBest = 1; }
+				if (s.it > 1 && crit >= s.last) ++s.rising; else s.rising = 0;
+				s.last = crit;
+			}
+			if (crit < s.tol) s.done = CONVERGED;
+			else if (s.it >= s.maxit) s.done = MAXIT;
+			else if (returnBest && s.rising >= RISING_CUTOFF) s.done = RISING;
+			else {
+				s.beta = red[0] / s.rho;
+				s.rho = red[0];
+				if (!fin(s.beta)) s.done = NONFINITE;
+			}
+		});
+		if (threadIdx.x == 0) setLoop(lc, ctrl);
+	}
+}
+
+// BiCGStab phase 1 (kBicgP + kBicgV, krylov.cu:599-676): p = r + beta (p - omega v) (p = r
+// on restart) evaluated at the stencil points, v = A p, (r0, v); last CTA: alpha
+template <typename T, int D, int K>
+__global__ void __launch_bounds__(PHB_TILE) kBicgV(Dom<double, D> dom, const T *__restrict__ A, const T *__restrict__ r,
+		const T *__restrict__ pIn, const T *__restrict__ vIn, T *__restrict__ pOut, T *__restrict__ vOut, const T *__restrict__ r0,
+		SysState *st, double *partial, Control *ctrl) {
+	__shared__ int32_t sB[PHB_BREC];
+	Cell c;
+	const bool valid = loadCell<double, D>(dom, sB, c);
+	const int inst = sB[B_INST];
+	bool act[K], rs[K];
+	T beta[K], omega[K];
+#pragma unroll
+	for (int k = 0; k < K; ++k) {
+		const SysState &s = st[inst * K + k];
+		act[k] = s.done == RUNNING;
+		rs[k] = s.restart;
+		beta[k] = T(s.beta);
+		omega[k] = T(s.omega);
+	}
+	double acc[K];
+#pragma unroll
+	for (int k = 0; k < K; ++k) acc[k] = 0;
+	if (valid) {
+		int64_t nb[2 * D];
+		stencilNeighbors<D>(dom, c, nb);
+		auto pv = [&](int64_t g, int k) {
+			const int64_t o = vk<K>(c.B, g, k);
+			return rs[k] ? r[o] : r[o] + beta[k] * (pIn[o] - omega[k] * vIn[o]);
+		};
+		T y[K];
+		applyA<T, D, K>(A, dom.ncells, c, nb, act, pv, y);
+#pragma unroll
+		for (int k = 0; k < K; ++k) {
+			if (!act[k]) continue;
+			const int64_t o = vk<K>(c.B, c.g, k);
+			pOut[o] = pv(c.g, k);
+			vOut[o] = y[k];
+			acc[k] = double(r0[o]) * double(y[k]);
+		}
+	}
+	if (storePartials<K>(acc, partial, &ctrl->counter)) {
+		finalizeSystems<K, 1>(dom.insts, dom.ninst, partial, st, ctrl, [&](SysState &s, int, const double *red, double) {
+			const double alpha = s.rho / red[0];
+			s.restart = 0;
+			if (!fin(alpha)) { s.done = NONFINITE; s.usedIt = s.it; }
+			else s.alpha = alpha;
+		});
+	}
+}
+
+// BiCGStab phase 2 (kBicgT, krylov.cu:680-750): s = r - alpha v on the fly, t = A s,
+// (t,s), (t,t), (s,s); last CTA: omega, or convergence after the half step.
+template <typename T, int D, int K>
+__global__ void __launch_bounds__(PHB_TILE) kBicgT(Dom<double, D> dom, const T *__restrict__ A, const T *__restrict__ r,
+		const T *__restrict__ v, T *__restrict__ t, SysState *st, double *partial, Control *ctrl) {
+	__shared__ int32_t sB[PHB_BREC];
+	Cell c;
+	const bool valid = loadCell<double, D>(dom, sB, c);
+	const int inst = sB[B_INST];
+	bool act[K];
+	T alpha[K];
+#pragma unroll
+	for (int k = 0; k < K; ++k) {
+		const SysState &s = st[inst * K + k];
+		act[k] = s.done == RUNNING;
+		alpha[k] = T(s.alpha);
+	}
+	double acc[3 * K];
+#pragma unroll
+	for (int k = 0; k < 3 * K; ++k) acc[k] = 0;
+	if (valid) {
+		int64_t nb[2 * D];
+		stencilNeighbors<D>(dom, c, nb);
+		auto sv = [&](int64_t g, int k) {
+			const int64_t o = vk<K>(c.B, g, k);
+			return r[o] - alpha[k] * v[o];
+		};
+		T y[K];
+		applyA<T, D, K>(A, dom.ncells, c, nb, act, sv, y);
+#pragma unroll
+		for (int k = 0; k < K; ++k) {
+			if (!act[k]) continue;
+			const int64_t o = vk<K>(c.B, c.g, k);
+			const T si = sv(c.g, k);
+			t[o] = y[k];
+			acc[3 * k + 0] = double(y[k]) * double(si);
+			acc[3 * k + 1] = double(y[k]) * double(y[k]);
+			acc[3 * k + 2] = double(si) * double(si);
+		}
+	}
+	if (storePartials<3 * K>(acc, partial, &ctrl->counter)) {
+		finalizeSystems<K, 3>(dom.insts, dom.ninst, partial, st, ctrl, [&](SysState &s, int in, const double *red, double) {
+			const double critS = sqrt(red[2]) * normScale(dom.insts, in);
+			s.halfCrit = critS;
+			if (!fin(critS)) { s.done = NONFINITE; s.crit = critS; s.usedIt = s.it; }
+			else if (critS < s.tol) { s.halfDone = 1; s.omega = 0.0; }
+			else {
+				const double omega = red[0] / red[1];
+				if (!fin(omega)) { s.done = NONFINITE; s.crit = critS; s.usedIt = s.it; }
+				else s.omega = omega;
+			}
+		});
+	}
+}
+
+// BiCGStab phase 3 (kBicgUpdate, krylov.cu:754-824): x += alpha p + omega s, r = s - omega t,
+// (r0, r), (r, r); last CTA: convergence and beta.
+template <typename T, int D, int K>
+__global__ void __launch_bounds__(PHB_TILE) kBicgUpdate(Dom<double, D> dom, T *__restrict__ r, const T *__restrict__ r0,
+		const T *__restrict__ p, const T *__restrict__ v, const T *__restrict__ t, T *__restrict__ x, SysState *st,
+		double *partial, Control *ctrl, LoopCond lc) {
+	__shared__ int32_t sB[PHB_BREC];
+	Cell c;
+	const bool valid = loadCell<double, D>(dom, sB, c);
+	const int inst = sB[B_INST];
+	double acc[2 * K];
+#pragma unroll
+	for (int k = 0; k < 2 * K; ++k) acc[k] = 0;
+	if (valid) {
+#pragma unroll
+		for (int k = 0; k < K; ++k) {
+			const SysState &s = st[inst * K + k];
+			if (s.done != RUNNING) continue;
+			const T alpha = T(s.alpha), omega = T(s.omega);
+			const int64_t o = vk<K>(c.B, c.g, k);
+			const T si = r[o] - alpha * v[o];
+			if (s.halfDone) {
+				x[o] += alpha * p[o];
+				r[o] = si;
+			} else {
+				x[o] += alpha * p[o] + omega * si;
+				const T ri = si - omega * t[o];
+				r[o] = ri;
+				acc[2 * k + 0] = double(r0[o]) * double(ri);
+				acc[2 * k + 1] = double(ri) * double(ri);
+			}
+		}
+	}
+	if (storePartials<2 * K>(acc, partial, &ctrl->counter)) {
+		finalizeSystems<K, 2>(dom.insts, dom.ninst, partial, st, ctrl, [&](SysState &s, int in, const double *red, double) {
+			if (s.halfDone) { s.done = CONVERGED; s.crit = s.halfCrit; s.usedIt = s.it; return; }
+			const double crit = sqrt(red[1]) * normScale(dom.insts, in);
+			s.crit = crit;
+			if (!fin(crit)) { s.done = NONFINITE; s.usedIt = s.it; }
+			else if (crit < s.tol) { s.done = CONVERGED; s.usedIt = s.it + 1; }
+			else {
+				++s.it;
+				s.usedIt = s.it - 1;
+				const double beta = (red[0] / s.rho) * (s.alpha / s.omega);
+				s.rho = red[0];
+				s.beta = beta;
+				if (!fin(beta)) s.done = NONFINITE;
+				else if (s.it >= s.maxit) s.done = MAXIT;
+			}
+		});
+		if (threadIdx.x == 0) setLoop(lc, ctrl);
+	}
+}
+
+// kRestoreBest (krylov.cu:370-375): systems that stopped without converging return their
+// best iterate
+template <typename T, int K>
+__global__ void kRestoreBest(const int32_t *__restrict__ insts, int ninst, int64_t ncells, T *x, const T *xbest, const SysState *st) {
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ncells * K; i += (int64_t)gridDim.x * blockDim.x) {
+		// instance of vector entry i in the [inst][K][cells] layout
+		int lo = 0, hi = ninst - 1;
+		while (lo < hi) {
+			const int mid = (lo + hi + 1) >> 1;
+			if ((int64_t)K * insts[mid * PHB_IREC + I_CELLOFF] <= i) lo = mid; else hi = mid - 1;
+		}
+		const int64_t base = (int64_t)K * insts[lo * PHB_IREC + I_CELLOFF];
+		const int k = int((i - base) / insts[lo * PHB_IREC + I_NCELLS]);
+		const SysState &s = st[lo * K + k];
+		if ((s.done == MAXIT || s.done == RISING) && s.bestIt >= 0 && s.best < s.crit) x[i] = xbest[i];
+	}
+}
+
+// FP64 refinement residual: r64 = b - A64 x; r32 = float(r64), e32 = 0; last CTA: the
+// outer tolerance (resolved from b on the first sweep), outer convergence per system, the
+// inner tolerance innerRtol * ||r||/sqrt(n) (infinite for systems that are done) and the
+// outer loop condition.
+template <int D, int K>
+__global__ void __launch_bounds__(PHB_TILE) kRefineResidual(Dom<double, D> dom, const double *__restrict__ A, const double *__restrict__ b,
+		const double *__restrict__ x, float *__restrict__ r32, float *__restrict__ e32, SysState *st, double *partial, Control *ctrl,
+		double innerRtol, int maxOuter, phb_tolerance tol, SysState *inner, LoopCond lc) {
+	__shared__ int32_t sB[PHB_BREC];
+	Cell c;
+	const bool valid = loadCell<double, D>(dom, sB, c);
+	double acc[2 * K];
+#pragma unroll
+	for (int k = 0; k < 2 * K; ++k) acc[k] = 0;
+	if (valid) {
+		int64_t nb[2 * D];
+		stencilNeighbors<D>(dom, c, nb);
+		bool act[K];
+#pragma unroll
+		for (int k = 0; k < K; ++k) act[k] = true;
+		double y[K];
+		applyA<double, D, K>(A, dom.ncells, c, nb, act, [&](int64_t g, int k) { return x[vk<K>(c.B, g, k)]; }, y);
+#pragma unroll
+		for (int k = 0; k < K; ++k) {
+			const int64_t o = vk<K>(c.B, c.g, k);
+			const double bi = b[o];
+			const double ri = bi - y[k];
+			r32[o] = float(ri);
+			e32[o] = 0.f;
+			acc[2 * k] = ri * ri;
+			acc[2 * k + 1] = bi * bi;
+		}
+	}
+	if (storePartials<2 * K>(acc, partial, &ctrl->counter)) {
+		const int nsys = dom.ninst * K;
+		// every system is visited, also once done, so that the inner solve of a finished
+		// system sees an infinite tolerance and stops at once
+		__shared__ int running;
+		if (threadIdx.x == 0) running = 0;
+		__threadfence();
+		__syncthreads();
+		const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+		for (int s = warp; s < nsys; s += NWARPS) {
+			const int inst = s / K, k = s - inst * K;
+			const int t0 = dom.insts[inst * PHB_IREC + I_TILESTART], tc = dom.insts[inst * PHB_IREC + I_TILECOUNT];
+			double a = 0, bb = 0;
+			for (int t = lane; t < tc; t += 32) {
+				a += __ldcg(partial + ((size_t)(t0 + t) * K + k) * 2);
+#pragma unroll
+				for (int kk = 0; kk < K; ++kk) bb += __ldcg(partial + ((size_t)(t0 + t) * K + kk) * 2 + 1);
+			}
+			a = warpSum(a);
+			bb = warpSum(bb);
+			if (lane == 0) {
+				SysState &o = st[s];
+				const double ns = normScale(dom.insts, inst);
+				if (o.it == 0 && o.done == RUNNING && tol.mode == 1) o.tol = resolveTol(tol, sqrt(bb / double(K)) * ns);
+				const double crit = sqrt(a) * ns;
+				o.crit = crit;
+				if (o.done == RUNNING) {
+					if (!fin(crit)) o.done = NONFINITE;
+					else if (crit < o.tol) o.done = CONVERGED;
+					else if (o.it >= maxOuter) o.done = MAXIT;
+					else ++o.it;
+				}
+				o.usedIt = o.it;
+				inner[s].innerTol = o.done == RUNNING ? fmax(innerRtol * crit, 0.25 * o.tol) : INFINITY;
+				if (o.done == RUNNING) atomicAdd(&running, 1);
+			}
+		}
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			ctrl->allDone = running == 0;
+			ctrl->counter = 0;
+			setLoop(lc, ctrl);
+		}
+	}
+}
+
+template <int K>
+__global__ void kRefineUpdate(int64_t n, double *__restrict__ x, const float *__restrict__ e) {
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) x[i] += double(e[i]);
+}
+
+__global__ void kInitOuter(SysState *st, int nsys, phb_tolerance tol, Control *ctrl, int maxLoops) {
+	for (int s = threadIdx.x; s < nsys; s += blockDim.x) {
+		SysState z;
+		memset(&z, 0, sizeof(z));
+		z.tol = tol.mode == 0 ? tol.atol : tol.mode == 2 ? tol.values[s] : NAN;
+		st[s] = z;
+	}
+	if (threadIdx.x == 0) { ctrl->counter = 0; ctrl->allDone = 0; ctrl->loops = 0; ctrl->maxLoops = maxLoops; }
+}
+
+// host side --------------------------------------------------------------------------------
+static size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+struct Layout {
+	size_t off[12];
+	size_t total;
+};
+
+static int vecCount(int kind) { return kind == 0 ? 5 : 7; } // CG: r q p0 p1 xbest; BiCG: r r0 p0 p1 v0 v1 t
+
+static Layout solveLayout(const phb_domain *dom, int kind, int vecBytes, int nrhs) {
+	Layout L;
+	size_t o = 0;
+	const size_t vb = align256((size_t)dom->ncells * nrhs * vecBytes);
+	for (int i = 0; i < vecCount(kind); ++i) { L.off[i] = o; o += vb; }
+	L.off[10] = o; // partials
+	o += align256((size_t)dom->ntiles * nrhs * 3 * sizeof(double));
+	L.total = o;
+	return L;
+}
+
+struct StateLayout { size_t ctrl, st, ctrl2, st2, total; };
+static StateLayout stateLayout(const phb_domain *dom, int nrhs) {
+	StateLayout L;
+	const size_t nsys = (size_t)dom->ninst * nrhs;
+	L.ctrl = 0;
+	L.st = 256;
+	L.ctrl2 = align256(L.st + nsys * sizeof(SysState));
+	L.st2 = L.ctrl2 + 256;
+	L.total = align256(L.st2 + nsys * sizeof(SysState));
+	return L;
+}
+
+// capture helpers ----------------------------------------------------------------------------
+struct Streams { cudaStream_t s[3] = {nullptr, nullptr, nullptr}; int device = -1; };
+static thread_local Streams tlStreams;
+static int getStreams(Streams *&out) {
+	int dev;
+	PHB_CUDA(cudaGetDevice(&dev));
+	if (tlStreams.device != dev) {
+		for (auto &s : tlStreams.s) {
+			if (s) cudaStreamDestroy(s);
+			s = nullptr;
+		}
+		for (auto &s : tlStreams.s) PHB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+		tlStreams.device = dev;
+	}
+	out = &tlStreams;
+	return PHB_OK;
+}
+
+// Add a conditional WHILE node to the graph `cap` is capturing and capture `body` into it on
+// `bodyStream`. The condition starts true and the body's last kernel sets it.
+static int emitWhile(cudaStream_t cap, cudaStream_t bodyStream, const std::function<int(cudaStream_t, LoopCond)> &body) {
+	cudaStreamCaptureStatus status;
+	cudaGraph_t graph;
+	const cudaGraphNode_t *deps = nullptr;
+	size_t ndeps = 0;
+	PHB_CUDA(cudaStreamGetCaptureInfo(cap, &status, nullptr, &graph, &deps, &ndeps));
+	if (status != cudaStreamCaptureStatusActive) return setError(PHB_ERR_STATE, "emitWhile: stream is not capturing");
+	cudaGraphConditionalHandle handle;
+	PHB_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+	cudaGraphNodeParams params = {};
+	params.type = cudaGraphNodeTypeConditional;
+	params.conditional.handle = handle;
+	params.conditional.type = cudaGraphCondTypeWhile;
+	params.conditional.size = 1;
+	cudaGraphNode_t node;
+	PHB_CUDA(cudaGraphAddNode(&node, graph, deps, ndeps, &params));
+	PHB_CUDA(cudaStreamUpdateCaptureDependencies(cap, &node, 1, cudaStreamSetCaptureDependencies));
+	cudaGraph_t bodyGraph = params.conditional.phGraph_out[0];
+	PHB_CUDA(cudaStreamBeginCaptureToGraph(bodyStream, bodyGraph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+	const int st = body(bodyStream, LoopCond{handle, 1});
+	cudaGraph_t ended;
+	const cudaError_t e = cudaStreamEndCapture(bodyStream, &ended);
+	if (st != PHB_OK) return st;
+	PHB_CUDA(e);
+	return PHB_OK;
+}
+
+struct CachedGraph { cudaGraphExec_t exec; };
+static std::mutex gMutex;
+static std::map<std::string, CachedGraph> gGraphs;
+
+static int releaseGraphsLocked() {
+	for (auto &kv : gGraphs) cudaGraphExecDestroy(kv.second.exec);
+	gGraphs.clear();
+	return PHB_OK;
+}
+
+// Run `emit` (which records work on a capturing stream) either spliced into the caller's
+// ongoing capture, or as a cached graph launched on `stream`.
+static int runGraph(cudaStream_t stream, const std::string &key, const std::function<int(cudaStream_t, Streams &)> &emit) {
+	Streams *ss;
+	int rc = getStreams(ss);
+	if (rc) return rc;
+	cudaStreamCaptureStatus status;
+	PHB_CUDA(cudaStreamIsCapturing(stream, &status));
+	if (status == cudaStreamCaptureStatusActive) return emit(stream, *ss);
+	std::lock_guard<std::mutex> lock(gMutex);
+	auto it = gGraphs.find(key);
+	if (it == gGraphs.end()) {
+		if (gGraphs.size() >= 64) releaseGraphsLocked();
+		PHB_CUDA(cudaStreamBeginCapture(ss->s[0], cudaStreamCaptureModeThreadLocal));
+		rc = emit(ss->s[0], *ss);
+		cudaGraph_t graph = nullptr;
+		const cudaError_t e = cudaStreamEndCapture(ss->s[0], &graph);
+		if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+		PHB_CUDA(e);
+		CachedGraph cg;
+		const cudaError_t ei = cudaGraphInstantiate(&cg.exec, graph, 0);
+		cudaGraphDestroy(graph);
+		PHB_CUDA(ei);
+		it = gGraphs.emplace(key, cg).first;
+	}
+	PHB_CUDA(cudaGraphLaunch(it->second.exec, stream));
+	return PHB_OK;
+}
+
+template <typename A, typename B>
+static std::string makeKey(const char *tag, const A &a, const B &b) {
+	std::string k(tag);
+	k.append(reinterpret_cast<const char *>(&a), sizeof(A));
+	k.append(reinterpret_cast<const char *>(&b), sizeof(B));
+	return k;
+}
+
+static int gridFor(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 148 * 16); }
+
+// the Krylov loop for one solve, recorded on `s`
+template <typename T, int D, int K>
+static int emitSolve(const phb_domain *dom, const phb_solve *sv, cudaStream_t s, Streams &ss, int useGraph, bool stopStart, int fromInner = 0) {
+	Dom<double, D> dm(*dom);
+	const Layout L = solveLayout(dom, sv->kind, sizeof(T), K);
+	const StateLayout SL = stateLayout(dom, K);
+	char *w = (char *)sv->work;
+	char *sb = (char *)sv->state;
+	Control *ctrl = (Control *)(sb + SL.ctrl);
+	SysState *st = (SysState *)(sb + SL.st);
+	double *partial = (double *)(w + L.off[10]);
+	const T *A = (const T *)sv->A;
+	const T *b = (const T *)sv->b;
+	T *x = (T *)sv->x;
+	const int nsys = dom->ninst * K;
+	const int tiles = dom->ntiles;
+	const int maxit = std::max(1, sv->maxit);
+	if (sv->kind == 0) {
+		T *r = (T *)(w + L.off[0]), *q = (T *)(w + L.off[1]), *p0 = (T *)(w + L.off[2]), *p1 = (T *)(w + L.off[3]);
+		T *xbest = sv->return_best ? (T *)(w + L.off[4]) : nullptr;
+		const int maxLoops = maxit / 2 + 2;
+		kInit<<<1, 256, 0, s>>>(st, nsys, sv->tol, fromInner, maxit, ctrl, maxLoops);
+		if (stopStart) kResidual<T, D, K, false, true><<<tiles, PHB_TILE, 0, s>>>(dm, A, b, x, r, nullptr, st, partial, ctrl, sv->tol);
+		else kResidual<T, D, K, false, false><<<tiles, PHB_TILE, 0, s>>>(dm, A, b, x, r, nullptr, st, partial, ctrl, sv->tol);
+		int rc = checkLaunch("kResidual");
+		if (rc) return rc;
+		auto body = [&](cudaStream_t bs, LoopCond lc) -> int {
+			for (int half = 0; half < 2; ++half) {
+				T *pIn = half == 0 ? p0 : p1, *pOut = half == 0 ? p1 : p0;
+				kCgDirection<T, D, K><<<tiles, PHB_TILE, 0, bs>>>(dm, A, r, pIn, pOut, q, st, partial, ctrl);
+				LoopCond l2 = lc;
+				l2.active = half == 1 ? lc.active : 0;
+				kCgUpdate<T, D, K><<<tiles, PHB_TILE, 0, bs>>>(dm, r, pOut, q, x, xbest, st, partial, ctrl, sv->return_best, l2);
+			}
+			return checkLaunch("CG body");
+		};
+		if (useGraph) { rc = emitWhile(s, ss.s[useGraph == 2 ? 2 : 1], body); if (rc) return rc; }
+		else {
+			// host loop (no graph): poll allDone every check_every iterations
+			int *hflag = nullptr;
+			PHB_CUDA(cudaMallocHost(&hflag, sizeof(int)));
+			const int chk = std::max(1, sv->check_every);
+			for (int loops = 0; loops < maxLoops; loops += chk) {
+				for (int i = 0; i < chk; ++i) { rc = body(s, LoopCond{0, 0}); if (rc) break; }
+				if (rc) break;
+				cudaMemcpyAsync(hflag, &ctrl->allDone, sizeof(int), cudaMemcpyDeviceToHost, s);
+				cudaStreamSynchronize(s);
+				if (*hflag) break;
+			}
+			cudaFreeHost(hflag);
+			if (rc) return rc;
+		}
+		if (xbest) kRestoreBest<T, K><<<gridFor(dom->ncells * K), 256, 0, s>>>(dom->insts, dom->ninst, dom->ncells, x, xbest, st);
+		return checkLaunch("CG epilogue");
+	}
+	T *r = (T *)(w + L.off[0]), *r0 = (T *)(w + L.off[1]), *p0 = (T *)(w + L.off[2]), *p1 = (T *)(w + L.off[3]);
+	T *v0 = (T *)(w + L.off[4]), *v1 = (T *)(w + L.off[5]), *t = (T *)(w + L.off[6]);
+	const int maxLoops = maxit / 2 + 2;
+	kInit<<<1, 256, 0, s>>>(st, nsys, sv->tol, fromInner, maxit, ctrl, maxLoops);
+	kResidual<T, D, K, true, true><<<tiles, PHB_TILE, 0, s>>>(dm, A, b, x, r, r0, st, partial, ctrl, sv->tol);
+	int rc = checkLaunch("kResidual");
+	if (rc) return rc;
+	auto body = [&](cudaStream_t bs, LoopCond lc) -> int {
+		for (int half = 0; half < 2; ++half) {
+			T *pIn = half == 0 ? p0 : p1, *pOut = half == 0 ? p1 : p0;
+			T *vIn = half == 0 ? v0 : v1, *vOut = half == 0 ? v1 : v0;
+			kBicgV<T, D, K><<<tiles, PHB_TILE, 0, bs>>>(dm, A, r, pIn, vIn, pOut, vOut, r0, st, partial, ctrl);
+			kBicgT<T, D, K><<<tiles, PHB_TILE, 0, bs>>>(dm, A, r, vOut, t, st, partial, ctrl);
+			LoopCond l2 = lc;
+			l2.active = half == 1 ? lc.active : 0;
+			kBicgUpdate<T, D, K><<<tiles, PHB_TILE, 0, bs>>>(dm, r, r0, pOut, vOut, t, x, st, partial, ctrl, l2);
+		}
+		return checkLaunch("BiCGStab body");
+	};
+	if (useGraph) return emitWhile(s, ss.s[useGraph == 2 ? 2 : 1], body);
+	int *hflag = nullptr;
+	PHB_CUDA(cudaMallocHost(&hflag, sizeof(int)));
+	const int chk = std::max(1, sv->check_every);
+	for (int loops = 0; loops < maxLoops; loops += chk) {
+		for (int i = 0; i < chk; ++i) { rc = body(s, LoopCond{0, 0}); if (rc) break; }
+		if (rc) break;
+		cudaMemcpyAsync(hflag, &ctrl->allDone, sizeof(int), cudaMemcpyDeviceToHost, s);
+		cudaStreamSynchronize(s);
+		if (*hflag) break;
+	}
+	cudaFreeHost(hflag);
+	return rc;
+}
+
+#define PHB_SOLVE_DISPATCH(DIMS, VEC, K, ...)                                                   \
+	do {                                                                                        \
+		if ((DIMS) == 2 && (VEC) == PHB_F64 && (K) == 1) { using T = double; constexpr int D = 2, KK = 1; __VA_ARGS__; } \
+		else if ((DIMS) == 2 && (VEC) == PHB_F64 && (K) == 2) { using T = double; constexpr int D = 2, KK = 2; __VA_ARGS__; } \
+		else if ((DIMS) == 3 && (VEC) == PHB_F64 && (K) == 1) { using T = double; constexpr int D = 3, KK = 1; __VA_ARGS__; } \
+		else if ((DIMS) == 3 && (VEC) == PHB_F64 && (K) == 3) { using T = double; constexpr int D = 3, KK = 3; __VA_ARGS__; } \
+		else if ((DIMS) == 2 && (VEC) == PHB_F32 && (K) == 1) { using T = float; constexpr int D = 2, KK = 1; __VA_ARGS__; } \
+		else if ((DIMS) == 2 && (VEC) == PHB_F32 && (K) == 2) { using T = float; constexpr int D = 2, KK = 2; __VA_ARGS__; } \
+		else if ((DIMS) == 3 && (VEC) == PHB_F32 && (K) == 1) { using T = float; constexpr int D = 3, KK = 1; __VA_ARGS__; } \
+		else if ((DIMS) == 3 && (VEC) == PHB_F32 && (K) == 3) { using T = float; constexpr int D = 3, KK = 3; __VA_ARGS__; } \
+		else return setError(PHB_ERR_ARG, "unsupported dims/dtype/nrhs combination");            \
+	} while (0)
+
+} // namespace phb
+
+using namespace phb;
+
+extern "C" int64_t phb_solve_work_bytes(const phb_domain *dom, int kind, int vec_dtype, int nrhs) {
+	if (!dom) return -1;
+	return (int64_t)solveLayout(dom, kind, vec_dtype == PHB_F64 ? 8 : 4, nrhs).total;
+}
+extern "C" int64_t phb_solve_state_bytes(const phb_domain *dom, int nrhs) {
+	if (!dom) return -1;
+	return (int64_t)stateLayout(dom, nrhs).total;
+}
+
+extern "C" int phb_solve_run(const phb_domain *dom, const phb_solve *s, phb_stream stream) {
+	if (!dom || !s || !s->A || !s->b || !s->x || !s->work || !s->state || (s->tol.mode == 2 && !s->tol.values)) return setError(PHB_ERR_ARG, "phb_solve_run: null argument");
+	if (s->vec_dtype != s->mat_dtype) return setError(PHB_ERR_ARG, "phb_solve_run: matrix and vector dtype must match");
+	if (s->kind != 0 && s->kind != 1) return setError(PHB_ERR_ARG, "phb_solve_run: kind must be 0 (CG) or 1 (BiCGStab)");
+	if (dom->ntiles == 0) return PHB_OK;
+	cudaStream_t st = (cudaStream_t)stream;
+	const std::string key = makeKey("solve", *dom, *s);
+	PHB_SOLVE_DISPATCH(dom->dims, s->vec_dtype, s->nrhs, {
+		if (!s->use_graph) {
+			Streams *ss; int rc = getStreams(ss); if (rc) return rc;
+			return emitSolve<T, D, KK>(dom, s, st, *ss, 0, false);
+		}
+		return runGraph(st, key, [&](cudaStream_t cs, Streams &ss) { return emitSolve<T, D, KK>(dom, s, cs, ss, 1, false); });
+	});
+	return PHB_OK;
+}
+
+extern "C" int phb_solve_results(const phb_domain *dom, const phb_solve *s, phb_solve_result *out, phb_stream stream) {
+	if (!dom || !s || !out || !s->state) return setError(PHB_ERR_ARG, "phb_solve_results: null argument");
+	const int nsys = dom->ninst * s->nrhs;
+	std::vector<SysState> h(nsys);
+	const StateLayout SL = stateLayout(dom, s->nrhs);
+	PHB_CUDA(cudaMemcpyAsync(h.data(), (char *)s->state + SL.st, nsys * sizeof(SysState), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+	PHB_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+	for (int i = 0; i < nsys; ++i) {
+		const SysState &x = h[i];
+		phb_solve_result &o = out[i];
+		o.final_residual = x.crit;
+		o.used_iterations = x.usedIt;
+		o.converged = x.done == CONVERGED;
+		o.finite = std::isfinite(x.crit);
+		o.status = x.done;
+		if (s->return_best && (x.done == MAXIT || x.done == RISING) && x.bestIt >= 0 && x.best < x.crit) {
+			o.used_iterations = x.bestIt;
+			o.final_residual = x.best;
+		}
+	}
+	return PHB_OK;
+}
+
+extern "C" int phb_release_graphs(void) {
+	std::lock_guard<std::mutex> lock(gMutex);
+	return releaseGraphsLocked();
+}
+
+// refinement ------------------------------------------------------------------------------
+extern "C" int64_t phb_refine_work_bytes(const phb_domain *dom, int kind, int nrhs) {
+	if (!dom) return -1;
+	const size_t inner = solveLayout(dom, kind, 4, nrhs).total;
+	const size_t v = align256((size_t)dom->ncells * nrhs * 4);
+	return (int64_t)(inner + 2 * v + align256((size_t)dom->ntiles * nrhs * 2 * sizeof(double)));
+}
+
+template <int D, int K>
+static int emitRefine(const phb_domain *dom, const phb_refine *rf, cudaStream_t s, Streams &ss) {
+	Dom<double, D> dm(*dom);
+	const size_t inner = solveLayout(dom, rf->kind, 4, K).total;
+	const size_t vb = align256((size_t)dom->ncells * K * 4);
+	char *w = (char *)rf->work;
+	float *r32 = (float *)(w + inner);
+	float *e32 = (float *)(w + inner + vb);
+	double *partial = (double *)(w + inner + 2 * vb);
+	const StateLayout SL = stateLayout(dom, K);
+	char *sb = (char *)rf->state;
+	Control *ctrlO = (Control *)(sb + SL.ctrl2);
+	SysState *stO = (SysState *)(sb + SL.st2);
+	SysState *stI = (SysState *)(sb + SL.st);
+	const int nsys = dom->ninst * K;
+	phb_solve in = {};
+	in.kind = rf->kind;
+	in.vec_dtype = PHB_F32;
+	in.mat_dtype = PHB_F32;
+	in.nrhs = K;
+	in.maxit = rf->inner_maxit;
+	in.return_best = 0;
+	in.use_graph = 1;
+	in.A = rf->A32;
+	in.b = r32;
+	in.x = e32;
+	in.tol = phb_tolerance{}; // unused: the inner tolerance is SysState::innerTol
+	in.work = rf->work;
+	in.state = rf->state;
+	kInitOuter<<<1, 256, 0, s>>>(stO, nsys, rf->tol, ctrlO, rf->max_outer + 2);
+	PHB_CUDA(cudaGetLastError());
+	auto outer = [&](cudaStream_t os, LoopCond lc) -> int {
+		kRefineResidual<D, K><<<dom->ntiles, PHB_TILE, 0, os>>>(dm, rf->A64, rf->b, rf->x, r32, e32, stO, partial, ctrlO,
+			rf->inner_rtol, rf->max_outer, rf->tol, stI, lc);
+		int rc = checkLaunch("kRefineResidual");
+		if (rc) return rc;
+		rc = emitSolve<float, D, K>(dom, &in, os, ss, 2, true, 1);
+		if (rc) return rc;
+		kRefineUpdate<K><<<gridFor(dom->ncells * K), 256, 0, os>>>(dom->ncells * K, rf->x, e32);
+		return checkLaunch("kRefineUpdate");
+	};
+	return emitWhile(s, ss.s[1], outer);
+}
+
+extern "C" int phb_refine_results(const phb_domain *dom, const phb_refine *r, phb_solve_result *out, int *outer_used, phb_stream stream);
+
+extern "C" int phb_refine_run(const phb_domain *dom, const phb_refine *r, phb_solve_result *out, int *outer_used, phb_stream stream) {
+	if (!dom || !r || !r->A64 || !r->A32 || !r->b || !r->x || !r->work || !r->state || (r->tol.mode == 2 && !r->tol.values))
+		return setError(PHB_ERR_ARG, "phb_refine_run: null argument");
+	if (dom->ntiles == 0) return PHB_OK;
+	cudaStream_t st = (cudaStream_t)stream;
+	const std::string key = makeKey("refine", *dom, *r);
+	int rc = PHB_OK;
+	const int K = r->nrhs;
+	if (dom->dims == 2 && K == 1) rc = runGraph(st, key, [&](cudaStream_t cs, Streams &ss) { return emitRefine<2, 1>(dom, r, cs, ss); });
+	else if (dom->dims == 2 && K == 2) rc = runGraph(st, key, [&](cudaStream_t cs, Streams &ss) { return emitRefine<2, 2>(dom, r, cs, ss); });
+	else if (dom->dims == 3 && K == 1) rc = runGraph(st, key, [&](cudaStream_t cs, Streams &ss) { return emitRefine<3, 1>(dom, r, cs, ss); });
+	else if (dom->dims == 3 && K == 3) rc = runGraph(st, key, [&](cudaStream_t cs, Streams &ss) { return emitRefine<3, 3>(dom, r, cs, ss); });
+	else return setError(PHB_ERR_ARG, "phb_refine_run: unsupported dims/nrhs");
+	if (rc) return rc;
+	if (out) return phb_refine_results(dom, r, out, outer_used, stream);
+	return PHB_OK;
+}
+
+extern "C" int phb_refine_results(const phb_domain *dom, const phb_refine *r, phb_solve_result *out, int *outer_used, phb_stream stream) {
+	if (!dom || !r || !out || !r->state) return setError(PHB_ERR_ARG, "phb_refine_results: null argument");
+	const int K = r->nrhs;
+	const int nsys = dom->ninst * K;
+	std::vector<SysState> h(nsys);
+	const StateLayout SL = stateLayout(dom, K);
+	cudaStream_t st = (cudaStream_t)stream;
+	PHB_CUDA(cudaMemcpyAsync(h.data(), (char *)r->state + SL.st2, nsys * sizeof(SysState), cudaMemcpyDeviceToHost, st));
+	PHB_CUDA(cudaStreamSynchronize(st));
+	int mo = 0;
+	for (int i = 0; i < nsys; ++i) {
+		out[i].final_residual = h[i].crit;
+		out[i].used_iterations = h[i].it;
+		out[i].converged = h[i].done == CONVERGED;
+		out[i].finite = std::isfinite(h[i].crit);
+		out[i].status = h[i].done;
+		mo = std::max(mo, h[i].it);
+	}
+	if (outer_used) *outer_used = mo;
+	return PHB_OK;
+}

@@ -1,0 +1,315 @@
+"""PISO simulation driver (phiPICT core/piso_simulation.py and simulation/simulation.py).
+
+``Simulation`` keeps phiPICT's constructor keywords and step semantics: one PISO step is
+the momentum predictor (advection matrix, right-hand side, BiCGStab solve warm-started
+from the last velocity), ``corrector_steps`` pressure correctors (pressure system, CG
+solve, mean projection, velocity correction) and the copy of the result to the blocks,
+with the same hook points (core/piso_simulation.py:3525-4169).
+
+What changes is the execution: every stage is a stream-ordered launch of the phipict_b200
+kernels with no host synchronisation inside the step; each solve is one CUDA-graph launch
+(or a node of a graph the caller is capturing). The solver outcomes are read back once at
+the end of the step, where phiPICT reads them after every solve.
+
+Extensions (keyword arguments phiPICT does not have):
+  ``mixed_precision``: with a float64 domain, every solve runs FP32 Krylov iterations
+      inside FP64 iterative refinement to the requested tolerance.
+  ``check_solves``: read the solver outcomes at the end of every step (default True).
+      With False the step never synchronises; failures surface through
+      :meth:`solve_report`.
+"""
+from __future__ import annotations
+
+import math
+from typing import Any, Literal
+
+import torch
+
+from . import _C as backend
+from .domain import Domain, FixedBoundary
+from .hooks import Hook, Hooks
+from .solvers import BICGSTAB, CG, LinearSolverResultInfo, LinsolveError, refiner_for, solver_for
+from .tolerance import SolverTolerance, parse_tolerance
+
+_UNSUPPORTED_TRUE = ("scipy_solve_advection", "scipy_solve_pressure", "differentiable_unsupported")
+
+
+class Simulation:
+    """A drop-in for ``phipict.Simulation`` on phipict_b200 kernels."""
+
+    def __init__(
+        self,
+        domain: Domain,
+        dt: float,
+        substeps: int | Literal["ADAPTIVE"] = 1,
+        corrector_steps: int = 2,
+        density_viscosity: float | None = None,
+        adaptive_CFL: float = 0.8,
+        adaptive_CFL_per_env: bool = True,
+        prep_fn: Hooks | dict | None = None,
+        advection_use_BiCG: bool = True,
+        pressure_use_BiCG: bool = False,
+        scipy_solve_advection: bool = False,
+        scipy_solve_pressure: bool = False,
+        preconditionBiCG: bool = False,
+        BiCG_precondition_fallback: bool = True,
+        advection_tol: float | SolverTolerance | None = None,
+        pressure_tol: float | SolverTolerance | None = None,
+        pressure_tol_intermediate: float | SolverTolerance | None = None,
+        pressure_warm_start: bool = False,
+        pressure_use_amg: bool | None = None,
+        pressure_amg_options: dict | None = None,
+        flux_balance_tol: float = 1e-5,
+        convergence_tol: float | None = None,
+        solver_double_fallback: bool = False,
+        advect_non_ortho_steps: int = 1,
+        pressure_non_ortho_steps: int = 1,
+        normalize_pressure_result: bool = True,
+        pressure_return_best_result: bool = False,
+        advect_passive_scalar: bool = True,
+        pressure_time_step_normalized: bool = False,
+        velocity_corrector: str = "FD",
+        non_orthogonal: bool = True,
+        differentiable: bool = False,
+        exclude_advection_solve_gradients: bool = False,
+        exclude_pressure_solve_gradients: bool = False,
+        output_resampling_shape: tuple[int, ...] | None = None,
+        output_resampling_fill_max_steps: int = 0,
+        hooks: Hooks | dict | None = None,
+        mixed_precision: bool = False,
+        check_solves: bool = True,
+    ) -> None:
+        if hooks is not None and prep_fn is not None:
+            raise ValueError("Pass hooks or its former name prep_fn, not both.")
+        if scipy_solve_advection or scipy_solve_pressure:
+            raise NotImplementedError("SciPy solves are not part of the phipict_b200 GPU path")
+        if velocity_corrector != "FD":
+            raise NotImplementedError("phipict_b200 implements the finite-difference velocity corrector ('FD')")
+        if pressure_time_step_normalized:
+            raise NotImplementedError("pressure_time_step_normalized is not implemented")
+        if substeps not in (1,) and not (isinstance(substeps, int) and substeps > 0):
+            raise NotImplementedError("phipict_b200 runs fixed substeps (substeps >= 1)")
+        if differentiable:
+            raise NotImplementedError(
+                "the differentiable step is provided by phipict_b200.adjoint.DifferentiableStep")
+        self.domain = domain
+        self.time_step = float(dt)
+        self.substeps = int(substeps)
+        self.corrector_steps = int(corrector_steps)
+        self.density_viscosity = density_viscosity
+        self.hooks = Hooks.coerce(hooks if hooks is not None else prep_fn)
+        self.advection_use_BiCG = advection_use_BiCG
+        self.pressure_use_BiCG = pressure_use_BiCG
+        self.advection_tol = parse_tolerance(advection_tol)
+        self.pressure_tol = parse_tolerance(pressure_tol)
+        self.pressure_tol_intermediate = parse_tolerance(pressure_tol_intermediate)
+        self.pressure_warm_start = pressure_warm_start
+        self.pressure_use_amg = pressure_use_amg
+        self.flux_balance_tol = flux_balance_tol
+        self.convergence_tol = convergence_tol
+        self.normalize_pressure_result = normalize_pressure_result
+        self.pressure_return_best_result = pressure_return_best_result
+        self.non_orthogonal = non_orthogonal
+        self.differentiable = False
+        self.linear_solve_max_iterations = 5000
+        self.mixed_precision = bool(mixed_precision)
+        self.check_solves = check_solves
+        self.total_step = 0
+        self.total_time = 0.0
+        self._pressure_guess: dict[int, torch.Tensor] = {}
+        self._pending: list[tuple[str, Any]] = []
+        self._last_report: list[tuple[str, list[LinearSolverResultInfo]]] = []
+        self._flux_checked_version = -1
+        if not domain.IsInitialized():
+            domain.PrepareSolve()
+        if self.mixed_precision and domain.getDtype() != torch.float64:
+            raise TypeError("mixed_precision refines float64 systems; create the domain with dtype=torch.float64")
+        domain._mixed = self.mixed_precision
+        if non_orthogonal:
+            self._require_orthogonal()
+
+    # --- helpers ---------------------------------------------------------------------
+    def _require_orthogonal(self) -> None:
+        """The non-orthogonal terms vanish on grids whose metric is diagonal; phipict_b200
+        assembles the orthogonal discretization only."""
+        d = self.domain.getSpatialDims()
+        M = self.domain._metrics[: d * d].view(d, d, -1)
+        off = M.clone()
+        for i in range(d):
+            off[i, i] = 0
+        scale = M.abs().amax()
+        if float(off.abs().amax()) > 1e-10 * float(scale):
+            raise NotImplementedError(
+                "non-orthogonal grid: phipict_b200 implements the orthogonal PISO step; "
+                "pass non_orthogonal=False to ignore the cross terms as phiPICT's orthogonal path does")
+
+    def _time_step_tensor(self, time_step: float | torch.Tensor | None) -> torch.Tensor:
+        if time_step is None:
+            time_step = self.time_step
+        if isinstance(time_step, torch.Tensor):
+            return time_step.detach().reshape(-1).to("cpu", torch.float64)
+        return torch.tensor([float(time_step)], dtype=torch.float64)
+
+    def _run_hooks(self, hook: Hook, **kw) -> None:
+        if self.hooks:
+            self.hooks.run(hook, domain=self.domain, total_step=self.total_step, total_time=self.total_time, **kw)
+
+    def _pressure_tol_for(self, cstep: int):
+        if self.pressure_tol_intermediate is None or cstep == self.corrector_steps - 1:
+            return self.pressure_tol
+        return self.pressure_tol_intermediate
+
+    def solve(self, which: str, rhs: torch.Tensor, x: torch.Tensor, *, use_BiCG: bool, tol, tag: str,
+              nrhs: int = 1, return_best: bool = False, max_iter: int | None = None) -> None:
+        """Launch one solve of a domain matrix (stencil) into ``x`` (the initial guess)."""
+        d = self.domain
+        maxit = self.linear_solve_max_iterations if max_iter is None else int(max_iter)
+        kind = BICGSTAB if use_BiCG else CG
+        if self.mixed_precision:
+            lo = backend._lo(d, which)
+            r = refiner_for(d, kind, nrhs, tag=tag)
+            r.solve(d._stencil(which), lo, rhs, x, tol, maxit)
+            self._pending.append((tag, r))
+        else:
+            s = solver_for(d, kind, d.getDtype(), nrhs, tag=tag)
+            s.solve(d._stencil(which), rhs, x, tol, maxit, return_best=return_best)
+            self._pending.append((tag, s))
+
+    def collect_solves(self, raise_on_failure: bool = True) -> bool:
+        """Read the outcomes of the solves launched since the last call (synchronises)."""
+        ok = True
+        report = []
+        for tag, s in self._pending:
+            infos = s.results()
+            report.append((tag, infos))
+            good = all(i.converged or (tag.startswith("epot") and self._accept_best(i)) for i in infos)
+            if not good:
+                ok = False
+        self._pending.clear()
+        self._last_report = report
+        if not ok and raise_on_failure:
+            bad = [(t, [str(i) for i in infos if not i.converged]) for t, infos in report]
+            raise LinsolveError(f"linear solve failed: {bad}", tag="step")
+        return ok
+
+    def _accept_best(self, info: LinearSolverResultInfo) -> bool:
+        return False
+
+    def solve_report(self) -> list[tuple[str, list[LinearSolverResultInfo]]]:
+        return list(self._last_report)
+
+    def _check_flux_balance(self) -> None:
+        d = self.domain
+        if d._version == self._flux_checked_version:
+            return
+        if any(isinstance(b, FixedBoundary) for blk in d.getBlocks() for b in blk.getBoundaries()):
+            bal = d.GetBoundaryFluxBalance()
+            if float(bal.abs().max()) > float(self.flux_balance_tol):
+                raise RuntimeError(
+                    f"Domain boundary fluxes not balanced, cannot proceed with simulation step. "
+                    f"Flux balance: {bal}, flux_balance_tol: {self.flux_balance_tol}")
+        self._flux_checked_version = d._version
+
+    # --- the step ----------------------------------------------------------------------
+    def single_step(self, static: bool = False) -> bool:
+        """One simulation step of ``substeps`` PISO steps (simulation/simulation.py:262-333)."""
+        self._check_flux_balance()
+        try:
+            return self._PISO_split_step(self.substeps)
+        except LinsolveError:
+            return False
+
+    def run(self, iterations: int) -> bool:
+        for _ in range(int(iterations)):
+            if not self.single_step():
+                return False
+        return True
+
+    def _PISO_split_step(self, iterations: int, time_step=None) -> bool:
+        d = self.domain
+        ts = self._time_step_tensor(time_step)
+        dims = d.getSpatialDims()
+        for step in range(int(iterations)):
+            if self.convergence_tol is not None:
+                last_vel = d._u_block.clone()
+            self._run_hooks(Hook.PRE, local_step=step, time_step=ts)
+            self._run_hooks(Hook.PRE_VELOCITY_SETUP, local_step=step, time_step=ts)
+            backend.SetupAdvectionMatrix(d, ts, 0)
+            backend.SetupAdvectionVelocity(d, ts, 0, False)
+            self._run_hooks(Hook.POST_VELOCITY_SETUP, local_step=step, time_step=ts, no_step=0)
+            self.solve("C", d.velocityRHS, d.velocityResult, use_BiCG=self.advection_use_BiCG,
+                       tol=self.advection_tol, tag="velocity", nrhs=dims)
+            self._run_hooks(Hook.POST_PREDICTION, local_step=step, time_step=ts)
+            for cstep in range(self.corrector_steps):
+                if cstep == 0:
+                    # P depends on A and the metrics only, so every corrector of a step would
+                    # rebuild the same values (pressure.cu:882-927 rebuilds it each time)
+                    backend.SetupPressureMatrix(d, ts, 0, False)
+                backend.SetupPressureRHS(d, ts, 0, False, False)
+                self._run_hooks(Hook.POST_PRESSURE_SETUP, local_step=step, time_step=ts)
+                guess = self._pressure_guess.get(cstep) if self.pressure_warm_start else None
+                if guess is not None:
+                    d.pressureResult.copy_(guess)
+                else:
+                    d.pressureResult.zero_()
+                self.solve("P", d.pressureRHSdiv, d.pressureResult, use_BiCG=self.pressure_use_BiCG,
+                           tol=self._pressure_tol_for(cstep), tag=f"pressure{cstep}",
+                           return_best=self.pressure_return_best_result)
+                if self.normalize_pressure_result:
+                    d._subtract_mean(d.pressureResult, 1)
+                if self.pressure_warm_start:
+                    g = self._pressure_guess.get(cstep)
+                    if g is None:
+                        self._pressure_guess[cstep] = d.pressureResult.clone()
+                    else:
+                        g.copy_(d.pressureResult)
+                self._run_hooks(Hook.POST_PRESSURE_RESULT, local_step=step, time_step=ts)
+                backend.CopyPressureResultToBlocks(d)
+                backend.CorrectVelocity(d, ts, version=1)
+                self._run_hooks(Hook.POST_VELOCITY_CORRECTION, local_step=step, time_step=ts)
+            backend.CopyVelocityResultToBlocks(d)
+            self._run_hooks(Hook.POST, local_step=step, time_step=ts)
+            ok = self.collect_solves() if self.check_solves else True
+            self.total_step += 1
+            self.total_time += float(ts[0])
+            if self.convergence_tol is not None:
+                diff = float((last_vel - d._u_block).abs().max())
+                if diff < self.convergence_tol:
+                    return False
+            if not ok:
+                return False
+        return True
+
+    def make_divergence_free(self, iterations: int = 1, max_iter: int = 1000) -> bool:
+        """Project the block velocity onto a divergence-free field with A = 1, dt = 1
+        (core/piso_simulation.py:3355-3523)."""
+        d = self.domain
+        ts = torch.tensor([1.0], dtype=torch.float64)
+        d.setTimeStep(ts)
+        backend.CopyVelocityResultFromBlocks(d)
+        for _ in range(int(iterations)):
+            d.A.fill_(1.0)
+            backend.SetupPressureMatrix(d, ts, 0, False)
+            # with A = 1 the projection's HbyA is the velocity itself
+            d.pressureRHS.copy_(d.velocityResult)
+            backend.SetupPressureRHSdiv(d, ts)
+            d.pressureResult.zero_()
+            self.solve("P", d.pressureRHSdiv, d.pressureResult, use_BiCG=self.pressure_use_BiCG,
+                       tol=self.pressure_tol, tag="projection", max_iter=max_iter)
+            if self.normalize_pressure_result:
+                d._subtract_mean(d.pressureResult, 1)
+            backend.CopyPressureResultToBlocks(d)
+            backend.CorrectVelocity(d, ts, version=1)
+        backend.CopyVelocityResultToBlocks(d)
+        return self.collect_solves(raise_on_failure=False)
+
+
+def get_max_time_step(domain: Domain, time_step_target: float, CFL_cond: float = 0.8, with_transformations: bool = True):
+    """Largest stable step for the current velocity and the substeps to reach the target."""
+    umax = float(domain.getMaxVelocity(True, False))
+    hmin = float(domain._metrics[2 * domain.getSpatialDims() ** 2].abs().min()) ** (1.0 / domain.getSpatialDims())
+    if umax <= 0:
+        return time_step_target, 1
+    dt = CFL_cond * hmin / umax
+    n = max(1, math.ceil(time_step_target / dt))
+    return time_step_target / n, n
