@@ -1,0 +1,362 @@
+"""Benchmark of the phipict_b200 PISO/MHD step (one JSON line on rank 0).
+
+Workload (default ``duct3d``): the 3D MHD rectangular duct of 3 connected blocks of
+64x48x48 cells (442,368 cells), tanh wall stretching beta=2 in y and z, Ha=100, Re=1000
+(N = 10), inflow u=1 plus seeded 1e-2 noise with a flux-balancing outflow, insulating walls
+and an open-potential outflow. Fields are float64; every solve runs float32 Krylov
+iterations inside float64 iterative refinement to a relative residual of 1e-10.
+Synthetic inputs (seeded), no dataset. A step is one PISO step (momentum predictor,
+2 pressure correctors) plus the potential step and the Lorentz force.
+
+``--impl reference`` times the CPU oracle (the restatement of phiPICT's step; phiPICT has no
+CPU path) on the same workload with all host threads, on rank 0.
+
+Multi-GPU: independent replicas (one instance per rank, no collective in the step);
+``value`` counts the cells of all ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        d["source"] = "measured"
+        return d
+    return dict(PEAKS_FALLBACK)
+
+
+def make_duct(device, dtype, nx=64, ny=48, nz=48, nblocks=3, seed=0):
+    import phipict_b200 as pb
+    from phipict_b200.grid import make_weights_tanh, rectilinear_vertices, span
+
+    ys = span(-1.0, 1.0, make_weights_tanh(ny, 2.0))
+    zs = span(-1.0, 1.0, make_weights_tanh(nz, 2.0))
+    Re = 1000.0
+    dom = pb.Domain(3, torch.tensor([1.0 / Re]), name="duct", device=device, dtype=dtype)
+    blocks = []
+    for i in range(nblocks):
+        xs = np.linspace(2.0 * i, 2.0 * (i + 1), nx + 1)
+        blocks.append(dom.CreateBlock(vertexCoordinates=rectilinear_vertices(xs, ys, zs, dtype=dtype), name=f"b{i}"))
+    for i in range(nblocks - 1):
+        blocks[i].ConnectBlock("+x", blocks[i + 1], "-x", "-y", "-z")
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    inflow = torch.zeros(1, 3, nz, ny, 1, dtype=dtype)
+    inflow[0, 0] = 1.0 + 1e-2 * torch.randn(nz, ny, 1, generator=g, dtype=dtype)
+    blocks[0].CloseBoundary("-x", inflow.to(device))
+    blocks[-1].CloseBoundary("+x", inflow.clone().to(device))
+    blocks[-1].getBoundary("+x").setPotentialBC(pb.PotentialBC.OPEN)
+    for b in blocks:
+        for f in ("-y", "+y", "-z", "+z"):
+            b.CloseBoundary(f)
+    for b in blocks:
+        v = torch.zeros(b.velocity.shape, dtype=dtype)
+        v[:, 0] = 1.0
+        v += 1e-2 * torch.randn(v.shape, generator=g, dtype=dtype)
+        b.velocity.copy_(v.to(device))
+    return dom
+
+
+WORKLOADS = {
+    "duct3d": dict(nx=64, ny=48, nz=48, nblocks=3, Ha=100.0, Re=1000.0, dt=0.01, rtol=1e-10),
+}
+
+
+def algorithmic_cg_bytes(dims: int, s_A: int, s_v: int) -> int:
+    """Bytes per cell of one fused CG iteration (kCgDirection + kCgUpdate): the stencil
+    (2d+1 values, no indices) and 10 vector passes (r, p_in read / p_out, q written; x, p, r,
+    q read / x, r written)."""
+    return (2 * dims + 1) * s_A + 10 * s_v
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"phb_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append(dict(sm=float(parts[1]), smmax=float(parts[2]), power=float(parts[3]), hw=parts[5],
+                                 hwt=parts[6], swt=parts[7], swp=parts[8]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        reasons = []
+        for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"), ("swt", "sw_thermal_slowdown"),
+                          ("swp", "sw_power_cap")):
+            if any(r[key].lower() == "active" for r in rows):
+                reasons.append(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in rows), "sm_max_mhz": max(r["smmax"] for r in rows),
+                "power_w_max": max(r["power"] for r in rows), "samples": len(rows), "reasons": reasons}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        backend = "nccl" if args.impl != "reference" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def max_over_ranks(v: float, world: int) -> float:
+    if world == 1:
+        return v
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def build_sim(wl: dict, device, mixed: bool):
+    import phipict_b200 as pb
+
+    dtype = torch.float64
+    dom = make_duct(device, dtype, wl["nx"], wl["ny"], wl["nz"], wl["nblocks"])
+    dom.PrepareSolve()
+    N = wl["Ha"] ** 2 / wl["Re"]
+    tol = pb.SolverTolerance(rtol=wl["rtol"])
+
+    def reset_source(domain, **kw):
+        # the Lorentz force is added onto the velocity source (simulation/mhd.py:583-593);
+        # the benchmark resets it each step, as phiPICT's examples/hartmann.py does
+        for b in domain.getBlocks():
+            if b.velocitySource is not None:
+                b.velocitySource.zero_()
+
+    hooks = pb.Hooks().append(pb.Hook.PRE_VELOCITY_SETUP, reset_source)
+    sim = pb.MHDSimulation(dom, wl["dt"], torch.tensor(N), torch.tensor([0.0, 1.0, 0.0], dtype=dtype),
+                           non_orthogonal=False, advection_tol=tol, pressure_tol=tol, potential_tol=tol,
+                           mixed_precision=mixed, hooks=hooks)
+    return dom, sim
+
+
+def run_ours(args, rank, world, local):
+    wl = WORKLOADS[args.workload]
+    device = torch.device("cuda", local)
+    mixed = not args.plain_fp64
+    dom, sim = build_sim(wl, device, mixed)
+    cells = dom.getTotalSize()
+    stream = torch.cuda.current_stream(device)
+    for _ in range(args.warmup):
+        if not sim.single_step():
+            raise RuntimeError("warm-up step failed")
+    torch.cuda.synchronize()
+    # solve timing: CUDA events around each solve graph launch (on the launching stream)
+    sim._solve_events = []
+    infos = []
+    orig_collect = sim.collect_solves
+
+    def collect(raise_on_failure=True):
+        ok = orig_collect(raise_on_failure)
+        infos.extend(sim.solve_report())
+        return ok
+
+    sim.collect_solves = collect
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        if not sim.single_step():
+            raise RuntimeError("timed step failed")
+    t1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = t0.elapsed_time(t1)
+    ms = max_over_ranks(ms, world)
+    # solver statistics of the timed steps
+    solve_ms = 0.0
+    for a, b in sim._solve_events:
+        solve_ms += a.elapsed_time(b)
+    inner_its = sum(i.innerIterations if mixed else i.usedIterations for _, lst in infos for i in lst)
+    sweeps = sum(i.usedIterations for _, lst in infos for i in lst) if mixed else 0
+    sim._solve_events = None
+    # end-to-end: the state comes from pinned host memory each step, u, p and phi go back
+    d = dom.getSpatialDims()
+    h_u = torch.empty(dom._u_block.shape, dtype=dom.getDtype(), pin_memory=True)
+    h_u.copy_(dom._u_block)
+    h_out = torch.empty(dom._u_block.numel() + 2 * cells, dtype=dom.getDtype(), pin_memory=True)
+    nu = dom._u_block.numel()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e_steps = max(1, min(args.steps, 5))
+    e0.record(stream)
+    for _ in range(e_steps):
+        dom._u_block.copy_(h_u, non_blocking=True)
+        sim.single_step()
+        h_out[:nu].copy_(dom._u_block.view(-1), non_blocking=True)
+        h_out[nu:nu + cells].copy_(dom.pressureResult, non_blocking=True)
+        h_out[nu + cells:].copy_(dom.epotResult, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world) / e_steps
+    total_cells = cells * world
+    value = total_cells * args.steps / (ms / 1e3) / 1e6
+    # roofline of the dominant kernel pair: the float32 (or float64) CG iteration
+    s = 4 if mixed else 8
+    per_cell = algorithmic_cg_bytes(d, s, s)
+    it_time_ms = solve_ms / max(1, inner_its)
+    achieved = per_cell * cells / (it_time_ms / 1e3) / 1e9 if inner_its else None
+    pk = peaks()
+    launches_per_step = 26  # assembly, mean projections and copies per PISO+MHD step
+    gpu_launches = args.steps * launches_per_step + 2 * inner_its + 6 * max(1, sweeps) + 3 * len(infos)
+    return dict(
+        metric="Mcell-steps/s", value=round(value, 4), unit="Mcell-steps/s", n_gpus=world, steps=args.steps,
+        warmup=args.warmup, ms_per_step=round(ms / args.steps, 4), higher_is_better=True, scaling="weak",
+        vs_baseline=None, dtype="f64 fields, f32 Krylov + f64 refinement" if mixed else "f64",
+        data="synthetic (seeded inflow noise 1e-2, seeded initial state)",
+        config={"workload": f"{args.workload}: 3 blocks 64x48x48 (442,368 cells), Ha=100, Re=1000, dt=0.01, "
+                            f"rtol 1e-10, {'mixed precision' if mixed else 'plain fp64'}",
+                "cells_per_gpu": cells, "l2": "working set ~60 MB f32 fits L2; HBM claims on the roofline sweep",
+                "parallelism": f"replicas x{world}"},
+        clocks=clk,
+        e2e={"value": round(total_cells / (e2e_ms / 1e3) / 1e6, 4), "unit": "Mcell-steps/s",
+             "h2d_bytes_per_step": int(h_u.numel() * h_u.element_size()),
+             "d2h_bytes_per_step": int(h_out.numel() * h_out.element_size())},
+        roofline={"bound": "hbm", "kernel": "CG iteration (kCgDirection + kCgUpdate)",
+                  "achieved": round(achieved, 1) if achieved else None, "peak": pk.get("hbm_gbs"),
+                  "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4) if achieved else None,
+                  "traffic": None, "bytes_per_cell": per_cell, "peak_source": pk["source"],
+                  "iterations": inner_its, "solve_ms": round(solve_ms, 3)},
+        gpu_launches=int(gpu_launches),
+        solver={"inner_iterations_per_step": round(inner_its / args.steps, 1),
+                "refinement_sweeps_per_step": round(sweeps / args.steps, 2)},
+    )
+
+
+def cpu_baseline(wl, sample_steps=1) -> dict:
+    """The oracle's FP64 step on the host cores (bounded sample)."""
+    from oracle.oracle import OracleDomain, OracleSim
+    import phipict_b200 as pb
+
+    dom = make_duct("cpu", torch.float64, wl["nx"], wl["ny"], wl["nz"], wl["nblocks"])
+    od = OracleDomain(dom)
+    u0 = np.concatenate([b.velocity.reshape(3, -1).numpy() for b in dom.getBlocks()], axis=1).reshape(-1)
+    tol = pb.SolverTolerance(rtol=wl["rtol"])
+    N = wl["Ha"] ** 2 / wl["Re"]
+    sim = OracleSim(od, u0, wl["dt"], 1.0 / wl["Re"], advection_tol=tol, pressure_tol=tol,
+                    mhd=dict(stuart=N, e_b=[0.0, 1.0, 0.0], singular=True, potential_tol=tol))
+    t = time.perf_counter()
+    for _ in range(sample_steps):
+        sim.src = None
+        sim.step()
+    el = time.perf_counter() - t
+    return {"value": round(od.n * sample_steps / el / 1e6, 5), "unit": "Mcell-steps/s",
+            "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)), "kind": "port",
+            "sample": f"{sample_steps} oracle PISO+MHD step(s) of the {od.n}-cell duct, float64, {el:.1f} s",
+            "seconds": round(el, 2)}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    wl = WORKLOADS[args.workload]
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    for _ in range(args.warmup):
+        pass  # the oracle has no warm-up state; its first step is representative
+    steps = max(1, args.steps if args.steps <= 2 else 2)
+    base = cpu_baseline(wl, steps)
+    line = dict(metric="Mcell-steps/s", value=base["value"], unit="Mcell-steps/s", n_gpus=world, steps=steps,
+                warmup=args.warmup, ms_per_step=round(base["seconds"] * 1e3 / steps, 1), higher_is_better=True,
+                scaling="weak", vs_baseline=None, dtype="f64", data="synthetic", impl="reference",
+                config={"workload": f"{args.workload}: 3 blocks 64x48x48 (442,368 cells), Ha=100, Re=1000",
+                        "parallelism": "host cores"},
+                cpu_baseline=base,
+                e2e={"value": base["value"], "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="duct3d", choices=list(WORKLOADS))
+    ap.add_argument("--plain-fp64", action="store_true", help="the plain float64 path (no refinement)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_setup(args)
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
+    line = run_ours(args, rank, world, local)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(WORKLOADS[args.workload], 1)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -170,6 +170,8 @@ typedef struct phb_solve_result {
 	int32_t converged;
 	int32_t finite;
 	int32_t status;       /* 1 converged, 2 non-finite, 3 max iterations, 4 rising */
+	int32_t inner_iterations; /* refinement: inner Krylov iterations of all sweeps */
+	int32_t pad;
 } phb_solve_result;
 
 int64_t phb_solve_work_bytes(const phb_domain *dom, int kind, int vec_dtype, int nrhs);

@@ -624,6 +624,7 @@ static int cg(int n, const int *row, const int *col, const S *val, const S *b, S
 	double rho = rr, beta = 0;
 	bool restart = true;
 	for (int it = 1;; ++it) {
+		#pragma omp parallel for schedule(static)
 		for (int i = 0; i < n; ++i) p[i] = restart ? r[i] : r[i] + S(beta) * p[i];
 		restart = false;
 		spmv(n, row, col, val, p.data(), q.data());
@@ -631,6 +632,7 @@ static int cg(int n, const int *row, const int *col, const S *val, const S *b, S
 		const double alpha = rho / pq;
 		if (!std::isfinite(alpha)) { *iters = it - 1; return 2; }
 		const S a = S(alpha);
+		#pragma omp parallel for schedule(static)
 		for (int i = 0; i < n; ++i) { x[i] += a * p[i]; r[i] -= a * q[i]; }
 		rr = dotd(n, r.data(), r.data());
 		crit = std::sqrt(rr) * ns;
@@ -658,11 +660,13 @@ static int bicgstab(int n, const int *row, const int *col, const S *val, const S
 	bool restart = true;
 	int it = 0;
 	for (;;) {
+		#pragma omp parallel for schedule(static)
 		for (int i = 0; i < n; ++i) p[i] = restart ? r[i] : r[i] + S(beta) * (p[i] - S(omega) * v[i]);
 		restart = false;
 		spmv(n, row, col, val, p.data(), v.data());
 		alpha = rho / dotd(n, r0.data(), v.data());
 		if (!std::isfinite(alpha)) { *iters = it; return 2; }
+		#pragma omp parallel for schedule(static)
 		for (int i = 0; i < n; ++i) s[i] = r[i] - S(alpha) * v[i];
 		spmv(n, row, col, val, s.data(), t.data());
 		const double critS = std::sqrt(dotd(n, s.data(), s.data())) * ns;
@@ -673,6 +677,7 @@ static int bicgstab(int n, const int *row, const int *col, const S *val, const S
 		}
 		omega = dotd(n, t.data(), s.data()) / dotd(n, t.data(), t.data());
 		if (!std::isfinite(omega)) { *critOut = critS; *iters = it; return 2; }
+		#pragma omp parallel for schedule(static)
 		for (int i = 0; i < n; ++i) { x[i] += S(alpha) * p[i] + S(omega) * s[i]; r[i] = s[i] - S(omega) * t[i]; }
 		const double rhoNew = dotd(n, r0.data(), r.data());
 		crit = std::sqrt(dotd(n, r.data(), r.data())) * ns;

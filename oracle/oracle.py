@@ -149,6 +149,8 @@ class OracleDomain:
         self._f("orc_row_pointers")(*self._dargs(), _p(self.row))
         self.nnz = int(self.row[-1])
         self.col = np.zeros(self.nnz, dtype=np.int32)
+        # the column pattern shared by all matrices of the domain
+        _, self.col = self.laplace_matrix(epot=True)
         del torch
 
     # --- plumbing ---

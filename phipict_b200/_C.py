@@ -49,6 +49,9 @@ def _lo(domain: Domain, which: str) -> torch.Tensor | None:
     st = domain._stencil(which)
     if t is None or t.shape != st.shape:
         t = torch.empty(st.shape, dtype=torch.float32, device=st.device)
+        # the momentum and pressure kernels refresh their copies at every assembly; the
+        # potential matrix is assembled once, so its copy is taken here
+        t.copy_(st)
         setattr(domain, key, t)
     return t
 

@@ -64,7 +64,7 @@ class PhbSolve(ct.Structure):
 class PhbSolveResult(ct.Structure):
     _fields_ = [
         ("final_residual", ct.c_double), ("used_iterations", ct.c_int32), ("converged", ct.c_int32),
-        ("finite", ct.c_int32), ("status", ct.c_int32),
+        ("finite", ct.c_int32), ("status", ct.c_int32), ("inner_iterations", ct.c_int32), ("pad", ct.c_int32),
     ]
 
 

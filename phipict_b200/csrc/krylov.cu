@@ -34,8 +34,8 @@ constexpr int RISING_CUTOFF = 100;
 
 struct SysState {
 	double tol, rho, alpha, beta, omega, crit, best, last, halfCrit, innerTol;
-	int it, maxit, bestIt, rising, done, restart, saveBest, halfDone, usedIt, pad1;
-	int pad2[2];
+	int it, maxit, bestIt, rising, done, restart, saveBest, halfDone, usedIt, innerIts;
+	int launched, pad2;
 };
 static_assert(sizeof(SysState) == 128, "SysState layout");
 
@@ -209,7 +209,8 @@ __global__ void kInit(SysState *st, int nsys, phb_tolerance tol, int fromInner, 
 // crit < tol.
 template <typename T, int D, int K, bool BICG, bool STOPSTART>
 __global__ void __launch_bounds__(PHB_TILE) kResidual(Dom<double, D> dom, const T *__restrict__ A, const T *__restrict__ b,
-		const T *__restrict__ x, T *__restrict__ r, T *__restrict__ r0, SysState *st, double *partial, Control *ctrl, phb_tolerance tol) {
+		const T *__restrict__ x, T *__restrict__ r, T *__restrict__ r0, SysState *st, double *partial, Control *ctrl, phb_tolerance tol,
+		LoopCond arm) {
 	__shared__ int32_t sB[PHB_BREC];
 	Cell c;
 	const bool valid = loadCell<double, D>(dom, sB, c);
@@ -250,6 +251,8 @@ __global__ void __launch_bounds__(PHB_TILE) kResidual(Dom<double, D> dom, const 
 			if (!fin(crit)) { s.done = NONFINITE; s.usedIt = 0; }
 			else if ((BICG || STOPSTART) ? crit < s.tol : crit == 0.0) { s.done = CONVERGED; s.usedIt = BICG ? -1 : 0; }
 		});
+		// arm the WHILE loop that follows: run its body only if a system is still running
+		if (threadIdx.x == 0 && arm.active) cudaGraphSetConditional(arm.handle, ctrl->allDone ? 0u : 1u);
 	}
 }
 
@@ -594,11 +597,12 @@ __global__ void __launch_bounds__(PHB_TILE) kRefineResidual(Dom<double, D> dom, 
 				if (o.it == 0 && o.done == RUNNING && tol.mode == 1) o.tol = resolveTol(tol, sqrt(bb / double(K)) * ns);
 				const double crit = sqrt(a) * ns;
 				o.crit = crit;
+				if (o.launched) { o.innerIts += max(inner[s].usedIt, 0); o.launched = 0; }
 				if (o.done == RUNNING) {
 					if (!fin(crit)) o.done = NONFINITE;
 					else if (crit < o.tol) o.done = CONVERGED;
 					else if (o.it >= maxOuter) o.done = MAXIT;
-					else ++o.it;
+					else { ++o.it; o.launched = 1; }
 				}
 				o.usedIt = o.it;
 				inner[s].innerTol = o.done == RUNNING ? fmax(innerRtol * crit, 0.25 * o.tol) : INFINITY;
@@ -619,14 +623,17 @@ __global__ void kRefineUpdate(int64_t n, double *__restrict__ x, const float *__
 	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) x[i] += double(e[i]);
 }
 
-__global__ void kInitOuter(SysState *st, int nsys, phb_tolerance tol, Control *ctrl, int maxLoops) {
+__global__ void kInitOuter(SysState *st, int nsys, phb_tolerance tol, Control *ctrl, int maxLoops, LoopCond arm) {
 	for (int s = threadIdx.x; s < nsys; s += blockDim.x) {
 		SysState z;
 		memset(&z, 0, sizeof(z));
 		z.tol = tol.mode == 0 ? tol.atol : tol.mode == 2 ? tol.values[s] : NAN;
 		st[s] = z;
 	}
-	if (threadIdx.x == 0) { ctrl->counter = 0; ctrl->allDone = 0; ctrl->loops = 0; ctrl->maxLoops = maxLoops; }
+	if (threadIdx.x == 0) {
+		ctrl->counter = 0; ctrl->allDone = 0; ctrl->loops = 0; ctrl->maxLoops = maxLoops;
+		if (arm.active) cudaGraphSetConditional(arm.handle, 1u);
+	}
 }
 
 // host side --------------------------------------------------------------------------------
@@ -680,17 +687,29 @@ static int getStreams(Streams *&out) {
 	return PHB_OK;
 }
 
-// Add a conditional WHILE node to the graph `cap` is capturing and capture `body` into it on
-// `bodyStream`. The condition starts true and the body's last kernel sets it.
-static int emitWhile(cudaStream_t cap, cudaStream_t bodyStream, const std::function<int(cudaStream_t, LoopCond)> &body) {
+// Create the condition handle of a WHILE loop on the graph `cap` is capturing. The kernel
+// launched just before the loop sets it (armCondition), so that a loop nested in another
+// conditional body is re-armed on every pass of the outer body: a handle's default value is
+// only applied when the graph that owns it is launched.
+static int createCondition(cudaStream_t cap, cudaGraphConditionalHandle *handle) {
+	cudaStreamCaptureStatus status;
+	cudaGraph_t graph;
+	PHB_CUDA(cudaStreamGetCaptureInfo(cap, &status, nullptr, &graph, nullptr, nullptr));
+	if (status != cudaStreamCaptureStatusActive) return setError(PHB_ERR_STATE, "createCondition: stream is not capturing");
+	PHB_CUDA(cudaGraphConditionalHandleCreate(handle, graph, 1, cudaGraphCondAssignDefault));
+	return PHB_OK;
+}
+
+// Add a conditional WHILE node on `handle` to the graph `cap` is capturing and capture
+// `body` into it on `bodyStream`; the body's last kernel sets the condition.
+static int addWhile(cudaStream_t cap, cudaStream_t bodyStream, cudaGraphConditionalHandle handle,
+		const std::function<int(cudaStream_t, LoopCond)> &body) {
 	cudaStreamCaptureStatus status;
 	cudaGraph_t graph;
 	const cudaGraphNode_t *deps = nullptr;
 	size_t ndeps = 0;
 	PHB_CUDA(cudaStreamGetCaptureInfo(cap, &status, nullptr, &graph, &deps, &ndeps));
-	if (status != cudaStreamCaptureStatusActive) return setError(PHB_ERR_STATE, "emitWhile: stream is not capturing");
-	cudaGraphConditionalHandle handle;
-	PHB_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+	if (status != cudaStreamCaptureStatusActive) return setError(PHB_ERR_STATE, "addWhile: stream is not capturing");
 	cudaGraphNodeParams params = {};
 	params.type = cudaGraphNodeTypeConditional;
 	params.conditional.handle = handle;
@@ -779,9 +798,15 @@ static int emitSolve(const phb_domain *dom, const phb_solve *sv, cudaStream_t s,
 		T *r = (T *)(w + L.off[0]), *q = (T *)(w + L.off[1]), *p0 = (T *)(w + L.off[2]), *p1 = (T *)(w + L.off[3]);
 		T *xbest = sv->return_best ? (T *)(w + L.off[4]) : nullptr;
 		const int maxLoops = maxit / 2 + 2;
+		LoopCond arm{0, 0};
+		if (useGraph) {
+			const int rc0 = createCondition(s, &arm.handle);
+			if (rc0) return rc0;
+			arm.active = 1;
+		}
 		kInit<<<1, 256, 0, s>>>(st, nsys, sv->tol, fromInner, maxit, ctrl, maxLoops);
-		if (stopStart) kResidual<T, D, K, false, true><<<tiles, PHB_TILE, 0, s>>>(dm, A, b, x, r, nullptr, st, partial, ctrl, sv->tol);
-		else kResidual<T, D, K, false, false><<<tiles, PHB_TILE, 0, s>>>(dm, A, b, x, r, nullptr, st, partial, ctrl, sv->tol);
+		if (stopStart) kResidual<T, D, K, false, true><<<tiles, PHB_TILE, 0, s>>>(dm, A, b, x, r, nullptr, st, partial, ctrl, sv->tol, arm);
+		else kResidual<T, D, K, false, false><<<tiles, PHB_TILE, 0, s>>>(dm, A, b, x, r, nullptr, st, partial, ctrl, sv->tol, arm);
 		int rc = checkLaunch("kResidual");
 		if (rc) return rc;
 		auto body = [&](cudaStream_t bs, LoopCond lc) -> int {
@@ -794,7 +819,7 @@ static int emitSolve(const phb_domain *dom, const phb_solve *sv, cudaStream_t s,
 			}
 			return checkLaunch("CG body");
 		};
-		if (useGraph) { rc = emitWhile(s, ss.s[useGraph == 2 ? 2 : 1], body); if (rc) return rc; }
+		if (useGraph) { rc = addWhile(s, ss.s[useGraph == 2 ? 2 : 1], arm.handle, body); if (rc) return rc; }
 		else {
 			// host loop (no graph): poll allDone every check_every iterations
 			int *hflag = nullptr;
@@ -816,8 +841,14 @@ static int emitSolve(const phb_domain *dom, const phb_solve *sv, cudaStream_t s,
 	T *r = (T *)(w + L.off[0]), *r0 = (T *)(w + L.off[1]), *p0 = (T *)(w + L.off[2]), *p1 = (T *)(w + L.off[3]);
 	T *v0 = (T *)(w + L.off[4]), *v1 = (T *)(w + L.off[5]), *t = (T *)(w + L.off[6]);
 	const int maxLoops = maxit / 2 + 2;
+	LoopCond arm{0, 0};
+	if (useGraph) {
+		const int rc0 = createCondition(s, &arm.handle);
+		if (rc0) return rc0;
+		arm.active = 1;
+	}
 	kInit<<<1, 256, 0, s>>>(st, nsys, sv->tol, fromInner, maxit, ctrl, maxLoops);
-	kResidual<T, D, K, true, true><<<tiles, PHB_TILE, 0, s>>>(dm, A, b, x, r, r0, st, partial, ctrl, sv->tol);
+	kResidual<T, D, K, true, true><<<tiles, PHB_TILE, 0, s>>>(dm, A, b, x, r, r0, st, partial, ctrl, sv->tol, arm);
 	int rc = checkLaunch("kResidual");
 	if (rc) return rc;
 	auto body = [&](cudaStream_t bs, LoopCond lc) -> int {
@@ -832,7 +863,7 @@ static int emitSolve(const phb_domain *dom, const phb_solve *sv, cudaStream_t s,
 		}
 		return checkLaunch("BiCGStab body");
 	};
-	if (useGraph) return emitWhile(s, ss.s[useGraph == 2 ? 2 : 1], body);
+	if (useGraph) return addWhile(s, ss.s[useGraph == 2 ? 2 : 1], arm.handle, body);
 	int *hflag = nullptr;
 	PHB_CUDA(cudaMallocHost(&hflag, sizeof(int)));
 	const int chk = std::max(1, sv->check_every);
@@ -905,6 +936,7 @@ extern "C" int phb_solve_results(const phb_domain *dom, const phb_solve *s, phb_
 		o.converged = x.done == CONVERGED;
 		o.finite = std::isfinite(x.crit);
 		o.status = x.done;
+		o.inner_iterations = 0;
 		if (s->return_best && (x.done == MAXIT || x.done == RISING) && x.bestIt >= 0 && x.best < x.crit) {
 			o.used_iterations = x.bestIt;
 			o.final_residual = x.best;
@@ -955,7 +987,10 @@ static int emitRefine(const phb_domain *dom, const phb_refine *rf, cudaStream_t 
 	in.tol = phb_tolerance{}; // unused: the inner tolerance is SysState::innerTol
 	in.work = rf->work;
 	in.state = rf->state;
-	kInitOuter<<<1, 256, 0, s>>>(stO, nsys, rf->tol, ctrlO, rf->max_outer + 2);
+	cudaGraphConditionalHandle outerHandle;
+	int rc0 = createCondition(s, &outerHandle);
+	if (rc0) return rc0;
+	kInitOuter<<<1, 256, 0, s>>>(stO, nsys, rf->tol, ctrlO, rf->max_outer + 2, LoopCond{outerHandle, 1});
 	PHB_CUDA(cudaGetLastError());
 	auto outer = [&](cudaStream_t os, LoopCond lc) -> int {
 		kRefineResidual<D, K><<<dom->ntiles, PHB_TILE, 0, os>>>(dm, rf->A64, rf->b, rf->x, r32, e32, stO, partial, ctrlO,
@@ -967,7 +1002,7 @@ static int emitRefine(const phb_domain *dom, const phb_refine *rf, cudaStream_t 
 		kRefineUpdate<K><<<gridFor(dom->ncells * K), 256, 0, os>>>(dom->ncells * K, rf->x, e32);
 		return checkLaunch("kRefineUpdate");
 	};
-	return emitWhile(s, ss.s[1], outer);
+	return addWhile(s, ss.s[1], outerHandle, outer);
 }
 
 extern "C" int phb_refine_results(const phb_domain *dom, const phb_refine *r, phb_solve_result *out, int *outer_used, phb_stream stream);
@@ -1006,6 +1041,7 @@ extern "C" int phb_refine_results(const phb_domain *dom, const phb_refine *r, ph
 		out[i].converged = h[i].done == CONVERGED;
 		out[i].finite = std::isfinite(h[i].crit);
 		out[i].status = h[i].done;
+		out[i].inner_iterations = h[i].innerIts;
 		mo = std::max(mo, h[i].it);
 	}
 	if (outer_used) *outer_used = mo;

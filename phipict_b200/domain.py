@@ -1106,6 +1106,7 @@ class Domain:
         self._epot_block = e
         _lib.call("phb_epot_matrix", ct.byref(self._desc), self._E_st.data_ptr(), None, _lib.stream_ptr(self._device))
         self.Epot = CSRmatrix(_domain=self, _which="E")
+        self.Epot.row, self.Epot.index = self._csr_row, self._csr_col
         self._csr_cache.pop("E", None)
 
     def hasEpot(self) -> bool:

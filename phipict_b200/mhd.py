@@ -124,7 +124,9 @@ class MHDSimulation(Simulation):
             self._potential_stale = True
 
     def _accept_best(self, info: LinearSolverResultInfo) -> bool:
-        return self._potential_return_best_result and info.isFiniteResidual
+        # a non-converged plain solve returns its best iterate (mhd.py:430-433); a refined
+        # solve has no best iterate, so it has to converge
+        return self._potential_return_best_result and info.isFiniteResidual and not self.mixed_precision
 
     # --- hooks -------------------------------------------------------------------------
     def _add_lorentz_force(self, domain: Domain, **kwargs) -> None:

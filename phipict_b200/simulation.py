@@ -120,6 +120,8 @@ class Simulation:
         self._pending: list[tuple[str, Any]] = []
         self._last_report: list[tuple[str, list[LinearSolverResultInfo]]] = []
         self._flux_checked_version = -1
+        self._solve_events: list | None = None  # (start, end) CUDA events per solve when a list
+        self.last_error: str | None = None
         if not domain.IsInitialized():
             domain.PrepareSolve()
         if self.mixed_precision and domain.getDtype() != torch.float64:
@@ -165,6 +167,17 @@ class Simulation:
         d = self.domain
         maxit = self.linear_solve_max_iterations if max_iter is None else int(max_iter)
         kind = BICGSTAB if use_BiCG else CG
+        ev = None
+        if self._solve_events is not None:
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            ev[0].record()
+            self._solve_events.append(ev)
+        self._solve_launch(which, rhs, x, kind, tol, tag, nrhs, return_best, maxit)
+        if ev is not None:
+            ev[1].record()
+
+    def _solve_launch(self, which, rhs, x, kind, tol, tag, nrhs, return_best, maxit) -> None:
+        d = self.domain
         if self.mixed_precision:
             lo = backend._lo(d, which)
             r = refiner_for(d, kind, nrhs, tag=tag)
@@ -216,7 +229,8 @@ class Simulation:
         self._check_flux_balance()
         try:
             return self._PISO_split_step(self.substeps)
-        except LinsolveError:
+        except LinsolveError as e:
+            self.last_error = str(e)
             return False
 
     def run(self, iterations: int) -> bool:

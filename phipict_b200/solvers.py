@@ -29,6 +29,7 @@ class LinearSolverResultInfo:
     converged: bool
     isFiniteResidual: bool
     status: int = 1
+    innerIterations: int = 0
 
     def __str__(self) -> str:
         return (f"LinearSolverResultInfo(residual={self.finalResidual:.3e}, iterations={self.usedIterations}, "
@@ -91,8 +92,8 @@ class StencilSolver:
         nsys = d.getBatchSize() * self.nrhs
         out = (_lib.PhbSolveResult * nsys)()
         _lib.call("phb_solve_results", ct.byref(d.desc()), ct.byref(self._s), out, _lib.stream_ptr(d.getDevice()))
-        return [LinearSolverResultInfo(o.final_residual, o.used_iterations, bool(o.converged), bool(o.finite), o.status)
-                for o in out]
+        return [LinearSolverResultInfo(o.final_residual, o.used_iterations, bool(o.converged), bool(o.finite), o.status,
+                                       o.inner_iterations) for o in out]
 
 
 class RefinedSolver:
@@ -135,8 +136,8 @@ class RefinedSolver:
         used = ct.c_int(0)
         _lib.call("phb_refine_run", ct.byref(d.desc()), ct.byref(r), out, ct.byref(used), _lib.stream_ptr(d.getDevice()))
         self.outer_used = used.value
-        return [LinearSolverResultInfo(o.final_residual, o.used_iterations, bool(o.converged), bool(o.finite), o.status)
-                for o in out]
+        return [LinearSolverResultInfo(o.final_residual, o.used_iterations, bool(o.converged), bool(o.finite), o.status,
+                                       o.inner_iterations) for o in out]
 
     def results(self) -> list[LinearSolverResultInfo]:
         """Outer results of the last solve (synchronises)."""
@@ -147,8 +148,8 @@ class RefinedSolver:
         _lib.call("phb_refine_results", ct.byref(d.desc()), ct.byref(self._r), out, ct.byref(used),
                   _lib.stream_ptr(d.getDevice()))
         self.outer_used = used.value
-        return [LinearSolverResultInfo(o.final_residual, o.used_iterations, bool(o.converged), bool(o.finite), o.status)
-                for o in out]
+        return [LinearSolverResultInfo(o.final_residual, o.used_iterations, bool(o.converged), bool(o.finite), o.status,
+                                       o.inner_iterations) for o in out]
 
 
 def solver_for(domain, kind: int, dtype: torch.dtype, nrhs: int, tag: str = "") -> StencilSolver:

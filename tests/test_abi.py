@@ -36,6 +36,6 @@ def test_version_and_error_text():
 
 def test_struct_layouts_match_header():
     assert ct.sizeof(_lib.PhbTolerance) == 48
-    assert ct.sizeof(_lib.PhbSolveResult) == 24
+    assert ct.sizeof(_lib.PhbSolveResult) == 32
     assert _lib.PhbSolve.tol.offset == 32
     assert _lib.PhbDomain.blocks.offset == 48
