@@ -43,7 +43,8 @@ enum phb_dtype { PHB_F32 = 0, PHB_F64 = 1 };
 #define PHB_BREC 48   /* block record  */
 #define PHB_FREC 16   /* fixed-face record */
 #define PHB_IREC 8    /* instance record */
-#define PHB_TILE 256  /* cells per tile (one CTA of the per-cell kernels) */
+#define PHB_TILE 256  /* threads per CTA of the per-cell kernels */
+#define PHB_TILE_CELLS 1024 /* cells per tile: one CTA, 4 cells per thread */
 
 /* Domain descriptor: device pointers produced by Domain.PrepareSolve(). It plays the
  * part of phiPICT's DomainGPU/BlockGPU atlas (domain/domain_structs_gpu.h:168-447). */
@@ -55,7 +56,7 @@ typedef struct phb_domain {
 	int64_t metric_stride;  /* cells in the metric array */
 	int64_t face_metric_stride;
 	const int32_t *blocks;  /* [nblocks][PHB_BREC] */
-	const int32_t *tiles;   /* [ntiles][2] = (block, first local cell) */
+	const int32_t *tiles;   /* [ntiles][2] = (block, first local cell), PHB_TILE_CELLS cells each */
 	const int32_t *fixed;   /* [nfixed][PHB_FREC] */
 	const int32_t *insts;   /* [ninst][PHB_IREC] */
 	const void *metrics;    /* [2d^2+1][metric_stride] */
@@ -191,6 +192,8 @@ typedef struct phb_refine {
 	int32_t nrhs;
 	int32_t max_outer;
 	int32_t inner_maxit;
+	int32_t use_graph;    /* 1: nested conditional-WHILE graph; 0: host loops (profiling) */
+	int32_t pad;
 	double inner_rtol;
 	phb_tolerance tol;    /* outer tolerance, on the float64 residual */
 	const double *A64;

@@ -230,11 +230,21 @@ def SolveLinear(A: CSRmatrix, RHS: torch.Tensor, x: torch.Tensor, maxit, tol, co
 
 
 def GetKrylovSettings() -> dict:
-    return {"enabled": True, "useGraphs": True}
+    from .solvers import SETTINGS
+
+    return {"enabled": True, "useGraphs": SETTINGS["use_graphs"], "checkInterval": SETTINGS["check_interval"]}
 
 
-def SetKrylovSettings(*args, **kwargs) -> None:
-    pass
+def SetKrylovSettings(enabled: bool = True, checkInterval: int = 8, useGraphs: bool = True,
+                      cgPreconditioner=None, bicgPreconditioner=None) -> None:
+    """Solver launch settings (bindings.cpp:739-751). Only the fused solvers exist here, so
+    ``enabled`` must stay True; preconditioners other than none are not implemented."""
+    from .solvers import SETTINGS
+
+    if not enabled:
+        raise NotImplementedError("phipict_b200 has no legacy (cuBLAS/cuSPARSE) solvers")
+    SETTINGS["use_graphs"] = bool(useGraphs)
+    SETTINGS["check_interval"] = max(1, int(checkInterval))
 
 
 def ReleaseKrylovWorkspaces() -> None:

@@ -15,7 +15,7 @@ _PKG = Path(__file__).resolve().parent
 LIB_PATH = _PKG / "libphipict_b200.so"
 
 PHB_F32, PHB_F64 = 0, 1
-BREC, FREC, IREC, TILE = 48, 16, 8, 256
+BREC, FREC, IREC, TILE = 48, 16, 8, 1024  # TILE: cells per tile (PHB_TILE_CELLS)
 
 # every exported symbol of include/phipict_b200.h
 EXPORTS = (
@@ -71,7 +71,7 @@ class PhbSolveResult(ct.Structure):
 class PhbRefine(ct.Structure):
     _fields_ = [
         ("kind", ct.c_int32), ("nrhs", ct.c_int32), ("max_outer", ct.c_int32), ("inner_maxit", ct.c_int32),
-        ("inner_rtol", ct.c_double),
+        ("use_graph", ct.c_int32), ("pad", ct.c_int32), ("inner_rtol", ct.c_double),
         ("tol", PhbTolerance),
         ("A64", ct.c_void_p), ("A32", ct.c_void_p), ("b", ct.c_void_p), ("x", ct.c_void_p),
         ("work", ct.c_void_p), ("state", ct.c_void_p),

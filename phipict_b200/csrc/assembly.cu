@@ -42,8 +42,11 @@ template <typename S, int D>
 __global__ void __launch_bounds__(PHB_TILE) kAdvectionMatrix(Dom<S, D> dom, const S *__restrict__ u, S *__restrict__ C,
 		S *__restrict__ Adiag, float *__restrict__ Clo) {
 	__shared__ int32_t sB[PHB_BREC];
+	int l0_, nc_;
+	loadTile<S, D>(dom, sB, l0_, nc_);
+	for (int j_ = 0; j_ < CPT; ++j_) {
 	Cell c;
-	if (!loadCell<S, D>(dom, sB, c)) return;
+	if (!cellAt<D>(sB, l0_, nc_, j_, c)) return;
 	const int inst = c.B[B_INST];
 	const S dt = S(dom.dt[inst]);
 	const S nu = S(dom.nu[inst]);
@@ -85,6 +88,7 @@ __global__ void __launch_bounds__(PHB_TILE) kAdvectionMatrix(Dom<S, D> dom, cons
 		if (Clo) Clo[s * N + c.g] = float(v);
 	}
 	Adiag[c.g] = rv[0] / det;
+	}
 }
 
 // boundary source of the momentum equation at fixed faces (advection.cu:834-866, the same
@@ -119,8 +123,11 @@ template <typename S, int D>
 __global__ void __launch_bounds__(PHB_TILE) kAdvectionRhs(Dom<S, D> dom, const S *__restrict__ u, const S *__restrict__ src,
 		int srcMode, S *__restrict__ rhs) {
 	__shared__ int32_t sB[PHB_BREC];
+	int l0_, nc_;
+	loadTile<S, D>(dom, sB, l0_, nc_);
+	for (int j_ = 0; j_ < CPT; ++j_) {
 	Cell c;
-	if (!loadCell<S, D>(dom, sB, c)) return;
+	if (!cellAt<D>(sB, l0_, nc_, j_, c)) return;
 	const int inst = c.B[B_INST];
 	const S dt = S(dom.dt[inst]);
 	const S nu = S(dom.nu[inst]);
@@ -134,6 +141,7 @@ __global__ void __launch_bounds__(PHB_TILE) kAdvectionRhs(Dom<S, D> dom, const S
 		r += sourceAt<S, D>(c, src, srcMode, dim);
 		rhs[o] = r;
 	}
+	}
 }
 
 // PISO_build_pressure_matrix (pressure.cu:26-191) with raP = 1/A, and
@@ -143,8 +151,11 @@ template <typename S, int D, bool EPOT>
 __global__ void __launch_bounds__(PHB_TILE) kLaplaceMatrix(Dom<S, D> dom, const S *__restrict__ Adiag, S *__restrict__ P,
 		float *__restrict__ Plo) {
 	__shared__ int32_t sB[PHB_BREC];
+	int l0_, nc_;
+	loadTile<S, D>(dom, sB, l0_, nc_);
+	for (int j_ = 0; j_ < CPT; ++j_) {
 	Cell c;
-	if (!loadCell<S, D>(dom, sB, c)) return;
+	if (!cellAt<D>(sB, l0_, nc_, j_, c)) return;
 	S alphaP[D];
 #pragma unroll
 	for (int d = 0; d < D; ++d) alphaP[d] = alphaAt<S, D>(dom, c.mi, d);
@@ -217,6 +228,7 @@ __global__ void __launch_bounds__(PHB_TILE) kLaplaceMatrix(Dom<S, D> dom, const 
 		P[s * N + c.g] = rv[s];
 		if (Plo) Plo[s * N + c.g] = float(rv[s]);
 	}
+	}
 }
 
 // PISO_build_pressure_rhs (pressure.cu:350-521): HbyA = (u/dt - H(u*) + S)/A per component
@@ -224,8 +236,11 @@ template <typename S, int D>
 __global__ void __launch_bounds__(PHB_TILE) kPressureRhs(Dom<S, D> dom, const S *__restrict__ C, const S *__restrict__ Adiag,
 		const S *__restrict__ u, const S *__restrict__ ustar, const S *__restrict__ src, int srcMode, S *__restrict__ hbya) {
 	__shared__ int32_t sB[PHB_BREC];
+	int l0_, nc_;
+	loadTile<S, D>(dom, sB, l0_, nc_);
+	for (int j_ = 0; j_ < CPT; ++j_) {
 	Cell c;
-	if (!loadCell<S, D>(dom, sB, c)) return;
+	if (!cellAt<D>(sB, l0_, nc_, j_, c)) return;
 	const int inst = c.B[B_INST];
 	const S dt = S(dom.dt[inst]);
 	const S nu = S(dom.nu[inst]);
@@ -252,20 +267,25 @@ __global__ void __launch_bounds__(PHB_TILE) kPressureRhs(Dom<S, D> dom, const S 
 		Ssum += sourceAt<S, D>(c, src, srcMode, dim);
 		hbya[o] = rDiag * (velOld - H + Ssum);
 	}
+	}
 }
 
 // k_computePressureRHSdivergenceFromFlux (pressure.cu:756-801), no face transforms
 template <typename S, int D>
 __global__ void __launch_bounds__(PHB_TILE) kDivergence(Dom<S, D> dom, const S *__restrict__ field, S *__restrict__ div) {
 	__shared__ int32_t sB[PHB_BREC];
+	int l0_, nc_;
+	loadTile<S, D>(dom, sB, l0_, nc_);
+	for (int j_ = 0; j_ < CPT; ++j_) {
 	Cell c;
-	if (!loadCell<S, D>(dom, sB, c)) return;
+	if (!cellAt<D>(sB, l0_, nc_, j_, c)) return;
 	S fl[2 * D];
 	faceFluxes<S, D>(dom, c, field, fl);
 	S dv = 0;
 #pragma unroll
 	for (int d = 0; d < D; ++d) dv += fl[d * 2 + 1] - fl[d * 2];
 	div[c.g] = dv;
+	}
 }
 
 // getPressureAtWithBounds for the +-1 neighbours (nonortho_laplace.cuh:302-381)
@@ -281,8 +301,11 @@ template <typename S, int D>
 __global__ void __launch_bounds__(PHB_TILE) kCorrectVelocity(Dom<S, D> dom, const S *__restrict__ p, const S *__restrict__ hbya,
 		const S *__restrict__ Adiag, S *__restrict__ u) {
 	__shared__ int32_t sB[PHB_BREC];
+	int l0_, nc_;
+	loadTile<S, D>(dom, sB, l0_, nc_);
+	for (int j_ = 0; j_ < CPT; ++j_) {
 	Cell c;
-	if (!loadCell<S, D>(dom, sB, c)) return;
+	if (!cellAt<D>(sB, l0_, nc_, j_, c)) return;
 	const S rDiag = S(1) / Adiag[c.g];
 	S gr[D];
 #pragma unroll
@@ -306,6 +329,7 @@ __global__ void __launch_bounds__(PHB_TILE) kCorrectVelocity(Dom<S, D> dom, cons
 	for (int d = 0; d < D; ++d) {
 		const int64_t o = vidx<D>(c.B, c.g, d);
 		u[o] = -rDiag * grad[d] + hbya[o];
+	}
 	}
 }
 
@@ -335,8 +359,11 @@ template <typename S, int D>
 __global__ void __launch_bounds__(PHB_TILE) kUxbEpotRhs(Dom<S, D> dom, const S *__restrict__ u, const double *__restrict__ eb,
 		S *__restrict__ uxb, S *__restrict__ rhs) {
 	__shared__ int32_t sB[PHB_BREC];
+	int l0_, nc_;
+	loadTile<S, D>(dom, sB, l0_, nc_);
+	for (int j_ = 0; j_ < CPT; ++j_) {
 	Cell c;
-	if (!loadCell<S, D>(dom, sB, c)) return;
+	if (!cellAt<D>(sB, l0_, nc_, j_, c)) return;
 	const double *e = eb + 3 * c.B[B_INST];
 	S x[3];
 	uCrossB<S, D>(c.B, c.g, u, e, x);
@@ -377,14 +404,18 @@ __global__ void __launch_bounds__(PHB_TILE) kUxbEpotRhs(Dom<S, D> dom, const S *
 		dv -= alphaAt<S, D>(dom, c.mi, f >> 1) * gv;
 	}
 	rhs[c.g] = dv;
+	}
 }
 
 // k_computeEpotRHS (mhd/potential.cu:273-323) of a given in-plane field [inst][dims][cells]
 template <typename S, int D>
 __global__ void __launch_bounds__(PHB_TILE) kEpotRhs(Dom<S, D> dom, const S *__restrict__ field, S *__restrict__ rhs) {
 	__shared__ int32_t sB[PHB_BREC];
+	int l0_, nc_;
+	loadTile<S, D>(dom, sB, l0_, nc_);
+	for (int j_ = 0; j_ < CPT; ++j_) {
 	Cell c;
-	if (!loadCell<S, D>(dom, sB, c)) return;
+	if (!cellAt<D>(sB, l0_, nc_, j_, c)) return;
 	S fl[2 * D];
 #pragma unroll
 	for (int dim = 0; dim < D; ++dim) {
@@ -418,6 +449,7 @@ __global__ void __launch_bounds__(PHB_TILE) kEpotRhs(Dom<S, D> dom, const S *__r
 		dv -= alphaAt<S, D>(dom, c.mi, f >> 1) * gv;
 	}
 	rhs[c.g] = dv;
+	}
 }
 
 // computeCurrentDensityFaceBased (mhd/potential.cu:718-880) fused with the Lorentz force
@@ -426,8 +458,11 @@ template <typename S, int D>
 __global__ void __launch_bounds__(PHB_TILE) kCurrentLorentz(Dom<S, D> dom, const S *__restrict__ phi, const S *__restrict__ uxb,
 		const double *__restrict__ eb, const double *__restrict__ stuart, S *__restrict__ Jout, S *__restrict__ src, int accumulate) {
 	__shared__ int32_t sB[PHB_BREC];
+	int l0_, nc_;
+	loadTile<S, D>(dom, sB, l0_, nc_);
+	for (int j_ = 0; j_ < CPT; ++j_) {
 	Cell c;
-	if (!loadCell<S, D>(dom, sB, c)) return;
+	if (!cellAt<D>(sB, l0_, nc_, j_, c)) return;
 	const int inst = c.B[B_INST];
 	const S phiP = phi[c.g];
 	S alphaP[D], cvelP[D];
@@ -491,6 +526,7 @@ __global__ void __launch_bounds__(PHB_TILE) kCurrentLorentz(Dom<S, D> dom, const
 			const S v = N * F[d];
 			src[o] = accumulate ? v + src[o] : v;
 		}
+	}
 	}
 }
 

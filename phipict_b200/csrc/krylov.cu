@@ -84,43 +84,68 @@ __device__ __forceinline__ bool storePartials(double (&v)[NV], double *partial, 
 	return isLast;
 }
 
-// In the last CTA: one warp per running system sums its instance's CTA partials in a fixed
-// order and lane 0 calls fn(state, inst, sums, instSum); then allDone is updated and the
-// ticket counter reset for the next kernel. With INSTQ >= 0 the warp also sums quantity
-// INSTQ over all K systems of the instance (instSum), e.g. the whole right-hand side norm.
+// In the last CTA: the warps are split into groups of G (a power of two, as many as fit
+// NWARPS/nsys); each group sums the CTA partials of one system's instance in a fixed order
+// (lanes strided over the tiles, two accumulators in flight, then warp and group sums) and
+// its leader calls fn(state, inst, sums, instSum). allDone is updated and the ticket
+// counter reset for the next kernel. With INSTQ >= 0 the group also sums quantity INSTQ over
+// all K systems of the instance (instSum), e.g. the whole right-hand side norm.
 template <int K, int NQ, int INSTQ = -1, typename Fn>
 __device__ __forceinline__ void finalizeSystems(const int32_t *insts, int ninst, const double *partial, SysState *st, Control *ctrl, Fn fn) {
+	constexpr int NV = NQ + 1;
 	__shared__ int running;
+	__shared__ double gsm[NWARPS][NV];
 	if (threadIdx.x == 0) running = 0;
 	__threadfence();
 	__syncthreads();
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	const int nsys = ninst * K;
-	for (int s = warp; s < nsys; s += NWARPS) {
-		const int inst = s / K, k = s - inst * K;
-		if (st[s].done == RUNNING) {
+	int G = NWARPS;
+	while (G > 1 && G * nsys > NWARPS) G >>= 1;
+	const int NG = NWARPS / G;
+	const int group = warp / G, wg = warp - group * G;
+	for (int base = 0; base < nsys; base += NG) {
+		const int s = base + group;
+		const bool act = s < nsys && st[s].done == RUNNING;
+		double a0[NV], a1[NV];
+#pragma unroll
+		for (int q = 0; q < NV; ++q) { a0[q] = 0; a1[q] = 0; }
+		if (act) {
+			const int inst = s / K, k = s - inst * K;
 			const int t0 = insts[inst * PHB_IREC + I_TILESTART], tc = insts[inst * PHB_IREC + I_TILECOUNT];
-			double acc[NQ];
-			double inst_acc = 0;
+			const int stride = G * 32;
+			auto load = [&](int t, double *a) {
+				const double *pp = partial + (size_t)(t0 + t) * K * NQ;
 #pragma unroll
-			for (int q = 0; q < NQ; ++q) acc[q] = 0;
-			for (int t = lane; t < tc; t += 32) {
-#pragma unroll
-				for (int q = 0; q < NQ; ++q) acc[q] += __ldcg(partial + ((size_t)(t0 + t) * K + k) * NQ + q);
+				for (int q = 0; q < NQ; ++q) a[q] += __ldcg(pp + k * NQ + q);
 				if (INSTQ >= 0) {
 #pragma unroll
-					for (int kk = 0; kk < K; ++kk) inst_acc += __ldcg(partial + ((size_t)(t0 + t) * K + kk) * NQ + (INSTQ < 0 ? 0 : INSTQ));
+					for (int kk = 0; kk < K; ++kk) a[NQ] += __ldcg(pp + kk * NQ + (INSTQ < 0 ? 0 : INSTQ));
 				}
-			}
-#pragma unroll
-			for (int q = 0; q < NQ; ++q) acc[q] = warpSum(acc[q]);
-			if (INSTQ >= 0) inst_acc = warpSum(inst_acc);
-			if (lane == 0) fn(st[s], inst, acc, inst_acc);
-			__syncwarp();
+			};
+			int t = wg * 32 + lane;
+			for (; t + stride < tc; t += 2 * stride) { load(t, a0); load(t + stride, a1); }
+			if (t < tc) load(t, a0);
 		}
-		if (lane == 0 && st[s].done == RUNNING) atomicAdd(&running, 1);
+#pragma unroll
+		for (int q = 0; q < NV; ++q) {
+			const double v = warpSum(a0[q] + a1[q]);
+			if (lane == 0) gsm[warp][q] = v;
+		}
+		__syncthreads();
+		if (act && wg == 0 && lane == 0) {
+			double red[NV];
+#pragma unroll
+			for (int q = 0; q < NV; ++q) {
+				double v = 0;
+				for (int w = 0; w < G; ++w) v += gsm[group * G + w][q];
+				red[q] = v;
+			}
+			fn(st[s], s / K, red, red[NQ]);
+		}
+		if (wg == 0 && lane == 0 && s < nsys && st[s].done == RUNNING) atomicAdd(&running, 1);
+		__syncthreads();
 	}
-	__syncthreads();
 	if (threadIdx.x == 0) {
 		ctrl->allDone = running == 0;
 		ctrl->counter = 0;
@@ -212,8 +237,8 @@ __global__ void __launch_bounds__(PHB_TILE) kResidual(Dom<double, D> dom, const 
 		const T *__restrict__ x, T *__restrict__ r, T *__restrict__ r0, SysState *st, double *partial, Control *ctrl, phb_tolerance tol,
 		LoopCond arm) {
 	__shared__ int32_t sB[PHB_BREC];
-	Cell c;
-	const bool valid = loadCell<double, D>(dom, sB, c);
+	int l0_, nc_;
+	loadTile<double, D>(dom, sB, l0_, nc_);
 	const int inst = sB[B_INST];
 	bool act[K];
 #pragma unroll
@@ -221,7 +246,9 @@ __global__ void __launch_bounds__(PHB_TILE) kResidual(Dom<double, D> dom, const 
 	double acc[2 * K];
 #pragma unroll
 	for (int k = 0; k < 2 * K; ++k) acc[k] = 0;
-	if (valid) {
+	for (int j_ = 0; j_ < CPT; ++j_) {
+		Cell c;
+		if (!cellAt<D>(sB, l0_, nc_, j_, c)) break;
 		int64_t nb[2 * D];
 		stencilNeighbors<D>(dom, c, nb);
 		T y[K];
@@ -234,8 +261,8 @@ __global__ void __launch_bounds__(PHB_TILE) kResidual(Dom<double, D> dom, const 
 			const T ri = bi - y[k];
 			r[o] = ri;
 			if (BICG) r0[o] = ri;
-			acc[2 * k] = double(ri) * double(ri);
-			acc[2 * k + 1] = double(bi) * double(bi);
+			acc[2 * k] += double(ri) * double(ri);
+			acc[2 * k + 1] += double(bi) * double(bi);
 		}
 	}
 	if (storePartials<2 * K>(acc, partial, &ctrl->counter)) {
@@ -262,8 +289,8 @@ template <typename T, int D, int K>
 __global__ void __launch_bounds__(PHB_TILE) kCgDirection(Dom<double, D> dom, const T *__restrict__ A, const T *__restrict__ r,
 		const T *__restrict__ pIn, T *__restrict__ pOut, T *__restrict__ q, SysState *st, double *partial, Control *ctrl) {
 	__shared__ int32_t sB[PHB_BREC];
-	Cell c;
-	const bool valid = loadCell<double, D>(dom, sB, c);
+	int l0_, nc_;
+	loadTile<double, D>(dom, sB, l0_, nc_);
 	const int inst = sB[B_INST];
 	bool act[K], rs[K];
 	T beta[K];
@@ -277,7 +304,9 @@ __global__ void __launch_bounds__(PHB_TILE) kCgDirection(Dom<double, D> dom, con
 	double acc[K];
 #pragma unroll
 	for (int k = 0; k < K; ++k) acc[k] = 0;
-	if (valid) {
+	for (int j_ = 0; j_ < CPT; ++j_) {
+		Cell c;
+		if (!cellAt<D>(sB, l0_, nc_, j_, c)) break;
 		int64_t nb[2 * D];
 		stencilNeighbors<D>(dom, c, nb);
 		auto pv = [&](int64_t g, int k) {
@@ -293,7 +322,7 @@ __global__ void __launch_bounds__(PHB_TILE) kCgDirection(Dom<double, D> dom, con
 			const T pi = pv(c.g, k);
 			pOut[o] = pi;
 			q[o] = y[k];
-			acc[k] = double(pi) * double(y[k]);
+			acc[k] += double(pi) * double(y[k]);
 		}
 	}
 	if (storePartials<K>(acc, partial, &ctrl->counter)) {
@@ -313,13 +342,15 @@ __global__ void __launch_bounds__(PHB_TILE) kCgUpdate(Dom<double, D> dom, T *__r
 		const T *__restrict__ q, T *__restrict__ x, T *__restrict__ xbest, SysState *st, double *partial, Control *ctrl,
 		int returnBest, LoopCond lc) {
 	__shared__ int32_t sB[PHB_BREC];
-	Cell c;
-	const bool valid = loadCell<double, D>(dom, sB, c);
+	int l0_, nc_;
+	loadTile<double, D>(dom, sB, l0_, nc_);
 	const int inst = sB[B_INST];
 	double acc[K];
 #pragma unroll
 	for (int k = 0; k < K; ++k) acc[k] = 0;
-	if (valid) {
+	for (int j_ = 0; j_ < CPT; ++j_) {
+		Cell c;
+		if (!cellAt<D>(sB, l0_, nc_, j_, c)) break;
 #pragma unroll
 		for (int k = 0; k < K; ++k) {
 			const SysState &s = st[inst * K + k];
@@ -331,7 +362,7 @@ __global__ void __launch_bounds__(PHB_TILE) kCgUpdate(Dom<double, D> dom, T *__r
 			x[o] = xi + alpha * p[o];
 			const T ri = r[o] - alpha * q[o];
 			r[o] = ri;
-			acc[k] = double(ri) * double(ri);
+			acc[k] += double(ri) * double(ri);
 		}
 	}
 	if (storePartials<K>(acc, partial, &ctrl->counter)) {
@@ -367,8 +398,8 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgV(Dom<double, D> dom, const T *
 		const T *__restrict__ pIn, const T *__restrict__ vIn, T *__restrict__ pOut, T *__restrict__ vOut, const T *__restrict__ r0,
 		SysState *st, double *partial, Control *ctrl) {
 	__shared__ int32_t sB[PHB_BREC];
-	Cell c;
-	const bool valid = loadCell<double, D>(dom, sB, c);
+	int l0_, nc_;
+	loadTile<double, D>(dom, sB, l0_, nc_);
 	const int inst = sB[B_INST];
 	bool act[K], rs[K];
 	T beta[K], omega[K];
@@ -383,7 +414,9 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgV(Dom<double, D> dom, const T *
 	double acc[K];
 #pragma unroll
 	for (int k = 0; k < K; ++k) acc[k] = 0;
-	if (valid) {
+	for (int j_ = 0; j_ < CPT; ++j_) {
+		Cell c;
+		if (!cellAt<D>(sB, l0_, nc_, j_, c)) break;
 		int64_t nb[2 * D];
 		stencilNeighbors<D>(dom, c, nb);
 		auto pv = [&](int64_t g, int k) {
@@ -398,7 +431,7 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgV(Dom<double, D> dom, const T *
 			const int64_t o = vk<K>(c.B, c.g, k);
 			pOut[o] = pv(c.g, k);
 			vOut[o] = y[k];
-			acc[k] = double(r0[o]) * double(y[k]);
+			acc[k] += double(r0[o]) * double(y[k]);
 		}
 	}
 	if (storePartials<K>(acc, partial, &ctrl->counter)) {
@@ -417,8 +450,8 @@ template <typename T, int D, int K>
 __global__ void __launch_bounds__(PHB_TILE) kBicgT(Dom<double, D> dom, const T *__restrict__ A, const T *__restrict__ r,
 		const T *__restrict__ v, T *__restrict__ t, SysState *st, double *partial, Control *ctrl) {
 	__shared__ int32_t sB[PHB_BREC];
-	Cell c;
-	const bool valid = loadCell<double, D>(dom, sB, c);
+	int l0_, nc_;
+	loadTile<double, D>(dom, sB, l0_, nc_);
 	const int inst = sB[B_INST];
 	bool act[K];
 	T alpha[K];
@@ -431,7 +464,9 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgT(Dom<double, D> dom, const T *
 	double acc[3 * K];
 #pragma unroll
 	for (int k = 0; k < 3 * K; ++k) acc[k] = 0;
-	if (valid) {
+	for (int j_ = 0; j_ < CPT; ++j_) {
+		Cell c;
+		if (!cellAt<D>(sB, l0_, nc_, j_, c)) break;
 		int64_t nb[2 * D];
 		stencilNeighbors<D>(dom, c, nb);
 		auto sv = [&](int64_t g, int k) {
@@ -446,9 +481,9 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgT(Dom<double, D> dom, const T *
 			const int64_t o = vk<K>(c.B, c.g, k);
 			const T si = sv(c.g, k);
 			t[o] = y[k];
-			acc[3 * k + 0] = double(y[k]) * double(si);
-			acc[3 * k + 1] = double(y[k]) * double(y[k]);
-			acc[3 * k + 2] = double(si) * double(si);
+			acc[3 * k + 0] += double(y[k]) * double(si);
+			acc[3 * k + 1] += double(y[k]) * double(y[k]);
+			acc[3 * k + 2] += double(si) * double(si);
 		}
 	}
 	if (storePartials<3 * K>(acc, partial, &ctrl->counter)) {
@@ -473,13 +508,15 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgUpdate(Dom<double, D> dom, T *_
 		const T *__restrict__ p, const T *__restrict__ v, const T *__restrict__ t, T *__restrict__ x, SysState *st,
 		double *partial, Control *ctrl, LoopCond lc) {
 	__shared__ int32_t sB[PHB_BREC];
-	Cell c;
-	const bool valid = loadCell<double, D>(dom, sB, c);
+	int l0_, nc_;
+	loadTile<double, D>(dom, sB, l0_, nc_);
 	const int inst = sB[B_INST];
 	double acc[2 * K];
 #pragma unroll
 	for (int k = 0; k < 2 * K; ++k) acc[k] = 0;
-	if (valid) {
+	for (int j_ = 0; j_ < CPT; ++j_) {
+		Cell c;
+		if (!cellAt<D>(sB, l0_, nc_, j_, c)) break;
 #pragma unroll
 		for (int k = 0; k < K; ++k) {
 			const SysState &s = st[inst * K + k];
@@ -494,8 +531,8 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgUpdate(Dom<double, D> dom, T *_
 				x[o] += alpha * p[o] + omega * si;
 				const T ri = si - omega * t[o];
 				r[o] = ri;
-				acc[2 * k + 0] = double(r0[o]) * double(ri);
-				acc[2 * k + 1] = double(ri) * double(ri);
+				acc[2 * k + 0] += double(r0[o]) * double(ri);
+				acc[2 * k + 1] += double(ri) * double(ri);
 			}
 		}
 	}
@@ -547,12 +584,14 @@ __global__ void __launch_bounds__(PHB_TILE) kRefineResidual(Dom<double, D> dom, 
 		const double *__restrict__ x, float *__restrict__ r32, float *__restrict__ e32, SysState *st, double *partial, Control *ctrl,
 		double innerRtol, int maxOuter, phb_tolerance tol, SysState *inner, LoopCond lc) {
 	__shared__ int32_t sB[PHB_BREC];
-	Cell c;
-	const bool valid = loadCell<double, D>(dom, sB, c);
+	int l0_, nc_;
+	loadTile<double, D>(dom, sB, l0_, nc_);
 	double acc[2 * K];
 #pragma unroll
 	for (int k = 0; k < 2 * K; ++k) acc[k] = 0;
-	if (valid) {
+	for (int j_ = 0; j_ < CPT; ++j_) {
+		Cell c;
+		if (!cellAt<D>(sB, l0_, nc_, j_, c)) break;
 		int64_t nb[2 * D];
 		stencilNeighbors<D>(dom, c, nb);
 		bool act[K];
@@ -567,8 +606,8 @@ __global__ void __launch_bounds__(PHB_TILE) kRefineResidual(Dom<double, D> dom, 
 			const double ri = bi - y[k];
 			r32[o] = float(ri);
 			e32[o] = 0.f;
-			acc[2 * k] = ri * ri;
-			acc[2 * k + 1] = bi * bi;
+			acc[2 * k] += ri * ri;
+			acc[2 * k + 1] += bi * bi;
 		}
 	}
 	if (storePartials<2 * K>(acc, partial, &ctrl->counter)) {
@@ -576,22 +615,37 @@ __global__ void __launch_bounds__(PHB_TILE) kRefineResidual(Dom<double, D> dom, 
 		// every system is visited, also once done, so that the inner solve of a finished
 		// system sees an infinite tolerance and stops at once
 		__shared__ int running;
+		__shared__ double gsm[NWARPS][2];
 		if (threadIdx.x == 0) running = 0;
 		__threadfence();
 		__syncthreads();
 		const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-		for (int s = warp; s < nsys; s += NWARPS) {
-			const int inst = s / K, k = s - inst * K;
-			const int t0 = dom.insts[inst * PHB_IREC + I_TILESTART], tc = dom.insts[inst * PHB_IREC + I_TILECOUNT];
+		int G = NWARPS;
+		while (G > 1 && G * nsys > NWARPS) G >>= 1;
+		const int NG = NWARPS / G;
+		const int group = warp / G, wg = warp - group * G;
+		for (int base = 0; base < nsys; base += NG) {
+			const int s = base + group;
 			double a = 0, bb = 0;
-			for (int t = lane; t < tc; t += 32) {
-				a += __ldcg(partial + ((size_t)(t0 + t) * K + k) * 2);
+			if (s < nsys) {
+				const int inst = s / K, k = s - inst * K;
+				const int t0 = dom.insts[inst * PHB_IREC + I_TILESTART], tc = dom.insts[inst * PHB_IREC + I_TILECOUNT];
+				for (int t = wg * 32 + lane; t < tc; t += G * 32) {
+					const double *pp = partial + (size_t)(t0 + t) * K * 2;
+					a += __ldcg(pp + k * 2);
 #pragma unroll
-				for (int kk = 0; kk < K; ++kk) bb += __ldcg(partial + ((size_t)(t0 + t) * K + kk) * 2 + 1);
+					for (int kk = 0; kk < K; ++kk) bb += __ldcg(pp + kk * 2 + 1);
+				}
 			}
 			a = warpSum(a);
 			bb = warpSum(bb);
-			if (lane == 0) {
+			if (lane == 0) { gsm[warp][0] = a; gsm[warp][1] = bb; }
+			__syncthreads();
+			if (s < nsys && wg == 0 && lane == 0) {
+				a = 0;
+				bb = 0;
+				for (int w = 0; w < G; ++w) { a += gsm[group * G + w][0]; bb += gsm[group * G + w][1]; }
+				const int inst = s / K;
 				SysState &o = st[s];
 				const double ns = normScale(dom.insts, inst);
 				if (o.it == 0 && o.done == RUNNING && tol.mode == 1) o.tol = resolveTol(tol, sqrt(bb / double(K)) * ns);
@@ -608,8 +662,8 @@ __global__ void __launch_bounds__(PHB_TILE) kRefineResidual(Dom<double, D> dom, 
 				inner[s].innerTol = o.done == RUNNING ? fmax(innerRtol * crit, 0.25 * o.tol) : INFINITY;
 				if (o.done == RUNNING) atomicAdd(&running, 1);
 			}
+			__syncthreads();
 		}
-		__syncthreads();
 		if (threadIdx.x == 0) {
 			ctrl->allDone = running == 0;
 			ctrl->counter = 0;
@@ -987,22 +1041,40 @@ static int emitRefine(const phb_domain *dom, const phb_refine *rf, cudaStream_t 
 	in.tol = phb_tolerance{}; // unused: the inner tolerance is SysState::innerTol
 	in.work = rf->work;
 	in.state = rf->state;
-	cudaGraphConditionalHandle outerHandle;
-	int rc0 = createCondition(s, &outerHandle);
-	if (rc0) return rc0;
-	kInitOuter<<<1, 256, 0, s>>>(stO, nsys, rf->tol, ctrlO, rf->max_outer + 2, LoopCond{outerHandle, 1});
+	const bool graph = rf->use_graph != 0;
+	in.use_graph = graph ? 1 : 0;
+	in.check_every = 8;
+	cudaGraphConditionalHandle outerHandle{};
+	if (graph) {
+		const int rc0 = createCondition(s, &outerHandle);
+		if (rc0) return rc0;
+	}
+	kInitOuter<<<1, 256, 0, s>>>(stO, nsys, rf->tol, ctrlO, rf->max_outer + 2, LoopCond{outerHandle, graph ? 1 : 0});
 	PHB_CUDA(cudaGetLastError());
 	auto outer = [&](cudaStream_t os, LoopCond lc) -> int {
 		kRefineResidual<D, K><<<dom->ntiles, PHB_TILE, 0, os>>>(dm, rf->A64, rf->b, rf->x, r32, e32, stO, partial, ctrlO,
 			rf->inner_rtol, rf->max_outer, rf->tol, stI, lc);
 		int rc = checkLaunch("kRefineResidual");
 		if (rc) return rc;
-		rc = emitSolve<float, D, K>(dom, &in, os, ss, 2, true, 1);
+		rc = emitSolve<float, D, K>(dom, &in, os, ss, graph ? 2 : 0, true, 1);
 		if (rc) return rc;
 		kRefineUpdate<K><<<gridFor(dom->ncells * K), 256, 0, os>>>(dom->ncells * K, rf->x, e32);
 		return checkLaunch("kRefineUpdate");
 	};
-	return addWhile(s, ss.s[1], outerHandle, outer);
+	if (graph) return addWhile(s, ss.s[1], outerHandle, outer);
+	// host loop: every kernel launched on its own (profilers see each launch)
+	int *hflag = nullptr;
+	PHB_CUDA(cudaMallocHost(&hflag, sizeof(int)));
+	int rc = PHB_OK;
+	for (int sweep = 0; sweep < rf->max_outer + 2; ++sweep) {
+		rc = outer(s, LoopCond{0, 0});
+		if (rc) break;
+		cudaMemcpyAsync(hflag, &ctrlO->allDone, sizeof(int), cudaMemcpyDeviceToHost, s);
+		cudaStreamSynchronize(s);
+		if (*hflag) break;
+	}
+	cudaFreeHost(hflag);
+	return rc;
 }
 
 extern "C" int phb_refine_results(const phb_domain *dom, const phb_refine *r, phb_solve_result *out, int *outer_used, phb_stream stream);
@@ -1015,6 +1087,19 @@ extern "C" int phb_refine_run(const phb_domain *dom, const phb_refine *r, phb_so
 	const std::string key = makeKey("refine", *dom, *r);
 	int rc = PHB_OK;
 	const int K = r->nrhs;
+	if (!r->use_graph) {
+		Streams *ss;
+		rc = getStreams(ss);
+		if (rc) return rc;
+		if (dom->dims == 2 && K == 1) rc = emitRefine<2, 1>(dom, r, st, *ss);
+		else if (dom->dims == 2 && K == 2) rc = emitRefine<2, 2>(dom, r, st, *ss);
+		else if (dom->dims == 3 && K == 1) rc = emitRefine<3, 1>(dom, r, st, *ss);
+		else if (dom->dims == 3 && K == 3) rc = emitRefine<3, 3>(dom, r, st, *ss);
+		else return setError(PHB_ERR_ARG, "phb_refine_run: unsupported dims/nrhs");
+		if (rc) return rc;
+		if (out) return phb_refine_results(dom, r, out, outer_used, stream);
+		return PHB_OK;
+	}
 	if (dom->dims == 2 && K == 1) rc = runGraph(st, key, [&](cudaStream_t cs, Streams &ss) { return emitRefine<2, 1>(dom, r, cs, ss); });
 	else if (dom->dims == 2 && K == 2) rc = runGraph(st, key, [&](cudaStream_t cs, Streams &ss) { return emitRefine<2, 2>(dom, r, cs, ss); });
 	else if (dom->dims == 3 && K == 1) rc = runGraph(st, key, [&](cudaStream_t cs, Streams &ss) { return emitRefine<3, 1>(dom, r, cs, ss); });

@@ -234,21 +234,29 @@ __device__ __forceinline__ S alphaFixed(const Dom<S, D> &dom, const int32_t *FR,
 	return dom.fm(Tr<D>::DET, fi) * s;
 }
 
-// Stage the CTA's block record into shared memory and locate this thread's cell.
-// Returns false for threads past the end of the block.
+// cells each thread handles per tile: a tile is PHB_TILE_CELLS consecutive cells of one
+// block, thread t takes cells t, t+PHB_TILE, ... (coalesced)
+constexpr int CPT = PHB_TILE_CELLS / PHB_TILE;
+
+// Stage the CTA's block record into shared memory; l0 = first local cell of the tile,
+// nc = cells of the block.
 template <typename S, int D>
-__device__ __forceinline__ bool loadCell(const Dom<S, D> &dom, int32_t *sB, Cell &c) {
+__device__ __forceinline__ void loadTile(const Dom<S, D> &dom, int32_t *sB, int &l0, int &nc) {
 	const int tile = blockIdx.x;
 	const int b = __ldg(dom.tiles + 2 * tile);
-	const int l0 = __ldg(dom.tiles + 2 * tile + 1);
+	l0 = __ldg(dom.tiles + 2 * tile + 1);
 	if (threadIdx.x < PHB_BREC) sB[threadIdx.x] = __ldg(dom.blocks + b * PHB_BREC + threadIdx.x);
 	__syncthreads();
-	c.B = sB;
-	c.b = b;
-	const int l = l0 + threadIdx.x;
+	nc = sB[B_NX] * sB[B_NY] * (D > 2 ? sB[B_NZ] : 1);
+}
+
+// The j-th cell of this thread in the tile; false past the end of the block.
+template <int D>
+__device__ __forceinline__ bool cellAt(const int32_t *sB, int l0, int nc, int j, Cell &c) {
+	const int l = l0 + threadIdx.x + j * PHB_TILE;
+	if (l >= nc || l >= l0 + PHB_TILE_CELLS) return false;
 	const int nx = sB[B_NX], ny = sB[B_NY];
-	const int nc = nx * ny * (D > 2 ? sB[B_NZ] : 1);
-	if (l >= nc) return false;
+	c.B = sB;
 	c.p[0] = l % nx;
 	c.p[1] = (l / nx) % ny;
 	c.p[2] = D > 2 ? l / (nx * ny) : 0;

@@ -27,13 +27,15 @@ __global__ void __launch_bounds__(PHB_TILE) kInstanceSums(Dom<S, D> dom, const S
 	__shared__ int32_t sB[PHB_BREC];
 	__shared__ double sm[3][NW];
 	__shared__ bool isLast;
-	Cell c;
-	const bool valid = loadCell<S, D>(dom, sB, c);
+	int l0_, nc_;
+	loadTile<S, D>(dom, sB, l0_, nc_);
 	double v[3] = {0, 0, 0};
-	if (valid) {
+	for (int j_ = 0; j_ < CPT; ++j_) {
+		Cell c;
+		if (!cellAt<D>(sB, l0_, nc_, j_, c)) break;
 		for (int k = 0; k < comps; ++k) {
 			const double a = double(x[c.g + (int64_t)(comps - 1) * c.B[B_INSTOFF] + (int64_t)k * c.B[B_INSTN]]);
-			v[k] = POW == 2 ? a * a : a;
+			v[k] += POW == 2 ? a * a : a;
 		}
 	}
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -77,13 +79,17 @@ __global__ void __launch_bounds__(PHB_TILE) kInstanceSums(Dom<S, D> dom, const S
 template <typename S, int D>
 __global__ void __launch_bounds__(PHB_TILE) kSubtractMean(Dom<S, D> dom, S *__restrict__ x, int comps, const double *__restrict__ scratch) {
 	__shared__ int32_t sB[PHB_BREC];
+	int l0_, nc_;
+	loadTile<S, D>(dom, sB, l0_, nc_);
+	for (int j_ = 0; j_ < CPT; ++j_) {
 	Cell c;
-	if (!loadCell<S, D>(dom, sB, c)) return;
+	if (!cellAt<D>(sB, l0_, nc_, j_, c)) return;
 	const double *res = scratch + 8;
 	const int inst = c.B[B_INST];
 	for (int k = 0; k < comps; ++k) {
 		const int64_t o = c.g + (int64_t)(comps - 1) * c.B[B_INSTOFF] + (int64_t)k * c.B[B_INSTN];
 		x[o] = S(double(x[o]) - res[inst * comps + k]);
+	}
 	}
 }
 
@@ -101,17 +107,24 @@ __global__ void kRmsFinish(const int32_t *insts, int ninst, int comps, const dou
 template <int D>
 __global__ void __launch_bounds__(PHB_TILE) kCsrRowSizes(Dom<double, D> dom, int32_t *rowsize) {
 	__shared__ int32_t sB[PHB_BREC];
+	int l0_, nc_;
+	loadTile<double, D>(dom, sB, l0_, nc_);
+	for (int j_ = 0; j_ < CPT; ++j_) {
 	Cell c;
-	if (!loadCell<double, D>(dom, sB, c)) return;
+	if (!cellAt<D>(sB, l0_, nc_, j_, c)) return;
 	int n = 2 * D + 1;
 	for (int f = 0; f < 2 * D; ++f) if (atBound(c.B, f, c.p) && fType(c.B, f) == FT_FIXED) --n;
 	rowsize[c.g] = n;
+	}
 }
 template <int D>
 __global__ void __launch_bounds__(PHB_TILE) kCsrPattern(Dom<double, D> dom, const int32_t *__restrict__ row, int32_t *col, int32_t *perm) {
 	__shared__ int32_t sB[PHB_BREC];
+	int l0_, nc_;
+	loadTile<double, D>(dom, sB, l0_, nc_);
+	for (int j_ = 0; j_ < CPT; ++j_) {
 	Cell c;
-	if (!loadCell<double, D>(dom, sB, c)) return;
+	if (!cellAt<D>(sB, l0_, nc_, j_, c)) return;
 	int64_t ci[2 * D + 1];
 	ci[0] = c.g;
 	for (int f = 0; f < 2 * D; ++f) ci[f + 1] = neighborIndex<double, D>(dom, c, f);
@@ -125,6 +138,7 @@ __global__ void __launch_bounds__(PHB_TILE) kCsrPattern(Dom<double, D> dom, cons
 		perm[w] = (int32_t)(best * dom.ncells + c.g);
 		ci[best] = -1;
 		++w;
+	}
 	}
 }
 template <typename T>

@@ -10,6 +10,7 @@ that synchronises.
 from __future__ import annotations
 
 import ctypes as ct
+import os
 from dataclasses import dataclass
 
 import torch
@@ -19,6 +20,11 @@ from .tolerance import to_device_tolerance
 
 CG, BICGSTAB = 0, 1
 STATUS = {0: "running", 1: "converged", 2: "non-finite", 3: "max iterations", 4: "rising"}
+
+# Global solver settings (phiPICT's SetKrylovSettings, bindings.cpp:739-751): with graphs
+# every solve is one CUDA-graph launch; without, every kernel is launched on its own and the
+# host polls for completion every `check_interval` iterations (what a profiler needs).
+SETTINGS = {"use_graphs": os.environ.get("PHIPICT_B200_GRAPHS", "1") != "0", "check_interval": 8}
 
 
 @dataclass
@@ -66,7 +72,7 @@ class StencilSolver:
         self._keep = None
 
     def solve(self, A: torch.Tensor, b: torch.Tensor, x: torch.Tensor, tol, maxit: int,
-              return_best: bool = False, use_graph: bool = True) -> None:
+              return_best: bool = False, use_graph: bool | None = None) -> None:
         """Launch the solve of ``A x = b`` (x: initial guess, overwritten). Asynchronous."""
         d = self.domain
         if A.dtype != self.dtype or b.dtype != self.dtype or x.dtype != self.dtype:
@@ -79,8 +85,8 @@ class StencilSolver:
         s.nrhs = self.nrhs
         s.maxit = int(maxit)
         s.return_best = int(bool(return_best)) if self.kind == CG else 0
-        s.use_graph = int(bool(use_graph))
-        s.check_every = 8
+        s.use_graph = int(bool(SETTINGS["use_graphs"] if use_graph is None else use_graph))
+        s.check_every = int(SETTINGS["check_interval"])
         nsys = d.getBatchSize() * self.nrhs
         s.tol, self._keep = to_device_tolerance(tol, d.getDtype(), nsys, d.getDevice())
         s.A, s.b, s.x = A.data_ptr(), b.data_ptr(), x.data_ptr()
@@ -125,6 +131,7 @@ class RefinedSolver:
         r.max_outer = self.max_outer
         r.inner_maxit = int(maxit)
         r.inner_rtol = self.inner_rtol
+        r.use_graph = int(bool(SETTINGS["use_graphs"]))
         nsys = d.getBatchSize() * self.nrhs
         r.tol, self._keep = to_device_tolerance(tol, torch.float64, nsys, d.getDevice())
         r.A64, r.A32, r.b, r.x = A64.data_ptr(), A32.data_ptr(), b.data_ptr(), x.data_ptr()
