@@ -209,6 +209,22 @@ int phb_refine_run(const phb_domain *dom, const phb_refine *r, phb_solve_result 
 /* per-system outer results of the last refinement (synchronises the stream) */
 int phb_refine_results(const phb_domain *dom, const phb_refine *r, phb_solve_result *out, int *outer_used, phb_stream stream);
 
+/* --- solve without device allocation ------------------------------------------------
+ * No counterpart in phiPICT. CG (as phb_solve_run with kind 0, host-polled, no CUDA graph)
+ * whose workspace lives in a static device array of PHB_NOALLOC_SCRATCH_BYTES inside this
+ * library, for hosts that cannot give the library device memory: programs that carve the
+ * GPU into fixed slices at start-up and allow no later allocation, or plugin hosts whose
+ * allocator is not reachable through a C ABI. It calls no allocator. The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with that device
+ * current, so make that first call before any stream capture. Sizes whose workspace
+ * (phb_cg_noalloc_bytes) exceeds the array are rejected with PHB_ERR_RANGE. All calls share
+ * the one array: calls that overlap on the GPU (two streams, two host threads) race.
+ * out (optional): per-system results, read back with synchronous copies. */
+#define PHB_NOALLOC_SCRATCH_BYTES (32u << 20)
+int64_t phb_cg_noalloc_bytes(const phb_domain *dom, int dtype, int nrhs);
+int phb_cg_solve_noalloc(const phb_domain *dom, int dtype, int nrhs, const void *A, const void *b, void *x,
+                         const phb_tolerance *tol, int maxit, int return_best, phb_solve_result *out, phb_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,6 +16,7 @@ LIB_PATH = _PKG / "libphipict_b200.so"
 
 PHB_F32, PHB_F64 = 0, 1
 BREC, FREC, IREC, TILE = 48, 16, 8, 1024  # TILE: cells per tile (PHB_TILE_CELLS)
+NOALLOC_SCRATCH_BYTES = 32 << 20  # PHB_NOALLOC_SCRATCH_BYTES
 
 # every exported symbol of include/phipict_b200.h
 EXPORTS = (
@@ -28,6 +29,7 @@ EXPORTS = (
     "phb_csr_row_sizes", "phb_csr_pattern", "phb_csr_gather",
     "phb_solve_work_bytes", "phb_solve_state_bytes", "phb_solve_run", "phb_solve_results",
     "phb_release_graphs", "phb_refine_work_bytes", "phb_refine_run", "phb_refine_results",
+    "phb_cg_noalloc_bytes", "phb_cg_solve_noalloc",
 )
 
 
@@ -122,6 +124,7 @@ def load() -> ct.CDLL:
         "phb_release_graphs": [],
         "phb_refine_run": [DP, ct.POINTER(PhbRefine), ct.POINTER(PhbSolveResult), ct.POINTER(ct.c_int), P],
         "phb_refine_results": [DP, ct.POINTER(PhbRefine), ct.POINTER(PhbSolveResult), ct.POINTER(ct.c_int), P],
+        "phb_cg_solve_noalloc": [DP, I, I, P, P, P, ct.POINTER(PhbTolerance), I, I, ct.POINTER(PhbSolveResult), P],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -132,6 +135,7 @@ def load() -> ct.CDLL:
         "phb_solve_work_bytes": [DP, I, I, I],
         "phb_solve_state_bytes": [DP, I],
         "phb_refine_work_bytes": [DP, I, I],
+        "phb_cg_noalloc_bytes": [DP, I, I],
     }.items():
         f = getattr(lib, name)
         f.argtypes = args

@@ -1132,3 +1132,137 @@ extern "C" int phb_refine_results(const phb_domain *dom, const phb_refine *r, ph
 	if (outer_used) *outer_used = mo;
 	return PHB_OK;
 }
+
+// no-allocation CG -------------------------------------------------------------------------
+// Some hosts cannot hand this library device memory for solver workspace: a program that
+// carves the GPU into fixed per-environment slices at start-up and forbids any later
+// allocation, or a plugin host whose device allocator is not reachable through a C ABI.
+// For them the CG solve below keeps its workspace (residual, search directions, partial
+// sums, per-system state) in this file-scope array instead of the caller-provided `work`
+// and `state` buffers of phb_solve_run. Every GPU that loads the library holds the array
+// until the process exits.
+static __device__ __align__(256) unsigned char gNoAllocScratch[PHB_NOALLOC_SCRATCH_BYTES];
+
+// Device address of the array on each device. In host code `gNoAllocScratch` names a
+// host-side stand-in, not device memory, so the address is looked up once per device, with
+// that device current, by the first call on it.
+static std::mutex gNoAllocMutex;
+static void *gNoAllocPtr[64] = {nullptr};
+
+static int noAllocScratch(void **out) {
+	int dev;
+	PHB_CUDA(cudaGetDevice(&dev));
+	if (dev < 0 || dev >= 64) return setError(PHB_ERR_RANGE, "phb_cg_solve_noalloc: device index out of range");
+	std::lock_guard<std::mutex> lock(gNoAllocMutex);
+	if (!gNoAllocPtr[dev]) {
+		void *p = nullptr;
+		PHB_CUDA(cudaGetSymbolAddress(&p, gNoAllocScratch));
+		gNoAllocPtr[dev] = p;
+	}
+	*out = gNoAllocPtr[dev];
+	return PHB_OK;
+}
+
+template <typename T, int D, int K>
+static int runCgNoAlloc(const phb_domain *dom, const phb_solve *sv, phb_solve_result *out, cudaStream_t s) {
+	Dom<double, D> dm(*dom);
+	const Layout L = solveLayout(dom, 0, sizeof(T), K);
+	const StateLayout SL = stateLayout(dom, K);
+	char *w = (char *)sv->work;
+	char *sb = (char *)sv->state;
+	Control *ctrl = (Control *)(sb + SL.ctrl);
+	SysState *st = (SysState *)(sb + SL.st);
+	double *partial = (double *)(w + L.off[10]);
+	const T *A = (const T *)sv->A;
+	const T *b = (const T *)sv->b;
+	T *x = (T *)sv->x;
+	T *r = (T *)(w + L.off[0]), *q = (T *)(w + L.off[1]), *p0 = (T *)(w + L.off[2]), *p1 = (T *)(w + L.off[3]);
+	T *xbest = sv->return_best ? (T *)(w + L.off[4]) : nullptr;
+	const int nsys = dom->ninst * K;
+	const int tiles = dom->ntiles;
+	const int maxit = std::max(1, sv->maxit);
+	const int maxLoops = maxit / 2 + 2;
+	// kInit resets the state and the ticket counter the reductions count with, so nothing
+	// left in the array by an earlier call is read before it is written
+	kInit<<<1, 256, 0, s>>>(st, nsys, sv->tol, 0, maxit, ctrl, maxLoops);
+	kResidual<T, D, K, false, false><<<tiles, PHB_TILE, 0, s>>>(dm, A, b, x, r, nullptr, st, partial, ctrl, sv->tol, LoopCond{0, 0});
+	PHB_CUDA(cudaGetLastError());
+	const int chk = std::max(1, sv->check_every);
+	for (int loops = 0; loops < maxLoops; loops += chk) {
+		for (int i = 0; i < chk; ++i) {
+			for (int half = 0; half < 2; ++half) {
+				T *pIn = half == 0 ? p0 : p1, *pOut = half == 0 ? p1 : p0;
+				kCgDirection<T, D, K><<<tiles, PHB_TILE, 0, s>>>(dm, A, r, pIn, pOut, q, st, partial, ctrl);
+				kCgUpdate<T, D, K><<<tiles, PHB_TILE, 0, s>>>(dm, r, pOut, q, x, xbest, st, partial, ctrl, sv->return_best, LoopCond{0, 0});
+			}
+		}
+		PHB_CUDA(cudaGetLastError());
+		int done = 0; // pageable stack copy: synchronous, no staging buffer of ours
+		PHB_CUDA(cudaMemcpyAsync(&done, &ctrl->allDone, sizeof(int), cudaMemcpyDeviceToHost, s));
+		PHB_CUDA(cudaStreamSynchronize(s));
+		if (done) break;
+	}
+	if (xbest) kRestoreBest<T, K><<<gridFor(dom->ncells * K), 256, 0, s>>>(dom->insts, dom->ninst, dom->ncells, x, xbest, st);
+	PHB_CUDA(cudaGetLastError());
+	if (out) {
+		for (int i = 0; i < nsys; ++i) {
+			SysState h;
+			PHB_CUDA(cudaMemcpyAsync(&h, st + i, sizeof(SysState), cudaMemcpyDeviceToHost, s));
+			PHB_CUDA(cudaStreamSynchronize(s));
+			phb_solve_result &o = out[i];
+			o.final_residual = h.crit;
+			o.used_iterations = h.usedIt;
+			o.converged = h.done == CONVERGED;
+			o.finite = std::isfinite(h.crit);
+			o.status = h.done;
+			o.inner_iterations = 0;
+			o.pad = 0;
+			if (sv->return_best && (h.done == MAXIT || h.done == RISING) && h.bestIt >= 0 && h.best < h.crit) {
+				o.used_iterations = h.bestIt;
+				o.final_residual = h.best;
+			}
+		}
+	}
+	return PHB_OK;
+}
+
+extern "C" int64_t phb_cg_noalloc_bytes(const phb_domain *dom, int dtype, int nrhs) {
+	if (!dom) return -1;
+	const int vb = dtype == PHB_F64 ? 8 : 4;
+	return (int64_t)(solveLayout(dom, 0, vb, nrhs).total + stateLayout(dom, nrhs).total);
+}
+
+extern "C" int phb_cg_solve_noalloc(const phb_domain *dom, int dtype, int nrhs, const void *A, const void *b, void *x,
+		const phb_tolerance *tol, int maxit, int return_best, phb_solve_result *out, phb_stream stream) {
+	if (!dom || !A || !b || !x || !tol || (tol->mode == 2 && !tol->values))
+		return setError(PHB_ERR_ARG, "phb_cg_solve_noalloc: null argument");
+	if (dtype != PHB_F32 && dtype != PHB_F64) return setError(PHB_ERR_ARG, "phb_cg_solve_noalloc: dtype");
+	const int64_t need = phb_cg_noalloc_bytes(dom, dtype, nrhs);
+	if (need > (int64_t)PHB_NOALLOC_SCRATCH_BYTES) {
+		char msg[256];
+		snprintf(msg, sizeof(msg), "phb_cg_solve_noalloc: the solve needs %lld bytes of scratch, more than the %lld of the "
+			"static array (PHB_NOALLOC_SCRATCH_BYTES)", (long long)need, (long long)PHB_NOALLOC_SCRATCH_BYTES);
+		return setError(PHB_ERR_RANGE, msg);
+	}
+	if (dom->ntiles == 0) return PHB_OK;
+	void *scratch = nullptr;
+	int rc = noAllocScratch(&scratch);
+	if (rc) return rc;
+	phb_solve sv = {};
+	sv.kind = 0;
+	sv.vec_dtype = sv.mat_dtype = dtype;
+	sv.nrhs = nrhs;
+	sv.maxit = maxit;
+	sv.return_best = return_best ? 1 : 0;
+	sv.use_graph = 0;
+	sv.check_every = 16;
+	sv.tol = *tol;
+	sv.A = A;
+	sv.b = b;
+	sv.x = x;
+	sv.work = scratch;
+	sv.state = (char *)scratch + solveLayout(dom, 0, dtype == PHB_F64 ? 8 : 4, nrhs).total;
+	cudaStream_t st = (cudaStream_t)stream;
+	PHB_SOLVE_DISPATCH(dom->dims, dtype, nrhs, return runCgNoAlloc<T, D, KK>(dom, &sv, out, st));
+	return PHB_OK;
+}
