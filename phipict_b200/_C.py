@@ -244,6 +244,10 @@ def SetKrylovSettings(enabled: bool = True, checkInterval: int = 8, useGraphs: b
     if not enabled:
         raise NotImplementedError("phipict_b200 has no legacy (cuBLAS/cuSPARSE) solvers")
     SETTINGS["use_graphs"] = bool(useGraphs)
+    if not useGraphs:
+        SETTINGS["mode"] = "host"
+    elif SETTINGS["mode"] == "host":
+        SETTINGS["mode"] = "persistent"
     SETTINGS["check_interval"] = max(1, int(checkInterval))
 
 

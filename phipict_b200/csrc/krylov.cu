@@ -44,7 +44,10 @@ struct Control {
 	int allDone;
 	int loops;
 	int maxLoops;
-	int pad[4];
+	unsigned int barCount; // grid barrier of the persistent solvers: arrivals,
+	unsigned int barGen;   // generation,
+	int barErr;            // set when a barrier wait ran out (the kernel then returns)
+	int pad;
 };
 static_assert(sizeof(Control) == 32, "Control layout");
 
@@ -225,7 +228,10 @@ __global__ void kInit(SysState *st, int nsys, phb_tolerance tol, int fromInner, 
 		z.bestIt = -1;
 		st[s] = z;
 	}
-	if (threadIdx.x == 0) { ctrl->counter = 0; ctrl->allDone = 0; ctrl->loops = 0; ctrl->maxLoops = maxLoops; }
+	if (threadIdx.x == 0) {
+		ctrl->counter = 0; ctrl->allDone = 0; ctrl->loops = 0; ctrl->maxLoops = maxLoops;
+		ctrl->barCount = 0; ctrl->barGen = 0; ctrl->barErr = 0;
+	}
 }
 
 // r = b - A x (and r0 = r for BiCGStab); rho = (r, r); the relative tolerance from (b, b);
@@ -690,6 +696,515 @@ __global__ void kInitOuter(SysState *st, int nsys, phb_tolerance tol, Control *c
 	}
 }
 
+// persistent solvers ---------------------------------------------------------------------
+// One cooperative launch runs a whole solve. The CTAs are co-resident (cooperative launch)
+// and meet at grid barriers instead of kernel boundaries, so an iteration costs a few
+// barrier round trips instead of kernel launches and the vectors stay in L2. Every barrier
+// wait is bounded: when it runs out it sets Control::barErr and every CTA leaves the kernel
+// (the systems then report non-finite). Each CTA keeps its own copy of the per-system
+// scalars in shared memory and reduces the per-tile partials itself, in the same fixed order
+// as every other CTA, so all CTAs take the same decisions without broadcasting them.
+constexpr unsigned int BARRIER_SPIN_LIMIT = 1u << 24;
+
+__device__ __forceinline__ bool gridBarrier(Control *ctrl, unsigned int &gen) {
+	__shared__ int sOk;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		int ok = *(volatile int *)&ctrl->barErr == 0;
+		if (ok) {
+			__threadfence();
+			const unsigned int g = gen;
+			if (atomicAdd(&ctrl->barCount, 1u) == gridDim.x - 1) {
+				atomicExch(&ctrl->barCount, 0u);
+				__threadfence();
+				atomicExch(&ctrl->barGen, g + 1);
+			} else {
+				unsigned int spins = 0;
+				while (*(volatile unsigned int *)&ctrl->barGen == g) {
+					if (++spins > BARRIER_SPIN_LIMIT || *(volatile int *)&ctrl->barErr) { atomicExch(&ctrl->barErr, 1); break; }
+					__nanosleep(32);
+				}
+			}
+			__threadfence();
+			gen = g + 1;
+			ok = *(volatile int *)&ctrl->barErr == 0;
+		}
+		sOk = ok;
+	}
+	__syncthreads();
+	return sOk;
+}
+
+// Block sum of NV values written to dst[0..NV) by the first threads.
+template <int NV>
+__device__ __forceinline__ void blockSumTo(double (&v)[NV], double *dst) {
+	__shared__ double sm[NV][NWARPS];
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+	for (int q = 0; q < NV; ++q) {
+		const double s = warpSum(v[q]);
+		if (lane == 0) sm[q][warp] = s;
+	}
+	__syncthreads();
+	if (threadIdx.x < NV) {
+		double s = 0;
+#pragma unroll
+		for (int w = 0; w < NWARPS; ++w) s += sm[threadIdx.x][w];
+		dst[threadIdx.x] = s;
+	}
+	__syncthreads();
+}
+
+// Visit this CTA's tiles with the block record staged in sB.
+template <int D, typename F>
+__device__ __forceinline__ void forMyTiles(const Dom<double, D> &dom, int32_t *sB, F f) {
+	for (int tile = blockIdx.x; tile < dom.ntiles; tile += gridDim.x) {
+		__syncthreads();
+		const int b = __ldg(dom.tiles + 2 * tile);
+		const int l0 = __ldg(dom.tiles + 2 * tile + 1);
+		if (threadIdx.x < PHB_BREC) sB[threadIdx.x] = __ldg(dom.blocks + b * PHB_BREC + threadIdx.x);
+		__syncthreads();
+		const int nc = sB[B_NX] * sB[B_NY] * (D > 2 ? sB[B_NZ] : 1);
+		f(tile, l0, nc);
+	}
+}
+
+// All CTAs: reduce every running system's partials (the group scheme of finalizeSystems) and
+// update the CTA's state copy; returns the number of systems still running.
+template <int K, int NQ, int INSTQ = -1, typename Fn>
+__device__ __forceinline__ int reduceStates(const int32_t *insts, int ninst, const double *partial, SysState *sst, Fn fn) {
+	constexpr int NV = NQ + 1;
+	__shared__ int running;
+	__shared__ double gsm[NWARPS][NV];
+	if (threadIdx.x == 0) running = 0;
+	__syncthreads();
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const int nsys = ninst * K;
+	int G = NWARPS;
+	while (G > 1 && G * nsys > NWARPS) G >>= 1;
+	const int NG = NWARPS / G;
+	const int group = warp / G, wg = warp - group * G;
+	for (int base = 0; base < nsys; base += NG) {
+		const int s = base + group;
+		const bool act = s < nsys && sst[s].done == RUNNING;
+		double a0[NV], a1[NV];
+#pragma unroll
+		for (int q = 0; q < NV; ++q) { a0[q] = 0; a1[q] = 0; }
+		if (act) {
+			const int inst = s / K, k = s - inst * K;
+			const int t0 = insts[inst * PHB_IREC + I_TILESTART], tc = insts[inst * PHB_IREC + I_TILECOUNT];
+			const int stride = G * 32;
+			auto load = [&](int t, double *a) {
+				const double *pp = partial + (size_t)(t0 + t) * K * NQ;
+#pragma unroll
+				for (int q = 0; q < NQ; ++q) a[q] += __ldcg(pp + k * NQ + q);
+				if (INSTQ >= 0) {
+#pragma unroll
+					for (int kk = 0; kk < K; ++kk) a[NQ] += __ldcg(pp + kk * NQ + (INSTQ < 0 ? 0 : INSTQ));
+				}
+			};
+			int t = wg * 32 + lane;
+			for (; t + stride < tc; t += 2 * stride) { load(t, a0); load(t + stride, a1); }
+			if (t < tc) load(t, a0);
+		}
+#pragma unroll
+		for (int q = 0; q < NV; ++q) {
+			const double v = warpSum(a0[q] + a1[q]);
+			if (lane == 0) gsm[warp][q] = v;
+		}
+		__syncthreads();
+		if (act && wg == 0 && lane == 0) {
+			double red[NV];
+#pragma unroll
+			for (int q = 0; q < NV; ++q) {
+				double v = 0;
+				for (int w = 0; w < G; ++w) v += gsm[group * G + w][q];
+				red[q] = v;
+			}
+			fn(sst[s], s / K, red, red[NQ]);
+		}
+		if (wg == 0 && lane == 0 && s < nsys && sst[s].done == RUNNING) atomicAdd(&running, 1);
+		__syncthreads();
+	}
+	const int r = running;
+	__syncthreads();
+	return r;
+}
+
+// The reference stop rule of the first residual (kResidual) applied to a CTA state copy.
+template <int K, bool BICG, bool STOPSTART>
+__device__ __forceinline__ void residualDecision(const Dom<double, 3> *, SysState &s, double ns, const double *red, double bb,
+		const phb_tolerance &tol) {
+	if (tol.mode == 1) s.tol = resolveTol(tol, sqrt(bb / double(K)) * ns);
+	const double crit = sqrt(red[0]) * ns;
+	s.rho = red[0];
+	s.restart = 1;
+	s.crit = crit;
+	if (!fin(crit)) { s.done = NONFINITE; s.usedIt = 0; }
+	else if ((BICG || STOPSTART) ? crit < s.tol : crit == 0.0) { s.done = CONVERGED; s.usedIt = BICG ? -1 : 0; }
+}
+
+template <typename T, int D, int K, bool STOPSTART>
+__global__ void __launch_bounds__(PHB_TILE) kCgPersistent(Dom<double, D> dom, const T *__restrict__ A, const T *__restrict__ b,
+		T *__restrict__ x, T *__restrict__ r, T *__restrict__ p0, T *__restrict__ p1, T *__restrict__ q, T *__restrict__ xbest,
+		SysState *st, double *partial, Control *ctrl, phb_tolerance tol, int returnBest, int maxit) {
+	extern __shared__ SysState sst[];
+	__shared__ int32_t sB[PHB_BREC];
+	const int nsys = dom.ninst * K;
+	for (int s = threadIdx.x; s < nsys; s += blockDim.x) sst[s] = st[s];
+	__syncthreads();
+	unsigned int gen = 0;
+	const int64_t N = dom.ncells;
+	// r = b - A x, (r, r), (b, b)
+	forMyTiles<D>(dom, sB, [&](int tile, int l0, int nc) {
+		const int inst = sB[B_INST];
+		bool act[K];
+#pragma unroll
+		for (int k = 0; k < K; ++k) act[k] = sst[inst * K + k].done == RUNNING;
+		double acc[2 * K];
+#pragma unroll
+		for (int k = 0; k < 2 * K; ++k) acc[k] = 0;
+		for (int j = 0; j < CPT; ++j) {
+			Cell c;
+			if (!cellAt<D>(sB, l0, nc, j, c)) break;
+			int64_t nb[2 * D];
+			stencilNeighbors<D>(dom, c, nb);
+			T y[K];
+			applyA<T, D, K>(A, N, c, nb, act, [&](int64_t g, int k) { return x[vk<K>(c.B, g, k)]; }, y);
+#pragma unroll
+			for (int k = 0; k < K; ++k) {
+				if (!act[k]) continue;
+				const int64_t o = vk<K>(c.B, c.g, k);
+				const T bi = b[o];
+				const T ri = bi - y[k];
+				r[o] = ri;
+				acc[2 * k] += double(ri) * double(ri);
+				acc[2 * k + 1] += double(bi) * double(bi);
+			}
+		}
+		blockSumTo<2 * K>(acc, partial + (size_t)tile * 2 * K);
+	});
+	if (!gridBarrier(ctrl, gen)) return;
+	int running = reduceStates<K, 2, 1>(dom.insts, dom.ninst, partial, sst, [&](SysState &s, int in, const double *red, double bb) {
+		residualDecision<K, false, STOPSTART>(nullptr, s, normScale(dom.insts, in), red, bb, tol);
+	});
+	T *pIn = p0, *pOut = p1;
+	for (int iter = 0; running > 0 && iter <= maxit + 1; ++iter) {
+		// p' = r + beta p, q = A p', (p', q)
+		forMyTiles<D>(dom, sB, [&](int tile, int l0, int nc) {
+			const int inst = sB[B_INST];
+			bool act[K], rs[K];
+			T beta[K];
+#pragma unroll
+			for (int k = 0; k < K; ++k) {
+				const SysState &s = sst[inst * K + k];
+				act[k] = s.done == RUNNING;
+				rs[k] = s.restart;
+				beta[k] = T(s.beta);
+			}
+			double acc[K];
+#pragma unroll
+			for (int k = 0; k < K; ++k) acc[k] = 0;
+			for (int j = 0; j < CPT; ++j) {
+				Cell c;
+				if (!cellAt<D>(sB, l0, nc, j, c)) break;
+				int64_t nb[2 * D];
+				stencilNeighbors<D>(dom, c, nb);
+				auto pv = [&](int64_t g, int k) {
+					const int64_t o = vk<K>(c.B, g, k);
+					return rs[k] ? r[o] : r[o] + beta[k] * pIn[o];
+				};
+				T y[K];
+				applyA<T, D, K>(A, N, c, nb, act, pv, y);
+#pragma unroll
+				for (int k = 0; k < K; ++k) {
+					if (!act[k]) continue;
+					const int64_t o = vk<K>(c.B, c.g, k);
+					const T pi = pv(c.g, k);
+					pOut[o] = pi;
+					q[o] = y[k];
+					acc[k] += double(pi) * double(y[k]);
+				}
+			}
+			blockSumTo<K>(acc, partial + (size_t)tile * K);
+		});
+		if (!gridBarrier(ctrl, gen)) return;
+		reduceStates<K, 1>(dom.insts, dom.ninst, partial, sst, [&](SysState &s, int, const double *red, double) {
+			const double alpha = s.rho / red[0];
+			s.restart = 0;
+			if (!fin(alpha)) { s.done = NONFINITE; s.usedIt = s.it; }
+			else s.alpha = alpha;
+		});
+		// x += alpha p', r -= alpha q, (r, r)
+		forMyTiles<D>(dom, sB, [&](int tile, int l0, int nc) {
+			const int inst = sB[B_INST];
+			double acc[K];
+#pragma unroll
+			for (int k = 0; k < K; ++k) acc[k] = 0;
+			for (int j = 0; j < CPT; ++j) {
+				Cell c;
+				if (!cellAt<D>(sB, l0, nc, j, c)) break;
+#pragma unroll
+				for (int k = 0; k < K; ++k) {
+					const SysState &s = sst[inst * K + k];
+					if (s.done != RUNNING) continue;
+					const T alpha = T(s.alpha);
+					const int64_t o = vk<K>(c.B, c.g, k);
+					const T xi = x[o];
+					if (s.saveBest && xbest) xbest[o] = xi;
+					x[o] = xi + alpha * pOut[o];
+					const T ri = r[o] - alpha * q[o];
+					r[o] = ri;
+					acc[k] += double(ri) * double(ri);
+				}
+			}
+			blockSumTo<K>(acc, partial + (size_t)tile * K);
+		});
+		if (!gridBarrier(ctrl, gen)) return;
+		running = reduceStates<K, 1>(dom.insts, dom.ninst, partial, sst, [&](SysState &s, int in, const double *red, double) {
+			const double crit = sqrt(red[0]) * normScale(dom.insts, in);
+			++s.it;
+			s.crit = crit;
+			s.saveBest = 0;
+			s.usedIt = s.it - 1;
+			if (!fin(crit)) { s.done = NONFINITE; return; }
+			if (returnBest) {
+				if (crit < s.best) { s.best = crit; s.bestIt = s.it - 1; s.saveBest = 1; }
+				if (s.it > 1 && crit >= s.last) ++s.rising; else s.rising = 0;
+				s.last = crit;
+			}
+			if (crit < s.tol) s.done = CONVERGED;
+			else if (s.it >= s.maxit) s.done = MAXIT;
+			else if (returnBest && s.rising >= RISING_CUTOFF) s.done = RISING;
+			else {
+				s.beta = red[0] / s.rho;
+				s.rho = red[0];
+				if (!fin(s.beta)) s.done = NONFINITE;
+			}
+		});
+		T *tmp = pIn; pIn = pOut; pOut = tmp;
+	}
+	// systems that stopped without converging return their best iterate (kRestoreBest)
+	if (xbest) {
+		forMyTiles<D>(dom, sB, [&](int, int l0, int nc) {
+			const int inst = sB[B_INST];
+			for (int j = 0; j < CPT; ++j) {
+				Cell c;
+				if (!cellAt<D>(sB, l0, nc, j, c)) break;
+#pragma unroll
+				for (int k = 0; k < K; ++k) {
+					const SysState &s = sst[inst * K + k];
+					if ((s.done == MAXIT || s.done == RISING) && s.bestIt >= 0 && s.best < s.crit) {
+						const int64_t o = vk<K>(c.B, c.g, k);
+						x[o] = xbest[o];
+					}
+				}
+			}
+		});
+	}
+	if (blockIdx.x == 0) {
+		__syncthreads();
+		for (int s = threadIdx.x; s < nsys; s += blockDim.x) st[s] = sst[s];
+	}
+}
+
+template <typename T, int D, int K>
+__global__ void __launch_bounds__(PHB_TILE) kBicgPersistent(Dom<double, D> dom, const T *__restrict__ A, const T *__restrict__ b,
+		T *__restrict__ x, T *__restrict__ r, T *__restrict__ r0, T *__restrict__ p0, T *__restrict__ p1, T *__restrict__ v0,
+		T *__restrict__ v1, T *__restrict__ t, SysState *st, double *partial, Control *ctrl, phb_tolerance tol, int maxit) {
+	extern __shared__ SysState sst[];
+	__shared__ int32_t sB[PHB_BREC];
+	const int nsys = dom.ninst * K;
+	for (int s = threadIdx.x; s < nsys; s += blockDim.x) sst[s] = st[s];
+	__syncthreads();
+	unsigned int gen = 0;
+	const int64_t N = dom.ncells;
+	forMyTiles<D>(dom, sB, [&](int tile, int l0, int nc) {
+		const int inst = sB[B_INST];
+		bool act[K];
+#pragma unroll
+		for (int k = 0; k < K; ++k) act[k] = sst[inst * K + k].done == RUNNING;
+		double acc[2 * K];
+#pragma unroll
+		for (int k = 0; k < 2 * K; ++k) acc[k] = 0;
+		for (int j = 0; j < CPT; ++j) {
+			Cell c;
+			if (!cellAt<D>(sB, l0, nc, j, c)) break;
+			int64_t nb[2 * D];
+			stencilNeighbors<D>(dom, c, nb);
+			T y[K];
+			applyA<T, D, K>(A, N, c, nb, act, [&](int64_t g, int k) { return x[vk<K>(c.B, g, k)]; }, y);
+#pragma unroll
+			for (int k = 0; k < K; ++k) {
+				if (!act[k]) continue;
+				const int64_t o = vk<K>(c.B, c.g, k);
+				const T bi = b[o];
+				const T ri = bi - y[k];
+				r[o] = ri;
+				r0[o] = ri;
+				acc[2 * k] += double(ri) * double(ri);
+				acc[2 * k + 1] += double(bi) * double(bi);
+			}
+		}
+		blockSumTo<2 * K>(acc, partial + (size_t)tile * 2 * K);
+	});
+	if (!gridBarrier(ctrl, gen)) return;
+	int running = reduceStates<K, 2, 1>(dom.insts, dom.ninst, partial, sst, [&](SysState &s, int in, const double *red, double bb) {
+		residualDecision<K, true, true>(nullptr, s, normScale(dom.insts, in), red, bb, tol);
+	});
+	T *pIn = p0, *pOut = p1, *vIn = v0, *vOut = v1;
+	for (int iter = 0; running > 0 && iter <= maxit + 1; ++iter) {
+		// p = r + beta (p - omega v), v = A p, (r0, v)
+		forMyTiles<D>(dom, sB, [&](int tile, int l0, int nc) {
+			const int inst = sB[B_INST];
+			bool act[K], rs[K];
+			T beta[K], omega[K];
+#pragma unroll
+			for (int k = 0; k < K; ++k) {
+				const SysState &s = sst[inst * K + k];
+				act[k] = s.done == RUNNING;
+				rs[k] = s.restart;
+				beta[k] = T(s.beta);
+				omega[k] = T(s.omega);
+			}
+			double acc[K];
+#pragma unroll
+			for (int k = 0; k < K; ++k) acc[k] = 0;
+			for (int j = 0; j < CPT; ++j) {
+				Cell c;
+				if (!cellAt<D>(sB, l0, nc, j, c)) break;
+				int64_t nb[2 * D];
+				stencilNeighbors<D>(dom, c, nb);
+				auto pv = [&](int64_t g, int k) {
+					const int64_t o = vk<K>(c.B, g, k);
+					return rs[k] ? r[o] : r[o] + beta[k] * (pIn[o] - omega[k] * vIn[o]);
+				};
+				T y[K];
+				applyA<T, D, K>(A, N, c, nb, act, pv, y);
+#pragma unroll
+				for (int k = 0; k < K; ++k) {
+					if (!act[k]) continue;
+					const int64_t o = vk<K>(c.B, c.g, k);
+					pOut[o] = pv(c.g, k);
+					vOut[o] = y[k];
+					acc[k] += double(r0[o]) * double(y[k]);
+				}
+			}
+			blockSumTo<K>(acc, partial + (size_t)tile * K);
+		});
+		if (!gridBarrier(ctrl, gen)) return;
+		reduceStates<K, 1>(dom.insts, dom.ninst, partial, sst, [&](SysState &s, int, const double *red, double) {
+			const double alpha = s.rho / red[0];
+			s.restart = 0;
+			if (!fin(alpha)) { s.done = NONFINITE; s.usedIt = s.it; }
+			else s.alpha = alpha;
+		});
+		// s = r - alpha v, t = A s, (t,s), (t,t), (s,s)
+		forMyTiles<D>(dom, sB, [&](int tile, int l0, int nc) {
+			const int inst = sB[B_INST];
+			bool act[K];
+			T alpha[K];
+#pragma unroll
+			for (int k = 0; k < K; ++k) {
+				const SysState &s = sst[inst * K + k];
+				act[k] = s.done == RUNNING;
+				alpha[k] = T(s.alpha);
+			}
+			double acc[3 * K];
+#pragma unroll
+			for (int k = 0; k < 3 * K; ++k) acc[k] = 0;
+			for (int j = 0; j < CPT; ++j) {
+				Cell c;
+				if (!cellAt<D>(sB, l0, nc, j, c)) break;
+				int64_t nb[2 * D];
+				stencilNeighbors<D>(dom, c, nb);
+				auto sv = [&](int64_t g, int k) {
+					const int64_t o = vk<K>(c.B, g, k);
+					return r[o] - alpha[k] * vOut[o];
+				};
+				T y[K];
+				applyA<T, D, K>(A, N, c, nb, act, sv, y);
+#pragma unroll
+				for (int k = 0; k < K; ++k) {
+					if (!act[k]) continue;
+					const int64_t o = vk<K>(c.B, c.g, k);
+					const T si = sv(c.g, k);
+					t[o] = y[k];
+					acc[3 * k + 0] += double(y[k]) * double(si);
+					acc[3 * k + 1] += double(y[k]) * double(y[k]);
+					acc[3 * k + 2] += double(si) * double(si);
+				}
+			}
+			blockSumTo<3 * K>(acc, partial + (size_t)tile * 3 * K);
+		});
+		if (!gridBarrier(ctrl, gen)) return;
+		reduceStates<K, 3>(dom.insts, dom.ninst, partial, sst, [&](SysState &s, int in, const double *red, double) {
+			const double critS = sqrt(red[2]) * normScale(dom.insts, in);
+			s.halfCrit = critS;
+			if (!fin(critS)) { s.done = NONFINITE; s.crit = critS; s.usedIt = s.it; }
+			else if (critS < s.tol) { s.halfDone = 1; s.omega = 0.0; }
+			else {
+				const double omega = red[0] / red[1];
+				if (!fin(omega)) { s.done = NONFINITE; s.crit = critS; s.usedIt = s.it; }
+				else s.omega = omega;
+			}
+		});
+		// x += alpha p + omega s, r = s - omega t, (r0, r), (r, r)
+		forMyTiles<D>(dom, sB, [&](int tile, int l0, int nc) {
+			const int inst = sB[B_INST];
+			double acc[2 * K];
+#pragma unroll
+			for (int k = 0; k < 2 * K; ++k) acc[k] = 0;
+			for (int j = 0; j < CPT; ++j) {
+				Cell c;
+				if (!cellAt<D>(sB, l0, nc, j, c)) break;
+#pragma unroll
+				for (int k = 0; k < K; ++k) {
+					const SysState &s = sst[inst * K + k];
+					if (s.done != RUNNING) continue;
+					const T alpha = T(s.alpha), omega = T(s.omega);
+					const int64_t o = vk<K>(c.B, c.g, k);
+					const T si = r[o] - alpha * vOut[o];
+					if (s.halfDone) {
+						x[o] += alpha * pOut[o];
+						r[o] = si;
+					} else {
+						x[o] += alpha * pOut[o] + omega * si;
+						const T ri = si - omega * t[o];
+						r[o] = ri;
+						acc[2 * k + 0] += double(r0[o]) * double(ri);
+						acc[2 * k + 1] += double(ri) * double(ri);
+					}
+				}
+			}
+			blockSumTo<2 * K>(acc, partial + (size_t)tile * 2 * K);
+		});
+		if (!gridBarrier(ctrl, gen)) return;
+		running = reduceStates<K, 2>(dom.insts, dom.ninst, partial, sst, [&](SysState &s, int in, const double *red, double) {
+			if (s.halfDone) { s.done = CONVERGED; s.crit = s.halfCrit; s.usedIt = s.it; return; }
+			const double crit = sqrt(red[1]) * normScale(dom.insts, in);
+			s.crit = crit;
+			if (!fin(crit)) { s.done = NONFINITE; s.usedIt = s.it; }
+			else if (crit < s.tol) { s.done = CONVERGED; s.usedIt = s.it + 1; }
+			else {
+				++s.it;
+				s.usedIt = s.it - 1;
+				const double beta = (red[0] / s.rho) * (s.alpha / s.omega);
+				s.rho = red[0];
+				s.beta = beta;
+				if (!fin(beta)) s.done = NONFINITE;
+				else if (s.it >= s.maxit) s.done = MAXIT;
+			}
+		});
+		T *tmp = pIn; pIn = pOut; pOut = tmp;
+		tmp = vIn; vIn = vOut; vOut = tmp;
+	}
+	if (blockIdx.x == 0) {
+		__syncthreads();
+		for (int s = threadIdx.x; s < nsys; s += blockDim.x) st[s] = sst[s];
+	}
+}
+
 // host side --------------------------------------------------------------------------------
 static size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
@@ -831,9 +1346,80 @@ static std::string makeKey(const char *tag, const A &a, const B &b) {
 
 static int gridFor(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 148 * 16); }
 
+static int numSMs() {
+	static int cache[64] = {0};
+	int dev = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+	if (!cache[dev]) {
+		int v = 0;
+		if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+		cache[dev] = v;
+	}
+	return cache[dev];
+}
+
+// A persistent solve: kInit, then one cooperative launch of the whole iteration (the grid is
+// sized so that every CTA is resident; the launch fails rather than deadlocks otherwise).
+template <typename T, int D, int K>
+static int launchPersistent(const phb_domain *dom, const phb_solve *sv, cudaStream_t s, bool stopStart, int fromInner) {
+	Dom<double, D> dm(*dom);
+	const Layout L = solveLayout(dom, sv->kind, sizeof(T), K);
+	const StateLayout SL = stateLayout(dom, K);
+	char *w = (char *)sv->work;
+	char *sb = (char *)sv->state;
+	Control *ctrl = (Control *)(sb + SL.ctrl);
+	SysState *st = (SysState *)(sb + SL.st);
+	double *partial = (double *)(w + L.off[10]);
+	const T *A = (const T *)sv->A;
+	const T *b = (const T *)sv->b;
+	T *x = (T *)sv->x;
+	const int nsys = dom->ninst * K;
+	const size_t smem = (size_t)nsys * sizeof(SysState);
+	if (smem > 160 * 1024) return setError(PHB_ERR_RANGE, "persistent solve: too many systems for the per-CTA state copy");
+	const int maxit = std::max(1, sv->maxit);
+	kInit<<<1, 256, 0, s>>>(st, nsys, sv->tol, fromInner, maxit, ctrl, maxit / 2 + 2);
+	PHB_CUDA(cudaGetLastError());
+	cudaLaunchConfig_t cfg = {};
+	cudaLaunchAttribute attr[1];
+	attr[0].id = cudaLaunchAttributeCooperative;
+	attr[0].val.cooperative = 1;
+	cfg.blockDim = dim3(PHB_TILE);
+	cfg.dynamicSmemBytes = smem;
+	cfg.stream = s;
+	cfg.attrs = attr;
+	cfg.numAttrs = 1;
+	auto grid = [&](const void *kern) -> int {
+		if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+		int perSM = 0;
+		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, PHB_TILE, smem) != cudaSuccess || perSM < 1) perSM = 1;
+		return std::max(1, std::min(dom->ntiles, perSM * numSMs()));
+	};
+	if (sv->kind == 0) {
+		T *r = (T *)(w + L.off[0]), *q = (T *)(w + L.off[1]), *p0 = (T *)(w + L.off[2]), *p1 = (T *)(w + L.off[3]);
+		T *xbest = sv->return_best ? (T *)(w + L.off[4]) : nullptr;
+		if (stopStart) {
+			auto kern = kCgPersistent<T, D, K, true>;
+			cfg.gridDim = dim3(grid((const void *)kern));
+			PHB_CUDA(cudaLaunchKernelEx(&cfg, kern, dm, A, b, x, r, p0, p1, q, xbest, st, partial, ctrl, sv->tol, sv->return_best, maxit));
+		} else {
+			auto kern = kCgPersistent<T, D, K, false>;
+			cfg.gridDim = dim3(grid((const void *)kern));
+			PHB_CUDA(cudaLaunchKernelEx(&cfg, kern, dm, A, b, x, r, p0, p1, q, xbest, st, partial, ctrl, sv->tol, sv->return_best, maxit));
+		}
+		return PHB_OK;
+	}
+	T *r = (T *)(w + L.off[0]), *r0 = (T *)(w + L.off[1]), *p0 = (T *)(w + L.off[2]), *p1 = (T *)(w + L.off[3]);
+	T *v0 = (T *)(w + L.off[4]), *v1 = (T *)(w + L.off[5]), *t = (T *)(w + L.off[6]);
+	auto kern = kBicgPersistent<T, D, K>;
+	cfg.gridDim = dim3(grid((const void *)kern));
+	PHB_CUDA(cudaLaunchKernelEx(&cfg, kern, dm, A, b, x, r, r0, p0, p1, v0, v1, t, st, partial, ctrl, sv->tol, maxit));
+	return PHB_OK;
+}
+
 // the Krylov loop for one solve, recorded on `s`
 template <typename T, int D, int K>
 static int emitSolve(const phb_domain *dom, const phb_solve *sv, cudaStream_t s, Streams &ss, int useGraph, bool stopStart, int fromInner = 0) {
+	if (sv->use_graph == 2) return launchPersistent<T, D, K>(dom, sv, s, stopStart, fromInner);
 	Dom<double, D> dm(*dom);
 	const Layout L = solveLayout(dom, sv->kind, sizeof(T), K);
 	const StateLayout SL = stateLayout(dom, K);
@@ -966,7 +1552,7 @@ extern "C" int phb_solve_run(const phb_domain *dom, const phb_solve *s, phb_stre
 	cudaStream_t st = (cudaStream_t)stream;
 	const std::string key = makeKey("solve", *dom, *s);
 	PHB_SOLVE_DISPATCH(dom->dims, s->vec_dtype, s->nrhs, {
-		if (!s->use_graph) {
+		if (s->use_graph != 1) {
 			Streams *ss; int rc = getStreams(ss); if (rc) return rc;
 			return emitSolve<T, D, KK>(dom, s, st, *ss, 0, false);
 		}
@@ -1042,7 +1628,7 @@ static int emitRefine(const phb_domain *dom, const phb_refine *rf, cudaStream_t 
 	in.work = rf->work;
 	in.state = rf->state;
 	const bool graph = rf->use_graph != 0;
-	in.use_graph = graph ? 1 : 0;
+	in.use_graph = rf->use_graph == 2 ? 2 : (graph ? 1 : 0);
 	in.check_every = 8;
 	cudaGraphConditionalHandle outerHandle{};
 	if (graph) {

@@ -24,7 +24,26 @@ STATUS = {0: "running", 1: "converged", 2: "non-finite", 3: "max iterations", 4:
 # Global solver settings (phiPICT's SetKrylovSettings, bindings.cpp:739-751): with graphs
 # every solve is one CUDA-graph launch; without, every kernel is launched on its own and the
 # host polls for completion every `check_interval` iterations (what a profiler needs).
-SETTINGS = {"use_graphs": os.environ.get("PHIPICT_B200_GRAPHS", "1") != "0", "check_interval": 8}
+# Solver launch modes: "persistent" (default) runs each Krylov solve as one cooperative
+# kernel with grid barriers; "graph" as a conditional-WHILE CUDA graph of per-phase kernels;
+# "host" launches every kernel on its own and polls (what a kernel profiler needs).
+MODES = {"host": 0, "graph": 1, "persistent": 2}
+SETTINGS = {
+    "use_graphs": os.environ.get("PHIPICT_B200_GRAPHS", "1") != "0",
+    "mode": os.environ.get("PHIPICT_B200_SOLVER_MODE", "persistent"),
+    "check_interval": 8,
+}
+if not SETTINGS["use_graphs"]:
+    SETTINGS["mode"] = "host"
+
+
+def mode_code(use_graph=None) -> int:
+    """phb_solve::use_graph for an explicit request (bool or mode code) or the settings."""
+    if use_graph is None:
+        return MODES[SETTINGS["mode"]]
+    if isinstance(use_graph, bool):
+        return 1 if use_graph else 0
+    return int(use_graph)
 
 
 @dataclass
@@ -85,7 +104,7 @@ class StencilSolver:
         s.nrhs = self.nrhs
         s.maxit = int(maxit)
         s.return_best = int(bool(return_best)) if self.kind == CG else 0
-        s.use_graph = int(bool(SETTINGS["use_graphs"] if use_graph is None else use_graph))
+        s.use_graph = mode_code(use_graph)
         s.check_every = int(SETTINGS["check_interval"])
         nsys = d.getBatchSize() * self.nrhs
         s.tol, self._keep = to_device_tolerance(tol, d.getDtype(), nsys, d.getDevice())
@@ -131,7 +150,7 @@ class RefinedSolver:
         r.max_outer = self.max_outer
         r.inner_maxit = int(maxit)
         r.inner_rtol = self.inner_rtol
-        r.use_graph = int(bool(SETTINGS["use_graphs"]))
+        r.use_graph = mode_code()
         nsys = d.getBatchSize() * self.nrhs
         r.tol, self._keep = to_device_tolerance(tol, torch.float64, nsys, d.getDevice())
         r.A64, r.A32, r.b, r.x = A64.data_ptr(), A32.data_ptr(), b.data_ptr(), x.data_ptr()

@@ -30,7 +30,7 @@ def rel(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
 
 
-@pytest.mark.parametrize("use_graph", [True, False])
+@pytest.mark.parametrize("use_graph", [0, 1, 2])
 @pytest.mark.parametrize("case", ["hartmann2d", "duct3d"])
 def test_pressure_cg_matches_direct_solve(cuda, case, use_graph):
     dom = hartmann_2d(14, 10) if case == "hartmann2d" else duct_3d(6, 5, 4, 2)
@@ -215,3 +215,33 @@ def test_mixed_precision_matches_fp64(cuda):
         results.append((host(dom._u_block).copy(), host(dom.pressureResult).copy()))
     assert rel(results[1][0], results[0][0]) < 1e-8
     assert rel(results[1][1], results[0][1]) < 1e-6
+
+
+@pytest.mark.parametrize("kind,nrhs", [(CG, 1), (BICGSTAB, 3)])
+def test_persistent_solver_matches_graph_solver(cuda, kind, nrhs):
+    """The persistent cooperative solve and the graph of per-phase kernels use the same
+    per-tile arithmetic and reduction order: identical iterations and solutions."""
+    dom = duct_3d(8, 6, 5, 2)
+    seeded_state(dom, 13, scale=0.2)
+    dom.PrepareSolve()
+    ts = torch.tensor([0.01], dtype=torch.float64)
+    _C.SetupAdvectionMatrix(dom, ts, 0)
+    _C.SetupAdvectionVelocity(dom, ts, 0, False)
+    _C.SetupPressureMatrix(dom, ts)
+    if kind == CG:
+        A, b = dom._P_st, dom.pressureRHSdiv.clone()
+        g = torch.Generator().manual_seed(3)
+        b.copy_(torch.randn(b.numel(), generator=g, dtype=torch.float64))
+        b -= b.mean()
+    else:
+        A, b = dom._C_st, dom.velocityRHS.clone()
+    out = []
+    for mode in (1, 2):
+        s = solver_for(dom, kind, torch.float64, nrhs, tag=f"mode{mode}")
+        x = torch.zeros_like(b)
+        s.solve(A, b, x, 1e-12, 5000, use_graph=mode)
+        out.append((x, s.results()))
+    (x1, i1), (x2, i2) = out
+    assert [i.usedIterations for i in i1] == [i.usedIterations for i in i2]
+    assert all(i.converged for i in i2)
+    assert torch.equal(x1, x2)
