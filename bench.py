@@ -87,6 +87,21 @@ def algorithmic_cg_bytes(dims: int, s_A: int, s_v: int) -> int:
     return (2 * dims + 1) * s_A + 10 * s_v
 
 
+def algorithmic_pcg_bytes(dims: int, levels: list[int]) -> float:
+    """Bytes per fine cell of one multigrid-preconditioned float32 CG iteration: the CG
+    passes (algorithmic_cg_bytes with z in place of r in the direction) plus, per level l of
+    n_l cells, the restriction (stencil + b read, coarse b written) and the prolongation
+    with its smoothing sweep (stencil, b and the coarse correction read, z written)."""
+    st = (2 * dims + 1) * 4
+    cyc = 0.0
+    for l in range(len(levels) - 1):
+        frac = levels[l] / levels[0]
+        coarse = levels[l + 1] / levels[0]
+        cyc += frac * (st + 4) + coarse * 4          # restriction
+        cyc += frac * (st + 4 + 4) + coarse * 4      # prolongation + post-smoothing
+    return algorithmic_cg_bytes(dims, 4, 4) + cyc
+
+
 class ClockSampler:
     """nvidia-smi clock/throttle samples during the timed region."""
 
@@ -168,7 +183,7 @@ def barrier(world: int):
         dist.barrier()
 
 
-def build_sim(wl: dict, device, mixed: bool):
+def build_sim(wl: dict, device, mixed: bool, amg: bool = True):
     import phipict_b200 as pb
 
     dtype = torch.float64
@@ -187,7 +202,8 @@ def build_sim(wl: dict, device, mixed: bool):
     hooks = pb.Hooks().append(pb.Hook.PRE_VELOCITY_SETUP, reset_source)
     sim = pb.MHDSimulation(dom, wl["dt"], torch.tensor(N), torch.tensor([0.0, 1.0, 0.0], dtype=dtype),
                            non_orthogonal=False, advection_tol=tol, pressure_tol=tol, potential_tol=tol,
-                           mixed_precision=mixed, hooks=hooks)
+                           mixed_precision=mixed, hooks=hooks, pressure_use_amg=amg and mixed,
+                           potential_use_preconditioner=amg and mixed)
     return dom, sim
 
 
@@ -195,7 +211,8 @@ def run_ours(args, rank, world, local):
     wl = WORKLOADS[args.workload]
     device = torch.device("cuda", local)
     mixed = not args.plain_fp64
-    dom, sim = build_sim(wl, device, mixed)
+    amg = mixed and not args.no_amg
+    dom, sim = build_sim(wl, device, mixed, amg)
     cells = dom.getTotalSize()
     stream = torch.cuda.current_stream(device)
     for _ in range(args.warmup):
@@ -257,28 +274,39 @@ def run_ours(args, rank, world, local):
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), world) / e_steps
     total_cells = cells * world
     value = total_cells * args.steps / (ms / 1e3) / 1e6
-    # roofline of the dominant kernel pair: the float32 (or float64) CG iteration
+    # roofline of the dominant kernel: the (preconditioned) Krylov iteration, float32 when
+    # mixed; solve time / inner iterations (the momentum BiCGStab iterations are counted as
+    # CG-sized, a slight overestimate of their bytes)
     s = 4 if mixed else 8
-    per_cell = algorithmic_cg_bytes(d, s, s)
+    levels = sim._amg_cache["P"].sizes if amg and "P" in sim._amg_cache else None
+    per_cell = algorithmic_pcg_bytes(d, levels) if levels else algorithmic_cg_bytes(d, s, s)
     it_time_ms = solve_ms / max(1, inner_its)
     achieved = per_cell * cells / (it_time_ms / 1e3) / 1e9 if inner_its else None
     pk = peaks()
-    launches_per_step = 26  # assembly, mean projections and copies per PISO+MHD step
-    gpu_launches = args.steps * launches_per_step + 2 * inner_its + 6 * max(1, sweeps) + 3 * len(infos)
+    # launches: assembly, mean projections and copies per PISO+MHD step; per solve kInit(Outer)
+    # and per refinement sweep kRefineResidual, kInit, the persistent solve and kRefineUpdate;
+    # per step the pressure hierarchy's setup (Galerkin per level, dense, inverse)
+    launches_per_step = 26
+    setup = (len(levels) + 1) if levels else 0
+    gpu_launches = args.steps * (launches_per_step + setup) + 4 * max(1, sweeps) + len(infos)
     return dict(
         metric="Mcell-steps/s", value=round(value, 4), unit="Mcell-steps/s", n_gpus=world, steps=args.steps,
         warmup=args.warmup, ms_per_step=round(ms / args.steps, 4), higher_is_better=True, scaling="weak",
         vs_baseline=None, dtype="f64 fields, f32 Krylov + f64 refinement" if mixed else "f64",
         data="synthetic (seeded inflow noise 1e-2, seeded initial state)",
         config={"workload": f"{args.workload}: 3 blocks 64x48x48 (442,368 cells), Ha=100, Re=1000, dt=0.01, "
-                            f"rtol 1e-10, {'mixed precision' if mixed else 'plain fp64'}",
+                            f"rtol 1e-10, {'mixed precision' if mixed else 'plain fp64'}"
+                            f"{', multigrid-preconditioned pressure and potential CG' if amg else ''}",
+                "amg_levels": levels,
                 "cells_per_gpu": cells, "l2": "working set ~60 MB f32 fits L2; HBM claims on the roofline sweep",
                 "parallelism": f"replicas x{world}"},
         clocks=clk,
         e2e={"value": round(total_cells / (e2e_ms / 1e3) / 1e6, 4), "unit": "Mcell-steps/s",
              "h2d_bytes_per_step": int(h_u.numel() * h_u.element_size()),
              "d2h_bytes_per_step": int(h_out.numel() * h_out.element_size())},
-        roofline={"bound": "hbm", "kernel": "CG iteration (kCgDirection + kCgUpdate)",
+        roofline={"bound": "hbm",
+                  "kernel": ("persistent PCG iteration (V-cycle + direction + update, kCgPersistent)" if amg
+                             else "CG iteration (kCgDirection + kCgUpdate)"),
                   "achieved": round(achieved, 1) if achieved else None, "peak": pk.get("hbm_gbs"),
                   "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4) if achieved else None,
                   "traffic": None, "bytes_per_cell": per_cell, "peak_source": pk["source"],
@@ -340,6 +368,7 @@ def main():
     ap.add_argument("--workload", default="duct3d", choices=list(WORKLOADS))
     ap.add_argument("--plain-fp64", action="store_true", help="the plain float64 path (no refinement)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-amg", action="store_true", help="unpreconditioned CG for pressure and potential")
     args = ap.parse_args()
     rank, world, local = dist_setup(args)
     if args.impl == "reference":

@@ -147,6 +147,38 @@ typedef struct phb_tolerance {
 	const double *values;
 } phb_tolerance;
 
+/* --- aggregation multigrid preconditioner -------------------------------------------
+ * Replaces phiPICT's AMG hierarchy (solvers/amg.py:450-712 hierarchy_for /
+ * galerkin_refresh, built with pyamg on the host) and its device V-cycle
+ * (solvers/krylov/krylov.cu:1248-1546, bound as amg_pcg_solve, solvers/amg.py:1544).
+ * Every level is a multi-block stencil grid: level l+1 halves each block of level l along
+ * every axis longer than one cell (ceil), keeps the block topology, and its operator is the
+ * Galerkin product P^T A_l P with piecewise-constant P, times coarse_scale. The coarsest
+ * level is solved with a dense generalised inverse per instance (FP64). The host builds the
+ * level descriptors and buffers; phb_amg_setup fills the coarse operators from levels[0].A
+ * on the device. One V-cycle: a damped Jacobi sweep from zero, restriction, the coarse
+ * cycle, prolongation, a damped Jacobi sweep: symmetric, so it can precondition CG. */
+#define PHB_AMG_MAX_LEVELS 12
+typedef struct phb_amg_level {
+	phb_domain dom;       /* blocks, tiles, insts of the level (level 0: the domain's own) */
+	float *A;             /* stencil [2d+1][ncells]; level 0: the float32 system matrix */
+	float *b;             /* restricted residual [ncells] (levels >= 1) */
+	float *x;             /* correction [ncells] (levels >= 1); level 0: z of phb_amg_vcycle */
+	float *wdinv;         /* omega / diagonal [ncells], written by phb_amg_setup */
+} phb_amg_level;
+typedef struct phb_amg {
+	int32_t nlevels;      /* 2..PHB_AMG_MAX_LEVELS */
+	int32_t coarse_n;     /* row stride of the coarsest inverses, >= cells of any instance (<= 1024) */
+	float omega;          /* damping of the Jacobi sweeps */
+	float coarse_scale;   /* factor on every Galerkin product (0.5: rediscretisation scaling) */
+	double *coarse_inv;   /* [ninst][coarse_n][coarse_n], written by phb_amg_setup */
+	phb_amg_level levels[PHB_AMG_MAX_LEVELS];
+} phb_amg;
+/* Galerkin products of levels 1.., dense coarsest operators and their inverses. */
+int phb_amg_setup(const phb_amg *amg, phb_stream stream);
+/* z = one V-cycle applied to r (both [ncells] of level 0, float32). */
+int phb_amg_vcycle(const phb_amg *amg, const float *r, float *z, phb_stream stream);
+
 typedef struct phb_solve {
 	int32_t kind;         /* 0 CG, 1 BiCGStab */
 	int32_t vec_dtype;    /* phb_dtype of the Krylov vectors */
@@ -162,6 +194,8 @@ typedef struct phb_solve {
 	void *x;              /* in: initial guess, out: solution */
 	void *work;           /* >= phb_solve_work_bytes() bytes, 256-byte aligned */
 	void *state;          /* >= phb_solve_state_bytes() bytes */
+	const phb_amg *amg;   /* optional (CG, float32, nrhs 1): precondition with one V-cycle of
+	                         this hierarchy (set up for A); its level-0 x holds z */
 } phb_solve;
 
 /* per-system result, mirrors LinearSolverResultInfo (bindings.cpp:727-732) */
@@ -202,6 +236,7 @@ typedef struct phb_refine {
 	double *x;
 	void *work;           /* >= phb_refine_work_bytes() */
 	void *state;          /* >= phb_solve_state_bytes() */
+	const phb_amg *amg;   /* optional (inner CG, nrhs 1): AMG-preconditioned inner solves, set up for A32 */
 } phb_refine;
 int64_t phb_refine_work_bytes(const phb_domain *dom, int kind, int nrhs);
 /* out (optional): per-system outer results, as phb_refine_results (synchronises) */

@@ -47,13 +47,26 @@ def _lo(domain: Domain, which: str) -> torch.Tensor | None:
     key = "_" + which + "_lo"
     t = getattr(domain, key, None)
     st = domain._stencil(which)
+    ver = domain._matrix_version(which)
+    lover = domain.__dict__.setdefault("_lo_ver", {})
     if t is None or t.shape != st.shape:
         t = torch.empty(st.shape, dtype=torch.float32, device=st.device)
-        # the momentum and pressure kernels refresh their copies at every assembly; the
-        # potential matrix is assembled once, so its copy is taken here
-        t.copy_(st)
         setattr(domain, key, t)
+        lover[which] = None
+    if lover.get(which) != ver:
+        # the momentum and pressure kernels refresh their copies at every assembly; the
+        # potential matrix (assembled once) and values set through the CSR views are
+        # copied here
+        t.copy_(st)
+        lover[which] = ver
     return t
+
+
+def _assembled(domain: Domain, which: str, lo: torch.Tensor | None) -> None:
+    """A kernel rewrote stencil ``which`` (and its float32 copy ``lo`` when given)."""
+    ver = domain._bump_matrix(which)
+    if lo is not None:
+        domain.__dict__.setdefault("_lo_ver", {})[which] = ver
 
 
 def _src(domain: Domain) -> tuple[int | None, int]:
@@ -72,6 +85,7 @@ def SetupAdvectionMatrix(domain: Domain, timeStep, nonOrthoFlags=0, forPassiveSc
     lo = _lo(domain, "C")
     _lib.call("phb_advection_matrix", ct.byref(domain.desc()), domain._u_block.data_ptr(), domain._C_st.data_ptr(),
               domain.A.data_ptr(), lo.data_ptr() if lo is not None else None, _S(domain))
+    _assembled(domain, "C", lo)
 
 
 def SetupAdvectionVelocity(domain: Domain, timeStep, nonOrthoFlags=0, applyPressureGradient: bool = False) -> None:
@@ -97,6 +111,7 @@ def SetupPressureMatrix(domain: Domain, timeStep, nonOrthoMode=0, useFaceTransfo
     lo = _lo(domain, "P")
     _lib.call("phb_pressure_matrix", ct.byref(domain.desc()), domain.A.data_ptr(), domain._P_st.data_ptr(),
               lo.data_ptr() if lo is not None else None, _S(domain))
+    _assembled(domain, "P", lo)
 
 
 def SetupPressureRHS(domain: Domain, timeStep, nonOrthoMode=0, useFaceTransform: bool = False,

@@ -17,6 +17,7 @@ LIB_PATH = _PKG / "libphipict_b200.so"
 PHB_F32, PHB_F64 = 0, 1
 BREC, FREC, IREC, TILE = 48, 16, 8, 1024  # TILE: cells per tile (PHB_TILE_CELLS)
 NOALLOC_SCRATCH_BYTES = 32 << 20  # PHB_NOALLOC_SCRATCH_BYTES
+AMG_MAX_LEVELS = 12  # PHB_AMG_MAX_LEVELS
 
 # every exported symbol of include/phipict_b200.h
 EXPORTS = (
@@ -30,6 +31,7 @@ EXPORTS = (
     "phb_solve_work_bytes", "phb_solve_state_bytes", "phb_solve_run", "phb_solve_results",
     "phb_release_graphs", "phb_refine_work_bytes", "phb_refine_run", "phb_refine_results",
     "phb_cg_noalloc_bytes", "phb_cg_solve_noalloc",
+    "phb_amg_setup", "phb_amg_vcycle",
 )
 
 
@@ -60,6 +62,7 @@ class PhbSolve(ct.Structure):
         ("tol", PhbTolerance),
         ("A", ct.c_void_p), ("b", ct.c_void_p), ("x", ct.c_void_p),
         ("work", ct.c_void_p), ("state", ct.c_void_p),
+        ("amg", ct.c_void_p),
     ]
 
 
@@ -77,6 +80,19 @@ class PhbRefine(ct.Structure):
         ("tol", PhbTolerance),
         ("A64", ct.c_void_p), ("A32", ct.c_void_p), ("b", ct.c_void_p), ("x", ct.c_void_p),
         ("work", ct.c_void_p), ("state", ct.c_void_p),
+        ("amg", ct.c_void_p),
+    ]
+
+
+class PhbAmgLevel(ct.Structure):
+    _fields_ = [("dom", PhbDomain), ("A", ct.c_void_p), ("b", ct.c_void_p), ("x", ct.c_void_p), ("wdinv", ct.c_void_p)]
+
+
+class PhbAmg(ct.Structure):
+    _fields_ = [
+        ("nlevels", ct.c_int32), ("coarse_n", ct.c_int32), ("omega", ct.c_float), ("coarse_scale", ct.c_float),
+        ("coarse_inv", ct.c_void_p),
+        ("levels", PhbAmgLevel * AMG_MAX_LEVELS),
     ]
 
 
@@ -125,6 +141,8 @@ def load() -> ct.CDLL:
         "phb_refine_run": [DP, ct.POINTER(PhbRefine), ct.POINTER(PhbSolveResult), ct.POINTER(ct.c_int), P],
         "phb_refine_results": [DP, ct.POINTER(PhbRefine), ct.POINTER(PhbSolveResult), ct.POINTER(ct.c_int), P],
         "phb_cg_solve_noalloc": [DP, I, I, P, P, P, ct.POINTER(PhbTolerance), I, I, ct.POINTER(PhbSolveResult), P],
+        "phb_amg_setup": [ct.POINTER(PhbAmg), P],
+        "phb_amg_vcycle": [ct.POINTER(PhbAmg), P, P, P],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

@@ -1,0 +1,271 @@
+// Setup of the aggregation multigrid hierarchy on the device (the numeric part of phiPICT's
+// hierarchy_for / galerkin_refresh, solvers/amg.py:450-712): Galerkin products level by
+// level, the dense coarsest operator of every instance and its (generalised) inverse. The
+// cycle itself is in phb_amg.cuh.
+#include <algorithm>
+#include <cmath>
+#include "phb_amg.cuh"
+#include "phb_launch.cuh"
+
+namespace phb {
+
+// omega / diagonal of a level (a zero diagonal counts as one)
+__global__ void kWdinv(int64_t n, const float *__restrict__ A, float *__restrict__ wd, float omega) {
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+		const float d = A[i];
+		wd[i] = omega / (d != 0.f ? d : 1.f);
+	}
+}
+
+// Ac = scale * P^T Af P for coarse tile `blockIdx.x`: each coarse stencil entry sums the
+// fine entries of the aggregate's cells; couplings between two cells of one aggregate fold
+// into the diagonal. scale applies on coarsened blocks only.
+template <int D>
+__global__ void __launch_bounds__(PHB_TILE) kGalerkin(Dom<float, D> fd, Dom<float, D> cd, const float *__restrict__ Af,
+		float *__restrict__ Ac, float scale) {
+	__shared__ int32_t sB[PHB_BREC];
+	const int tile = blockIdx.x;
+	const int bi = __ldg(cd.tiles + 2 * tile);
+	const int l0 = __ldg(cd.tiles + 2 * tile + 1);
+	const int nc = stageBlock<D>(cd, bi, sB);
+	const int32_t *FB = fd.blk(bi);
+	const int64_t N = fd.ncells, NC = cd.ncells;
+	bool coarsened = false;
+#pragma unroll
+	for (int a = 0; a < D; ++a) coarsened |= sB[B_NX + a] < FB[B_NX + a];
+	const double sc = coarsened ? double(scale) : 1.0;
+	for (int j = 0; j < CPT; ++j) {
+		Cell cc;
+		if (!cellAt<D>(sB, l0, nc, j, cc)) break;
+		int base[3], cnt[3];
+#pragma unroll
+		for (int a = 0; a < 3; ++a) {
+			const bool co = a < D && sB[B_NX + a] < FB[B_NX + a];
+			base[a] = co ? 2 * cc.p[a] : cc.p[a];
+			cnt[a] = (co && base[a] + 1 < FB[B_NX + a]) ? 2 : 1;
+		}
+		double acc[2 * D + 1];
+#pragma unroll
+		for (int s = 0; s < 2 * D + 1; ++s) acc[s] = 0;
+		for (int oz = 0; oz < cnt[2]; ++oz)
+			for (int oy = 0; oy < cnt[1]; ++oy)
+				for (int ox = 0; ox < cnt[0]; ++ox) {
+					const int o[3] = {ox, oy, oz};
+					const int p[3] = {base[0] + ox, base[1] + oy, base[2] + oz};
+					const int64_t g = FB[B_CELLOFF] + flat(FB, p);
+					acc[0] += Af[g];
+#pragma unroll
+					for (int f = 0; f < 2 * D; ++f) {
+						const int a = f >> 1;
+						// the neighbour across f is the other cell of the aggregate
+						const bool inside = cnt[a] == 2 && ((f & 1) ? o[a] == 0 : o[a] == 1);
+						const double v = Af[(f + 1) * N + g];
+						if (inside) acc[0] += v;
+						else acc[f + 1] += v;
+					}
+				}
+#pragma unroll
+		for (int s = 0; s < 2 * D + 1; ++s) Ac[s * NC + cc.g] = float(sc * acc[s]);
+	}
+}
+
+// Dense operator of the coarsest level per instance: dense[inst][row][col] (local cells).
+template <int D>
+__global__ void __launch_bounds__(PHB_TILE) kDense(Dom<float, D> cd, const float *__restrict__ Ac, int cn, double *__restrict__ dense) {
+	__shared__ int32_t sB[PHB_BREC];
+	int l0, nc;
+	loadTile<float, D>(cd, sB, l0, nc);
+	const int64_t N = cd.ncells;
+	for (int j = 0; j < CPT; ++j) {
+		Cell c;
+		if (!cellAt<D>(sB, l0, nc, j, c)) break;
+		const int inst = c.B[B_INST];
+		const int off = c.B[B_INSTOFF];
+		if (c.g - off >= cn) continue; // an instance larger than the stride: rejected by the host
+		double *row = dense + ((size_t)inst * cn + (c.g - off)) * cn;
+		atomicAdd(row + (c.g - off), double(Ac[c.g]));
+#pragma unroll
+		for (int f = 0; f < 2 * D; ++f) {
+			const int64_t nb = neighborIndex<float, D>(cd, c, f);
+			if (nb >= 0 && nb - off < cn) atomicAdd(row + (nb - off), double(Ac[(f + 1) * N + c.g]));
+		}
+	}
+}
+
+// In-place Gauss-Jordan inversion of each instance's coarsest operator (one CTA per
+// instance). The operators are symmetric and (semi)definite, so no pivoting is needed.
+// A pure-Neumann pressure or potential system is singular with the constant as null space
+// (phiPICT's rank-deficient systems, whose V-cycle projects the constant out,
+// solvers/amg.py hierarchy_for(project_constant=...)). Its coarse operator is built from
+// float32 stencils, so its row sums are roundoff rather than zero and the null pivot would
+// be inverted into a huge eigenvalue of either sign. Such an operator (every row sum below
+// ZERO_ROWSUM of the largest diagonal) is inverted as A + c 1 1^T with c n = sign(diag) *
+// max|diag|: the constant then has an eigenvalue of the operator's own sign and size, and the
+// inverse is a definite operator that solves every consistent coarse system. A pivot that
+// still falls to roundoff (a second null direction, e.g. two unconnected blocks) is left out:
+// that row and column of the inverse are zero.
+constexpr int INV_THREADS = 512;
+constexpr int INV_MAX = 1024;
+constexpr double ZERO_ROWSUM = 1e-4;
+// instances whose n x n operator fits are inverted in shared memory
+constexpr size_t INV_SMEM_MAX = 200 * 1024;
+
+// M: the n x n operator with row stride ld (shared or global memory), inverted in place
+__device__ void invertDense(double *M, int n, int ld) {
+	__shared__ double rowk[INV_MAX], colk[INV_MAX];
+	__shared__ unsigned char skip[INV_MAX];
+	__shared__ double red[3][INV_THREADS / 32];
+	__shared__ double sThr, sShift;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	// largest |diagonal|, largest |row sum| and the sum of the diagonal (its sign), one warp per row
+	double m = 0, rs = 0, ds = 0;
+	for (int i = warp; i < n; i += INV_THREADS / 32) {
+		double s = 0;
+		for (int j = lane; j < n; j += 32) s += M[(size_t)i * ld + j];
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+		const double dg = M[(size_t)i * ld + i];
+		m = fmax(m, fabs(dg));
+		rs = fmax(rs, fabs(s));
+		ds += dg;
+	}
+	if (lane == 0) { red[0][warp] = m; red[1][warp] = rs; red[2][warp] = ds; }
+	for (int i = threadIdx.x; i < n; i += blockDim.x) skip[i] = 0;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double v = 0, r = 0, d = 0;
+		for (int w = 0; w < INV_THREADS / 32; ++w) { v = fmax(v, red[0][w]); r = fmax(r, red[1][w]); d += red[2][w]; }
+		sThr = 1e-10 * v;
+		sShift = (n > 1 && v > 0 && r <= ZERO_ROWSUM * v) ? (d < 0 ? -v : v) / n : 0.0;
+	}
+	__syncthreads();
+	const double thr = sThr;
+	const double shift = sShift;
+	if (shift != 0.0) {
+		for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) M[(size_t)(idx / n) * ld + idx % n] += shift;
+		__syncthreads();
+	}
+	for (int k = 0; k < n; ++k) {
+		const double p = M[(size_t)k * ld + k];
+		if (!(fabs(p) > thr)) {
+			if (threadIdx.x == 0) skip[k] = 1;
+			__syncthreads();
+			continue;
+		}
+		for (int j = threadIdx.x; j < n; j += blockDim.x) {
+			rowk[j] = M[(size_t)k * ld + j] / p;
+			colk[j] = M[(size_t)j * ld + k];
+		}
+		__syncthreads();
+		for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+			const int i = idx / n, j = idx - i * n;
+			double *e = M + (size_t)i * ld + j;
+			if (i == k && j == k) *e = 1.0 / p;
+			else if (i == k) *e = rowk[j];
+			else if (j == k) *e = -colk[i] / p;
+			else *e -= colk[i] * rowk[j];
+		}
+		__syncthreads();
+	}
+	for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+		const int i = idx / n, j = idx - i * n;
+		if (skip[i] || skip[j]) M[(size_t)i * ld + j] = 0.0;
+	}
+	__syncthreads();
+}
+
+// One CTA per instance: dense[inst] is cn x cn, of which the instance's n x n block is used.
+// SHARED: the block is staged through dynamic shared memory.
+template <bool SHARED>
+__global__ void __launch_bounds__(INV_THREADS) kInvert(double *dense, int cn, const int32_t *insts) {
+	extern __shared__ double sm[];
+	double *G = dense + (size_t)blockIdx.x * cn * cn;
+	const int n = min(cn, insts[blockIdx.x * PHB_IREC + I_NCELLS]);
+	if (SHARED) {
+		for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) sm[idx] = G[(size_t)(idx / n) * cn + idx % n];
+		__syncthreads();
+		invertDense(sm, n, n);
+		for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) G[(size_t)(idx / n) * cn + idx % n] = sm[idx];
+	} else {
+		invertDense(G, n, cn);
+	}
+}
+
+template <int D>
+static int setup(const phb_amg *amg, cudaStream_t s) {
+	const int L = amg->nlevels;
+	for (int l = 0; l + 1 < L; ++l) {
+		const phb_amg_level &F = amg->levels[l], &C = amg->levels[l + 1];
+		if (C.dom.ntiles == 0) continue;
+		kGalerkin<D><<<C.dom.ntiles, PHB_TILE, 0, s>>>(Dom<float, D>(F.dom), Dom<float, D>(C.dom), F.A, C.A, amg->coarse_scale);
+		const int rc = checkLaunch("kGalerkin");
+		if (rc) return rc;
+	}
+	for (int l = 0; l < L; ++l) {
+		const phb_amg_level &v = amg->levels[l];
+		const int64_t n = v.dom.ncells;
+		kWdinv<<<(int)std::min<int64_t>((n + 255) / 256, 148 * 8), 256, 0, s>>>(n, v.A, v.wdinv, amg->omega);
+	}
+	int rc = checkLaunch("kWdinv");
+	if (rc) return rc;
+	const phb_amg_level &C = amg->levels[L - 1];
+	const int cn = amg->coarse_n;
+	PHB_CUDA(cudaMemsetAsync(amg->coarse_inv, 0, sizeof(double) * (size_t)C.dom.ninst * cn * cn, s));
+	if (C.dom.ntiles) kDense<D><<<C.dom.ntiles, PHB_TILE, 0, s>>>(Dom<float, D>(C.dom), C.A, cn, amg->coarse_inv);
+	rc = checkLaunch("kDense");
+	if (rc) return rc;
+	const size_t smem = (size_t)cn * cn * sizeof(double);
+	if (smem <= INV_SMEM_MAX) {
+		static int configured[64] = {0};
+		int dev = 0;
+		PHB_CUDA(cudaGetDevice(&dev));
+		if (dev >= 0 && dev < 64 && !configured[dev]) {
+			PHB_CUDA(cudaFuncSetAttribute(kInvert<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INV_SMEM_MAX));
+			configured[dev] = 1;
+		}
+		kInvert<true><<<C.dom.ninst, INV_THREADS, smem, s>>>(amg->coarse_inv, cn, C.dom.insts);
+	} else {
+		kInvert<false><<<C.dom.ninst, INV_THREADS, 0, s>>>(amg->coarse_inv, cn, C.dom.insts);
+	}
+	return checkLaunch("kInvert");
+}
+
+} // namespace phb
+
+using namespace phb;
+
+// Shared with the Krylov solvers: validates a hierarchy before any launch.
+int phbCheckAmg(const phb_amg *amg) {
+	if (!amg) return setError(PHB_ERR_ARG, "AMG: null hierarchy");
+	if (amg->nlevels < 2 || amg->nlevels > PHB_AMG_MAX_LEVELS) return setError(PHB_ERR_RANGE, "AMG: nlevels must be 2..PHB_AMG_MAX_LEVELS");
+	if (amg->coarse_n < 1 || amg->coarse_n > INV_MAX) return setError(PHB_ERR_RANGE, "AMG: coarse_n must be 1..1024");
+	if (!amg->coarse_inv) return setError(PHB_ERR_ARG, "AMG: coarse_inv missing");
+	const int d = amg->levels[0].dom.dims;
+	if (d != 2 && d != 3) return setError(PHB_ERR_ARG, "AMG: dims must be 2 or 3");
+	for (int l = 0; l < amg->nlevels; ++l) {
+		const phb_amg_level &v = amg->levels[l];
+		if (v.dom.dims != d || !v.dom.blocks || !v.dom.tiles || !v.dom.insts || !v.A || !v.wdinv) return setError(PHB_ERR_ARG, "AMG: incomplete level");
+		if (l > 0 && (!v.b || !v.x)) return setError(PHB_ERR_ARG, "AMG: level vectors missing");
+		if (v.dom.ninst != amg->levels[0].dom.ninst) return setError(PHB_ERR_ARG, "AMG: levels disagree on the instance count");
+	}
+	const phb_amg_level &C = amg->levels[amg->nlevels - 1];
+	if (C.dom.ncells > (int64_t)C.dom.ninst * amg->coarse_n) return setError(PHB_ERR_RANGE, "AMG: coarsest level larger than coarse_n per instance");
+	return PHB_OK;
+}
+
+extern "C" int phb_amg_setup(const phb_amg *amg, phb_stream stream) {
+	const int rc = phbCheckAmg(amg);
+	if (rc) return rc;
+	cudaStream_t s = (cudaStream_t)stream;
+	return amg->levels[0].dom.dims == 2 ? setup<2>(amg, s) : setup<3>(amg, s);
+}
+
+extern "C" int phb_amg_vcycle(const phb_amg *amg, const float *r, float *z, phb_stream stream) {
+	const int rc = phbCheckAmg(amg);
+	if (rc) return rc;
+	if (!r || !z) return setError(PHB_ERR_ARG, "phb_amg_vcycle: null vector");
+	cudaStream_t s = (cudaStream_t)stream;
+	if (amg->levels[0].dom.dims == 2) PHB_CUDA(launchAmgCycle<2>(makeAmgView<2>(*amg, r, z), s, 0));
+	else PHB_CUDA(launchAmgCycle<3>(makeAmgView<3>(*amg, r, z), s, 0));
+	return PHB_OK;
+}

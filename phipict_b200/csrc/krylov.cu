@@ -23,8 +23,12 @@
 #include <cstring>
 #include <cmath>
 #include <functional>
+#include <type_traits>
 #include "phb_device.cuh"
+#include "phb_amg.cuh"
 #include "phb_launch.cuh"
+
+int phbCheckAmg(const phb_amg *amg); // amg.cu
 
 namespace phb {
 
@@ -342,8 +346,9 @@ __global__ void __launch_bounds__(PHB_TILE) kCgDirection(Dom<double, D> dom, con
 }
 
 // CG phase 2 (kCgUpdate, krylov.cu:502-568): x += alpha p, r -= alpha q, (r, r); last CTA:
-// convergence, beta = (r, r)_new / (r, r)_old, optional best-iterate tracking.
-template <typename T, int D, int K>
+// convergence, beta = (r, r)_new / (r, r)_old, optional best-iterate tracking. Preconditioned
+// (PC): beta comes from (r, z) after the next V-cycle instead (kPcgPrecond).
+template <typename T, int D, int K, bool PC = false>
 __global__ void __launch_bounds__(PHB_TILE) kCgUpdate(Dom<double, D> dom, T *__restrict__ r, const T *__restrict__ p,
 		const T *__restrict__ q, T *__restrict__ x, T *__restrict__ xbest, SysState *st, double *partial, Control *ctrl,
 		int returnBest, LoopCond lc) {
@@ -387,13 +392,36 @@ __global__ void __launch_bounds__(PHB_TILE) kCgUpdate(Dom<double, D> dom, T *__r
 			if (crit < s.tol) s.done = CONVERGED;
 			else if (s.it >= s.maxit) s.done = MAXIT;
 			else if (returnBest && s.rising >= RISING_CUTOFF) s.done = RISING;
-			else {
+			else if (!PC) {
 				s.beta = red[0] / s.rho;
 				s.rho = red[0];
 				if (!fin(s.beta)) s.done = NONFINITE;
 			}
 		});
 		if (threadIdx.x == 0) setLoop(lc, ctrl);
+	}
+}
+
+// rho/beta of a running system from the new (r, z) (the preconditioned CG of
+// amg_pcg_solve, solvers/amg.py:1544): the first iteration after a restart takes rho only.
+__device__ __forceinline__ void pcgRho(SysState &s, double rz) {
+	if (s.restart) s.rho = rz;
+	else {
+		s.beta = rz / s.rho;
+		s.rho = rz;
+		if (!fin(s.beta)) s.done = NONFINITE;
+	}
+	if (!fin(rz)) s.done = NONFINITE;
+}
+
+// Last step of the V-cycle on level 0 (prolongation and post-smoothing, z written to the
+// hierarchy's level-0 x) fused with (r, z); last CTA: rho and beta (pcgRho).
+template <int D>
+__global__ void __launch_bounds__(PHB_TILE) kPcgPrecond(Dom<double, D> dom, AmgView<D> mg, SysState *st, double *partial, Control *ctrl) {
+	__shared__ int32_t sB[PHB_BREC];
+	double acc[1] = {amgProlongTile<D>(mg, 0, blockIdx.x, sB, mg.x[0])};
+	if (storePartials<1>(acc, partial, &ctrl->counter)) {
+		finalizeSystems<1, 1>(dom.insts, dom.ninst, partial, st, ctrl, [&](SysState &s, int, const double *red, double) { pcgRho(s, red[0]); });
 	}
 }
 
@@ -844,10 +872,13 @@ __device__ __forceinline__ void residualDecision(const Dom<double, 3> *, SysStat
 	else if ((BICG || STOPSTART) ? crit < s.tol : crit == 0.0) { s.done = CONVERGED; s.usedIt = BICG ? -1 : 0; }
 }
 
-template <typename T, int D, int K, bool STOPSTART>
+// PC: AMG-preconditioned CG (float, one right-hand side): every iteration first runs the
+// V-cycle of `mg` on r, level by level between grid barriers, and takes the direction from z.
+template <typename T, int D, int K, bool STOPSTART, bool PC = false>
 __global__ void __launch_bounds__(PHB_TILE) kCgPersistent(Dom<double, D> dom, const T *__restrict__ A, const T *__restrict__ b,
 		T *__restrict__ x, T *__restrict__ r, T *__restrict__ p0, T *__restrict__ p1, T *__restrict__ q, T *__restrict__ xbest,
-		SysState *st, double *partial, Control *ctrl, phb_tolerance tol, int returnBest, int maxit) {
+		SysState *st, double *partial, Control *ctrl, phb_tolerance tol, int returnBest, int maxit, AmgView<D> mg) {
+	static_assert(!PC || (std::is_same<T, float>::value && K == 1), "the V-cycle preconditions float single-rhs CG");
 	extern __shared__ SysState sst[];
 	__shared__ int32_t sB[PHB_BREC];
 	const int nsys = dom.ninst * K;
@@ -855,7 +886,13 @@ __global__ void __launch_bounds__(PHB_TILE) kCgPersistent(Dom<double, D> dom, co
 	__syncthreads();
 	unsigned int gen = 0;
 	const int64_t N = dom.ncells;
+	// consecutive phases write alternate halves of the partials, so that a CTA that has left
+	// a barrier cannot overwrite partials another CTA is still reducing
+	const size_t half = (size_t)dom.ntiles * K * 3;
+	int ph = 0;
+	double *pp = partial;
 	// r = b - A x, (r, r), (b, b)
+	pp = partial + (size_t)(ph++ & 1) * half;
 	forMyTiles<D>(dom, sB, [&](int tile, int l0, int nc) {
 		const int inst = sB[B_INST];
 		bool act[K];
@@ -882,15 +919,42 @@ __global__ void __launch_bounds__(PHB_TILE) kCgPersistent(Dom<double, D> dom, co
 				acc[2 * k + 1] += double(bi) * double(bi);
 			}
 		}
-		blockSumTo<2 * K>(acc, partial + (size_t)tile * 2 * K);
+		blockSumTo<2 * K>(acc, pp + (size_t)tile * 2 * K);
 	});
 	if (!gridBarrier(ctrl, gen)) return;
-	int running = reduceStates<K, 2, 1>(dom.insts, dom.ninst, partial, sst, [&](SysState &s, int in, const double *red, double bb) {
+	int running = reduceStates<K, 2, 1>(dom.insts, dom.ninst, pp, sst, [&](SysState &s, int in, const double *red, double bb) {
 		residualDecision<K, false, STOPSTART>(nullptr, s, normScale(dom.insts, in), red, bb, tol);
 	});
 	T *pIn = p0, *pOut = p1;
+	// the direction is built from z = M r when preconditioned, from r otherwise
+	const T *dsrc = r;
+	if constexpr (PC) dsrc = (const T *)mg.x[0];
 	for (int iter = 0; running > 0 && iter <= maxit + 1; ++iter) {
-		// p' = r + beta p, q = A p', (p', q)
+		if constexpr (PC) {
+			const int L = mg.nlevels;
+			for (int l = 0; l + 1 < L; ++l) {
+				for (int sub = blockIdx.x; sub < mg.lv[l + 1].ntiles * Restrict<D>::PER_TILE; sub += gridDim.x) amgRestrictSub<D>(mg, l, sub, sB);
+				if (!gridBarrier(ctrl, gen)) return;
+			}
+			amgCoarseRows<D>(mg, int(blockIdx.x * NWARPS + (threadIdx.x >> 5)), int(gridDim.x * NWARPS));
+			if (!gridBarrier(ctrl, gen)) return;
+			for (int l = L - 2; l >= 1; --l) {
+				for (int sub = blockIdx.x; sub < mg.lv[l].ntiles * AMG_SUBTILES; sub += gridDim.x) {
+					const int q = sub % AMG_SUBTILES;
+					amgProlongTile<D>(mg, l, sub / AMG_SUBTILES, sB, mg.x[l], q, q + 1);
+				}
+				if (!gridBarrier(ctrl, gen)) return;
+			}
+			pp = partial + (size_t)(ph++ & 1) * half;
+			for (int tile = blockIdx.x; tile < dom.ntiles; tile += gridDim.x) {
+				double acc[1] = {amgProlongTile<D>(mg, 0, tile, sB, mg.x[0])};
+				blockSumTo<1>(acc, pp + tile);
+			}
+			if (!gridBarrier(ctrl, gen)) return;
+			reduceStates<1, 1>(dom.insts, dom.ninst, pp, sst, [&](SysState &s, int, const double *red, double) { pcgRho(s, red[0]); });
+		}
+		// p' = z + beta p (z = r without preconditioner), q = A p', (p', q)
+		pp = partial + (size_t)(ph++ & 1) * half;
 		forMyTiles<D>(dom, sB, [&](int tile, int l0, int nc) {
 			const int inst = sB[B_INST];
 			bool act[K], rs[K];
@@ -912,7 +976,7 @@ __global__ void __launch_bounds__(PHB_TILE) kCgPersistent(Dom<double, D> dom, co
 				stencilNeighbors<D>(dom, c, nb);
 				auto pv = [&](int64_t g, int k) {
 					const int64_t o = vk<K>(c.B, g, k);
-					return rs[k] ? r[o] : r[o] + beta[k] * pIn[o];
+					return rs[k] ? dsrc[o] : dsrc[o] + beta[k] * pIn[o];
 				};
 				T y[K];
 				applyA<T, D, K>(A, N, c, nb, act, pv, y);
@@ -926,16 +990,17 @@ __global__ void __launch_bounds__(PHB_TILE) kCgPersistent(Dom<double, D> dom, co
 					acc[k] += double(pi) * double(y[k]);
 				}
 			}
-			blockSumTo<K>(acc, partial + (size_t)tile * K);
+			blockSumTo<K>(acc, pp + (size_t)tile * K);
 		});
 		if (!gridBarrier(ctrl, gen)) return;
-		reduceStates<K, 1>(dom.insts, dom.ninst, partial, sst, [&](SysState &s, int, const double *red, double) {
+		reduceStates<K, 1>(dom.insts, dom.ninst, pp, sst, [&](SysState &s, int, const double *red, double) {
 			const double alpha = s.rho / red[0];
 			s.restart = 0;
 			if (!fin(alpha)) { s.done = NONFINITE; s.usedIt = s.it; }
 			else s.alpha = alpha;
 		});
 		// x += alpha p', r -= alpha q, (r, r)
+		pp = partial + (size_t)(ph++ & 1) * half;
 		forMyTiles<D>(dom, sB, [&](int tile, int l0, int nc) {
 			const int inst = sB[B_INST];
 			double acc[K];
@@ -958,10 +1023,10 @@ __global__ void __launch_bounds__(PHB_TILE) kCgPersistent(Dom<double, D> dom, co
 					acc[k] += double(ri) * double(ri);
 				}
 			}
-			blockSumTo<K>(acc, partial + (size_t)tile * K);
+			blockSumTo<K>(acc, pp + (size_t)tile * K);
 		});
 		if (!gridBarrier(ctrl, gen)) return;
-		running = reduceStates<K, 1>(dom.insts, dom.ninst, partial, sst, [&](SysState &s, int in, const double *red, double) {
+		running = reduceStates<K, 1>(dom.insts, dom.ninst, pp, sst, [&](SysState &s, int in, const double *red, double) {
 			const double crit = sqrt(red[0]) * normScale(dom.insts, in);
 			++s.it;
 			s.crit = crit;
@@ -976,7 +1041,7 @@ __global__ void __launch_bounds__(PHB_TILE) kCgPersistent(Dom<double, D> dom, co
 			if (crit < s.tol) s.done = CONVERGED;
 			else if (s.it >= s.maxit) s.done = MAXIT;
 			else if (returnBest && s.rising >= RISING_CUTOFF) s.done = RISING;
-			else {
+			else if (!PC) {
 				s.beta = red[0] / s.rho;
 				s.rho = red[0];
 				if (!fin(s.beta)) s.done = NONFINITE;
@@ -1019,6 +1084,12 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgPersistent(Dom<double, D> dom, 
 	__syncthreads();
 	unsigned int gen = 0;
 	const int64_t N = dom.ncells;
+	// consecutive phases write alternate halves of the partials, so that a CTA that has left
+	// a barrier cannot overwrite partials another CTA is still reducing
+	const size_t half = (size_t)dom.ntiles * K * 3;
+	int ph = 0;
+	double *pp = partial;
+	pp = partial + (size_t)(ph++ & 1) * half;
 	forMyTiles<D>(dom, sB, [&](int tile, int l0, int nc) {
 		const int inst = sB[B_INST];
 		bool act[K];
@@ -1046,15 +1117,16 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgPersistent(Dom<double, D> dom, 
 				acc[2 * k + 1] += double(bi) * double(bi);
 			}
 		}
-		blockSumTo<2 * K>(acc, partial + (size_t)tile * 2 * K);
+		blockSumTo<2 * K>(acc, pp + (size_t)tile * 2 * K);
 	});
 	if (!gridBarrier(ctrl, gen)) return;
-	int running = reduceStates<K, 2, 1>(dom.insts, dom.ninst, partial, sst, [&](SysState &s, int in, const double *red, double bb) {
+	int running = reduceStates<K, 2, 1>(dom.insts, dom.ninst, pp, sst, [&](SysState &s, int in, const double *red, double bb) {
 		residualDecision<K, true, true>(nullptr, s, normScale(dom.insts, in), red, bb, tol);
 	});
 	T *pIn = p0, *pOut = p1, *vIn = v0, *vOut = v1;
 	for (int iter = 0; running > 0 && iter <= maxit + 1; ++iter) {
 		// p = r + beta (p - omega v), v = A p, (r0, v)
+		pp = partial + (size_t)(ph++ & 1) * half;
 		forMyTiles<D>(dom, sB, [&](int tile, int l0, int nc) {
 			const int inst = sB[B_INST];
 			bool act[K], rs[K];
@@ -1090,16 +1162,17 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgPersistent(Dom<double, D> dom, 
 					acc[k] += double(r0[o]) * double(y[k]);
 				}
 			}
-			blockSumTo<K>(acc, partial + (size_t)tile * K);
+			blockSumTo<K>(acc, pp + (size_t)tile * K);
 		});
 		if (!gridBarrier(ctrl, gen)) return;
-		reduceStates<K, 1>(dom.insts, dom.ninst, partial, sst, [&](SysState &s, int, const double *red, double) {
+		reduceStates<K, 1>(dom.insts, dom.ninst, pp, sst, [&](SysState &s, int, const double *red, double) {
 			const double alpha = s.rho / red[0];
 			s.restart = 0;
 			if (!fin(alpha)) { s.done = NONFINITE; s.usedIt = s.it; }
 			else s.alpha = alpha;
 		});
 		// s = r - alpha v, t = A s, (t,s), (t,t), (s,s)
+		pp = partial + (size_t)(ph++ & 1) * half;
 		forMyTiles<D>(dom, sB, [&](int tile, int l0, int nc) {
 			const int inst = sB[B_INST];
 			bool act[K];
@@ -1135,10 +1208,10 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgPersistent(Dom<double, D> dom, 
 					acc[3 * k + 2] += double(si) * double(si);
 				}
 			}
-			blockSumTo<3 * K>(acc, partial + (size_t)tile * 3 * K);
+			blockSumTo<3 * K>(acc, pp + (size_t)tile * 3 * K);
 		});
 		if (!gridBarrier(ctrl, gen)) return;
-		reduceStates<K, 3>(dom.insts, dom.ninst, partial, sst, [&](SysState &s, int in, const double *red, double) {
+		reduceStates<K, 3>(dom.insts, dom.ninst, pp, sst, [&](SysState &s, int in, const double *red, double) {
 			const double critS = sqrt(red[2]) * normScale(dom.insts, in);
 			s.halfCrit = critS;
 			if (!fin(critS)) { s.done = NONFINITE; s.crit = critS; s.usedIt = s.it; }
@@ -1150,6 +1223,7 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgPersistent(Dom<double, D> dom, 
 			}
 		});
 		// x += alpha p + omega s, r = s - omega t, (r0, r), (r, r)
+		pp = partial + (size_t)(ph++ & 1) * half;
 		forMyTiles<D>(dom, sB, [&](int tile, int l0, int nc) {
 			const int inst = sB[B_INST];
 			double acc[2 * K];
@@ -1177,10 +1251,10 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgPersistent(Dom<double, D> dom, 
 					}
 				}
 			}
-			blockSumTo<2 * K>(acc, partial + (size_t)tile * 2 * K);
+			blockSumTo<2 * K>(acc, pp + (size_t)tile * 2 * K);
 		});
 		if (!gridBarrier(ctrl, gen)) return;
-		running = reduceStates<K, 2>(dom.insts, dom.ninst, partial, sst, [&](SysState &s, int in, const double *red, double) {
+		running = reduceStates<K, 2>(dom.insts, dom.ninst, pp, sst, [&](SysState &s, int in, const double *red, double) {
 			if (s.halfDone) { s.done = CONVERGED; s.crit = s.halfCrit; s.usedIt = s.it; return; }
 			const double crit = sqrt(red[1]) * normScale(dom.insts, in);
 			s.crit = crit;
@@ -1220,8 +1294,8 @@ static Layout solveLayout(const phb_domain *dom, int kind, int vecBytes, int nrh
 	size_t o = 0;
 	const size_t vb = align256((size_t)dom->ncells * nrhs * vecBytes);
 	for (int i = 0; i < vecCount(kind); ++i) { L.off[i] = o; o += vb; }
-	L.off[10] = o; // partials
-	o += align256((size_t)dom->ntiles * nrhs * 3 * sizeof(double));
+	L.off[10] = o; // partials: two halves of up to 3 values per tile and right-hand side
+	o += align256((size_t)dom->ntiles * nrhs * 3 * 2 * sizeof(double));
 	L.total = o;
 	return L;
 }
@@ -1397,16 +1471,19 @@ static int launchPersistent(const phb_domain *dom, const phb_solve *sv, cudaStre
 	if (sv->kind == 0) {
 		T *r = (T *)(w + L.off[0]), *q = (T *)(w + L.off[1]), *p0 = (T *)(w + L.off[2]), *p1 = (T *)(w + L.off[3]);
 		T *xbest = sv->return_best ? (T *)(w + L.off[4]) : nullptr;
-		if (stopStart) {
-			auto kern = kCgPersistent<T, D, K, true>;
+		AmgView<D> mg = {};
+		auto launch = [&](auto kern) -> int {
 			cfg.gridDim = dim3(grid((const void *)kern));
-			PHB_CUDA(cudaLaunchKernelEx(&cfg, kern, dm, A, b, x, r, p0, p1, q, xbest, st, partial, ctrl, sv->tol, sv->return_best, maxit));
-		} else {
-			auto kern = kCgPersistent<T, D, K, false>;
-			cfg.gridDim = dim3(grid((const void *)kern));
-			PHB_CUDA(cudaLaunchKernelEx(&cfg, kern, dm, A, b, x, r, p0, p1, q, xbest, st, partial, ctrl, sv->tol, sv->return_best, maxit));
+			PHB_CUDA(cudaLaunchKernelEx(&cfg, kern, dm, A, b, x, r, p0, p1, q, xbest, st, partial, ctrl, sv->tol, sv->return_best, maxit, mg));
+			return PHB_OK;
+		};
+		if constexpr (std::is_same<T, float>::value && K == 1) {
+			if (sv->amg) {
+				mg = makeAmgView<D>(*sv->amg, (const float *)r, sv->amg->levels[0].x);
+				return stopStart ? launch(kCgPersistent<T, D, K, true, true>) : launch(kCgPersistent<T, D, K, false, true>);
+			}
 		}
-		return PHB_OK;
+		return stopStart ? launch(kCgPersistent<T, D, K, true>) : launch(kCgPersistent<T, D, K, false>);
 	}
 	T *r = (T *)(w + L.off[0]), *r0 = (T *)(w + L.off[1]), *p0 = (T *)(w + L.off[2]), *p1 = (T *)(w + L.off[3]);
 	T *v0 = (T *)(w + L.off[4]), *v1 = (T *)(w + L.off[5]), *t = (T *)(w + L.off[6]);
@@ -1449,13 +1526,32 @@ static int emitSolve(const phb_domain *dom, const phb_solve *sv, cudaStream_t s,
 		else kResidual<T, D, K, false, false><<<tiles, PHB_TILE, 0, s>>>(dm, A, b, x, r, nullptr, st, partial, ctrl, sv->tol, arm);
 		int rc = checkLaunch("kResidual");
 		if (rc) return rc;
+		// preconditioned (float, one right-hand side): V-cycle on r down to level 1, then level
+		// 0's prolongation with (r, z) and beta, and the direction taken from z
+		bool pc = false;
+		AmgView<D> mg = {};
+		const T *dsrc = r;
+		if constexpr (std::is_same<T, float>::value && K == 1) {
+			if (sv->amg) {
+				pc = true;
+				mg = makeAmgView<D>(*sv->amg, (const float *)r, sv->amg->levels[0].x);
+				dsrc = (const T *)mg.x[0];
+			}
+		}
 		auto body = [&](cudaStream_t bs, LoopCond lc) -> int {
 			for (int half = 0; half < 2; ++half) {
 				T *pIn = half == 0 ? p0 : p1, *pOut = half == 0 ? p1 : p0;
-				kCgDirection<T, D, K><<<tiles, PHB_TILE, 0, bs>>>(dm, A, r, pIn, pOut, q, st, partial, ctrl);
 				LoopCond l2 = lc;
 				l2.active = half == 1 ? lc.active : 0;
-				kCgUpdate<T, D, K><<<tiles, PHB_TILE, 0, bs>>>(dm, r, pOut, q, x, xbest, st, partial, ctrl, sv->return_best, l2);
+				if (pc) {
+					PHB_CUDA(launchAmgCycle<D>(mg, bs, 1));
+					kPcgPrecond<D><<<tiles, PHB_TILE, 0, bs>>>(dm, mg, st, partial, ctrl);
+					kCgDirection<T, D, K><<<tiles, PHB_TILE, 0, bs>>>(dm, A, dsrc, pIn, pOut, q, st, partial, ctrl);
+					kCgUpdate<T, D, K, true><<<tiles, PHB_TILE, 0, bs>>>(dm, r, pOut, q, x, xbest, st, partial, ctrl, sv->return_best, l2);
+				} else {
+					kCgDirection<T, D, K><<<tiles, PHB_TILE, 0, bs>>>(dm, A, r, pIn, pOut, q, st, partial, ctrl);
+					kCgUpdate<T, D, K><<<tiles, PHB_TILE, 0, bs>>>(dm, r, pOut, q, x, xbest, st, partial, ctrl, sv->return_best, l2);
+				}
 			}
 			return checkLaunch("CG body");
 		};
@@ -1548,9 +1644,16 @@ extern "C" int phb_solve_run(const phb_domain *dom, const phb_solve *s, phb_stre
 	if (!dom || !s || !s->A || !s->b || !s->x || !s->work || !s->state || (s->tol.mode == 2 && !s->tol.values)) return setError(PHB_ERR_ARG, "phb_solve_run: null argument");
 	if (s->vec_dtype != s->mat_dtype) return setError(PHB_ERR_ARG, "phb_solve_run: matrix and vector dtype must match");
 	if (s->kind != 0 && s->kind != 1) return setError(PHB_ERR_ARG, "phb_solve_run: kind must be 0 (CG) or 1 (BiCGStab)");
+	if (s->amg) {
+		if (s->kind != 0 || s->vec_dtype != PHB_F32 || s->nrhs != 1) return setError(PHB_ERR_ARG, "phb_solve_run: the AMG preconditioner takes float32 CG with one right-hand side");
+		const int rc = phbCheckAmg(s->amg);
+		if (rc) return rc;
+		if (s->amg->levels[0].dom.ncells != dom->ncells || !s->amg->levels[0].x) return setError(PHB_ERR_ARG, "phb_solve_run: hierarchy does not match the domain");
+	}
 	if (dom->ntiles == 0) return PHB_OK;
 	cudaStream_t st = (cudaStream_t)stream;
-	const std::string key = makeKey("solve", *dom, *s);
+	std::string key = makeKey("solve", *dom, *s);
+	if (s->amg) key.append(reinterpret_cast<const char *>(s->amg), sizeof(phb_amg));
 	PHB_SOLVE_DISPATCH(dom->dims, s->vec_dtype, s->nrhs, {
 		if (s->use_graph != 1) {
 			Streams *ss; int rc = getStreams(ss); if (rc) return rc;
@@ -1627,6 +1730,7 @@ static int emitRefine(const phb_domain *dom, const phb_refine *rf, cudaStream_t 
 	in.tol = phb_tolerance{}; // unused: the inner tolerance is SysState::innerTol
 	in.work = rf->work;
 	in.state = rf->state;
+	in.amg = rf->amg;
 	const bool graph = rf->use_graph != 0;
 	in.use_graph = rf->use_graph == 2 ? 2 : (graph ? 1 : 0);
 	in.check_every = 8;
@@ -1668,9 +1772,16 @@ extern "C" int phb_refine_results(const phb_domain *dom, const phb_refine *r, ph
 extern "C" int phb_refine_run(const phb_domain *dom, const phb_refine *r, phb_solve_result *out, int *outer_used, phb_stream stream) {
 	if (!dom || !r || !r->A64 || !r->A32 || !r->b || !r->x || !r->work || !r->state || (r->tol.mode == 2 && !r->tol.values))
 		return setError(PHB_ERR_ARG, "phb_refine_run: null argument");
+	if (r->amg) {
+		if (r->kind != 0 || r->nrhs != 1) return setError(PHB_ERR_ARG, "phb_refine_run: the AMG preconditioner takes CG with one right-hand side");
+		const int rc = phbCheckAmg(r->amg);
+		if (rc) return rc;
+		if (r->amg->levels[0].dom.ncells != dom->ncells || !r->amg->levels[0].x) return setError(PHB_ERR_ARG, "phb_refine_run: hierarchy does not match the domain");
+	}
 	if (dom->ntiles == 0) return PHB_OK;
 	cudaStream_t st = (cudaStream_t)stream;
-	const std::string key = makeKey("refine", *dom, *r);
+	std::string key = makeKey("refine", *dom, *r);
+	if (r->amg) key.append(reinterpret_cast<const char *>(r->amg), sizeof(phb_amg));
 	int rc = PHB_OK;
 	const int K = r->nrhs;
 	if (!r->use_graph) {

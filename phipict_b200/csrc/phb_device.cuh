@@ -47,6 +47,7 @@ struct Dom {
 	int64_t ms, fms, ncells;
 	int nblocks, ninst, ntiles;
 
+	Dom() = default;
 	__host__ Dom(const phb_domain &d)
 		: blocks(d.blocks), tiles(d.tiles), fixed(d.fixed), insts(d.insts),
 		  met((const S *)d.metrics), fmet((const S *)d.face_metrics), fvel((const S *)d.fvel),

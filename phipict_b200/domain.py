@@ -1016,6 +1016,7 @@ class Domain:
                 r[7] = venv[e]
                 r[8] = self._fixed_cells[k]
                 r[9] = self._fixed_toff[k]
+        self._blocks_host, self._insts_host = blocks, insts
         self._blocks_dev = blocks.to(self._device)
         self._fixed_dev = fixed.to(self._device)
         self._insts_dev = insts.to(self._device)
@@ -1105,6 +1106,7 @@ class Domain:
                 b.epot.copy_(old)
         self._epot_block = e
         _lib.call("phb_epot_matrix", ct.byref(self._desc), self._E_st.data_ptr(), None, _lib.stream_ptr(self._device))
+        self._bump_matrix("E")
         self.Epot = CSRmatrix(_domain=self, _which="E")
         self.Epot.row, self.Epot.index = self._csr_row, self._csr_col
         self._csr_cache.pop("E", None)
@@ -1154,6 +1156,17 @@ class Domain:
     def _set_csr_values(self, which: str, v: torch.Tensor) -> None:
         st = self._stencil(which)
         st.view(-1).scatter_(0, self._csr_perm.long(), v.to(self._dtype).reshape(-1))
+        self._bump_matrix(which)
+
+    def _bump_matrix(self, which: str) -> int:
+        """A new version of stencil ``which`` (its float32 copy and multigrid operators
+        follow on their next use)."""
+        ver = self.__dict__.setdefault("_mver", {})
+        ver[which] = ver.get(which, 0) + 1
+        return ver[which]
+
+    def _matrix_version(self, which: str) -> int:
+        return self.__dict__.get("_mver", {}).get(which, 0)
 
     # --- per-instance vector helpers ------------------------------------------------------
     def _subtract_mean(self, x: torch.Tensor, comps: int) -> None:

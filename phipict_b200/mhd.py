@@ -72,6 +72,10 @@ class MHDSimulation(Simulation):
             from .amg import require_amg
 
             require_amg()
+            if not self._amg_dtype_ok():
+                raise NotImplementedError(
+                    "the multigrid V-cycle runs in float32: use a float32 domain or mixed_precision=True")
+        self._potential_amg_options = dict(potential_amg_options or {})
         self._stuart_number = stuart_number
         self.potential_tol = parse_tolerance(potential_tol)
         self._potential_use_BiCG = potential_use_BiCG
@@ -93,6 +97,15 @@ class MHDSimulation(Simulation):
         self._potential_stale = False
         self.hooks.append(Hook.POST, self._magnetic_step_callback)
         self.hooks.append(Hook.PRE_VELOCITY_SETUP, self._add_lorentz_force)
+
+    # potential solves use the multigrid preconditioner when asked (mhd.py:673-712)
+    def _amg_wanted(self, which: str) -> bool:
+        if which == "E":
+            return bool(self._potential_use_preconditioner) and not self._potential_use_BiCG
+        return super()._amg_wanted(which)
+
+    def _amg_options(self, which: str) -> dict:
+        return self._potential_amg_options if which == "E" else super()._amg_options(which)
 
     def _set_field(self, e_b: torch.Tensor) -> None:
         d = self.domain

@@ -37,6 +37,11 @@ _UNSUPPORTED_TRUE = ("scipy_solve_advection", "scipy_solve_pressure", "different
 class Simulation:
     """A drop-in for ``phipict.Simulation`` on phipict_b200 kernels."""
 
+    # pressure systems at least this large use the multigrid preconditioner when
+    # pressure_use_amg is None (core/piso_simulation.py:1118-1122)
+    PRESSURE_AMG_AUTO_MIN_ROWS = 200_000
+    PRESSURE_AMG_AUTO_MIN_ROWS_BATCHED = 400_000
+
     def __init__(
         self,
         domain: Domain,
@@ -105,6 +110,8 @@ class Simulation:
         self.pressure_tol_intermediate = parse_tolerance(pressure_tol_intermediate)
         self.pressure_warm_start = pressure_warm_start
         self.pressure_use_amg = pressure_use_amg
+        self._pressure_amg_options = dict(pressure_amg_options or {})
+        self._amg_cache: dict = {}
         self.flux_balance_tol = flux_balance_tol
         self.convergence_tol = convergence_tol
         self.normalize_pressure_result = normalize_pressure_result
@@ -127,6 +134,8 @@ class Simulation:
         if self.mixed_precision and domain.getDtype() != torch.float64:
             raise TypeError("mixed_precision refines float64 systems; create the domain with dtype=torch.float64")
         domain._mixed = self.mixed_precision
+        if pressure_use_amg and not self._amg_dtype_ok():
+            raise NotImplementedError("the multigrid V-cycle runs in float32: use a float32 domain or mixed_precision=True")
         if non_orthogonal:
             self._require_orthogonal()
 
@@ -178,15 +187,45 @@ class Simulation:
 
     def _solve_launch(self, which, rhs, x, kind, tol, tag, nrhs, return_best, maxit) -> None:
         d = self.domain
+        pc = kind == CG and nrhs == 1 and self._amg_wanted(which)
         if self.mixed_precision:
             lo = backend._lo(d, which)
+            amg = self._amg_for(which, lo) if pc else None
             r = refiner_for(d, kind, nrhs, tag=tag)
-            r.solve(d._stencil(which), lo, rhs, x, tol, maxit)
+            r.solve(d._stencil(which), lo, rhs, x, tol, maxit, amg=amg)
             self._pending.append((tag, r))
         else:
+            A = d._stencil(which)
+            amg = self._amg_for(which, A) if pc else None
             s = solver_for(d, kind, d.getDtype(), nrhs, tag=tag)
-            s.solve(d._stencil(which), rhs, x, tol, maxit, return_best=return_best)
+            s.solve(A, rhs, x, tol, maxit, return_best=return_best, amg=amg)
             self._pending.append((tag, s))
+
+    # --- multigrid preconditioner ------------------------------------------------------
+    def _amg_dtype_ok(self) -> bool:
+        return self.domain.getDtype() == torch.float32 or self.mixed_precision
+
+    def _amg_wanted(self, which: str) -> bool:
+        """pressure_use_amg: True/False, or None for automatic from PRESSURE_AMG_AUTO_MIN_ROWS
+        unknowns (core/piso_simulation.py:2222-2300)."""
+        if which != "P" or self.pressure_use_BiCG or not self._amg_dtype_ok():
+            return False
+        use = self.pressure_use_amg
+        if use is None:
+            d = self.domain
+            rows = d.getTotalSize() * d.getBatchSize()
+            limit = self.PRESSURE_AMG_AUTO_MIN_ROWS if d.getBatchSize() == 1 else self.PRESSURE_AMG_AUTO_MIN_ROWS_BATCHED
+            return rows >= limit
+        return bool(use)
+
+    def _amg_options(self, which: str) -> dict:
+        return self._pressure_amg_options
+
+    def _amg_for(self, which: str, A32: torch.Tensor):
+        from .amg import hierarchy_for
+
+        d = self.domain
+        return hierarchy_for(d, which, A32, d._matrix_version(which), self._amg_cache, self._amg_options(which))
 
     def collect_solves(self, raise_on_failure: bool = True) -> bool:
         """Read the outcomes of the solves launched since the last call (synchronises)."""

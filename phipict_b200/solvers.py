@@ -91,8 +91,10 @@ class StencilSolver:
         self._keep = None
 
     def solve(self, A: torch.Tensor, b: torch.Tensor, x: torch.Tensor, tol, maxit: int,
-              return_best: bool = False, use_graph: bool | None = None) -> None:
-        """Launch the solve of ``A x = b`` (x: initial guess, overwritten). Asynchronous."""
+              return_best: bool = False, use_graph: bool | None = None, amg=None) -> None:
+        """Launch the solve of ``A x = b`` (x: initial guess, overwritten). Asynchronous.
+        ``amg``: an :class:`~phipict_b200.amg.AmgHierarchy` set up for ``A`` (float32 CG
+        with one right-hand side) preconditions every iteration with one V-cycle."""
         d = self.domain
         if A.dtype != self.dtype or b.dtype != self.dtype or x.dtype != self.dtype:
             raise TypeError("matrix, right-hand side and solution must share the solver dtype")
@@ -110,6 +112,8 @@ class StencilSolver:
         s.tol, self._keep = to_device_tolerance(tol, d.getDtype(), nsys, d.getDevice())
         s.A, s.b, s.x = A.data_ptr(), b.data_ptr(), x.data_ptr()
         s.work, s.state = self.work.data_ptr(), self.state.data_ptr()
+        s.amg = amg.address() if amg is not None else None
+        self._amg = amg
         _lib.call("phb_solve_run", ct.byref(d.desc()), ct.byref(s), _lib.stream_ptr(d.getDevice()))
 
     def results(self) -> list[LinearSolverResultInfo]:
@@ -142,7 +146,9 @@ class RefinedSolver:
         self.outer_used = 0
 
     def solve(self, A64: torch.Tensor, A32: torch.Tensor, b: torch.Tensor, x: torch.Tensor, tol, maxit: int,
-              fetch: bool = False) -> list[LinearSolverResultInfo] | None:
+              fetch: bool = False, amg=None) -> list[LinearSolverResultInfo] | None:
+        """Launch the refined solve; ``amg`` (a hierarchy set up for ``A32``) preconditions
+        the inner CG."""
         d = self.domain
         r = self._r
         r.kind = self.kind
@@ -155,6 +161,8 @@ class RefinedSolver:
         r.tol, self._keep = to_device_tolerance(tol, torch.float64, nsys, d.getDevice())
         r.A64, r.A32, r.b, r.x = A64.data_ptr(), A32.data_ptr(), b.data_ptr(), x.data_ptr()
         r.work, r.state = self.work.data_ptr(), self.state.data_ptr()
+        r.amg = amg.address() if amg is not None else None
+        self._amg = amg
         if not fetch:
             _lib.call("phb_refine_run", ct.byref(d.desc()), ct.byref(r), None, None, _lib.stream_ptr(d.getDevice()))
             return None
