@@ -213,6 +213,8 @@ def run_ours(args, rank, world, local):
     mixed = not args.plain_fp64
     amg = mixed and not args.no_amg
     dom, sim = build_sim(wl, device, mixed, amg)
+    if args.inner_rtol:
+        sim.refinement_inner_rtol = args.inner_rtol
     cells = dom.getTotalSize()
     stream = torch.cuda.current_stream(device)
     for _ in range(args.warmup):
@@ -247,8 +249,14 @@ def run_ours(args, rank, world, local):
     ms = max_over_ranks(ms, world)
     # solver statistics of the timed steps
     solve_ms = 0.0
-    for a, b in sim._solve_events:
-        solve_ms += a.elapsed_time(b)
+    per_tag: dict = {}
+    for a, b, tag in sim._solve_events:
+        t = a.elapsed_time(b)
+        solve_ms += t
+        per_tag[tag] = per_tag.get(tag, 0.0) + t / args.steps
+    tag_its: dict = {}
+    for tag, lst in infos:
+        tag_its[tag] = tag_its.get(tag, 0) + sum(i.innerIterations if mixed else i.usedIterations for i in lst) / args.steps
     inner_its = sum(i.innerIterations if mixed else i.usedIterations for _, lst in infos for i in lst)
     sweeps = sum(i.usedIterations for _, lst in infos for i in lst) if mixed else 0
     sim._solve_events = None
@@ -313,7 +321,9 @@ def run_ours(args, rank, world, local):
                   "iterations": inner_its, "solve_ms": round(solve_ms, 3)},
         gpu_launches=int(gpu_launches),
         solver={"inner_iterations_per_step": round(inner_its / args.steps, 1),
-                "refinement_sweeps_per_step": round(sweeps / args.steps, 2)},
+                "refinement_sweeps_per_step": round(sweeps / args.steps, 2),
+                "ms_per_step_by_solve": {k: round(v, 3) for k, v in per_tag.items()},
+                "iterations_per_step_by_solve": {k: round(v, 1) for k, v in tag_its.items()}},
     )
 
 
@@ -369,6 +379,7 @@ def main():
     ap.add_argument("--plain-fp64", action="store_true", help="the plain float64 path (no refinement)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-amg", action="store_true", help="unpreconditioned CG for pressure and potential")
+    ap.add_argument("--inner-rtol", type=float, default=None, help="inner FP32 reduction per refinement sweep")
     args = ap.parse_args()
     rank, world, local = dist_setup(args)
     if args.impl == "reference":

@@ -170,7 +170,10 @@ typedef struct phb_amg {
 	int32_t nlevels;      /* 2..PHB_AMG_MAX_LEVELS */
 	int32_t coarse_n;     /* row stride of the coarsest inverses, >= cells of any instance (<= 1024) */
 	float omega;          /* damping of the Jacobi sweeps */
-	float coarse_scale;   /* factor on every Galerkin product (0.5: rediscretisation scaling) */
+	float coarse_scale;   /* factor on every Galerkin product (1: plain Galerkin) */
+	int32_t tail_level;   /* levels from this one down are cycled by one CTA per instance
+	                         (1..nlevels-1; 0: the coarse solve alone) */
+	int32_t pad;
 	double *coarse_inv;   /* [ninst][coarse_n][coarse_n], written by phb_amg_setup */
 	phb_amg_level levels[PHB_AMG_MAX_LEVELS];
 } phb_amg;

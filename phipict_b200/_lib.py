@@ -91,7 +91,7 @@ class PhbAmgLevel(ct.Structure):
 class PhbAmg(ct.Structure):
     _fields_ = [
         ("nlevels", ct.c_int32), ("coarse_n", ct.c_int32), ("omega", ct.c_float), ("coarse_scale", ct.c_float),
-        ("coarse_inv", ct.c_void_p),
+        ("tail_level", ct.c_int32), ("pad", ct.c_int32), ("coarse_inv", ct.c_void_p),
         ("levels", PhbAmgLevel * AMG_MAX_LEVELS),
     ]
 

@@ -30,7 +30,14 @@ import torch
 
 from . import _lib
 
-DEFAULT_OPTIONS = {"omega": 0.8, "coarse_scale": 0.5, "coarse_cells": 128, "max_levels": _lib.AMG_MAX_LEVELS}
+# omega 0.8 and the unscaled Galerkin product gave the fewest iterations on the graded
+# 3D duct's pressure and potential systems (omega 1 is not a convergent Jacobi smoother,
+# scaled coarse operators over-correct on the deeper levels)
+# tail_cells: levels with at most this many cells per instance are cycled by one CTA per
+# instance instead of grid-wide phases; off by default (0): one CTA is slower than a
+# grid-wide phase plus its barrier unless many instances run their tails side by side
+DEFAULT_OPTIONS = {"omega": 0.8, "coarse_scale": 1.0, "coarse_cells": 128, "max_levels": _lib.AMG_MAX_LEVELS,
+                   "tail_cells": 0}
 MAX_COARSE_CELLS = 1024  # largest dense coarsest operator per instance (phb_amg::coarse_n)
 
 
@@ -115,6 +122,16 @@ class AmgHierarchy:
         s.coarse_n = cn
         s.omega = float(opts["omega"])
         s.coarse_scale = float(opts["coarse_scale"])
+        # the small levels (at most tail_cells cells per instance) are cycled by one CTA per
+        # instance; level 0 never is
+        inst_max = [int(r[2][:, 1].max()) for r in records]
+        tail = len(records) - 1
+        while tail > 1 and inst_max[tail - 1] <= int(opts["tail_cells"]):
+            tail -= 1
+        if int(opts["tail_cells"]) <= 0:
+            tail = 0
+        s.tail_level = tail
+        self.tail_level = tail
         ninst = insts.shape[0]
         self.coarse_inv = torch.zeros(ninst * cn * cn, dtype=torch.float64, device=dev)
         s.coarse_inv = self.coarse_inv.data_ptr()

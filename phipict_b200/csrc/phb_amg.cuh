@@ -6,8 +6,8 @@
 // levels. Here every level stays a structured multi-block stencil: a coarse cell
 // aggregates up to 2^d cells of one block (2 per axis, 1 at an odd end), the coarse blocks
 // keep the topology of the fine ones (periodic and connected faces), and the coarse operator
-// is the Galerkin product P^T A P with piecewise-constant P, scaled per coarsening (a scale
-// of 0.5 turns it into the rediscretised operator). Neighbours come from the same index
+// is the Galerkin product P^T A P with piecewise-constant P (optionally scaled per coarsening;
+// 0.5 would give the rediscretised operator). Neighbours come from the same index
 // arithmetic on every level; there are no column indices. The coarsest level is solved with
 // a dense inverse per instance, as phiPICT's coarse pseudo-inverse (solvers/amg.py:579-585).
 //
@@ -38,6 +38,7 @@ struct AmgView {
 	float *x[AMG_MAX_LEVELS];
 	const double *inv;
 	int cn, nlevels;
+	int tail; // first level of the single-CTA tail (nlevels-1: the coarse solve alone)
 	float omega;
 };
 
@@ -56,6 +57,7 @@ __host__ inline AmgView<D> makeAmgView(const phb_amg &a, const float *r, float *
 	v.inv = a.coarse_inv;
 	v.cn = a.coarse_n;
 	v.nlevels = a.nlevels;
+	v.tail = (a.tail_level >= 1 && a.tail_level < a.nlevels) ? a.tail_level : a.nlevels - 1;
 	v.omega = a.omega;
 	return v;
 }
@@ -101,22 +103,17 @@ template <int D> struct Restrict {
 	static constexpr int PER_TILE = PHB_TILE_CELLS / CELLS; // CTAs per coarse tile
 };
 
-// Restriction for coarse sub-tile `sub` of level l+1: b_{l+1} = P^T (b_l - A_l omega D^-1 b_l).
-// Level vectors are read with plain loads: in the persistent solver other CTAs wrote them
-// earlier in the same launch.
+// One part (Restrict::CELLS coarse cells) of a coarse tile whose block `bi` (nc cells, tile
+// starting at l0) is staged in sB.
 template <int D>
-__device__ __forceinline__ void amgRestrictSub(const AmgView<D> &mg, int l, int sub, int32_t *sB) {
+__device__ __forceinline__ void amgRestrictPart(const AmgView<D> &mg, int l, int bi, int l0, int nc, int part, const int32_t *sB) {
 	using R = Restrict<D>;
-	const Dom<float, D> &fd = mg.lv[l], &cd = mg.lv[l + 1];
+	const Dom<float, D> &fd = mg.lv[l];
 	const float *A = mg.A[l];
 	const float *wd = mg.wd[l];
 	const float *b = mg.b[l];
 	float *bc = mg.b[l + 1];
 	const float w = mg.omega;
-	const int tile = sub / R::PER_TILE, part = sub - tile * R::PER_TILE;
-	const int bi = __ldg(cd.tiles + 2 * tile);
-	const int l0 = __ldg(cd.tiles + 2 * tile + 1);
-	const int nc = stageBlock<D>(cd, bi, sB);
 	const int32_t *FB = fd.blk(bi);
 	const int64_t N = fd.ncells;
 	const int lc = l0 + part * R::CELLS + int(threadIdx.x) / R::G; // coarse cell of the block
@@ -154,6 +151,26 @@ __device__ __forceinline__ void amgRestrictSub(const AmgView<D> &mg, int l, int 
 #pragma unroll
 	for (int m = 1; m < R::G; m <<= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
 	if (cvalid && o == 0) bc[sB[B_CELLOFF] + lc] = v;
+}
+
+// parts of coarse tile (l0, nc) that hold cells
+template <int D>
+__device__ __forceinline__ int restrictParts(int l0, int nc) {
+	const int cells = min(PHB_TILE_CELLS, nc - l0);
+	return (cells + Restrict<D>::CELLS - 1) / Restrict<D>::CELLS;
+}
+
+// Restriction for coarse sub-tile `sub` (part sub % PER_TILE of tile sub / PER_TILE) of level
+// l+1: b_{l+1} = P^T (b_l - A_l omega D^-1 b_l). Level vectors are read with plain loads: in
+// the persistent solver other CTAs wrote them earlier in the same launch.
+template <int D>
+__device__ __forceinline__ void amgRestrictSub(const AmgView<D> &mg, int l, int sub, int32_t *sB) {
+	const Dom<float, D> &cd = mg.lv[l + 1];
+	const int tile = sub / Restrict<D>::PER_TILE, part = sub - tile * Restrict<D>::PER_TILE;
+	const int bi = __ldg(cd.tiles + 2 * tile);
+	const int l0 = __ldg(cd.tiles + 2 * tile + 1);
+	const int nc = stageBlock<D>(cd, bi, sB);
+	if (part < restrictParts<D>(l0, nc)) amgRestrictPart<D>(mg, l, bi, l0, nc, part, sB);
 }
 
 // Prolongation and post-smoothing for fine tile `tile` of level l (l < nlevels-1), cells
@@ -213,15 +230,15 @@ __device__ __forceinline__ double amgProlongTile(const AmgView<D> &mg, int l, in
 // Coarsest level: x = inverse * b per instance, one warp per row; rows are dealt out to
 // warps `warp`, `warp + nwarps`, ...
 template <int D>
-__device__ __forceinline__ void amgCoarseRows(const AmgView<D> &mg, int warp, int nwarps) {
+__device__ __forceinline__ void amgCoarseRows(const AmgView<D> &mg, int warp, int nwarps, int row0 = 0, int row1 = -1) {
 	const int L = mg.nlevels - 1;
 	const Dom<float, D> &cd = mg.lv[L];
 	const int lane = threadIdx.x & 31;
 	const int cn = mg.cn;
 	const float *b = mg.b[L];
 	float *x = mg.x[L];
-	const int rows = cd.ninst * cn;
-	for (int row = warp; row < rows; row += nwarps) {
+	const int rows = row1 < 0 ? cd.ninst * cn : row1;
+	for (int row = row0 + warp; row < rows; row += nwarps) {
 		const int inst = row / cn, r = row - inst * cn;
 		const int off = __ldg(cd.insts + inst * PHB_IREC + I_CELLOFF);
 		const int n = min(cn, __ldg(cd.insts + inst * PHB_IREC + I_NCELLS));
@@ -258,16 +275,59 @@ __global__ void __launch_bounds__(PHB_TILE) kAmgCoarse(AmgView<D> mg) {
 	amgCoarseRows<D>(mg, int(blockIdx.x * (PHB_TILE / 32) + (threadIdx.x >> 5)), int(gridDim.x * (PHB_TILE / 32)));
 }
 
+// The tail of the cycle: the levels from `first` down are small (the host picks `first` so
+// that they hold at most about a thousand cells per instance), and coarse levels never mix
+// instances, so one CTA runs an instance's whole sub-cycle below level `first` (restrictions,
+// coarse solve, prolongations) with CTA barriers instead of grid-wide phases. b_first must be
+// in place; x_first is written.
+
+template <int D>
+__device__ __forceinline__ void amgTail(const AmgView<D> &mg, int first, int inst, int32_t *sB) {
+	const int L = mg.nlevels;
+	for (int l = first; l + 1 < L; ++l) {
+		const Dom<float, D> &cd = mg.lv[l + 1];
+		const int32_t *rec = cd.insts + inst * PHB_IREC;
+		const int t0 = __ldg(rec + I_TILESTART), tc = __ldg(rec + I_TILECOUNT);
+		for (int tile = t0; tile < t0 + tc; ++tile) {
+			const int bi = __ldg(cd.tiles + 2 * tile);
+			const int l0 = __ldg(cd.tiles + 2 * tile + 1);
+			const int nc = stageBlock<D>(cd, bi, sB);
+			const int parts = restrictParts<D>(l0, nc);
+			for (int part = 0; part < parts; ++part) amgRestrictPart<D>(mg, l, bi, l0, nc, part, sB);
+		}
+		__syncthreads();
+	}
+	amgCoarseRows<D>(mg, int(threadIdx.x >> 5), int(blockDim.x >> 5), inst * mg.cn, (inst + 1) * mg.cn);
+	__syncthreads();
+	for (int l = L - 2; l >= first; --l) {
+		const int32_t *rec = mg.lv[l].insts + inst * PHB_IREC;
+		const int t0 = __ldg(rec + I_TILESTART), tc = __ldg(rec + I_TILECOUNT);
+		for (int tile = t0; tile < t0 + tc; ++tile) amgProlongTile<D>(mg, l, tile, sB, mg.x[l]);
+		__syncthreads();
+	}
+}
+
+template <int D>
+__global__ void __launch_bounds__(PHB_TILE) kAmgTail(AmgView<D> mg, int first) {
+	__shared__ int32_t sB[PHB_BREC];
+	amgTail<D>(mg, first, blockIdx.x, sB);
+}
+
 // Launch the cycle down to the coarsest level and back up to level `stop` (0: the whole
 // cycle; 1: the caller runs level 0's prolongation itself).
 template <int D>
 __host__ inline cudaError_t launchAmgCycle(const AmgView<D> &mg, cudaStream_t s, int stop) {
 	const int L = mg.nlevels;
-	for (int l = 0; l + 1 < L; ++l) kAmgRestrict<D><<<mg.lv[l + 1].ntiles * Restrict<D>::PER_TILE, PHB_TILE, 0, s>>>(mg, l);
-	const int rows = mg.lv[L - 1].ninst * mg.cn;
-	const int warpsPerCta = PHB_TILE / 32;
-	kAmgCoarse<D><<<(rows + warpsPerCta - 1) / warpsPerCta, PHB_TILE, 0, s>>>(mg);
-	for (int l = L - 2; l >= stop; --l) kAmgProlong<D><<<mg.lv[l].ntiles * AMG_SUBTILES, PHB_TILE, 0, s>>>(mg, l);
+	const int tail = mg.tail;
+	for (int l = 0; l < tail; ++l) kAmgRestrict<D><<<mg.lv[l + 1].ntiles * Restrict<D>::PER_TILE, PHB_TILE, 0, s>>>(mg, l);
+	if (tail == L - 1) {
+		const int rows = mg.lv[L - 1].ninst * mg.cn;
+		const int warpsPerCta = PHB_TILE / 32;
+		kAmgCoarse<D><<<(rows + warpsPerCta - 1) / warpsPerCta, PHB_TILE, 0, s>>>(mg);
+	} else {
+		kAmgTail<D><<<mg.lv[tail].ninst, PHB_TILE, 0, s>>>(mg, tail);
+	}
+	for (int l = tail - 1; l >= stop; --l) kAmgProlong<D><<<mg.lv[l].ntiles * AMG_SUBTILES, PHB_TILE, 0, s>>>(mg, l);
 	return cudaGetLastError();
 }
 

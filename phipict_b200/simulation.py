@@ -120,6 +120,8 @@ class Simulation:
         self.differentiable = False
         self.linear_solve_max_iterations = 5000
         self.mixed_precision = bool(mixed_precision)
+        # mixed precision: each inner FP32 solve reduces the outer residual by this factor
+        self.refinement_inner_rtol = 1e-4
         self.check_solves = check_solves
         self.total_step = 0
         self.total_time = 0.0
@@ -178,7 +180,7 @@ class Simulation:
         kind = BICGSTAB if use_BiCG else CG
         ev = None
         if self._solve_events is not None:
-            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True), tag)
             ev[0].record()
             self._solve_events.append(ev)
         self._solve_launch(which, rhs, x, kind, tol, tag, nrhs, return_best, maxit)
@@ -192,6 +194,7 @@ class Simulation:
             lo = backend._lo(d, which)
             amg = self._amg_for(which, lo) if pc else None
             r = refiner_for(d, kind, nrhs, tag=tag)
+            r.inner_rtol = self.refinement_inner_rtol
             r.solve(d._stencil(which), lo, rhs, x, tol, maxit, amg=amg)
             self._pending.append((tag, r))
         else:
