@@ -154,10 +154,13 @@ typedef struct phb_tolerance {
  * Every level is a multi-block stencil grid: level l+1 halves each block of level l along
  * every axis longer than one cell (ceil), keeps the block topology, and its operator is the
  * Galerkin product P^T A_l P with piecewise-constant P, times coarse_scale. The coarsest
- * level is solved with a dense generalised inverse per instance (FP64). The host builds the
- * level descriptors and buffers; phb_amg_setup fills the coarse operators from levels[0].A
- * on the device. One V-cycle: a damped Jacobi sweep from zero, restriction, the coarse
- * cycle, prolongation, a damped Jacobi sweep: symmetric, so it can precondition CG. */
+ * level is solved with a dense generalised inverse per instance (FP64), and the whole cycle
+ * below a small level T (at most 1024 cells per instance) is folded into one dense operator
+ * C_T = S~ + W C_{T+1} W^T (W = (I - S A) P, S = omega D^-1, S~ = 2S - S A S), so that a
+ * cycle reaches level T and applies C_T in one step. The host builds the level descriptors
+ * and buffers; phb_amg_setup fills the coarse operators from levels[0].A on the device. One
+ * V-cycle: a damped Jacobi sweep from zero, restriction, the coarse cycle, prolongation, a
+ * damped Jacobi sweep: symmetric, so it can precondition CG. */
 #define PHB_AMG_MAX_LEVELS 12
 typedef struct phb_amg_level {
 	phb_domain dom;       /* blocks, tiles, insts of the level (level 0: the domain's own) */
@@ -165,18 +168,25 @@ typedef struct phb_amg_level {
 	float *b;             /* restricted residual [ncells] (levels >= 1) */
 	float *x;             /* correction [ncells] (levels >= 1); level 0: z of phb_amg_vcycle */
 	float *wdinv;         /* omega / diagonal [ncells], written by phb_amg_setup */
+	int32_t inst_cells;   /* cells of the largest instance on this level */
+	int32_t pad;
 } phb_amg_level;
 typedef struct phb_amg {
 	int32_t nlevels;      /* 2..PHB_AMG_MAX_LEVELS */
 	int32_t coarse_n;     /* row stride of the coarsest inverses, >= cells of any instance (<= 1024) */
 	float omega;          /* damping of the Jacobi sweeps */
 	float coarse_scale;   /* factor on every Galerkin product (1: plain Galerkin) */
-	int32_t tail_level;   /* levels from this one down are cycled by one CTA per instance
-	                         (1..nlevels-1; 0: the coarse solve alone) */
+	int32_t tail_level;   /* T: the cycle below level T is applied as one dense operator per
+	                         instance (1..nlevels-1; 0 means nlevels-1: the coarsest inverse) */
 	int32_t pad;
-	double *coarse_inv;   /* [ninst][coarse_n][coarse_n], written by phb_amg_setup */
+	double *coarse_inv;   /* [ninst][coarse_n][coarse_n]: the dense operator of level T,
+	                         coarse_n >= levels[T].inst_cells; written by phb_amg_setup */
+	double *work;         /* setup scratch of phb_amg_work_doubles() doubles */
+	int64_t work_doubles;
 	phb_amg_level levels[PHB_AMG_MAX_LEVELS];
 } phb_amg;
+/* Doubles of setup scratch a hierarchy needs (the dense operators of levels T..nlevels-1). */
+int64_t phb_amg_work_doubles(const phb_amg *amg);
 /* Galerkin products of levels 1.., dense coarsest operators and their inverses. */
 int phb_amg_setup(const phb_amg *amg, phb_stream stream);
 /* z = one V-cycle applied to r (both [ncells] of level 0, float32). */

@@ -31,7 +31,7 @@ EXPORTS = (
     "phb_solve_work_bytes", "phb_solve_state_bytes", "phb_solve_run", "phb_solve_results",
     "phb_release_graphs", "phb_refine_work_bytes", "phb_refine_run", "phb_refine_results",
     "phb_cg_noalloc_bytes", "phb_cg_solve_noalloc",
-    "phb_amg_setup", "phb_amg_vcycle",
+    "phb_amg_setup", "phb_amg_vcycle", "phb_amg_work_doubles",
 )
 
 
@@ -85,13 +85,15 @@ class PhbRefine(ct.Structure):
 
 
 class PhbAmgLevel(ct.Structure):
-    _fields_ = [("dom", PhbDomain), ("A", ct.c_void_p), ("b", ct.c_void_p), ("x", ct.c_void_p), ("wdinv", ct.c_void_p)]
+    _fields_ = [("dom", PhbDomain), ("A", ct.c_void_p), ("b", ct.c_void_p), ("x", ct.c_void_p), ("wdinv", ct.c_void_p),
+                ("inst_cells", ct.c_int32), ("pad", ct.c_int32)]
 
 
 class PhbAmg(ct.Structure):
     _fields_ = [
         ("nlevels", ct.c_int32), ("coarse_n", ct.c_int32), ("omega", ct.c_float), ("coarse_scale", ct.c_float),
         ("tail_level", ct.c_int32), ("pad", ct.c_int32), ("coarse_inv", ct.c_void_p),
+        ("work", ct.c_void_p), ("work_doubles", ct.c_int64),
         ("levels", PhbAmgLevel * AMG_MAX_LEVELS),
     ]
 
@@ -154,6 +156,7 @@ def load() -> ct.CDLL:
         "phb_solve_state_bytes": [DP, I],
         "phb_refine_work_bytes": [DP, I, I],
         "phb_cg_noalloc_bytes": [DP, I, I],
+        "phb_amg_work_doubles": [ct.POINTER(PhbAmg)],
     }.items():
         f = getattr(lib, name)
         f.argtypes = args

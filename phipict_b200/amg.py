@@ -33,11 +33,12 @@ from . import _lib
 # omega 0.8 and the unscaled Galerkin product gave the fewest iterations on the graded
 # 3D duct's pressure and potential systems (omega 1 is not a convergent Jacobi smoother,
 # scaled coarse operators over-correct on the deeper levels)
-# tail_cells: levels with at most this many cells per instance are cycled by one CTA per
-# instance instead of grid-wide phases; off by default (0): one CTA is slower than a
-# grid-wide phase plus its barrier unless many instances run their tails side by side
+# dense_cells / dense_bytes: the cycle below the first level with at most dense_cells cells per
+# instance (and dense operators of at most dense_bytes for all instances) is applied as one
+# dense operator, which saves two grid-wide phases per folded level; 0 folds nothing (the
+# cycle runs down to the coarsest inverse)
 DEFAULT_OPTIONS = {"omega": 0.8, "coarse_scale": 1.0, "coarse_cells": 128, "max_levels": _lib.AMG_MAX_LEVELS,
-                   "tail_cells": 0}
+                   "dense_cells": 1024, "dense_bytes": 32 << 20}
 MAX_COARSE_CELLS = 1024  # largest dense coarsest operator per instance (phb_amg::coarse_n)
 
 
@@ -122,17 +123,20 @@ class AmgHierarchy:
         s.coarse_n = cn
         s.omega = float(opts["omega"])
         s.coarse_scale = float(opts["coarse_scale"])
-        # the small levels (at most tail_cells cells per instance) are cycled by one CTA per
-        # instance; level 0 never is
+        # the dense level T: the first small enough one below level 0 (else the coarsest)
         inst_max = [int(r[2][:, 1].max()) for r in records]
-        tail = len(records) - 1
-        while tail > 1 and inst_max[tail - 1] <= int(opts["tail_cells"]):
-            tail -= 1
-        if int(opts["tail_cells"]) <= 0:
-            tail = 0
-        s.tail_level = tail
-        self.tail_level = tail
         ninst = insts.shape[0]
+        T = len(records) - 1
+        if int(opts["dense_cells"]) > 0:
+            for t in range(1, len(records)):
+                n_t = inst_max[t]
+                if n_t <= min(int(opts["dense_cells"]), MAX_COARSE_CELLS) and ninst * n_t * n_t * 8 <= int(opts["dense_bytes"]):
+                    T = t
+                    break
+        s.tail_level = T
+        self.tail_level = T
+        cn = inst_max[T]
+        s.coarse_n = cn
         self.coarse_inv = torch.zeros(ninst * cn * cn, dtype=torch.float64, device=dev)
         s.coarse_inv = self.coarse_inv.data_ptr()
         self._keep: list[torch.Tensor] = []
@@ -144,6 +148,7 @@ class AmgHierarchy:
         self.z = torch.zeros(N0, dtype=torch.float32, device=dev)
         for l, (blk, tiles, ins) in enumerate(records):
             lv = s.levels[l]
+            lv.inst_cells = inst_max[l]
             if l == 0:
                 lv.dom = _lib.PhbDomain.from_buffer_copy(fine)
                 lv.x = self.z.data_ptr()
@@ -178,6 +183,10 @@ class AmgHierarchy:
             lv.A, lv.b, lv.x = A.data_ptr(), b.data_ptr(), x.data_ptr()
         self._struct = s
         self.coarse_n = cn
+        wd = int(_lib.load().phb_amg_work_doubles(ct.byref(s)))
+        self.work = torch.zeros(max(1, wd), dtype=torch.float64, device=dev)
+        s.work = self.work.data_ptr()
+        s.work_doubles = self.work.numel()
         self._fine_blocks = domain._blocks_dev
         self._A0 = None
 

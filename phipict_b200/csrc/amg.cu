@@ -191,6 +191,131 @@ __global__ void __launch_bounds__(INV_THREADS) kInvert(double *dense, int cn, co
 	}
 }
 
+// --- the cycle below a small level as one dense operator --------------------------------
+// One cycle at level l (x0 = S b, restriction, the coarse correction C_{l+1}, prolongation,
+// a second sweep) is the linear map
+//   C_l = S~ + W C_{l+1} W^T,   S = omega D^-1,  S~ = 2S - S A S,  W = (I - S A) P,
+// so the levels below a small level T fold, from the coarsest inverse up, into one dense
+// matrix per instance (FP64, rows and columns indexed by the instance's local cells).
+
+// W [inst][n][nc] = (I - S A) P of level l (zeroed by the caller): the row of cell i holds
+// 1 - wd_i A_ii at its own aggregate and -wd_i A_ij at the aggregate of each neighbour j
+template <int D>
+__global__ void __launch_bounds__(PHB_TILE) kTailW(Dom<float, D> fd, Dom<float, D> cd, const float *__restrict__ A,
+		const float *__restrict__ wd, double *__restrict__ W, int n, int nc) {
+	__shared__ int32_t sB[PHB_BREC];
+	int l0, ncb;
+	loadTile<float, D>(fd, sB, l0, ncb);
+	const int bi = __ldg(fd.tiles + 2 * blockIdx.x);
+	const int32_t *CB = cd.blk(bi);
+	const int64_t N = fd.ncells;
+	for (int j = 0; j < CPT; ++j) {
+		Cell c;
+		if (!cellAt<D>(sB, l0, ncb, j, c)) break;
+		const int inst = sB[B_INST];
+		const int64_t i = c.g - sB[B_INSTOFF];
+		if (i >= n) continue;
+		const int coff = CB[B_INSTOFF];
+		double *row = W + ((size_t)inst * n + i) * nc;
+		const double wi = wd[c.g];
+		const int64_t ai = coarseCell<D>(CB, sB, c.p) - coff;
+		if (ai < nc) row[ai] += 1.0 - wi * A[c.g];
+#pragma unroll
+		for (int f = 0; f < 2 * D; ++f) {
+			if (atBound(sB, f, c.p) && fType(sB, f) == FT_FIXED) continue;
+			const Nbr nb = neighbor<float, D>(fd, c, f);
+			const int32_t *nCB = nb.B == sB ? CB : cd.blk(int((nb.B - fd.blocks) / PHB_BREC));
+			const int64_t aj = coarseCell<D>(nCB, nb.B, nb.p) - coff;
+			if (aj < nc) row[aj] -= wi * A[(f + 1) * N + c.g];
+		}
+	}
+}
+
+// C [inst][n][n] += S~ of level l: 2 wd_i - wd_i A_ii wd_i on the diagonal, -wd_i A_ij wd_j
+// at each neighbour j
+template <int D>
+__global__ void __launch_bounds__(PHB_TILE) kTailSbar(Dom<float, D> fd, const float *__restrict__ A, const float *__restrict__ wd,
+		double *__restrict__ C, int n) {
+	__shared__ int32_t sB[PHB_BREC];
+	int l0, ncb;
+	loadTile<float, D>(fd, sB, l0, ncb);
+	const int64_t N = fd.ncells;
+	for (int j = 0; j < CPT; ++j) {
+		Cell c;
+		if (!cellAt<D>(sB, l0, ncb, j, c)) break;
+		const int inst = sB[B_INST];
+		const int off = sB[B_INSTOFF];
+		const int64_t i = c.g - off;
+		if (i >= n) continue;
+		double *row = C + ((size_t)inst * n + i) * n;
+		const double wi = wd[c.g];
+		row[i] += 2.0 * wi - wi * A[c.g] * wi;
+#pragma unroll
+		for (int f = 0; f < 2 * D; ++f) {
+			const int64_t nb = neighborIndex<float, D>(fd, c, f);
+			if (nb >= 0 && nb - off < n) row[nb - off] -= wi * A[(f + 1) * N + c.g] * double(wd[nb]);
+		}
+	}
+}
+
+// Batched C = A op(B) over instances (blockIdx.z): A [m][k], op(B) [k][n] (TB: B stored
+// [n][k]), C [m][n], each instance's matrices `stride*` apart. Setup only, FP64.
+constexpr int GT = 16;
+template <bool TB>
+__global__ void __launch_bounds__(GT * GT) kGemm(int m, int n, int k, const double *__restrict__ A, size_t sA,
+		const double *__restrict__ B, size_t sB, double *__restrict__ C, size_t sC) {
+	__shared__ double As[GT][GT + 1], Bs[GT][GT + 1];
+	const int tx = threadIdx.x % GT, ty = threadIdx.x / GT;
+	const int row = blockIdx.y * GT + ty, col = blockIdx.x * GT + tx;
+	const double *Ai = A + blockIdx.z * sA;
+	const double *Bi = B + blockIdx.z * sB;
+	double acc = 0;
+	for (int kk = 0; kk < k; kk += GT) {
+		As[ty][tx] = (row < m && kk + tx < k) ? Ai[(size_t)row * k + kk + tx] : 0.0;
+		const int bk = kk + ty;
+		if (TB) Bs[ty][tx] = (bk < k && col < n) ? Bi[(size_t)col * k + bk] : 0.0;
+		else Bs[ty][tx] = (bk < k && col < n) ? Bi[(size_t)bk * n + col] : 0.0;
+		__syncthreads();
+#pragma unroll
+		for (int t = 0; t < GT; ++t) acc += As[ty][t] * Bs[t][tx];
+		__syncthreads();
+	}
+	if (row < m && col < n) C[blockIdx.z * sC + (size_t)row * n + col] = acc;
+}
+
+static int gemm(bool tb, int ninst, int m, int n, int k, const double *A, const double *B, double *C, cudaStream_t s) {
+	dim3 grid((n + GT - 1) / GT, (m + GT - 1) / GT, ninst);
+	if (tb) kGemm<true><<<grid, GT * GT, 0, s>>>(m, n, k, A, (size_t)m * k, B, (size_t)n * k, C, (size_t)m * n);
+	else kGemm<false><<<grid, GT * GT, 0, s>>>(m, n, k, A, (size_t)m * k, B, (size_t)k * n, C, (size_t)m * n);
+	return checkLaunch("kGemm");
+}
+
+static int tailLevel(const phb_amg *amg) {
+	return (amg->tail_level >= 1 && amg->tail_level < amg->nlevels) ? amg->tail_level : amg->nlevels - 1;
+}
+
+// rows of the dense operator of level l >= T per instance (level T: the coarse_n stride)
+static int denseN(const phb_amg *amg, int l) { return l == tailLevel(amg) ? amg->coarse_n : amg->levels[l].inst_cells; }
+
+// dense operator buffers: the coarsest inverse and the folded levels above it are built in
+// `work` ([C_a | C_b | W | Tmp], each sized for the largest level) and the last one, C_T,
+// in coarse_inv
+static void tailSizes(const phb_amg *amg, int64_t &cmax, int64_t &wmax) {
+	const int T = tailLevel(amg), L = amg->nlevels;
+	cmax = 0;
+	wmax = 0;
+	for (int l = T; l < L; ++l) {
+		const int64_t n = denseN(amg, l);
+		cmax = std::max(cmax, n * n);
+		if (l + 1 < L) wmax = std::max(wmax, n * (int64_t)denseN(amg, l + 1));
+	}
+}
+static int64_t tailWorkDoubles(const phb_amg *amg) {
+	int64_t c, w;
+	tailSizes(amg, c, w);
+	return (int64_t)amg->levels[0].dom.ninst * (2 * c + 2 * w);
+}
+
 template <int D>
 static int setup(const phb_amg *amg, cudaStream_t s) {
 	const int L = amg->nlevels;
@@ -208,13 +333,17 @@ static int setup(const phb_amg *amg, cudaStream_t s) {
 	}
 	int rc = checkLaunch("kWdinv");
 	if (rc) return rc;
+	// the coarsest inverse (into coarse_inv when it is the last level of the cycle)
+	const int T = tailLevel(amg);
+	const int ninst = amg->levels[0].dom.ninst;
 	const phb_amg_level &C = amg->levels[L - 1];
-	const int cn = amg->coarse_n;
-	PHB_CUDA(cudaMemsetAsync(amg->coarse_inv, 0, sizeof(double) * (size_t)C.dom.ninst * cn * cn, s));
-	if (C.dom.ntiles) kDense<D><<<C.dom.ntiles, PHB_TILE, 0, s>>>(Dom<float, D>(C.dom), C.A, cn, amg->coarse_inv);
+	const int nL = denseN(amg, L - 1);
+	double *cur = T == L - 1 ? amg->coarse_inv : amg->work;
+	PHB_CUDA(cudaMemsetAsync(cur, 0, sizeof(double) * (size_t)ninst * nL * nL, s));
+	if (C.dom.ntiles) kDense<D><<<C.dom.ntiles, PHB_TILE, 0, s>>>(Dom<float, D>(C.dom), C.A, nL, cur);
 	rc = checkLaunch("kDense");
 	if (rc) return rc;
-	const size_t smem = (size_t)cn * cn * sizeof(double);
+	const size_t smem = (size_t)nL * nL * sizeof(double);
 	if (smem <= INV_SMEM_MAX) {
 		static int configured[64] = {0};
 		int dev = 0;
@@ -223,11 +352,37 @@ static int setup(const phb_amg *amg, cudaStream_t s) {
 			PHB_CUDA(cudaFuncSetAttribute(kInvert<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INV_SMEM_MAX));
 			configured[dev] = 1;
 		}
-		kInvert<true><<<C.dom.ninst, INV_THREADS, smem, s>>>(amg->coarse_inv, cn, C.dom.insts);
+		kInvert<true><<<ninst, INV_THREADS, smem, s>>>(cur, nL, C.dom.insts);
 	} else {
-		kInvert<false><<<C.dom.ninst, INV_THREADS, 0, s>>>(amg->coarse_inv, cn, C.dom.insts);
+		kInvert<false><<<ninst, INV_THREADS, 0, s>>>(cur, nL, C.dom.insts);
 	}
-	return checkLaunch("kInvert");
+	rc = checkLaunch("kInvert");
+	if (rc) return rc;
+	// fold the levels above it: C_l = S~_l + W_l C_{l+1} W_l^T, down to level T
+	int64_t cmax, wmax;
+	tailSizes(amg, cmax, wmax);
+	double *bufA = amg->work, *bufB = amg->work + ninst * cmax;
+	double *W = amg->work + 2 * ninst * cmax, *Tm = W + ninst * wmax;
+	int ncur = nL;
+	for (int l = L - 2; l >= T; --l) {
+		const phb_amg_level &F = amg->levels[l], &G = amg->levels[l + 1];
+		const int n = denseN(amg, l);
+		double *next = l == T ? amg->coarse_inv : (cur == bufA ? bufB : bufA);
+		PHB_CUDA(cudaMemsetAsync(W, 0, sizeof(double) * (size_t)ninst * n * ncur, s));
+		kTailW<D><<<F.dom.ntiles, PHB_TILE, 0, s>>>(Dom<float, D>(F.dom), Dom<float, D>(G.dom), F.A, F.wdinv, W, n, ncur);
+		rc = checkLaunch("kTailW");
+		if (rc) return rc;
+		rc = gemm(false, ninst, n, ncur, ncur, W, cur, Tm, s); // Tm = W C_{l+1}
+		if (rc) return rc;
+		rc = gemm(true, ninst, n, n, ncur, Tm, W, next, s);    // C_l = Tm W^T
+		if (rc) return rc;
+		kTailSbar<D><<<F.dom.ntiles, PHB_TILE, 0, s>>>(Dom<float, D>(F.dom), F.A, F.wdinv, next, n);
+		rc = checkLaunch("kTailSbar");
+		if (rc) return rc;
+		cur = next;
+		ncur = n;
+	}
+	return PHB_OK;
 }
 
 } // namespace phb
@@ -248,9 +403,21 @@ int phbCheckAmg(const phb_amg *amg) {
 		if (l > 0 && (!v.b || !v.x)) return setError(PHB_ERR_ARG, "AMG: level vectors missing");
 		if (v.dom.ninst != amg->levels[0].dom.ninst) return setError(PHB_ERR_ARG, "AMG: levels disagree on the instance count");
 	}
-	const phb_amg_level &C = amg->levels[amg->nlevels - 1];
-	if (C.dom.ncells > (int64_t)C.dom.ninst * amg->coarse_n) return setError(PHB_ERR_RANGE, "AMG: coarsest level larger than coarse_n per instance");
+	const int T = tailLevel(amg);
+	for (int l = T; l < amg->nlevels; ++l) {
+		const phb_amg_level &v = amg->levels[l];
+		if (v.inst_cells < 1 || v.inst_cells > INV_MAX || v.dom.ncells > (int64_t)v.dom.ninst * v.inst_cells)
+			return setError(PHB_ERR_RANGE, "AMG: inst_cells of a dense level missing, too small, or above 1024");
+	}
+	if (amg->coarse_n < amg->levels[T].inst_cells) return setError(PHB_ERR_RANGE, "AMG: coarse_n below the cells of an instance on the dense level");
+	if (T < amg->nlevels - 1 && (!amg->work || amg->work_doubles < tailWorkDoubles(amg)))
+		return setError(PHB_ERR_ARG, "AMG: setup work buffer missing or smaller than phb_amg_work_doubles()");
 	return PHB_OK;
+}
+
+extern "C" int64_t phb_amg_work_doubles(const phb_amg *amg) {
+	if (!amg || amg->nlevels < 2 || amg->nlevels > PHB_AMG_MAX_LEVELS) return -1;
+	return tailWorkDoubles(amg);
 }
 
 extern "C" int phb_amg_setup(const phb_amg *amg, phb_stream stream) {

@@ -931,18 +931,14 @@ __global__ void __launch_bounds__(PHB_TILE) kCgPersistent(Dom<double, D> dom, co
 	if constexpr (PC) dsrc = (const T *)mg.x[0];
 	for (int iter = 0; running > 0 && iter <= maxit + 1; ++iter) {
 		if constexpr (PC) {
-			const int L = mg.nlevels, TL = mg.tail;
-			for (int l = 0; l < TL; ++l) {
+			const int L = mg.nlevels;
+			for (int l = 0; l + 1 < L; ++l) {
 				for (int sub = blockIdx.x; sub < mg.lv[l + 1].ntiles * Restrict<D>::PER_TILE; sub += gridDim.x) amgRestrictSub<D>(mg, l, sub, sB);
 				if (!gridBarrier(ctrl, gen)) return;
 			}
-			if (TL == L - 1) {
-				amgCoarseRows<D>(mg, int(blockIdx.x * NWARPS + (threadIdx.x >> 5)), int(gridDim.x * NWARPS));
-			} else {
-				for (int inst = blockIdx.x; inst < mg.lv[TL].ninst; inst += gridDim.x) amgTail<D>(mg, TL, inst, sB);
-			}
+			amgCoarseRows<D>(mg, int(blockIdx.x * NWARPS + (threadIdx.x >> 5)), int(gridDim.x * NWARPS));
 			if (!gridBarrier(ctrl, gen)) return;
-			for (int l = TL - 1; l >= 1; --l) {
+			for (int l = L - 2; l >= 1; --l) {
 				for (int sub = blockIdx.x; sub < mg.lv[l].ntiles * AMG_SUBTILES; sub += gridDim.x) {
 					const int q = sub % AMG_SUBTILES;
 					amgProlongTile<D>(mg, l, sub / AMG_SUBTILES, sB, mg.x[l], q, q + 1);

@@ -36,9 +36,8 @@ struct AmgView {
 	const float *wd[AMG_MAX_LEVELS]; // omega / diagonal
 	float *b[AMG_MAX_LEVELS];
 	float *x[AMG_MAX_LEVELS];
-	const double *inv;
-	int cn, nlevels;
-	int tail; // first level of the single-CTA tail (nlevels-1: the coarse solve alone)
+	const double *inv; // dense operator of the last level of the cycle, per instance
+	int cn, nlevels;   // its row stride; levels of the cycle (the last one dense)
 	float omega;
 };
 
@@ -56,8 +55,8 @@ __host__ inline AmgView<D> makeAmgView(const phb_amg &a, const float *r, float *
 	v.x[0] = z;
 	v.inv = a.coarse_inv;
 	v.cn = a.coarse_n;
-	v.nlevels = a.nlevels;
-	v.tail = (a.tail_level >= 1 && a.tail_level < a.nlevels) ? a.tail_level : a.nlevels - 1;
+	// the cycle ends at level T, whose dense operator stands for everything below it
+	v.nlevels = ((a.tail_level >= 1 && a.tail_level < a.nlevels) ? a.tail_level : a.nlevels - 1) + 1;
 	v.omega = a.omega;
 	return v;
 }
@@ -227,8 +226,9 @@ __device__ __forceinline__ double amgProlongTile(const AmgView<D> &mg, int l, in
 	return dot;
 }
 
-// Coarsest level: x = inverse * b per instance, one warp per row; rows are dealt out to
-// warps `warp`, `warp + nwarps`, ...
+// Last level of the cycle: x = C b per instance with its dense operator C (the coarsest
+// inverse, or the folded cycle below it), one warp per row; rows are dealt out to warps
+// `warp`, `warp + nwarps`, ...
 template <int D>
 __device__ __forceinline__ void amgCoarseRows(const AmgView<D> &mg, int warp, int nwarps, int row0 = 0, int row1 = -1) {
 	const int L = mg.nlevels - 1;
@@ -275,59 +275,16 @@ __global__ void __launch_bounds__(PHB_TILE) kAmgCoarse(AmgView<D> mg) {
 	amgCoarseRows<D>(mg, int(blockIdx.x * (PHB_TILE / 32) + (threadIdx.x >> 5)), int(gridDim.x * (PHB_TILE / 32)));
 }
 
-// The tail of the cycle: the levels from `first` down are small (the host picks `first` so
-// that they hold at most about a thousand cells per instance), and coarse levels never mix
-// instances, so one CTA runs an instance's whole sub-cycle below level `first` (restrictions,
-// coarse solve, prolongations) with CTA barriers instead of grid-wide phases. b_first must be
-// in place; x_first is written.
-
-template <int D>
-__device__ __forceinline__ void amgTail(const AmgView<D> &mg, int first, int inst, int32_t *sB) {
-	const int L = mg.nlevels;
-	for (int l = first; l + 1 < L; ++l) {
-		const Dom<float, D> &cd = mg.lv[l + 1];
-		const int32_t *rec = cd.insts + inst * PHB_IREC;
-		const int t0 = __ldg(rec + I_TILESTART), tc = __ldg(rec + I_TILECOUNT);
-		for (int tile = t0; tile < t0 + tc; ++tile) {
-			const int bi = __ldg(cd.tiles + 2 * tile);
-			const int l0 = __ldg(cd.tiles + 2 * tile + 1);
-			const int nc = stageBlock<D>(cd, bi, sB);
-			const int parts = restrictParts<D>(l0, nc);
-			for (int part = 0; part < parts; ++part) amgRestrictPart<D>(mg, l, bi, l0, nc, part, sB);
-		}
-		__syncthreads();
-	}
-	amgCoarseRows<D>(mg, int(threadIdx.x >> 5), int(blockDim.x >> 5), inst * mg.cn, (inst + 1) * mg.cn);
-	__syncthreads();
-	for (int l = L - 2; l >= first; --l) {
-		const int32_t *rec = mg.lv[l].insts + inst * PHB_IREC;
-		const int t0 = __ldg(rec + I_TILESTART), tc = __ldg(rec + I_TILECOUNT);
-		for (int tile = t0; tile < t0 + tc; ++tile) amgProlongTile<D>(mg, l, tile, sB, mg.x[l]);
-		__syncthreads();
-	}
-}
-
-template <int D>
-__global__ void __launch_bounds__(PHB_TILE) kAmgTail(AmgView<D> mg, int first) {
-	__shared__ int32_t sB[PHB_BREC];
-	amgTail<D>(mg, first, blockIdx.x, sB);
-}
-
 // Launch the cycle down to the coarsest level and back up to level `stop` (0: the whole
 // cycle; 1: the caller runs level 0's prolongation itself).
 template <int D>
 __host__ inline cudaError_t launchAmgCycle(const AmgView<D> &mg, cudaStream_t s, int stop) {
 	const int L = mg.nlevels;
-	const int tail = mg.tail;
-	for (int l = 0; l < tail; ++l) kAmgRestrict<D><<<mg.lv[l + 1].ntiles * Restrict<D>::PER_TILE, PHB_TILE, 0, s>>>(mg, l);
-	if (tail == L - 1) {
-		const int rows = mg.lv[L - 1].ninst * mg.cn;
-		const int warpsPerCta = PHB_TILE / 32;
-		kAmgCoarse<D><<<(rows + warpsPerCta - 1) / warpsPerCta, PHB_TILE, 0, s>>>(mg);
-	} else {
-		kAmgTail<D><<<mg.lv[tail].ninst, PHB_TILE, 0, s>>>(mg, tail);
-	}
-	for (int l = tail - 1; l >= stop; --l) kAmgProlong<D><<<mg.lv[l].ntiles * AMG_SUBTILES, PHB_TILE, 0, s>>>(mg, l);
+	for (int l = 0; l + 1 < L; ++l) kAmgRestrict<D><<<mg.lv[l + 1].ntiles * Restrict<D>::PER_TILE, PHB_TILE, 0, s>>>(mg, l);
+	const int rows = mg.lv[L - 1].ninst * mg.cn;
+	const int warpsPerCta = PHB_TILE / 32;
+	kAmgCoarse<D><<<(rows + warpsPerCta - 1) / warpsPerCta, PHB_TILE, 0, s>>>(mg);
+	for (int l = L - 2; l >= stop; --l) kAmgProlong<D><<<mg.lv[l].ntiles * AMG_SUBTILES, PHB_TILE, 0, s>>>(mg, l);
 	return cudaGetLastError();
 }
 

@@ -85,7 +85,7 @@ def _prolongation(fine, coarse, dims) -> sp.csr_matrix:
 def test_coarse_operators_are_scaled_galerkin_products(cuda, case):
     dom = CASES[case](torch.float32)
     _pressure_system(dom, 3)
-    h = AmgHierarchy(dom, coarse_cells=4)
+    h = AmgHierarchy(dom, coarse_cells=4, dense_cells=0)
     h.setup(dom._P_st)
     torch.cuda.synchronize()
     dims = dom.getSpatialDims()
@@ -105,6 +105,24 @@ def test_coarse_operators_are_scaled_galerkin_products(cuda, case):
     y = np.random.default_rng(0).standard_normal(n)
     rhs = Ac @ y
     assert np.abs(Ac @ (inv @ rhs) - rhs).max() <= 1e-8 * np.abs(rhs).max()
+
+
+@pytest.mark.parametrize("case", ["hartmann2d", "duct3d", "rotated2d"])
+def test_folded_levels_give_the_same_cycle(cuda, case):
+    """The cycle below the dense level T applied as one dense operator equals running it
+    level by level down to the coarsest inverse (float32 roundoff apart)."""
+    dom = {"hartmann2d": lambda: hartmann_2d(64, 48, dtype=torch.float32),
+           "duct3d": lambda: duct_3d(16, 12, 10, 2, dtype=torch.float32),
+           "rotated2d": lambda: rotated_pair_2d(32, dtype=torch.float32)}[case]()
+    _pressure_system(dom, 23)
+    h0 = AmgHierarchy(dom, dense_cells=0)
+    h1 = AmgHierarchy(dom)
+    assert h1.tail_level < h1.nlevels - 1 == h0.tail_level, (h1.sizes, h1.tail_level)
+    h0.setup(dom._P_st)
+    h1.setup(dom._P_st)
+    r = torch.randn(dom.getTotalSize(), generator=torch.Generator().manual_seed(4)).cuda()
+    z0, z1 = h0.vcycle(r).double(), h1.vcycle(r).double()
+    assert float((z0 - z1).abs().max() / z0.abs().max()) < 1e-5
 
 
 @pytest.mark.parametrize("case", ["hartmann2d", "duct3d"])
