@@ -87,11 +87,12 @@ def algorithmic_cg_bytes(dims: int, s_A: int, s_v: int) -> int:
     return (2 * dims + 1) * s_A + 10 * s_v
 
 
-def algorithmic_pcg_bytes(dims: int, levels: list[int]) -> float:
+def algorithmic_pcg_bytes(dims: int, levels: list[int], dense_doubles: int = 0) -> float:
     """Bytes per fine cell of one multigrid-preconditioned float32 CG iteration: the CG
-    passes (algorithmic_cg_bytes with z in place of r in the direction) plus, per level l of
-    n_l cells, the restriction (stencil + b read, coarse b written) and the prolongation
-    with its smoothing sweep (stencil, b and the coarse correction read, z written)."""
+    passes (algorithmic_cg_bytes with z in place of r in the direction) plus, per cycle level
+    l of n_l cells, the restriction (stencil + b read, coarse b written) and the prolongation
+    with its smoothing sweep (stencil, b and the coarse correction read, z written), plus the
+    dense operator of the last cycle level (dense_doubles FP64 values)."""
     st = (2 * dims + 1) * 4
     cyc = 0.0
     for l in range(len(levels) - 1):
@@ -99,7 +100,13 @@ def algorithmic_pcg_bytes(dims: int, levels: list[int]) -> float:
         coarse = levels[l + 1] / levels[0]
         cyc += frac * (st + 4) + coarse * 4          # restriction
         cyc += frac * (st + 4 + 4) + coarse * 4      # prolongation + post-smoothing
-    return algorithmic_cg_bytes(dims, 4, 4) + cyc
+    return algorithmic_cg_bytes(dims, 4, 4) + cyc + 8.0 * dense_doubles / levels[0]
+
+
+# DRAM bytes per preconditioned CG iteration on the duct workload, from the full ncu capture
+# of one persistent launch (25.74 MB read + 0.44 MB written in a 24-iteration inner solve,
+# profiles/kCgPersistent_pcg_duct3d_full.md): the working set is L2-resident
+PCG_DRAM_BYTES_PER_ITERATION_DUCT3D = (25.74e6 + 0.44e6) / 24
 
 
 class ClockSampler:
@@ -286,8 +293,13 @@ def run_ours(args, rank, world, local):
     # mixed; solve time / inner iterations (the momentum BiCGStab iterations are counted as
     # CG-sized, a slight overestimate of their bytes)
     s = 4 if mixed else 8
-    levels = sim._amg_cache["P"].sizes if amg and "P" in sim._amg_cache else None
-    per_cell = algorithmic_pcg_bytes(d, levels) if levels else algorithmic_cg_bytes(d, s, s)
+    hier = sim._amg_cache.get("P") if amg else None
+    levels = hier.sizes if hier is not None else None
+    if hier is not None:
+        cycle = hier.sizes[:hier.tail_level + 1]
+        per_cell = algorithmic_pcg_bytes(d, cycle, hier.coarse_inv.numel())
+    else:
+        per_cell = algorithmic_cg_bytes(d, s, s)
     it_time_ms = solve_ms / max(1, inner_its)
     achieved = per_cell * cells / (it_time_ms / 1e3) / 1e9 if inner_its else None
     pk = peaks()
@@ -295,7 +307,7 @@ def run_ours(args, rank, world, local):
     # and per refinement sweep kRefineResidual, kInit, the persistent solve and kRefineUpdate;
     # per step the pressure hierarchy's setup (Galerkin per level, dense, inverse)
     launches_per_step = 26
-    setup = (len(levels) + 1) if levels else 0
+    setup = (2 * len(levels) + 6) if levels else 0
     gpu_launches = args.steps * (launches_per_step + setup) + 4 * max(1, sweeps) + len(infos)
     return dict(
         metric="Mcell-steps/s", value=round(value, 4), unit="Mcell-steps/s", n_gpus=world, steps=args.steps,
@@ -317,7 +329,11 @@ def run_ours(args, rank, world, local):
                              else "CG iteration (kCgDirection + kCgUpdate)"),
                   "achieved": round(achieved, 1) if achieved else None, "peak": pk.get("hbm_gbs"),
                   "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4) if achieved else None,
-                  "traffic": None, "bytes_per_cell": per_cell, "peak_source": pk["source"],
+                  "traffic": (round(PCG_DRAM_BYTES_PER_ITERATION_DUCT3D) if hier is not None and args.workload == "duct3d"
+                              else None),
+                  "traffic_unit": "DRAM bytes per iteration (ncu capture)",
+                  "algorithmic_bytes_per_iteration": round(per_cell * cells),
+                  "bytes_per_cell": round(per_cell, 2), "peak_source": pk["source"],
                   "iterations": inner_its, "solve_ms": round(solve_ms, 3)},
         gpu_launches=int(gpu_launches),
         solver={"inner_iterations_per_step": round(inner_its / args.steps, 1),

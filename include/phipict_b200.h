@@ -199,7 +199,7 @@ typedef struct phb_solve {
 	int32_t nrhs;         /* right-hand sides per instance sharing its matrix (1..3) */
 	int32_t maxit;
 	int32_t return_best;  /* CG only: keep the iterate with the lowest residual */
-	int32_t use_graph;    /* 2: persistent cooperative kernel; 1: conditional-WHILE CUDA graph; 0: host loop */
+	int32_t use_graph;    /* 2 (or 3): persistent cooperative kernel; 1: conditional-WHILE CUDA graph; 0: host loop */
 	int32_t check_every;  /* host loop only: iterations between completion checks */
 	phb_tolerance tol;
 	const void *A;        /* stencil [2d+1][ncells] */
@@ -239,7 +239,8 @@ typedef struct phb_refine {
 	int32_t nrhs;
 	int32_t max_outer;
 	int32_t inner_maxit;
-	int32_t use_graph;    /* 2: graph outer loop, persistent inner solves; 1: nested graph loops; 0: host loops */
+	int32_t use_graph;    /* 2: graph outer loop, persistent inner solves; 3: host outer loop, persistent inner
+	                         solves (profilers see every launch); 1: nested graph loops; 0: host loops */
 	int32_t pad;
 	double inner_rtol;
 	phb_tolerance tol;    /* outer tolerance, on the float64 residual */

@@ -1496,7 +1496,7 @@ static int launchPersistent(const phb_domain *dom, const phb_solve *sv, cudaStre
 // the Krylov loop for one solve, recorded on `s`
 template <typename T, int D, int K>
 static int emitSolve(const phb_domain *dom, const phb_solve *sv, cudaStream_t s, Streams &ss, int useGraph, bool stopStart, int fromInner = 0) {
-	if (sv->use_graph == 2) return launchPersistent<T, D, K>(dom, sv, s, stopStart, fromInner);
+	if (sv->use_graph >= 2) return launchPersistent<T, D, K>(dom, sv, s, stopStart, fromInner);
 	Dom<double, D> dm(*dom);
 	const Layout L = solveLayout(dom, sv->kind, sizeof(T), K);
 	const StateLayout SL = stateLayout(dom, K);
@@ -1731,8 +1731,10 @@ static int emitRefine(const phb_domain *dom, const phb_refine *rf, cudaStream_t 
 	in.work = rf->work;
 	in.state = rf->state;
 	in.amg = rf->amg;
-	const bool graph = rf->use_graph != 0;
-	in.use_graph = rf->use_graph == 2 ? 2 : (graph ? 1 : 0);
+	// 1: nested graph loops; 2: graph outer loop, persistent inner solves; 3: host outer loop,
+	// persistent inner solves (every launch visible to a kernel profiler); 0: host loops
+	const bool graph = rf->use_graph == 1 || rf->use_graph == 2;
+	in.use_graph = rf->use_graph >= 2 ? 2 : (graph ? 1 : 0);
 	in.check_every = 8;
 	cudaGraphConditionalHandle outerHandle{};
 	if (graph) {
@@ -1784,7 +1786,7 @@ extern "C" int phb_refine_run(const phb_domain *dom, const phb_refine *r, phb_so
 	if (r->amg) key.append(reinterpret_cast<const char *>(r->amg), sizeof(phb_amg));
 	int rc = PHB_OK;
 	const int K = r->nrhs;
-	if (!r->use_graph) {
+	if (r->use_graph == 0 || r->use_graph == 3) {
 		Streams *ss;
 		rc = getStreams(ss);
 		if (rc) return rc;

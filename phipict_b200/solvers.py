@@ -26,8 +26,10 @@ STATUS = {0: "running", 1: "converged", 2: "non-finite", 3: "max iterations", 4:
 # host polls for completion every `check_interval` iterations (what a profiler needs).
 # Solver launch modes: "persistent" (default) runs each Krylov solve as one cooperative
 # kernel with grid barriers; "graph" as a conditional-WHILE CUDA graph of per-phase kernels;
-# "host" launches every kernel on its own and polls (what a kernel profiler needs).
-MODES = {"host": 0, "graph": 1, "persistent": 2}
+# "host" launches every kernel on its own and polls; "persistent-host" keeps the persistent
+# solves but runs the refinement's outer loop on the host. Kernel profilers cannot see
+# kernels inside graphs with conditional nodes, so they need "host" or "persistent-host".
+MODES = {"host": 0, "graph": 1, "persistent": 2, "persistent-host": 3}
 SETTINGS = {
     "use_graphs": os.environ.get("PHIPICT_B200_GRAPHS", "1") != "0",
     "mode": os.environ.get("PHIPICT_B200_SOLVER_MODE", "persistent"),
