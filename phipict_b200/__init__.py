@@ -6,6 +6,7 @@ module ``phipict_b200._C``. The compute runs in the in-tree CUDA library
 ``libphipict_b200.so`` (C ABI: ``include/phipict_b200.h``); there is no CPU fallback.
 """
 from . import _C
+from .batch import DomainBatch
 from .domain import (
     AdvectionScheme,
     Block,
@@ -27,6 +28,6 @@ from .tolerance import SolverTolerance
 
 __all__ = [
     "AdvectionScheme", "Block", "Boundary", "BoundaryConditionType", "BoundaryType", "ConnectedBoundary",
-    "CSRmatrix", "Domain", "FixedBoundary", "Hook", "Hooks", "LinearSolverResultInfo", "LinsolveError",
+    "CSRmatrix", "Domain", "DomainBatch", "FixedBoundary", "Hook", "Hooks", "LinearSolverResultInfo", "LinsolveError",
     "MHDSimulation", "PeriodicBoundary", "PotentialBC", "Simulation", "SolverTolerance", "_C",
 ]

@@ -107,7 +107,8 @@ class AmgHierarchy:
         blocks, insts = domain._blocks_host.numpy(), domain._insts_host.numpy()
         records = [(blocks, None, insts)]
         max_levels = max(2, min(int(opts["max_levels"]), _lib.AMG_MAX_LEVELS))
-        while len(records) < max_levels and int(records[-1][2][:, 1].max()) > int(opts["coarse_cells"]):
+        # at least one coarse level, then down to coarse_cells cells per instance
+        while len(records) < max_levels and (len(records) == 1 or int(records[-1][2][:, 1].max()) > int(opts["coarse_cells"])):
             nxt = coarsen_records(records[-1][0], records[-1][2], dims)
             if nxt is None:
                 break

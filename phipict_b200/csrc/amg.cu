@@ -141,8 +141,12 @@ __device__ void invertDense(double *M, int n, int ld) {
 	__syncthreads();
 	const double thr = sThr;
 	const double shift = sShift;
+	// element loops: warp w takes rows w, w + NW, ..., lane c columns c, c + 32, ... (no
+	// integer division in the hot loop)
+	constexpr int NW = INV_THREADS / 32;
 	if (shift != 0.0) {
-		for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) M[(size_t)(idx / n) * ld + idx % n] += shift;
+		for (int i = warp; i < n; i += NW)
+			for (int j = lane; j < n; j += 32) M[(size_t)i * ld + j] += shift;
 		__syncthreads();
 	}
 	for (int k = 0; k < n; ++k) {
@@ -157,20 +161,21 @@ __device__ void invertDense(double *M, int n, int ld) {
 			colk[j] = M[(size_t)j * ld + k];
 		}
 		__syncthreads();
-		for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
-			const int i = idx / n, j = idx - i * n;
-			double *e = M + (size_t)i * ld + j;
-			if (i == k && j == k) *e = 1.0 / p;
-			else if (i == k) *e = rowk[j];
-			else if (j == k) *e = -colk[i] / p;
-			else *e -= colk[i] * rowk[j];
+		const double rp = 1.0 / p;
+		for (int i = warp; i < n; i += NW) {
+			double *Mi = M + (size_t)i * ld;
+			const double ci = colk[i];
+			if (i == k) {
+				for (int j = lane; j < n; j += 32) Mi[j] = j == k ? rp : rowk[j];
+			} else {
+				for (int j = lane; j < n; j += 32) Mi[j] = j == k ? -ci * rp : Mi[j] - ci * rowk[j];
+			}
 		}
 		__syncthreads();
 	}
-	for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
-		const int i = idx / n, j = idx - i * n;
-		if (skip[i] || skip[j]) M[(size_t)i * ld + j] = 0.0;
-	}
+	for (int i = warp; i < n; i += NW)
+		for (int j = lane; j < n; j += 32)
+			if (skip[i] || skip[j]) M[(size_t)i * ld + j] = 0.0;
 	__syncthreads();
 }
 
@@ -182,10 +187,13 @@ __global__ void __launch_bounds__(INV_THREADS) kInvert(double *dense, int cn, co
 	double *G = dense + (size_t)blockIdx.x * cn * cn;
 	const int n = min(cn, insts[blockIdx.x * PHB_IREC + I_NCELLS]);
 	if (SHARED) {
-		for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) sm[idx] = G[(size_t)(idx / n) * cn + idx % n];
+		const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+		for (int i = warp; i < n; i += INV_THREADS / 32)
+			for (int j = lane; j < n; j += 32) sm[i * n + j] = G[(size_t)i * cn + j];
 		__syncthreads();
 		invertDense(sm, n, n);
-		for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) G[(size_t)(idx / n) * cn + idx % n] = sm[idx];
+		for (int i = warp; i < n; i += INV_THREADS / 32)
+			for (int j = lane; j < n; j += 32) G[(size_t)i * cn + j] = sm[i * n + j];
 	} else {
 		invertDense(G, n, cn);
 	}

@@ -632,6 +632,10 @@ class Domain:
     def getTotalSize(self) -> int:
         return sum(b.ncells() for b in self._blocks)
 
+    def numCells(self) -> int:
+        """Cells of all batched environments (the length of a scalar field)."""
+        return self.getTotalSize() * self._batch
+
     def IsInitialized(self) -> bool:
         return self._prepared
 

@@ -23,6 +23,10 @@ from .tolerance import SolverTolerance, parse_tolerance
 
 def epot_matrix_is_anchored(domain: Domain) -> bool:
     """True if a Dirichlet potential face makes the potential matrix non-singular (mhd.py:48-80)."""
+    if hasattr(domain, "members"):  # a DomainBatch: its instances must agree
+        from .batch import potential_anchoring
+
+        return potential_anchoring(domain)
     for block in domain.getBlocks():
         for _, bound in block.getFixedBoundaries():
             if bound.hasPotentialDirichlet():
@@ -90,10 +94,9 @@ class MHDSimulation(Simulation):
         self._stuart_dev = stuart_number.detach().to(dev, torch.float64).reshape(-1).expand(B).contiguous()
         domain.SetupEpotOnDomain(potential_non_ortho_flags, potential_use_face_transform)
         self._potential_rank_deficient = not epot_matrix_is_anchored(domain)
-        N = domain.getTotalSize()
         # u x e_b of the last potential step, [B][3][cells]; phiPICT initialises it from
         # domain.velocityResult, which is zero until a step has run (mhd.py:526-533)
-        self._uxb = torch.zeros(B * 3 * N, dtype=domain.getDtype(), device=dev)
+        self._uxb = torch.zeros(3 * domain.numCells(), dtype=domain.getDtype(), device=dev)
         self._potential_stale = False
         self.hooks.append(Hook.POST, self._magnetic_step_callback)
         self.hooks.append(Hook.PRE_VELOCITY_SETUP, self._add_lorentz_force)

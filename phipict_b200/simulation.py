@@ -216,7 +216,7 @@ class Simulation:
         use = self.pressure_use_amg
         if use is None:
             d = self.domain
-            rows = d.getTotalSize() * d.getBatchSize()
+            rows = d.numCells()
             limit = self.PRESSURE_AMG_AUTO_MIN_ROWS if d.getBatchSize() == 1 else self.PRESSURE_AMG_AUTO_MIN_ROWS_BATCHED
             return rows >= limit
         return bool(use)
@@ -225,10 +225,18 @@ class Simulation:
         return self._pressure_amg_options
 
     def _amg_for(self, which: str, A32: torch.Tensor):
+        """The multigrid hierarchy of matrix `which`, or None for a grid that cannot be
+        coarsened (single cells, or a coarsest level above the dense limit): plain CG then."""
         from .amg import hierarchy_for
 
         d = self.domain
-        return hierarchy_for(d, which, A32, d._matrix_version(which), self._amg_cache, self._amg_options(which))
+        if self._amg_cache.get(("unavailable", which)) is d._blocks_dev:
+            return None
+        try:
+            return hierarchy_for(d, which, A32, d._matrix_version(which), self._amg_cache, self._amg_options(which))
+        except ValueError:
+            self._amg_cache[("unavailable", which)] = d._blocks_dev
+            return None
 
     def collect_solves(self, raise_on_failure: bool = True) -> bool:
         """Read the outcomes of the solves launched since the last call (synchronises)."""
