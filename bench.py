@@ -75,8 +75,49 @@ def make_duct(device, dtype, nx=64, ny=48, nz=48, nblocks=3, seed=0):
     return dom
 
 
+def make_hartmann2d(device, dtype, nx, ny, Re, seed=0, length=4.0):
+    """Periodic 2D channel [0, length] x [-1, 1], no-slip insulating walls, u = 1 + 1e-3 noise."""
+    import phipict_b200 as pb
+    from phipict_b200.grid import rectilinear_vertices
+
+    dom = pb.Domain(2, torch.tensor([1.0 / Re]), name="hartmann", device=device, dtype=dtype)
+    b = dom.CreateBlock(vertexCoordinates=rectilinear_vertices(np.linspace(0.0, length, nx + 1),
+                                                               np.linspace(-1.0, 1.0, ny + 1), dtype=dtype), name="channel")
+    b.CloseBoundary("-y")
+    b.CloseBoundary("+y")
+    b.MakePeriodic("x")
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    v = torch.zeros(b.velocity.shape, dtype=dtype)
+    v[:, 0] = 1.0
+    v += 1e-3 * torch.randn(v.shape, generator=g, dtype=dtype)
+    b.velocity.copy_(v.to(device))
+    return dom
+
+
+def make_cavity2d(device, dtype, n, Re, seed=0):
+    """Lid-driven cavity [0, 1]^2 from rest: four no-slip insulating walls, the +y lid at u = 1."""
+    import phipict_b200 as pb
+    from phipict_b200.grid import rectilinear_vertices
+
+    dom = pb.Domain(2, torch.tensor([1.0 / Re]), name="cavity", device=device, dtype=dtype)
+    xs = np.linspace(0.0, 1.0, n + 1)
+    b = dom.CreateBlock(vertexCoordinates=rectilinear_vertices(xs, xs, dtype=dtype), name="cavity")
+    for f in ("-x", "+x", "-y"):
+        b.CloseBoundary(f)
+    lid = torch.zeros(1, 2, 1, n, dtype=dtype)
+    lid[0, 0] = 1.0
+    b.CloseBoundary("+y", lid.to(device))
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    b.velocity.copy_((1e-3 * torch.randn(b.velocity.shape, generator=g, dtype=dtype)).to(device))
+    return dom
+
+
 WORKLOADS = {
     "duct3d": dict(nx=64, ny=48, nz=48, nblocks=3, Ha=100.0, Re=1000.0, dt=0.01, rtol=1e-10),
+    # 64 heterogeneous 2D instances (Hartmann channels and lid-driven cavities) in one batch
+    "batch64": dict(instances=64, sides=(32, 48, 64, 96, 128, 192, 256), rtol=1e-8),
+    # a served Poisson stream of 2D and 3D requests
+    "serve": dict(requests=24, rate=20.0, steps=100, rtol=1e-8),
 }
 
 
@@ -385,6 +426,150 @@ def run_reference(args, rank, world):
     return line
 
 
+def batch64_instances(wl, device, dtype, seed=0):
+    """The seeded instance mix: (domain, stuart, dt) per instance; sides uniform over
+    wl['sides'], Hartmann channel or cavity by a fair coin, Ha log-uniform in [1, 1000],
+    Re uniform in [100, 2000]; dt = min(1e-3, 0.5 / N) keeps the explicit Lorentz force stable."""
+    g = torch.Generator().manual_seed(seed)
+    out = []
+    for k in range(wl["instances"]):
+        side = wl["sides"][int(torch.randint(len(wl["sides"]), (1,), generator=g))]
+        cavity = bool(torch.rand(1, generator=g) < 0.5)
+        Ha = float(10 ** (3 * torch.rand(1, generator=g)))
+        Re = float(100 + 1900 * torch.rand(1, generator=g))
+        dom = make_cavity2d(device, dtype, side, Re, seed=k) if cavity else make_hartmann2d(device, dtype, side, side, Re, seed=k)
+        dom.PrepareSolve()
+        N = Ha * Ha / Re
+        out.append((dom, N, min(1e-3, 0.5 / N)))
+    return out
+
+
+def reset_cell_source(domain, **kw):
+    """The Lorentz force is added onto the velocity source (simulation/mhd.py:583-593); the
+    benchmarks reset the source every step, as phiPICT's examples/hartmann.py does."""
+    if getattr(domain, "_src", None) is not None:
+        domain._src.zero_()
+
+
+def run_batch64(args, rank, world, local):
+    import phipict_b200 as pb
+
+    wl = WORKLOADS["batch64"]
+    device = torch.device("cuda", local)
+    inst = batch64_instances(wl, device, torch.float64, seed=rank)
+    cells = sum(d.numCells() for d, _, _ in inst)
+    batch = pb.DomainBatch([d for d, _, _ in inst])
+    tol = pb.SolverTolerance(rtol=wl["rtol"])
+    sim = pb.MHDSimulation(batch, inst[0][2], torch.tensor([n for _, n, _ in inst], dtype=torch.float64),
+                           torch.tensor([0.0, 1.0, 0.0], dtype=torch.float64), non_orthogonal=False,
+                           advection_tol=tol, pressure_tol=tol, potential_tol=tol, mixed_precision=not args.plain_fp64,
+                           pressure_use_amg=not args.plain_fp64 and not args.no_amg,
+                           potential_use_preconditioner=not args.plain_fp64 and not args.no_amg,
+                           hooks=pb.Hooks().append(pb.Hook.PRE_VELOCITY_SETUP, reset_cell_source))
+    sim.time_step = torch.tensor([dt for _, _, dt in inst], dtype=torch.float64)
+    stream = torch.cuda.current_stream(device)
+    for _ in range(args.warmup):
+        if not sim.single_step():
+            raise RuntimeError(f"warm-up step failed: {sim.last_error}")
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        if not sim.single_step():
+            raise RuntimeError(f"timed step failed: {sim.last_error}")
+    t1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = max_over_ranks(t0.elapsed_time(t1), world)
+    # the same instances one at a time (plain FP64 path, one timed step each after a warm-up)
+    alone_ms = 0.0
+    if not args.no_alone:
+        for dom, N, dt in batch64_instances(wl, device, torch.float64, seed=rank):
+            s1 = pb.MHDSimulation(dom, dt, torch.tensor([N], dtype=torch.float64),
+                                  torch.tensor([0.0, 1.0, 0.0], dtype=torch.float64), non_orthogonal=False,
+                                  advection_tol=tol, pressure_tol=tol, potential_tol=tol,
+                                  hooks=pb.Hooks().append(pb.Hook.PRE_VELOCITY_SETUP, reset_cell_source))
+            s1.single_step()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            s1.single_step()
+            b.record(stream)
+            torch.cuda.synchronize()
+            alone_ms += a.elapsed_time(b)
+    value = cells * world * args.steps / (ms / 1e3) / 1e6
+    return dict(metric="Mcell-steps/s", value=round(value, 4), unit="Mcell-steps/s", n_gpus=world, steps=args.steps,
+                warmup=args.warmup, ms_per_step=round(ms / args.steps, 4), higher_is_better=True, scaling="weak",
+                vs_baseline=None, dtype="f64 fields, f32 Krylov + f64 refinement" if not args.plain_fp64 else "f64",
+                data="synthetic (seeded instance mix)",
+                config={"workload": f"batch64: {len(inst)} 2D Hartmann/cavity instances, sides in {wl['sides']}, "
+                                    f"Ha log-uniform [1,1000], Re U(100,2000), one DomainBatch, rtol {wl['rtol']}",
+                        "cells_per_gpu": cells, "parallelism": f"replicas x{world}"},
+                clocks=clk,
+                one_at_a_time={"ms_per_step": round(alone_ms, 3) if alone_ms else None,
+                               "value": round(cells / (alone_ms / 1e3) / 1e6, 4) if alone_ms else None,
+                               "path": "plain FP64, each instance alone"},
+                gpu_launches=None)
+
+
+def serve_requests(wl, device, seed=0):
+    """The seeded request stream: half 2D Hartmann channels with side U[64, 512], half 3D
+    ducts of one block with side U[32, 128]; Ha log-uniform in [1, 1000], Re = 1000."""
+    from phipict_b200.serve import Request, poisson_arrivals
+
+    g = torch.Generator().manual_seed(seed)
+    arrivals = poisson_arrivals(wl["requests"], wl["rate"], seed)
+    reqs = []
+    for k in range(wl["requests"]):
+        three = bool(torch.rand(1, generator=g) < 0.5)
+        side = int(32 + 96 * torch.rand(1, generator=g)) if three else int(64 + 448 * torch.rand(1, generator=g))
+        Ha = float(10 ** (3 * torch.rand(1, generator=g)))
+        N = Ha * Ha / 1000.0
+        dt = min(0.01 if three else 1e-3, 0.5 / N)
+
+        def build(k=k, three=three, side=side):
+            dom = (make_duct(device, torch.float64, side, side, side, 1, seed=k) if three
+                   else make_hartmann2d(device, torch.float64, side, side, 1000.0, seed=k))
+            dom.PrepareSolve()
+            return dom
+        reqs.append(Request(rid=k, build=build, stuart=N, e_b=(0.0, 1.0, 0.0), steps=wl["steps"], dt=dt,
+                            arrival=arrivals[k]))
+    return reqs
+
+
+def run_serve(args, rank, world, local):
+    import phipict_b200 as pb
+    from phipict_b200.serve import Server
+
+    wl = dict(WORKLOADS["serve"])
+    if args.requests:
+        wl["requests"] = args.requests
+    device = torch.device("cuda", local)
+    tol = pb.SolverTolerance(rtol=wl["rtol"])
+    kw = dict(non_orthogonal=False, advection_tol=tol, pressure_tol=tol, potential_tol=tol,
+              mixed_precision=not args.plain_fp64, pressure_use_amg=not args.plain_fp64,
+              potential_use_preconditioner=not args.plain_fp64,
+              hooks=pb.Hooks().append(pb.Hook.PRE_VELOCITY_SETUP, reset_cell_source))
+    server = Server(device=device, hbm_budget=150e9, sim_kwargs=kw)
+    rep = server.run(serve_requests(wl, device, seed=rank))
+    cells = sum(r.cells for r in server.finished)
+    return dict(metric="Mcell-steps/s", value=round(rep["mcell_steps_per_s"] * world, 4), unit="Mcell-steps/s",
+                n_gpus=world, steps=wl["steps"], warmup=0, higher_is_better=True, scaling="weak", vs_baseline=None,
+                dtype="f64 fields, f32 Krylov + f64 refinement" if not args.plain_fp64 else "f64",
+                data="synthetic (seeded Poisson request stream)",
+                config={"workload": f"serve: {wl['requests']} requests at {wl['rate']}/s, 50% 2D side U[64,512], "
+                                    f"50% 3D side U[32,128], Ha log-uniform [1,1000], {wl['steps']} steps each, "
+                                    f"rtol {wl['rtol']}, admission against 150 GB", "parallelism": f"replicas x{world}"},
+                served={"p50_s": rep["p50_s"], "p99_s": rep["p99_s"], "wall_s": round(rep["wall_s"], 3),
+                        "failed": rep["failed"], "batch_steps": rep["batch_steps"], "cells_total": cells,
+                        "failures": [f"{r.rid}: {r.failed[:160]}" for r in server.finished if r.failed][:4],
+                        "peak_held_bytes": rep["peak_held_bytes"]},
+                gpu_launches=None)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -396,6 +581,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-amg", action="store_true", help="unpreconditioned CG for pressure and potential")
     ap.add_argument("--inner-rtol", type=float, default=None, help="inner FP32 reduction per refinement sweep")
+    ap.add_argument("--no-alone", action="store_true", help="batch64: skip the one-at-a-time comparison")
+    ap.add_argument("--requests", type=int, default=None, help="serve: number of requests")
     args = ap.parse_args()
     rank, world, local = dist_setup(args)
     if args.impl == "reference":
@@ -403,8 +590,13 @@ def main():
         if rank == 0:
             print(json.dumps(line), flush=True)
         return
-    line = run_ours(args, rank, world, local)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if args.workload == "batch64":
+        line = run_batch64(args, rank, world, local)
+    elif args.workload == "serve":
+        line = run_serve(args, rank, world, local)
+    else:
+        line = run_ours(args, rank, world, local)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "duct3d":
         line["cpu_baseline"] = cpu_baseline(WORKLOADS[args.workload], 1)
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -9,11 +9,12 @@
 
 namespace phb {
 
-// omega / diagonal of a level (a zero diagonal counts as one)
+// omega / diagonal of a level; a zero row (an aggregate that is a whole closed instance, the
+// null space) is not smoothed: wd = 0
 __global__ void kWdinv(int64_t n, const float *__restrict__ A, float *__restrict__ wd, float omega) {
 	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
 		const float d = A[i];
-		wd[i] = omega / (d != 0.f ? d : 1.f);
+		wd[i] = d != 0.f ? omega / d : 0.f;
 	}
 }
 
@@ -45,6 +46,7 @@ __global__ void __launch_bounds__(PHB_TILE) kGalerkin(Dom<float, D> fd, Dom<floa
 			cnt[a] = (co && base[a] + 1 < FB[B_NX + a]) ? 2 : 1;
 		}
 		double acc[2 * D + 1];
+		double mag = 0; // size of the diagonal's contributions: a sum that cancels to roundoff is zero
 #pragma unroll
 		for (int s = 0; s < 2 * D + 1; ++s) acc[s] = 0;
 		for (int oz = 0; oz < cnt[2]; ++oz)
@@ -54,16 +56,33 @@ __global__ void __launch_bounds__(PHB_TILE) kGalerkin(Dom<float, D> fd, Dom<floa
 					const int p[3] = {base[0] + ox, base[1] + oy, base[2] + oz};
 					const int64_t g = FB[B_CELLOFF] + flat(FB, p);
 					acc[0] += Af[g];
+					mag += fabs(double(Af[g]));
 #pragma unroll
 					for (int f = 0; f < 2 * D; ++f) {
 						const int a = f >> 1;
 						// the neighbour across f is the other cell of the aggregate
 						const bool inside = cnt[a] == 2 && ((f & 1) ? o[a] == 0 : o[a] == 1);
 						const double v = Af[(f + 1) * N + g];
-						if (inside) acc[0] += v;
-						else acc[f + 1] += v;
+						if (inside) {
+							acc[0] += v;
+							mag += fabs(v);
+						} else acc[f + 1] += v;
 					}
 				}
+		// across a periodic face of a block one cell wide along that axis the neighbour is the
+		// cell itself: that coupling belongs to the diagonal (the stencil applies the same
+		// operator either way, but the smoother and the test below need the true diagonal)
+#pragma unroll
+		for (int f = 0; f < 2 * D; ++f) {
+			if (sB[B_NX + (f >> 1)] == 1 && fType(sB, f) == FT_PERIODIC) {
+				acc[0] += acc[f + 1];
+				mag += fabs(acc[f + 1]);
+				acc[f + 1] = 0.0;
+			}
+		}
+		// the fine values are float32: a diagonal below 1e-5 of its contributions is a
+		// cancellation (an aggregate with no coupling left outside it) and exactly zero
+		if (fabs(acc[0]) <= 1e-5 * mag) acc[0] = 0.0;
 #pragma unroll
 		for (int s = 0; s < 2 * D + 1; ++s) Ac[s * NC + cc.g] = float(sc * acc[s]);
 	}

@@ -112,7 +112,6 @@ __device__ __forceinline__ void amgRestrictPart(const AmgView<D> &mg, int l, int
 	const float *wd = mg.wd[l];
 	const float *b = mg.b[l];
 	float *bc = mg.b[l + 1];
-	const float w = mg.omega;
 	const int32_t *FB = fd.blk(bi);
 	const int64_t N = fd.ncells;
 	const int lc = l0 + part * R::CELLS + int(threadIdx.x) / R::G; // coarse cell of the block
@@ -138,7 +137,7 @@ __device__ __forceinline__ void amgRestrictPart(const AmgView<D> &mg, int l, int
 			c.g = __ldg(FB + B_CELLOFF) + flat(FB, c.p);
 			c.mi = c.g;
 			const float bi_ = b[c.g];
-			float y = w * bi_; // A_ii * (omega b_i / A_ii)
+			float y = __ldg(A + c.g) * (bi_ * __ldg(wd + c.g)); // A_ii x0_i
 #pragma unroll
 			for (int f = 0; f < 2 * D; ++f) {
 				const int64_t nb = neighborIndex<float, D>(fd, c, f);

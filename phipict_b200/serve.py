@@ -159,6 +159,19 @@ class Server:
         g.batch, g.sim, g.batch_requests = batch, sim, reqs
         g.dirty = False
 
+    @staticmethod
+    def _failed_instances(g: _Group) -> set[int]:
+        """Instances of the batch with a solve that did not converge in the last step (the
+        others' results are unaffected: every system of a batch is solved on its own)."""
+        B = g.batch.getBatchSize()
+        bad = set()
+        for tag, infos in g.sim.solve_report():
+            per = max(1, len(infos) // B)
+            for i, inf in enumerate(infos):
+                if not inf.converged and not (tag.startswith("epot") and g.sim._accept_best(inf)):
+                    bad.add(i // per)
+        return bad if bad else set(range(B))
+
     def _retire(self, g: _Group, now: float) -> None:
         done = [r for r in g.requests if r.done >= r.steps or r.failed]
         if not done:
@@ -192,10 +205,11 @@ class Server:
                 self._repack(g)
             ok = g.sim.single_step()
             self.steps_run += 1
-            for r in g.requests:
+            bad = set() if ok else self._failed_instances(g)
+            for k, r in enumerate(g.batch_requests):
                 r.done += 1
                 self.cell_steps += r.cells
-                if not ok:
+                if k in bad:
                     r.failed = g.sim.last_error or "step failed"
         now = self._now()
         for g in active:
