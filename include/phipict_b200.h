@@ -274,6 +274,43 @@ int64_t phb_cg_noalloc_bytes(const phb_domain *dom, int dtype, int nrhs);
 int phb_cg_solve_noalloc(const phb_domain *dom, int dtype, int nrhs, const void *A, const void *b, void *x,
                          const phb_tolerance *tol, int maxit, int return_best, phb_solve_result *out, phb_stream stream);
 
+/* --- adjoint of the step (float64 domains) ------------------------------------------
+ * Replace phiPICT's *Grad kernels (piso/advection.cu:310-544,958-1195; pressure.cu:196-345,
+ * 525-750; velocity_correction.cu:301-375; mhd/potential.cu:981-1329, bound at
+ * bindings.cpp:781-814) and the solve adjoint pieces of core/piso_diff.py:1154-1421
+ * (LinearSolveFunction, SparseOuterProduct, csrTranspose). Every *bar output is
+ * accumulated (+=): zero it before the first contribution. ubbar has the layout of the
+ * fixed-face velocity buffer (phb_domain::fvel). */
+/* CT = C^T as a stencil (the adjoint momentum solve) */
+int phb_transpose_stencil(const phb_domain *dom, const double *C, double *CT, phb_stream stream);
+/* Mbar[s][i] += scale * sum_k lam[i,k] x[nb_s(i),k] (ncomp 1 or dims): the adjoint of a
+ * solve M x = b with respect to M is -lam (x)^T on the stencil, lam = M^-T xbar */
+int phb_adj_outer(const phb_domain *dom, int ncomp, const double *lam, const double *x, double scale, double *Mbar,
+                  phb_stream stream);
+/* phb_advection_matrix: Cbar (slot 0 including the adjoint of Adiag) -> ubar */
+int phb_adj_advection_matrix(const phb_domain *dom, const double *Cbar, double *ubar, phb_stream stream);
+/* phb_advection_rhs (per-cell source): rhsbar -> ubar, srcbar (may be NULL), ubbar (may be NULL) */
+int phb_adj_advection_rhs(const phb_domain *dom, const double *rhsbar, double *ubar, double *srcbar, double *ubbar,
+                          phb_stream stream);
+/* phb_pressure_rhs: hbar -> ubar, ustarbar, Cbar (off-diagonal slots), Abar, srcbar, ubbar; h = the forward HbyA */
+int phb_adj_pressure_rhs(const phb_domain *dom, const double *C, const double *Adiag, const double *ustar, const double *h,
+                         const double *hbar, double *ubar, double *ustarbar, double *Cbar, double *Abar, double *srcbar,
+                         double *ubbar, phb_stream stream);
+/* phb_divergence: dbar -> fbar (the field) and ubbar (fixed faces) */
+int phb_adj_divergence(const phb_domain *dom, const double *dbar, double *fbar, double *ubbar, phb_stream stream);
+/* phb_correct_velocity: ubar -> hbar, pbar, Abar */
+int phb_adj_correct_velocity(const phb_domain *dom, const double *p, const double *Adiag, const double *ubar, double *hbar,
+                             double *pbar, double *Abar, phb_stream stream);
+/* phb_pressure_matrix: Pbar -> Abar */
+int phb_adj_pressure_matrix(const phb_domain *dom, const double *Adiag, const double *Pbar, double *Abar, phb_stream stream);
+/* phb_uxb_epot_rhs: rbar (may be NULL) -> xbar (+= the flux transpose; xbar may already hold
+ * the adjoint of the u x e_b output), then xbar -> ubar */
+int phb_adj_uxb_epot_rhs(const phb_domain *dom, const double *e_b, const double *rbar, double *xbar, double *ubar,
+                         phb_stream stream);
+/* phb_current_lorentz with accumulate = 0: srcbar -> phibar, xbar (u x e_b), stuartbar [ninst] */
+int phb_adj_lorentz(const phb_domain *dom, const double *phi, const double *uxb, const double *e_b, const double *stuart,
+                    const double *srcbar, double *phibar, double *xbar, double *stuartbar, phb_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

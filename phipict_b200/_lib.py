@@ -32,6 +32,9 @@ EXPORTS = (
     "phb_release_graphs", "phb_refine_work_bytes", "phb_refine_run", "phb_refine_results",
     "phb_cg_noalloc_bytes", "phb_cg_solve_noalloc",
     "phb_amg_setup", "phb_amg_vcycle", "phb_amg_work_doubles",
+    "phb_transpose_stencil", "phb_adj_outer", "phb_adj_advection_matrix", "phb_adj_advection_rhs",
+    "phb_adj_pressure_rhs", "phb_adj_divergence", "phb_adj_correct_velocity", "phb_adj_pressure_matrix",
+    "phb_adj_uxb_epot_rhs", "phb_adj_lorentz",
 )
 
 
@@ -144,6 +147,16 @@ def load() -> ct.CDLL:
         "phb_refine_results": [DP, ct.POINTER(PhbRefine), ct.POINTER(PhbSolveResult), ct.POINTER(ct.c_int), P],
         "phb_cg_solve_noalloc": [DP, I, I, P, P, P, ct.POINTER(PhbTolerance), I, I, ct.POINTER(PhbSolveResult), P],
         "phb_amg_setup": [ct.POINTER(PhbAmg), P],
+        "phb_transpose_stencil": [DP, P, P, P],
+        "phb_adj_outer": [DP, I, P, P, ct.c_double, P, P],
+        "phb_adj_advection_matrix": [DP, P, P, P],
+        "phb_adj_advection_rhs": [DP, P, P, P, P, P],
+        "phb_adj_pressure_rhs": [DP, P, P, P, P, P, P, P, P, P, P, P, P],
+        "phb_adj_divergence": [DP, P, P, P, P],
+        "phb_adj_correct_velocity": [DP, P, P, P, P, P, P, P],
+        "phb_adj_pressure_matrix": [DP, P, P, P, P],
+        "phb_adj_uxb_epot_rhs": [DP, P, P, P, P, P],
+        "phb_adj_lorentz": [DP, P, P, P, P, P, P, P, P, P],
         "phb_amg_vcycle": [ct.POINTER(PhbAmg), P, P, P],
     }
     for name, args in sig.items():

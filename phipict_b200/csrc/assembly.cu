@@ -343,15 +343,6 @@ __device__ __forceinline__ void uCrossB(const int32_t *B, int64_t g, const S *__
 	out[1] = u2 * e0 - u0 * e2;
 	out[2] = u0 * e1 - u1 * e0;
 }
-template <typename S, int D>
-__device__ __forceinline__ S contraVec(const Dom<S, D> &dom, int64_t mi, int c, const S *v) {
-	S s = 0;
-#pragma unroll
-	for (int j = 0; j < D; ++j) s += dom.m(Tr<D>::MINV + c * D + j, mi) * v[j];
-	return dom.m(Tr<D>::DET, mi) * s;
-}
-// [inst][3][cells] index
-__device__ __forceinline__ int64_t vidx3(const int32_t *B, int64_t g, int k) { return g + 2 * (int64_t)B[B_INSTOFF] + (int64_t)k * B[B_INSTN]; }
 
 // u x e_b fused with k_computeEpotRHS (mhd/potential.cu:273-323) and its face fluxes
 // computeEpotFluxesNDLoop (discretization.cuh:856-912)

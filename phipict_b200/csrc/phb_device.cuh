@@ -193,6 +193,17 @@ __device__ __forceinline__ S contraAt(const Dom<S, D> &dom, const int32_t *B, in
 	return dom.m(Tr<D>::DET, mi) * s;
 }
 
+// det * Minv[c] . v for a vector v given by value
+template <typename S, int D>
+__device__ __forceinline__ S contraVec(const Dom<S, D> &dom, int64_t mi, int c, const S *v) {
+	S s = 0;
+#pragma unroll
+	for (int j = 0; j < D; ++j) s += dom.m(Tr<D>::MINV + c * D + j, mi) * v[j];
+	return dom.m(Tr<D>::DET, mi) * s;
+}
+// [inst][3][cells] index (u x e_b and current density always have 3 components)
+__device__ __forceinline__ int64_t vidx3(const int32_t *B, int64_t g, int k) { return g + 2 * (int64_t)B[B_INSTOFF] + (int64_t)k * B[B_INSTN]; }
+
 // fixed face helpers (block_data.cuh:137-205, topology.cuh:46-66) --------------------
 __device__ __forceinline__ int faceCell(const int32_t *B, int f, const int *p) {
 	const int ax = f >> 1;
