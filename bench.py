@@ -118,6 +118,8 @@ WORKLOADS = {
     "batch64": dict(instances=64, sides=(32, 48, 64, 96, 128, 192, 256), rtol=1e-8),
     # a served Poisson stream of 2D and 3D requests
     "serve": dict(requests=24, rate=20.0, steps=100, rtol=1e-8),
+    # differentiable duct: 96^3 cells in 2 blocks, 50 steps with checkpoints every 10
+    "adjoint": dict(nx=48, ny=96, nz=96, nblocks=2, Ha=10.0, Re=1000.0, dt=0.01, rollout=50, every=10, rtol=1e-12),
 }
 
 
@@ -570,6 +572,85 @@ def run_serve(args, rank, world, local):
                 gpu_launches=None)
 
 
+def run_adjoint(args, rank, world, local):
+    """Gradient of L = ||u_outlet - target||^2 after the rollout with respect to the inflow
+    profile (applied to inflow and outflow, which keeps the mass balance) and the Stuart
+    number, by the hand-written adjoint; checked against fourth-order central differences
+    on seeded directions (8 by default). Target: u_x = 1 - y^2 z^2 plus 1e-2 seeded noise on the outlet."""
+    import phipict_b200 as pb
+    from phipict_b200.adjoint import AdjointMHD, rollout
+
+    wl = dict(WORKLOADS["adjoint"])
+    if args.rollout:
+        wl["rollout"] = args.rollout
+    device = torch.device("cuda", local)
+    dom = make_duct(device, torch.float64, wl["nx"], wl["ny"], wl["nz"], wl["nblocks"])
+    dom.PrepareSolve()
+    blocks = dom.getBlocks()
+    N0 = wl["Ha"] ** 2 / wl["Re"]
+    model = AdjointMHD(dom, wl["dt"], torch.tensor([N0]), torch.tensor([0.0, 1.0, 0.0], dtype=torch.float64),
+                       steps=wl["rollout"], faces=[(blocks[0], "-x"), (blocks[-1], "+x")], checkpoint_every=wl["every"],
+                       tol=wl["rtol"], mixed_precision=not args.plain_fp64)
+    initial = model._state()
+    last = blocks[-1]
+    nx, ny, nz = last.getSizes()[:3]
+    g = torch.Generator().manual_seed(7)
+    yy = torch.linspace(-1, 1, ny, dtype=torch.float64).view(1, ny, 1)
+    zz = torch.linspace(-1, 1, nz, dtype=torch.float64).view(nz, 1, 1)
+    target = (1 - yy ** 2 * zz ** 2) + 1e-2 * torch.randn(nz, ny, 1, generator=g, dtype=torch.float64)
+    target = target.to(device)
+    n = dom.getTotalSize()
+
+    def outlet(u):
+        ux = u.view(3, n)[0][last.globalOffset:last.globalOffset + last.ncells()].view(nz, ny, nx)
+        return ux[:, :, nx - 1:nx]
+
+    def loss_of(u):
+        return ((outlet(u) - target) ** 2).sum()
+
+    p0 = model.faces[0]._velocity.detach().clone()
+    prof = p0.clone().requires_grad_(True)
+    N = torch.tensor([N0], dtype=torch.float64, requires_grad=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    u = rollout(model, prof, N, initial=[t.clone() for t in initial])
+    L = loss_of(u)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    L.backward()
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    checks = []
+    for k in range(args.fd_directions):
+        vp = torch.randn(p0.shape, generator=g, dtype=torch.float64).to(device)
+        vp[:, 0] -= vp[:, 0].mean()
+        vp[:, 1:] = 0
+        vp /= vp.abs().max()  # unit max-norm direction: eps is the largest change of a face value
+        vN = N0 * float(torch.randn(1, generator=g))  # the same relative size as the profile change
+        eps = args.fd_eps
+
+        def L_at(h):
+            return float(loss_of(model.forward(p0 + h * vp, torch.tensor([N0 + h * vN]), [t.clone() for t in initial])))
+
+        # fourth-order central difference: (8 (L(h) - L(-h)) - (L(2h) - L(-2h))) / 12h
+        fd = (8 * (L_at(eps) - L_at(-eps)) - (L_at(2 * eps) - L_at(-2 * eps))) / (12 * eps)
+        an = float((prof.grad * vp).sum()) + float(N.grad.reshape(-1)[0]) * vN
+        checks.append({"analytic": an, "fd": fd, "rel_err": abs(an - fd) / max(abs(fd), 1e-300)})
+    cells = dom.numCells()
+    fwd, bwd = t1 - t0, t2 - t1
+    return dict(metric="Mcell-steps/s", value=round(cells * wl["rollout"] / (fwd + bwd) / 1e6, 4), unit="Mcell-steps/s",
+                n_gpus=world, steps=wl["rollout"], warmup=0, higher_is_better=True, scaling="weak", vs_baseline=None,
+                dtype="f64 (adjoint kernels); solves " + ("f32 Krylov + f64 refinement" if not args.plain_fp64 else "f64"),
+                data="synthetic (seeded inflow noise, seeded target)",
+                config={"workload": f"adjoint: 2 blocks {wl['nx']}x{wl['ny']}x{wl['nz']} ({cells} cells), Ha {wl['Ha']}, "
+                                    f"Re {wl['Re']}, {wl['rollout']} steps, checkpoints every {wl['every']}, rtol {wl['rtol']}",
+                        "parallelism": f"replicas x{world}"},
+                adjoint={"forward_s": round(fwd, 3), "backward_s": round(bwd, 3), "loss": float(L),
+                         "grad_N": float(N.grad.reshape(-1)[0]), "grad_profile_norm": float(prof.grad.norm()),
+                         "fd_checks": checks, "max_rel_err": max(c["rel_err"] for c in checks)},
+                gpu_launches=None)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -583,6 +664,9 @@ def main():
     ap.add_argument("--inner-rtol", type=float, default=None, help="inner FP32 reduction per refinement sweep")
     ap.add_argument("--no-alone", action="store_true", help="batch64: skip the one-at-a-time comparison")
     ap.add_argument("--requests", type=int, default=None, help="serve: number of requests")
+    ap.add_argument("--rollout", type=int, default=None, help="adjoint: steps of the differentiable rollout")
+    ap.add_argument("--fd-directions", type=int, default=8, help="adjoint: random directions of the FD check")
+    ap.add_argument("--fd-eps", type=float, default=3e-3, help="adjoint: central-difference step")
     args = ap.parse_args()
     rank, world, local = dist_setup(args)
     if args.impl == "reference":
@@ -594,6 +678,8 @@ def main():
         line = run_batch64(args, rank, world, local)
     elif args.workload == "serve":
         line = run_serve(args, rank, world, local)
+    elif args.workload == "adjoint":
+        line = run_adjoint(args, rank, world, local)
     else:
         line = run_ours(args, rank, world, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "duct3d":

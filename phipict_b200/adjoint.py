@@ -57,7 +57,11 @@ class AdjointMHD:
     outflow of a duct); stuart: [B] Stuart numbers; e_b: (3,) or (B, 3)."""
 
     def __init__(self, domain, dt: float, stuart: torch.Tensor, e_b: torch.Tensor, steps: int, faces,
-                 checkpoint_every: int = 10, tol: float = 1e-13, corrector_steps: int = 2, maxit: int = 20000):
+                 checkpoint_every: int = 10, tol: float = 1e-13, corrector_steps: int = 2, maxit: int = 20000,
+                 mixed_precision: bool = False):
+        """mixed_precision: every forward and adjoint solve runs FP32 Krylov iterations
+        (multigrid-preconditioned for the pressure and potential systems) inside FP64
+        refinement to the same tolerance; the adjoint kernels stay FP64."""
         if domain.getDtype() != torch.float64:
             raise TypeError("the adjoint step runs in float64")
         if not domain.IsInitialized():
@@ -86,6 +90,10 @@ class AdjointMHD:
         self.uxb = torch.zeros(3 * n, dtype=torch.float64, device=dev)
         self._ts = torch.tensor([self.dt], dtype=torch.float64)
         self.stream = _lib.stream_ptr(dev)
+        self.mixed = bool(mixed_precision)
+        self._amg_cache: dict = {}
+        if self.mixed:
+            domain._mixed = True
 
     # --- state ------------------------------------------------------------------------------
     def _state(self):
@@ -107,8 +115,23 @@ class AdjointMHD:
     # --- one forward step ---------------------------------------------------------------------
     def _solve(self, which, rhs, x, kind, nrhs, A=None):
         d = self.d
-        s = solver_for(d, kind, torch.float64, nrhs, tag=f"adjoint-{which}-{kind}-{nrhs}")
-        s.solve(d._stencil(which) if A is None else A, rhs, x, self.tol, self.maxit)
+        M = d._stencil(which) if A is None else A
+        if self.mixed:
+            from .amg import hierarchy_for
+            from .solvers import refiner_for
+
+            lo = backend._lo(d, which) if A is None else A.float()
+            amg = None
+            if A is None and kind == CG and nrhs == 1:
+                try:
+                    amg = hierarchy_for(d, which, lo, d._matrix_version(which), self._amg_cache)
+                except ValueError:
+                    amg = None
+            s = refiner_for(d, kind, nrhs, tag=f"adjoint-{which}-{kind}-{nrhs}", max_outer=30)
+            s.solve(M, lo, rhs, x, self.tol, self.maxit, amg=amg)
+        else:
+            s = solver_for(d, kind, torch.float64, nrhs, tag=f"adjoint-{which}-{kind}-{nrhs}")
+            s.solve(M, rhs, x, self.tol, self.maxit)
         bad = [str(i) for i in s.results() if not i.converged]
         if bad:
             raise RuntimeError(f"adjoint rollout: {which} solve did not converge: {bad}")

@@ -95,6 +95,27 @@ def test_rollout_gradient_matches_finite_differences(cuda, case):
     assert abs(fdp) > 1e-6 and abs(fdN) > 1e-6  # both directions move the loss
 
 
+def test_mixed_precision_adjoint_matches_fp64_adjoint(cuda):
+    """FP32 multigrid-preconditioned solves inside FP64 refinement give the FP64 gradient."""
+    grads = []
+    for mixed in (False, True):
+        dom = duct_3d(8, 6, 5, 2)
+        seeded_state(dom, 12, scale=0.1)
+        dom.PrepareSolve()
+        blocks = dom.getBlocks()
+        model = AdjointMHD(dom, 0.01, torch.tensor([1.5]), torch.tensor([0.0, 1.0, 0.0], dtype=torch.float64), steps=2,
+                           faces=[(blocks[0], "-x"), (blocks[-1], "+x")], checkpoint_every=1, tol=1e-12,
+                           mixed_precision=mixed)
+        prof = model.faces[0]._velocity.detach().clone().requires_grad_(True)
+        N = torch.tensor([1.5], dtype=torch.float64, requires_grad=True)
+        u = rollout(model, prof, N)
+        (u * u).sum().backward()
+        grads.append((prof.grad.clone(), N.grad.clone()))
+    rel = float((grads[1][0] - grads[0][0]).abs().max() / grads[0][0].abs().max())
+    assert rel < 1e-7, rel
+    assert abs(float(grads[1][1] - grads[0][1])) <= 1e-7 * abs(float(grads[0][1]))
+
+
 def test_checkpointing_does_not_change_the_gradient(cuda):
     grads = []
     for every in (1, 4):
