@@ -18,7 +18,7 @@ from .domain import Domain
 from .hooks import Hook, Hooks
 from .simulation import Simulation
 from .solvers import LinearSolverResultInfo
-from .tolerance import SolverTolerance, parse_tolerance
+from .tolerance import SolverTolerance, coerce_tolerance
 
 
 def epot_matrix_is_anchored(domain: Domain) -> bool:
@@ -81,7 +81,7 @@ class MHDSimulation(Simulation):
                     "the multigrid V-cycle runs in float32: use a float32 domain or mixed_precision=True")
         self._potential_amg_options = dict(potential_amg_options or {})
         self._stuart_number = stuart_number
-        self.potential_tol = parse_tolerance(potential_tol)
+        self.potential_tol = coerce_tolerance(potential_tol)
         self._potential_use_BiCG = potential_use_BiCG
         self._potential_normalize = potential_normalize
         self._potential_solve_max_iter = int(potential_solve_max_iter)

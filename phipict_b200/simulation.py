@@ -29,7 +29,7 @@ from . import _C as backend
 from .domain import Domain, FixedBoundary
 from .hooks import Hook, Hooks
 from .solvers import BICGSTAB, CG, LinearSolverResultInfo, LinsolveError, refiner_for, solver_for
-from .tolerance import SolverTolerance, parse_tolerance
+from .tolerance import SolverTolerance, coerce_tolerance
 
 _UNSUPPORTED_TRUE = ("scipy_solve_advection", "scipy_solve_pressure", "differentiable_unsupported")
 
@@ -105,9 +105,9 @@ class Simulation:
         self.hooks = Hooks.coerce(hooks if hooks is not None else prep_fn)
         self.advection_use_BiCG = advection_use_BiCG
         self.pressure_use_BiCG = pressure_use_BiCG
-        self.advection_tol = parse_tolerance(advection_tol)
-        self.pressure_tol = parse_tolerance(pressure_tol)
-        self.pressure_tol_intermediate = parse_tolerance(pressure_tol_intermediate)
+        self.advection_tol = coerce_tolerance(advection_tol)
+        self.pressure_tol = coerce_tolerance(pressure_tol)
+        self.pressure_tol_intermediate = coerce_tolerance(pressure_tol_intermediate)
         self.pressure_warm_start = pressure_warm_start
         self.pressure_use_amg = pressure_use_amg
         self._pressure_amg_options = dict(pressure_amg_options or {})

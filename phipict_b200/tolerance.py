@@ -53,10 +53,10 @@ class SolverTolerance:
             tol = default_tolerance(dtype)
         return float(tol)
 
+    _resolve_scale = resolve_scale  # the reference's name (tolerance.py:243)
+
     def resolve(self, rhs: torch.Tensor) -> float:
-        n = rhs.numel()
-        scale = float(torch.linalg.vector_norm(rhs.detach().to(torch.float64))) / math.sqrt(n) if n else 0.0
-        return self.resolve_scale(scale, rhs.dtype)
+        return self.resolve_scale(rhs_scale(rhs), rhs.dtype)
 
     def resolve_batched(self, rhs: torch.Tensor, batch_size: int) -> list[float]:
         slices = rhs.detach().reshape(batch_size, -1)
@@ -68,20 +68,56 @@ class SolverTolerance:
     def __str__(self) -> str:
         parts = []
         if self.rtol is not None:
-            parts.append(f"rtol={self.rtol:g}")
+            parts.append(f"rtol={self.rtol:.03e}")
         if self.atol is not None:
-            parts.append(f"atol={self.atol:g}")
+            parts.append(f"atol={self.atol:.03e}")
         return "SolverTolerance(" + ", ".join(parts) + ")"
 
 
-def parse_tolerance(tol) -> float | SolverTolerance | None:
-    if tol is None or isinstance(tol, SolverTolerance):
-        return tol
+def rhs_scale(rhs: torch.Tensor) -> float:
+    """||b||_2 / sqrt(n) accumulated in float64, 0.0 for an empty RHS (tolerance.py:116-139)."""
+    n = rhs.numel()
+    if n == 0:
+        return 0.0
+    return float(torch.linalg.vector_norm(rhs.detach().to(torch.float64))) / math.sqrt(n)
+
+
+def parse_tolerance(spec) -> float | SolverTolerance | None:
+    """Coerce a config value into a tolerance (tolerance.py:268-323): None and
+    SolverTolerance pass through, real numbers (not bools) become floats, a mapping with
+    `rtol`/`atol` keys becomes a SolverTolerance; other keys raise ValueError, anything
+    else TypeError."""
+    if spec is None or isinstance(spec, SolverTolerance):
+        return spec
+    if isinstance(spec, numbers.Real) and not isinstance(spec, bool):
+        return float(spec)
+    if hasattr(spec, "keys"):
+        unknown = set(spec.keys()) - {"rtol", "atol"}
+        if unknown:
+            raise ValueError(f"Unknown tolerance keys {sorted(unknown)}, expected 'rtol' and/or 'atol'.")
+        rtol, atol = spec.get("rtol", None), spec.get("atol", None)
+        return SolverTolerance(rtol=None if rtol is None else float(rtol), atol=None if atol is None else float(atol))
+    raise TypeError(f"Cannot interpret {spec!r} as a solver tolerance; expected None, a float, "
+                    "a SolverTolerance, or a mapping with rtol/atol.")
+
+
+def resolve_tolerance(tol, rhs: torch.Tensor, batch_size: int = 1):
+    """A SolverTolerance resolved against `rhs` (a list per environment when batch_size > 1);
+    any other value unchanged (tolerance.py:326-354). The solvers here resolve on the device
+    instead; this host form serves callers of the reference's function."""
+    if isinstance(tol, SolverTolerance):
+        if batch_size > 1:
+            return tol.resolve_batched(rhs, batch_size)
+        return tol.resolve(rhs)
+    return tol
+
+
+def coerce_tolerance(tol):
+    """The tolerance keyword of a simulation: what parse_tolerance accepts, or a tensor of
+    per-system absolute tolerances (which the reference's solvers take unchanged)."""
     if isinstance(tol, torch.Tensor):
         return tol
-    if not isinstance(tol, numbers.Real) or not tol > 0:
-        raise ValueError("tolerance must be a positive float, SolverTolerance or None")
-    return float(tol)
+    return parse_tolerance(tol)
 
 
 def set_adjoint_rtol(rtol: float | None) -> None:
