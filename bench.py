@@ -120,6 +120,8 @@ WORKLOADS = {
     "serve": dict(requests=24, rate=20.0, steps=100, rtol=1e-8),
     # differentiable duct: 96^3 cells in 2 blocks, 50 steps with checkpoints every 10
     "adjoint": dict(nx=48, ny=96, nz=96, nblocks=2, Ha=10.0, Re=1000.0, dt=0.01, rollout=50, every=10, rtol=1e-12),
+    # every kernel on single-block grids far larger than L2 (SWEEP_GRIDS)
+    "sweep": dict(),
 }
 
 
@@ -572,6 +574,165 @@ def run_serve(args, rank, world, local):
                 gpu_launches=None)
 
 
+SWEEP_GRIDS = [(3, 128), (3, 192), (3, 256), (2, 2048), (2, 4096)]
+
+
+def make_box(device, dims, n, Re=1000.0, seed=0):
+    """One block of n^dims cells on [0, 2] x [-1, 1]^(dims-1): periodic in x, no-slip
+    insulating walls elsewhere, u = (1, 0, 0) plus seeded 1e-2 noise."""
+    import phipict_b200 as pb
+    from phipict_b200.grid import rectilinear_vertices
+
+    dtype = torch.float64
+    dom = pb.Domain(dims, torch.tensor([1.0 / Re]), name="box", device=device, dtype=dtype)
+    xs = np.linspace(0.0, 2.0, n + 1)
+    ys = np.linspace(-1.0, 1.0, n + 1)
+    b = dom.CreateBlock(vertexCoordinates=rectilinear_vertices(xs, ys, *([ys] if dims == 3 else []), dtype=dtype), name="box")
+    for f in ("-y", "+y") + (("-z", "+z") if dims == 3 else ()):
+        b.CloseBoundary(f)
+    b.MakePeriodic("x")
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    v = torch.zeros(b.velocity.shape, dtype=dtype)
+    v[:, 0] = 1.0
+    v += 1e-2 * torch.randn(v.shape, generator=g, dtype=dtype)
+    b.velocity.copy_(v.to(device))
+    return dom
+
+
+def assembly_bytes(d: int, s: int = 8) -> dict:
+    """Algorithmic bytes per cell of the assembly kernels (float64 fields, s bytes a value):
+    every input and output once, per-cell transforms of 2d^2+1 values, stencils of 2d+1
+    values without indices; the matrix kernels also write the float32 copy the inner solves
+    use ((2d+1)*4 bytes)."""
+    return {"advection_matrix": (d + 2 * d * d + 1 + 2 * d + 1 + 1) * s + (2 * d + 1) * 4,
+            "advection_rhs": (3 * d + 1) * s,
+            "pressure_matrix": (1 + d * d + 1 + 2 * d + 1) * s + (2 * d + 1) * 4,
+            "pressure_rhs": (2 * d + 1 + 4 * d + 2) * s,
+            "divergence": (d + d * d + 1 + 1) * s,
+            "correct_velocity": (3 + d * d + 1 + 2 * d) * s,
+            "uxb_epot_rhs": (d + 3) * s + (d + d * d + 1 + 1) * s,
+            "current_lorentz": (1 + 3 + 2 * d * d + 1 + 3) * s + (3 + 2 * d) * s}
+
+
+def run_sweep(args, rank, world, local):
+    """Roofline sweep: every kernel of the step on single-block grids far larger than L2
+    (128^3 ... 256^3, 2048^2, 4096^2), each launch timed alone with CUDA events after an L2
+    flush; achieved = algorithmic bytes / time, frac = achieved / measured HBM peak. The
+    Krylov iterations run a fixed iteration count (float32, as inside the refinement)."""
+    import ctypes as ct
+
+    import phipict_b200 as pb
+    from phipict_b200 import _C as backend
+    from phipict_b200 import _lib
+    from phipict_b200.solvers import BICGSTAB, CG, MODES, solver_for
+
+    device = torch.device("cuda", local)
+    pk = peaks()
+    peak = pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
+    grids = SWEEP_GRIDS if not args.sweep_grids else [tuple(int(v) for v in g.split("x")) for g in args.sweep_grids.split(",")]
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=device)
+    reps = args.steps
+    rows = []
+    clocks = ClockSampler(local)
+    clocks.start()
+    for dims, n in grids:
+        dom = make_box(device, dims, n)
+        dom.PrepareSolve()
+        tol = pb.SolverTolerance(rtol=1e-6)
+        sim = pb.MHDSimulation(dom, 1e-3, torch.tensor(10.0), torch.tensor([0.0, 1.0, 0.0], dtype=torch.float64),
+                               non_orthogonal=False, advection_tol=tol, pressure_tol=tol, potential_tol=tol,
+                               mixed_precision=True, pressure_use_amg=True, potential_use_preconditioner=True)
+        for _ in range(max(1, args.warmup)):
+            if not sim.single_step():
+                raise RuntimeError(f"warm-up step failed on {n}^{dims}: {sim.last_error}")
+        cells = dom.numCells()
+        S = _lib.stream_ptr(device)
+        ts = sim._time_step_tensor(None)
+        desc = dom.desc()
+        kern = {
+            "advection_matrix": lambda: backend.SetupAdvectionMatrix(dom, ts, 0),
+            "advection_rhs": lambda: backend.SetupAdvectionVelocity(dom, ts, 0, False),
+            "pressure_matrix": lambda: backend.SetupPressureMatrix(dom, ts, 0, False),
+            "pressure_rhs": lambda: _lib.call("phb_pressure_rhs", ct.byref(desc), dom._C_st.data_ptr(), dom.A.data_ptr(),
+                                              dom._u_block.data_ptr(), dom.velocityResult.data_ptr(), *backend._src(dom),
+                                              dom.pressureRHS.data_ptr(), S),
+            "divergence": lambda: _lib.call("phb_divergence", ct.byref(desc), dom.pressureRHS.data_ptr(),
+                                            dom.pressureRHSdiv.data_ptr(), S),
+            "correct_velocity": lambda: backend.CorrectVelocity(dom, ts, version=1),
+            "uxb_epot_rhs": lambda: _lib.call("phb_uxb_epot_rhs", ct.byref(desc), dom.velocityResult.data_ptr(),
+                                              sim._e_b_dev.data_ptr(), sim._uxb.data_ptr(), dom.epotRHS.data_ptr(), S),
+            "current_lorentz": lambda: _lib.call("phb_current_lorentz", ct.byref(desc), dom.epotResult.data_ptr(),
+                                                 sim._uxb.data_ptr(), sim._e_b_dev.data_ptr(), sim._stuart_dev.data_ptr(),
+                                                 None, dom._src.data_ptr(), 1, S),
+        }
+        abytes = assembly_bytes(dims)
+
+        def timed(fn):
+            ms = []
+            for _ in range(reps):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                fn()
+                e1.record()
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            return statistics.median(ms)
+
+        for name, fn in kern.items():
+            ms = timed(fn)
+            gbs = abytes[name] * cells / (ms * 1e-3) / 1e9
+            rows.append({"grid": f"{n}^{dims}", "cells": cells, "kernel": name, "bytes_per_cell": abytes[name],
+                         "ms": round(ms, 4), "gbs": round(gbs, 1), "frac": round(gbs / peak, 3)})
+        # Krylov iterations: fixed count, float32 (the refinement's inner solves)
+        its = args.sweep_iterations
+        P32 = backend._lo(dom, "P")
+        C32 = backend._lo(dom, "C")
+        amg = sim._amg_for("P", P32)
+        bP = dom.pressureRHSdiv.float()
+        bC = dom.velocityRHS.float()
+        solves = [("cg_iteration", CG, 1, P32, bP, None, algorithmic_cg_bytes(dims, 4, 4)),
+                  ("bicgstab_iteration", BICGSTAB, dims, C32, bC, None, 2 * (2 * dims + 1) * 4 + 18 * dims * 4)]
+        if amg is not None:
+            solves.append(("pcg_iteration", CG, 1, P32, bP, amg,
+                           algorithmic_pcg_bytes(dims, amg.sizes[:amg.tail_level + 1], amg.coarse_inv.numel())))
+        modes = args.sweep_modes.split(",")
+        for name, kind, nrhs, A, b, mg, bpc in solves:
+            s = solver_for(dom, kind, torch.float32, nrhs, tag="sweep-" + name)
+            x = torch.zeros_like(b)
+            for mode in modes:
+                ms = []
+                used = []
+                for _ in range(reps):
+                    x.zero_()
+                    flush.zero_()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    s.solve(A, b, x, 1e-30, its, use_graph=MODES[mode], amg=mg)
+                    e1.record()
+                    e1.synchronize()
+                    ms.append(e0.elapsed_time(e1))
+                    used.append(max(i.usedIterations for i in s.results()))
+                it = statistics.median(used)
+                per = statistics.median(ms) / max(it, 1)
+                gbs = bpc * cells / (per * 1e-3) / 1e9
+                rows.append({"grid": f"{n}^{dims}", "cells": cells, "kernel": name + ("" if mode == "persistent" else f" ({mode})"),
+                             "bytes_per_cell": round(bpc, 2), "ms": round(per, 4), "iterations": it, "gbs": round(gbs, 1),
+                             "frac": round(gbs / peak, 3)})
+        for r in rows[-(len(kern) + len(solves) * len(modes)):]:
+            print(f"{r['grid']:>7} {r['kernel']:>20} {r['ms']:9.4f} ms {r['gbs']:8.1f} GB/s {r['frac']:6.3f}", file=sys.stderr)
+        del sim, dom, kern
+        torch.cuda.empty_cache()
+    clk = clocks.stop()
+    big = [r for r in rows if r["cells"] >= 16_000_000]
+    return dict(metric="HBM roofline fraction (kernels of the step, grids >> L2)", value=round(min(r["frac"] for r in big), 3) if big else None,
+                unit="fraction of measured HBM GB/s", n_gpus=world, steps=reps, warmup=args.warmup, higher_is_better=True,
+                scaling="weak", vs_baseline=None, dtype="f64 fields, f32 Krylov", data="synthetic (seeded)",
+                config={"workload": "roofline sweep: " + ", ".join(f"{n}^{d}" for d, n in grids) + "; L2 flushed before every launch",
+                        "parallelism": f"replicas x{world}"},
+                clocks=clk, peak={"hbm_gbs": peak, "source": pk.get("source")}, sweep=rows, gpu_launches=None)
+
+
 def run_adjoint(args, rank, world, local):
     """Gradient of L = ||u_outlet - target||^2 after the rollout with respect to the inflow
     profile (applied to inflow and outflow, which keeps the mass balance) and the Stuart
@@ -667,6 +828,9 @@ def main():
     ap.add_argument("--rollout", type=int, default=None, help="adjoint: steps of the differentiable rollout")
     ap.add_argument("--fd-directions", type=int, default=8, help="adjoint: random directions of the FD check")
     ap.add_argument("--fd-eps", type=float, default=3e-3, help="adjoint: central-difference step")
+    ap.add_argument("--sweep-grids", default=None, help="sweep: grids as dims x n, e.g. 3x128,2x2048")
+    ap.add_argument("--sweep-iterations", type=int, default=30, help="sweep: Krylov iterations per timed solve")
+    ap.add_argument("--sweep-modes", default="persistent", help="sweep: solver launch modes (persistent, graph, host)")
     args = ap.parse_args()
     rank, world, local = dist_setup(args)
     if args.impl == "reference":
@@ -680,6 +844,8 @@ def main():
         line = run_serve(args, rank, world, local)
     elif args.workload == "adjoint":
         line = run_adjoint(args, rank, world, local)
+    elif args.workload == "sweep":
+        line = run_sweep(args, rank, world, local)
     else:
         line = run_ours(args, rank, world, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "duct3d":

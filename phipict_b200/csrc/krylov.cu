@@ -173,21 +173,334 @@ __device__ __forceinline__ void stencilNeighbors(const Dom<double, D> &dom, cons
 	for (int f = 0; f < 2 * D; ++f) nb[f] = neighborIndex<double, D>(dom, c, f);
 }
 
-// y = A v at cell c, v(g, k) evaluated by `val` (also at the stencil neighbours).
-template <typename T, int D, int K, typename Val>
-__device__ __forceinline__ void applyA(const T *__restrict__ A, int64_t N, const Cell &c, const int64_t *nb, const bool *act, Val val, T *out) {
-	const T a0 = A[c.g];
-	T af[2 * D];
+// Krylov tile bodies on quads ------------------------------------------------------------
+// Fields evaluated at the stencil points: at(o) one value, at4(o) four consecutive values.
+// Every multiply-add is an explicit fma, so that the persistent kernel and the per-phase
+// kernels round identically whatever contraction the compiler would choose in each.
+template <typename T>
+struct FX { // a stored vector
+	const T *x;
+	__device__ __forceinline__ T at(int64_t o) const { return x[o]; }
+	__device__ __forceinline__ void at4(int64_t o, int n, bool al, T (&v)[4]) const { ld4(x + o, n, al, v); }
+};
+template <typename T>
+struct FDir { // CG direction p' = z + beta p (z after a restart)
+	const T *z, *p;
+	T beta;
+	bool rs;
+	__device__ __forceinline__ T at(int64_t o) const { return rs ? z[o] : fma(beta, p[o], z[o]); }
+	__device__ __forceinline__ void at4(int64_t o, int n, bool al, T (&v)[4]) const {
+		ld4(z + o, n, al, v);
+		if (rs) return;
+		T b[4];
+		ld4(p + o, n, al, b);
 #pragma unroll
-	for (int f = 0; f < 2 * D; ++f) af[f] = A[(f + 1) * N + c.g];
+		for (int i = 0; i < 4; ++i) v[i] = fma(beta, b[i], v[i]);
+	}
+};
+template <typename T>
+struct FBicgP { // BiCGStab direction p = r + beta (p - omega v) (r after a restart)
+	const T *r, *p, *v;
+	T beta, omega;
+	bool rs;
+	__device__ __forceinline__ T at(int64_t o) const { return rs ? r[o] : fma(beta, fma(-omega, v[o], p[o]), r[o]); }
+	__device__ __forceinline__ void at4(int64_t o, int n, bool al, T (&w)[4]) const {
+		ld4(r + o, n, al, w);
+		if (rs) return;
+		T a[4], b[4];
+		ld4(p + o, n, al, a);
+		ld4(v + o, n, al, b);
+#pragma unroll
+		for (int i = 0; i < 4; ++i) w[i] = fma(beta, fma(-omega, b[i], a[i]), w[i]);
+	}
+};
+template <typename T>
+struct FBicgS { // BiCGStab half step s = r - alpha v
+	const T *r, *v;
+	T alpha;
+	__device__ __forceinline__ T at(int64_t o) const { return fma(-alpha, v[o], r[o]); }
+	__device__ __forceinline__ void at4(int64_t o, int n, bool al, T (&w)[4]) const {
+		T b[4];
+		ld4(r + o, n, al, w);
+		ld4(v + o, n, al, b);
+#pragma unroll
+		for (int i = 0; i < 4; ++i) w[i] = fma(-alpha, b[i], w[i]);
+	}
+};
+
+// y = A f and f itself at the quad's cells for every active right-hand side (zeros for the
+// others and past q.n). On the fast path the four cells' stencil rows and neighbour groups
+// are loaded at once, slot by slot; elsewhere every cell resolves its neighbours across
+// faces. The products are summed in the same order on both paths (centre, then faces -x +x
+// -y +y -z +z, a face without neighbour skipped).
+template <typename T, int D, int K, typename F>
+__device__ __forceinline__ void quadApply(const Dom<double, D> &dom, const T *__restrict__ A, const Quad &q, const bool (&act)[K],
+		const F (&fld)[K], T (&y)[K][4], T (&f)[K][4]) {
+	const int64_t N = dom.ncells;
+	if (q.fast) {
+		// x neighbours of the row ends: across the block's x face when the quad touches it
+		int64_t gW = q.g - 1, gE = q.g + 4;
+		if (q.p[0] == 0 || q.p[0] + 3 == q.B[B_NX] - 1) {
+			Cell c;
+			c.B = q.B;
+			c.p[1] = q.p[1];
+			c.p[2] = q.p[2];
+			if (q.p[0] == 0) {
+				c.p[0] = 0;
+				c.g = (int)q.g;
+				gW = neighborIndex<double, D>(dom, c, 0);
+			}
+			if (q.p[0] + 3 == q.B[B_NX] - 1) {
+				c.p[0] = q.p[0] + 3;
+				c.g = (int)(q.g + 3);
+				gE = neighborIndex<double, D>(dom, c, 1);
+			}
+		}
+		int64_t o[K];
+#pragma unroll
+		for (int k = 0; k < K; ++k) o[k] = vk<K>(q.B, q.g, k);
+		T a[4];
+		ld4(A + q.g, 4, q.al, a);
+#pragma unroll
+		for (int k = 0; k < K; ++k) {
+			if (!act[k]) {
+#pragma unroll
+				for (int i = 0; i < 4; ++i) f[k][i] = 0;
+			} else {
+				fld[k].at4(o[k], 4, q.al, f[k]);
+			}
+#pragma unroll
+			for (int i = 0; i < 4; ++i) y[k][i] = a[i] * f[k][i];
+		}
+		ld4(A + N + q.g, 4, q.al, a);
+#pragma unroll
+		for (int k = 0; k < K; ++k) {
+			if (!act[k]) continue;
+			if (gW >= 0) y[k][0] = fma(a[0], fld[k].at(vk<K>(q.B, gW, k)), y[k][0]);
+#pragma unroll
+			for (int i = 1; i < 4; ++i) y[k][i] = fma(a[i], f[k][i - 1], y[k][i]);
+		}
+		ld4(A + 2 * N + q.g, 4, q.al, a);
+#pragma unroll
+		for (int k = 0; k < K; ++k) {
+			if (!act[k]) continue;
+#pragma unroll
+			for (int i = 0; i < 3; ++i) y[k][i] = fma(a[i], f[k][i + 1], y[k][i]);
+			if (gE >= 0) y[k][3] = fma(a[3], fld[k].at(vk<K>(q.B, gE, k)), y[k][3]);
+		}
+#pragma unroll
+		for (int sl = 3; sl < 2 * D + 1; ++sl) {
+			const int64_t off = sl == 3 ? -(int64_t)q.sy : sl == 4 ? (int64_t)q.sy : sl == 5 ? -(int64_t)q.sz : (int64_t)q.sz;
+			const bool al = sl < 5 ? q.alY : q.alZ;
+			ld4(A + sl * N + q.g, 4, q.al, a);
+#pragma unroll
+			for (int k = 0; k < K; ++k) {
+				if (!act[k]) continue;
+				T v[4];
+				fld[k].at4(o[k] + off, 4, al, v);
+#pragma unroll
+				for (int i = 0; i < 4; ++i) y[k][i] = fma(a[i], v[i], y[k][i]);
+			}
+		}
+		return;
+	}
+#pragma unroll
+	for (int i = 0; i < 4; ++i) {
+#pragma unroll
+		for (int k = 0; k < K; ++k) { y[k][i] = 0; f[k][i] = 0; }
+		if (i >= q.n) continue;
+		Cell c;
+		quadCell<D>(q, i, c);
+		int64_t nb[2 * D];
+		stencilNeighbors<D>(dom, c, nb);
+		const T a0 = A[c.g];
+		T af[2 * D];
+#pragma unroll
+		for (int fc = 0; fc < 2 * D; ++fc) af[fc] = A[(fc + 1) * N + c.g];
+#pragma unroll
+		for (int k = 0; k < K; ++k) {
+			if (!act[k]) continue;
+			const T ci = fld[k].at(vk<K>(c.B, c.g, k));
+			T s = a0 * ci;
+#pragma unroll
+			for (int fc = 0; fc < 2 * D; ++fc)
+				if (nb[fc] >= 0) s = fma(af[fc], fld[k].at(vk<K>(c.B, nb[fc], k)), s);
+			y[k][i] = s;
+			f[k][i] = ci;
+		}
+	}
+}
+
+// r = b - A x per right-hand side, (r, r) and (b, b) into acc[2k], acc[2k+1]; emit(k, o, q,
+// r[4]) stores r.
+template <typename T, int D, int K, typename Emit>
+__device__ __forceinline__ void tileResidual(const Dom<double, D> &dom, const int32_t *sB, int l0, int nc, const T *__restrict__ A,
+		const T *__restrict__ b, const T *__restrict__ x, const bool (&act)[K], double (&acc)[2 * K], Emit emit) {
+	Quad q;
+	quadAt<D, K>(dom.vec4, sB, l0, nc, q);
+	FX<T> fx[K];
+#pragma unroll
+	for (int k = 0; k < K; ++k) fx[k].x = x;
+	T y[K][4], f[K][4];
+	quadApply<T, D, K>(dom, A, q, act, fx, y, f);
 #pragma unroll
 	for (int k = 0; k < K; ++k) {
-		if (!act[k]) { out[k] = 0; continue; }
-		T s = a0 * val(c.g, k);
+		if (!act[k]) continue;
+		const int64_t o = vk<K>(q.B, q.g, k);
+		T bv[4], rv[4];
+		ld4(b + o, q.n, q.al, bv);
 #pragma unroll
-		for (int f = 0; f < 2 * D; ++f)
-			if (nb[f] >= 0) s += af[f] * val(nb[f], k);
-		out[k] = s;
+		for (int i = 0; i < 4; ++i) {
+			rv[i] = bv[i] - y[k][i];
+			acc[2 * k] = fma(double(rv[i]), double(rv[i]), acc[2 * k]);
+			acc[2 * k + 1] = fma(double(bv[i]), double(bv[i]), acc[2 * k + 1]);
+		}
+		emit(k, o, q, rv);
+	}
+}
+
+// CG phase 1 on a tile: p' = z + beta p, q = A p', (p', q)
+template <typename T, int D, int K>
+__device__ __forceinline__ void tileCgDirection(const Dom<double, D> &dom, const int32_t *sB, int l0, int nc, const T *__restrict__ A,
+		const T *z, const T *pIn, T *pOut, T *qv, const bool (&act)[K], const bool (&rs)[K], const T (&beta)[K], double (&acc)[K]) {
+	Quad q;
+	quadAt<D, K>(dom.vec4, sB, l0, nc, q);
+	FDir<T> fd[K];
+#pragma unroll
+	for (int k = 0; k < K; ++k) fd[k] = FDir<T>{z, pIn, beta[k], rs[k]};
+	T y[K][4], f[K][4];
+	quadApply<T, D, K>(dom, A, q, act, fd, y, f);
+#pragma unroll
+	for (int k = 0; k < K; ++k) {
+		if (!act[k]) continue;
+		const int64_t o = vk<K>(q.B, q.g, k);
+		st4(pOut + o, q.n, q.al, f[k]);
+		st4(qv + o, q.n, q.al, y[k]);
+#pragma unroll
+		for (int i = 0; i < 4; ++i) acc[k] = fma(double(f[k][i]), double(y[k][i]), acc[k]);
+	}
+}
+
+// CG phase 2 on a tile: x += alpha p, r -= alpha q, (r, r) (xbest = x before, when asked)
+template <typename T, int D, int K>
+__device__ __forceinline__ void tileCgUpdate(const Dom<double, D> &dom, const int32_t *sB, int l0, int nc, T *r, const T *p,
+		const T *qv, T *x, T *xbest, const SysState *sst, double (&acc)[K]) {
+	Quad q;
+	quadAt<D, K>(dom.vec4, sB, l0, nc, q);
+	const int inst = sB[B_INST];
+#pragma unroll
+	for (int k = 0; k < K; ++k) {
+		const SysState &s = sst[inst * K + k];
+		if (s.done != RUNNING) continue;
+		const T alpha = T(s.alpha);
+		const int64_t o = vk<K>(q.B, q.g, k);
+		T xv[4], pv[4], rv[4], qq[4];
+		ld4(x + o, q.n, q.al, xv);
+		ld4(p + o, q.n, q.al, pv);
+		ld4(r + o, q.n, q.al, rv);
+		ld4(qv + o, q.n, q.al, qq);
+		if (s.saveBest && xbest) st4(xbest + o, q.n, q.al, xv);
+#pragma unroll
+		for (int i = 0; i < 4; ++i) {
+			xv[i] = fma(alpha, pv[i], xv[i]);
+			rv[i] = fma(-alpha, qq[i], rv[i]);
+			acc[k] = fma(double(rv[i]), double(rv[i]), acc[k]);
+		}
+		st4(x + o, q.n, q.al, xv);
+		st4(r + o, q.n, q.al, rv);
+	}
+}
+
+// BiCGStab phase 1 on a tile: p = r + beta (p - omega v), v = A p, (r0, v)
+template <typename T, int D, int K>
+__device__ __forceinline__ void tileBicgV(const Dom<double, D> &dom, const int32_t *sB, int l0, int nc, const T *__restrict__ A,
+		const T *r, const T *pIn, const T *vIn, T *pOut, T *vOut, const T *r0, const bool (&act)[K], const bool (&rs)[K],
+		const T (&beta)[K], const T (&omega)[K], double (&acc)[K]) {
+	Quad q;
+	quadAt<D, K>(dom.vec4, sB, l0, nc, q);
+	FBicgP<T> fp[K];
+#pragma unroll
+	for (int k = 0; k < K; ++k) fp[k] = FBicgP<T>{r, pIn, vIn, beta[k], omega[k], rs[k]};
+	T y[K][4], f[K][4];
+	quadApply<T, D, K>(dom, A, q, act, fp, y, f);
+#pragma unroll
+	for (int k = 0; k < K; ++k) {
+		if (!act[k]) continue;
+		const int64_t o = vk<K>(q.B, q.g, k);
+		st4(pOut + o, q.n, q.al, f[k]);
+		st4(vOut + o, q.n, q.al, y[k]);
+		T r0v[4];
+		ld4(r0 + o, q.n, q.al, r0v);
+#pragma unroll
+		for (int i = 0; i < 4; ++i) acc[k] = fma(double(r0v[i]), double(y[k][i]), acc[k]);
+	}
+}
+
+// BiCGStab phase 2 on a tile: s = r - alpha v, t = A s, (t, s), (t, t), (s, s)
+template <typename T, int D, int K>
+__device__ __forceinline__ void tileBicgT(const Dom<double, D> &dom, const int32_t *sB, int l0, int nc, const T *__restrict__ A,
+		const T *r, const T *v, T *t, const bool (&act)[K], const T (&alpha)[K], double (&acc)[3 * K]) {
+	Quad q;
+	quadAt<D, K>(dom.vec4, sB, l0, nc, q);
+	FBicgS<T> fs[K];
+#pragma unroll
+	for (int k = 0; k < K; ++k) fs[k] = FBicgS<T>{r, v, alpha[k]};
+	T y[K][4], f[K][4];
+	quadApply<T, D, K>(dom, A, q, act, fs, y, f);
+#pragma unroll
+	for (int k = 0; k < K; ++k) {
+		if (!act[k]) continue;
+		const int64_t o = vk<K>(q.B, q.g, k);
+		st4(t + o, q.n, q.al, y[k]);
+#pragma unroll
+		for (int i = 0; i < 4; ++i) {
+			acc[3 * k + 0] = fma(double(y[k][i]), double(f[k][i]), acc[3 * k + 0]);
+			acc[3 * k + 1] = fma(double(y[k][i]), double(y[k][i]), acc[3 * k + 1]);
+			acc[3 * k + 2] = fma(double(f[k][i]), double(f[k][i]), acc[3 * k + 2]);
+		}
+	}
+}
+
+// BiCGStab phase 3 on a tile: x += alpha p + omega s, r = s - omega t, (r0, r), (r, r); after
+// a converged half step x += alpha p, r = s
+template <typename T, int D, int K>
+__device__ __forceinline__ void tileBicgUpdate(const Dom<double, D> &dom, const int32_t *sB, int l0, int nc, T *r, const T *r0,
+		const T *p, const T *v, const T *t, T *x, const SysState *sst, double (&acc)[2 * K]) {
+	Quad q;
+	quadAt<D, K>(dom.vec4, sB, l0, nc, q);
+	const int inst = sB[B_INST];
+#pragma unroll
+	for (int k = 0; k < K; ++k) {
+		const SysState &s = sst[inst * K + k];
+		if (s.done != RUNNING) continue;
+		const T alpha = T(s.alpha), omega = T(s.omega);
+		const int64_t o = vk<K>(q.B, q.g, k);
+		T rv[4], vv[4], pv[4], xv[4];
+		ld4(r + o, q.n, q.al, rv);
+		ld4(v + o, q.n, q.al, vv);
+		ld4(p + o, q.n, q.al, pv);
+		ld4(x + o, q.n, q.al, xv);
+		if (s.halfDone) {
+#pragma unroll
+			for (int i = 0; i < 4; ++i) {
+				xv[i] = fma(alpha, pv[i], xv[i]);
+				rv[i] = fma(-alpha, vv[i], rv[i]);
+			}
+		} else {
+			T tv[4], r0v[4];
+			ld4(t + o, q.n, q.al, tv);
+			ld4(r0 + o, q.n, q.al, r0v);
+#pragma unroll
+			for (int i = 0; i < 4; ++i) {
+				const T si = fma(-alpha, vv[i], rv[i]);
+				xv[i] = fma(omega, si, fma(alpha, pv[i], xv[i]));
+				rv[i] = fma(-omega, tv[i], si);
+				acc[2 * k + 0] = fma(double(r0v[i]), double(rv[i]), acc[2 * k + 0]);
+				acc[2 * k + 1] = fma(double(rv[i]), double(rv[i]), acc[2 * k + 1]);
+			}
+		}
+		st4(x + o, q.n, q.al, xv);
+		st4(r + o, q.n, q.al, rv);
 	}
 }
 
@@ -256,25 +569,10 @@ __global__ void __launch_bounds__(PHB_TILE) kResidual(Dom<double, D> dom, const 
 	double acc[2 * K];
 #pragma unroll
 	for (int k = 0; k < 2 * K; ++k) acc[k] = 0;
-	for (int j_ = 0; j_ < CPT; ++j_) {
-		Cell c;
-		if (!cellAt<D>(sB, l0_, nc_, j_, c)) break;
-		int64_t nb[2 * D];
-		stencilNeighbors<D>(dom, c, nb);
-		T y[K];
-		applyA<T, D, K>(A, dom.ncells, c, nb, act, [&](int64_t g, int k) { return x[vk<K>(c.B, g, k)]; }, y);
-#pragma unroll
-		for (int k = 0; k < K; ++k) {
-			if (!act[k]) continue;
-			const int64_t o = vk<K>(c.B, c.g, k);
-			const T bi = b[o];
-			const T ri = bi - y[k];
-			r[o] = ri;
-			if (BICG) r0[o] = ri;
-			acc[2 * k] += double(ri) * double(ri);
-			acc[2 * k + 1] += double(bi) * double(bi);
-		}
-	}
+	tileResidual<T, D, K>(dom, sB, l0_, nc_, A, b, x, act, acc, [&](int, int64_t o, const Quad &q, const T (&rv)[4]) {
+		st4(r + o, q.n, q.al, rv);
+		if (BICG) st4(r0 + o, q.n, q.al, rv);
+	});
 	if (storePartials<2 * K>(acc, partial, &ctrl->counter)) {
 		const bool relative = tol.mode == 1;
 		finalizeSystems<K, 2, 1>(dom.insts, dom.ninst, partial, st, ctrl, [&](SysState &s, int in, const double *red, double bb) {
@@ -314,27 +612,7 @@ __global__ void __launch_bounds__(PHB_TILE) kCgDirection(Dom<double, D> dom, con
 	double acc[K];
 #pragma unroll
 	for (int k = 0; k < K; ++k) acc[k] = 0;
-	for (int j_ = 0; j_ < CPT; ++j_) {
-		Cell c;
-		if (!cellAt<D>(sB, l0_, nc_, j_, c)) break;
-		int64_t nb[2 * D];
-		stencilNeighbors<D>(dom, c, nb);
-		auto pv = [&](int64_t g, int k) {
-			const int64_t o = vk<K>(c.B, g, k);
-			return rs[k] ? r[o] : r[o] + beta[k] * pIn[o];
-		};
-		T y[K];
-		applyA<T, D, K>(A, dom.ncells, c, nb, act, pv, y);
-#pragma unroll
-		for (int k = 0; k < K; ++k) {
-			if (!act[k]) continue;
-			const int64_t o = vk<K>(c.B, c.g, k);
-			const T pi = pv(c.g, k);
-			pOut[o] = pi;
-			q[o] = y[k];
-			acc[k] += double(pi) * double(y[k]);
-		}
-	}
+	tileCgDirection<T, D, K>(dom, sB, l0_, nc_, A, r, pIn, pOut, q, act, rs, beta, acc);
 	if (storePartials<K>(acc, partial, &ctrl->counter)) {
 		finalizeSystems<K, 1>(dom.insts, dom.ninst, partial, st, ctrl, [&](SysState &s, int, const double *red, double) {
 			const double alpha = s.rho / red[0];
@@ -355,27 +633,10 @@ __global__ void __launch_bounds__(PHB_TILE) kCgUpdate(Dom<double, D> dom, T *__r
 	__shared__ int32_t sB[PHB_BREC];
 	int l0_, nc_;
 	loadTile<double, D>(dom, sB, l0_, nc_);
-	const int inst = sB[B_INST];
 	double acc[K];
 #pragma unroll
 	for (int k = 0; k < K; ++k) acc[k] = 0;
-	for (int j_ = 0; j_ < CPT; ++j_) {
-		Cell c;
-		if (!cellAt<D>(sB, l0_, nc_, j_, c)) break;
-#pragma unroll
-		for (int k = 0; k < K; ++k) {
-			const SysState &s = st[inst * K + k];
-			if (s.done != RUNNING) continue;
-			const T alpha = T(s.alpha);
-			const int64_t o = vk<K>(c.B, c.g, k);
-			const T xi = x[o];
-			if (s.saveBest && xbest) xbest[o] = xi;
-			x[o] = xi + alpha * p[o];
-			const T ri = r[o] - alpha * q[o];
-			r[o] = ri;
-			acc[k] += double(ri) * double(ri);
-		}
-	}
+	tileCgUpdate<T, D, K>(dom, sB, l0_, nc_, r, p, q, x, xbest, st, acc);
 	if (storePartials<K>(acc, partial, &ctrl->counter)) {
 		finalizeSystems<K, 1>(dom.insts, dom.ninst, partial, st, ctrl, [&](SysState &s, int in, const double *red, double) {
 			const double crit = sqrt(red[0]) * normScale(dom.insts, in);
@@ -448,26 +709,7 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgV(Dom<double, D> dom, const T *
 	double acc[K];
 #pragma unroll
 	for (int k = 0; k < K; ++k) acc[k] = 0;
-	for (int j_ = 0; j_ < CPT; ++j_) {
-		Cell c;
-		if (!cellAt<D>(sB, l0_, nc_, j_, c)) break;
-		int64_t nb[2 * D];
-		stencilNeighbors<D>(dom, c, nb);
-		auto pv = [&](int64_t g, int k) {
-			const int64_t o = vk<K>(c.B, g, k);
-			return rs[k] ? r[o] : r[o] + beta[k] * (pIn[o] - omega[k] * vIn[o]);
-		};
-		T y[K];
-		applyA<T, D, K>(A, dom.ncells, c, nb, act, pv, y);
-#pragma unroll
-		for (int k = 0; k < K; ++k) {
-			if (!act[k]) continue;
-			const int64_t o = vk<K>(c.B, c.g, k);
-			pOut[o] = pv(c.g, k);
-			vOut[o] = y[k];
-			acc[k] += double(r0[o]) * double(y[k]);
-		}
-	}
+	tileBicgV<T, D, K>(dom, sB, l0_, nc_, A, r, pIn, vIn, pOut, vOut, r0, act, rs, beta, omega, acc);
 	if (storePartials<K>(acc, partial, &ctrl->counter)) {
 		finalizeSystems<K, 1>(dom.insts, dom.ninst, partial, st, ctrl, [&](SysState &s, int, const double *red, double) {
 			const double alpha = s.rho / red[0];
@@ -498,28 +740,7 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgT(Dom<double, D> dom, const T *
 	double acc[3 * K];
 #pragma unroll
 	for (int k = 0; k < 3 * K; ++k) acc[k] = 0;
-	for (int j_ = 0; j_ < CPT; ++j_) {
-		Cell c;
-		if (!cellAt<D>(sB, l0_, nc_, j_, c)) break;
-		int64_t nb[2 * D];
-		stencilNeighbors<D>(dom, c, nb);
-		auto sv = [&](int64_t g, int k) {
-			const int64_t o = vk<K>(c.B, g, k);
-			return r[o] - alpha[k] * v[o];
-		};
-		T y[K];
-		applyA<T, D, K>(A, dom.ncells, c, nb, act, sv, y);
-#pragma unroll
-		for (int k = 0; k < K; ++k) {
-			if (!act[k]) continue;
-			const int64_t o = vk<K>(c.B, c.g, k);
-			const T si = sv(c.g, k);
-			t[o] = y[k];
-			acc[3 * k + 0] += double(y[k]) * double(si);
-			acc[3 * k + 1] += double(y[k]) * double(y[k]);
-			acc[3 * k + 2] += double(si) * double(si);
-		}
-	}
+	tileBicgT<T, D, K>(dom, sB, l0_, nc_, A, r, v, t, act, alpha, acc);
 	if (storePartials<3 * K>(acc, partial, &ctrl->counter)) {
 		finalizeSystems<K, 3>(dom.insts, dom.ninst, partial, st, ctrl, [&](SysState &s, int in, const double *red, double) {
 			const double critS = sqrt(red[2]) * normScale(dom.insts, in);
@@ -544,32 +765,10 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgUpdate(Dom<double, D> dom, T *_
 	__shared__ int32_t sB[PHB_BREC];
 	int l0_, nc_;
 	loadTile<double, D>(dom, sB, l0_, nc_);
-	const int inst = sB[B_INST];
 	double acc[2 * K];
 #pragma unroll
 	for (int k = 0; k < 2 * K; ++k) acc[k] = 0;
-	for (int j_ = 0; j_ < CPT; ++j_) {
-		Cell c;
-		if (!cellAt<D>(sB, l0_, nc_, j_, c)) break;
-#pragma unroll
-		for (int k = 0; k < K; ++k) {
-			const SysState &s = st[inst * K + k];
-			if (s.done != RUNNING) continue;
-			const T alpha = T(s.alpha), omega = T(s.omega);
-			const int64_t o = vk<K>(c.B, c.g, k);
-			const T si = r[o] - alpha * v[o];
-			if (s.halfDone) {
-				x[o] += alpha * p[o];
-				r[o] = si;
-			} else {
-				x[o] += alpha * p[o] + omega * si;
-				const T ri = si - omega * t[o];
-				r[o] = ri;
-				acc[2 * k + 0] += double(r0[o]) * double(ri);
-				acc[2 * k + 1] += double(ri) * double(ri);
-			}
-		}
-	}
+	tileBicgUpdate<T, D, K>(dom, sB, l0_, nc_, r, r0, p, v, t, x, st, acc);
 	if (storePartials<2 * K>(acc, partial, &ctrl->counter)) {
 		finalizeSystems<K, 2>(dom.insts, dom.ninst, partial, st, ctrl, [&](SysState &s, int in, const double *red, double) {
 			if (s.halfDone) { s.done = CONVERGED; s.crit = s.halfCrit; s.usedIt = s.it; return; }
@@ -623,27 +822,16 @@ __global__ void __launch_bounds__(PHB_TILE) kRefineResidual(Dom<double, D> dom, 
 	double acc[2 * K];
 #pragma unroll
 	for (int k = 0; k < 2 * K; ++k) acc[k] = 0;
-	for (int j_ = 0; j_ < CPT; ++j_) {
-		Cell c;
-		if (!cellAt<D>(sB, l0_, nc_, j_, c)) break;
-		int64_t nb[2 * D];
-		stencilNeighbors<D>(dom, c, nb);
-		bool act[K];
+	bool act[K];
 #pragma unroll
-		for (int k = 0; k < K; ++k) act[k] = true;
-		double y[K];
-		applyA<double, D, K>(A, dom.ncells, c, nb, act, [&](int64_t g, int k) { return x[vk<K>(c.B, g, k)]; }, y);
+	for (int k = 0; k < K; ++k) act[k] = true;
+	tileResidual<double, D, K>(dom, sB, l0_, nc_, A, b, x, act, acc, [&](int, int64_t o, const Quad &q, const double (&rv)[4]) {
+		float r4[4], z4[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-		for (int k = 0; k < K; ++k) {
-			const int64_t o = vk<K>(c.B, c.g, k);
-			const double bi = b[o];
-			const double ri = bi - y[k];
-			r32[o] = float(ri);
-			e32[o] = 0.f;
-			acc[2 * k] += ri * ri;
-			acc[2 * k + 1] += bi * bi;
-		}
-	}
+		for (int i = 0; i < 4; ++i) r4[i] = float(rv[i]);
+		st4(r32 + o, q.n, q.al, r4);
+		st4(e32 + o, q.n, q.al, z4);
+	});
 	if (storePartials<2 * K>(acc, partial, &ctrl->counter)) {
 		const int nsys = dom.ninst * K;
 		// every system is visited, also once done, so that the inner solve of a finished
@@ -901,24 +1089,8 @@ __global__ void __launch_bounds__(PHB_TILE) kCgPersistent(Dom<double, D> dom, co
 		double acc[2 * K];
 #pragma unroll
 		for (int k = 0; k < 2 * K; ++k) acc[k] = 0;
-		for (int j = 0; j < CPT; ++j) {
-			Cell c;
-			if (!cellAt<D>(sB, l0, nc, j, c)) break;
-			int64_t nb[2 * D];
-			stencilNeighbors<D>(dom, c, nb);
-			T y[K];
-			applyA<T, D, K>(A, N, c, nb, act, [&](int64_t g, int k) { return x[vk<K>(c.B, g, k)]; }, y);
-#pragma unroll
-			for (int k = 0; k < K; ++k) {
-				if (!act[k]) continue;
-				const int64_t o = vk<K>(c.B, c.g, k);
-				const T bi = b[o];
-				const T ri = bi - y[k];
-				r[o] = ri;
-				acc[2 * k] += double(ri) * double(ri);
-				acc[2 * k + 1] += double(bi) * double(bi);
-			}
-		}
+		tileResidual<T, D, K>(dom, sB, l0, nc, A, b, x, act, acc,
+				[&](int, int64_t o, const Quad &q, const T (&rv)[4]) { st4(r + o, q.n, q.al, rv); });
 		blockSumTo<2 * K>(acc, pp + (size_t)tile * 2 * K);
 	});
 	if (!gridBarrier(ctrl, gen)) return;
@@ -969,27 +1141,7 @@ __global__ void __launch_bounds__(PHB_TILE) kCgPersistent(Dom<double, D> dom, co
 			double acc[K];
 #pragma unroll
 			for (int k = 0; k < K; ++k) acc[k] = 0;
-			for (int j = 0; j < CPT; ++j) {
-				Cell c;
-				if (!cellAt<D>(sB, l0, nc, j, c)) break;
-				int64_t nb[2 * D];
-				stencilNeighbors<D>(dom, c, nb);
-				auto pv = [&](int64_t g, int k) {
-					const int64_t o = vk<K>(c.B, g, k);
-					return rs[k] ? dsrc[o] : dsrc[o] + beta[k] * pIn[o];
-				};
-				T y[K];
-				applyA<T, D, K>(A, N, c, nb, act, pv, y);
-#pragma unroll
-				for (int k = 0; k < K; ++k) {
-					if (!act[k]) continue;
-					const int64_t o = vk<K>(c.B, c.g, k);
-					const T pi = pv(c.g, k);
-					pOut[o] = pi;
-					q[o] = y[k];
-					acc[k] += double(pi) * double(y[k]);
-				}
-			}
+			tileCgDirection<T, D, K>(dom, sB, l0, nc, A, dsrc, pIn, pOut, q, act, rs, beta, acc);
 			blockSumTo<K>(acc, pp + (size_t)tile * K);
 		});
 		if (!gridBarrier(ctrl, gen)) return;
@@ -1002,27 +1154,10 @@ __global__ void __launch_bounds__(PHB_TILE) kCgPersistent(Dom<double, D> dom, co
 		// x += alpha p', r -= alpha q, (r, r)
 		pp = partial + (size_t)(ph++ & 1) * half;
 		forMyTiles<D>(dom, sB, [&](int tile, int l0, int nc) {
-			const int inst = sB[B_INST];
 			double acc[K];
 #pragma unroll
 			for (int k = 0; k < K; ++k) acc[k] = 0;
-			for (int j = 0; j < CPT; ++j) {
-				Cell c;
-				if (!cellAt<D>(sB, l0, nc, j, c)) break;
-#pragma unroll
-				for (int k = 0; k < K; ++k) {
-					const SysState &s = sst[inst * K + k];
-					if (s.done != RUNNING) continue;
-					const T alpha = T(s.alpha);
-					const int64_t o = vk<K>(c.B, c.g, k);
-					const T xi = x[o];
-					if (s.saveBest && xbest) xbest[o] = xi;
-					x[o] = xi + alpha * pOut[o];
-					const T ri = r[o] - alpha * q[o];
-					r[o] = ri;
-					acc[k] += double(ri) * double(ri);
-				}
-			}
+			tileCgUpdate<T, D, K>(dom, sB, l0, nc, r, pOut, q, x, xbest, sst, acc);
 			blockSumTo<K>(acc, pp + (size_t)tile * K);
 		});
 		if (!gridBarrier(ctrl, gen)) return;
@@ -1098,25 +1233,10 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgPersistent(Dom<double, D> dom, 
 		double acc[2 * K];
 #pragma unroll
 		for (int k = 0; k < 2 * K; ++k) acc[k] = 0;
-		for (int j = 0; j < CPT; ++j) {
-			Cell c;
-			if (!cellAt<D>(sB, l0, nc, j, c)) break;
-			int64_t nb[2 * D];
-			stencilNeighbors<D>(dom, c, nb);
-			T y[K];
-			applyA<T, D, K>(A, N, c, nb, act, [&](int64_t g, int k) { return x[vk<K>(c.B, g, k)]; }, y);
-#pragma unroll
-			for (int k = 0; k < K; ++k) {
-				if (!act[k]) continue;
-				const int64_t o = vk<K>(c.B, c.g, k);
-				const T bi = b[o];
-				const T ri = bi - y[k];
-				r[o] = ri;
-				r0[o] = ri;
-				acc[2 * k] += double(ri) * double(ri);
-				acc[2 * k + 1] += double(bi) * double(bi);
-			}
-		}
+		tileResidual<T, D, K>(dom, sB, l0, nc, A, b, x, act, acc, [&](int, int64_t o, const Quad &q, const T (&rv)[4]) {
+			st4(r + o, q.n, q.al, rv);
+			st4(r0 + o, q.n, q.al, rv);
+		});
 		blockSumTo<2 * K>(acc, pp + (size_t)tile * 2 * K);
 	});
 	if (!gridBarrier(ctrl, gen)) return;
@@ -1142,26 +1262,7 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgPersistent(Dom<double, D> dom, 
 			double acc[K];
 #pragma unroll
 			for (int k = 0; k < K; ++k) acc[k] = 0;
-			for (int j = 0; j < CPT; ++j) {
-				Cell c;
-				if (!cellAt<D>(sB, l0, nc, j, c)) break;
-				int64_t nb[2 * D];
-				stencilNeighbors<D>(dom, c, nb);
-				auto pv = [&](int64_t g, int k) {
-					const int64_t o = vk<K>(c.B, g, k);
-					return rs[k] ? r[o] : r[o] + beta[k] * (pIn[o] - omega[k] * vIn[o]);
-				};
-				T y[K];
-				applyA<T, D, K>(A, N, c, nb, act, pv, y);
-#pragma unroll
-				for (int k = 0; k < K; ++k) {
-					if (!act[k]) continue;
-					const int64_t o = vk<K>(c.B, c.g, k);
-					pOut[o] = pv(c.g, k);
-					vOut[o] = y[k];
-					acc[k] += double(r0[o]) * double(y[k]);
-				}
-			}
+			tileBicgV<T, D, K>(dom, sB, l0, nc, A, r, pIn, vIn, pOut, vOut, r0, act, rs, beta, omega, acc);
 			blockSumTo<K>(acc, pp + (size_t)tile * K);
 		});
 		if (!gridBarrier(ctrl, gen)) return;
@@ -1186,28 +1287,7 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgPersistent(Dom<double, D> dom, 
 			double acc[3 * K];
 #pragma unroll
 			for (int k = 0; k < 3 * K; ++k) acc[k] = 0;
-			for (int j = 0; j < CPT; ++j) {
-				Cell c;
-				if (!cellAt<D>(sB, l0, nc, j, c)) break;
-				int64_t nb[2 * D];
-				stencilNeighbors<D>(dom, c, nb);
-				auto sv = [&](int64_t g, int k) {
-					const int64_t o = vk<K>(c.B, g, k);
-					return r[o] - alpha[k] * vOut[o];
-				};
-				T y[K];
-				applyA<T, D, K>(A, N, c, nb, act, sv, y);
-#pragma unroll
-				for (int k = 0; k < K; ++k) {
-					if (!act[k]) continue;
-					const int64_t o = vk<K>(c.B, c.g, k);
-					const T si = sv(c.g, k);
-					t[o] = y[k];
-					acc[3 * k + 0] += double(y[k]) * double(si);
-					acc[3 * k + 1] += double(y[k]) * double(y[k]);
-					acc[3 * k + 2] += double(si) * double(si);
-				}
-			}
+			tileBicgT<T, D, K>(dom, sB, l0, nc, A, r, vOut, t, act, alpha, acc);
 			blockSumTo<3 * K>(acc, pp + (size_t)tile * 3 * K);
 		});
 		if (!gridBarrier(ctrl, gen)) return;
@@ -1225,32 +1305,10 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgPersistent(Dom<double, D> dom, 
 		// x += alpha p + omega s, r = s - omega t, (r0, r), (r, r)
 		pp = partial + (size_t)(ph++ & 1) * half;
 		forMyTiles<D>(dom, sB, [&](int tile, int l0, int nc) {
-			const int inst = sB[B_INST];
 			double acc[2 * K];
 #pragma unroll
 			for (int k = 0; k < 2 * K; ++k) acc[k] = 0;
-			for (int j = 0; j < CPT; ++j) {
-				Cell c;
-				if (!cellAt<D>(sB, l0, nc, j, c)) break;
-#pragma unroll
-				for (int k = 0; k < K; ++k) {
-					const SysState &s = sst[inst * K + k];
-					if (s.done != RUNNING) continue;
-					const T alpha = T(s.alpha), omega = T(s.omega);
-					const int64_t o = vk<K>(c.B, c.g, k);
-					const T si = r[o] - alpha * vOut[o];
-					if (s.halfDone) {
-						x[o] += alpha * pOut[o];
-						r[o] = si;
-					} else {
-						x[o] += alpha * pOut[o] + omega * si;
-						const T ri = si - omega * t[o];
-						r[o] = ri;
-						acc[2 * k + 0] += double(r0[o]) * double(ri);
-						acc[2 * k + 1] += double(ri) * double(ri);
-					}
-				}
-			}
+			tileBicgUpdate<T, D, K>(dom, sB, l0, nc, r, r0, pOut, vOut, t, x, sst, acc);
 			blockSumTo<2 * K>(acc, pp + (size_t)tile * 2 * K);
 		});
 		if (!gridBarrier(ctrl, gen)) return;
@@ -1281,6 +1339,15 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgPersistent(Dom<double, D> dom, 
 
 // host side --------------------------------------------------------------------------------
 static size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+// Dom::vec4 of a launch: every operand on a 16-byte boundary and a cell count that keeps the
+// stencil's slot rows aligned
+static int vec4Ok(const phb_domain *dom, std::initializer_list<const void *> ptrs) {
+	if (dom->ncells % 4) return 0;
+	for (const void *p : ptrs)
+		if (p && ((uintptr_t)p & 15)) return 0;
+	return 1;
+}
 
 struct Layout {
 	size_t off[12];
@@ -1447,6 +1514,7 @@ static int launchPersistent(const phb_domain *dom, const phb_solve *sv, cudaStre
 	const T *A = (const T *)sv->A;
 	const T *b = (const T *)sv->b;
 	T *x = (T *)sv->x;
+	dm.vec4 = vec4Ok(dom, {A, b, x, w});
 	const int nsys = dom->ninst * K;
 	const size_t smem = (size_t)nsys * sizeof(SysState);
 	if (smem > 160 * 1024) return setError(PHB_ERR_RANGE, "persistent solve: too many systems for the per-CTA state copy");
@@ -1508,6 +1576,7 @@ static int emitSolve(const phb_domain *dom, const phb_solve *sv, cudaStream_t s,
 	const T *A = (const T *)sv->A;
 	const T *b = (const T *)sv->b;
 	T *x = (T *)sv->x;
+	dm.vec4 = vec4Ok(dom, {A, b, x, w});
 	const int nsys = dom->ninst * K;
 	const int tiles = dom->ntiles;
 	const int maxit = std::max(1, sv->maxit);
@@ -1710,6 +1779,7 @@ static int emitRefine(const phb_domain *dom, const phb_refine *rf, cudaStream_t 
 	float *r32 = (float *)(w + inner);
 	float *e32 = (float *)(w + inner + vb);
 	double *partial = (double *)(w + inner + 2 * vb);
+	dm.vec4 = vec4Ok(dom, {rf->A64, rf->b, rf->x, w});
 	const StateLayout SL = stateLayout(dom, K);
 	char *sb = (char *)rf->state;
 	Control *ctrlO = (Control *)(sb + SL.ctrl2);
@@ -1875,6 +1945,7 @@ static int runCgNoAlloc(const phb_domain *dom, const phb_solve *sv, phb_solve_re
 	const T *A = (const T *)sv->A;
 	const T *b = (const T *)sv->b;
 	T *x = (T *)sv->x;
+	dm.vec4 = vec4Ok(dom, {A, b, x, w});
 	T *r = (T *)(w + L.off[0]), *q = (T *)(w + L.off[1]), *p0 = (T *)(w + L.off[2]), *p1 = (T *)(w + L.off[3]);
 	T *xbest = sv->return_best ? (T *)(w + L.off[4]) : nullptr;
 	const int nsys = dom->ninst * K;

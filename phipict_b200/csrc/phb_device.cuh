@@ -46,6 +46,9 @@ struct Dom {
 	const double *dt, *nu;
 	int64_t ms, fms, ncells;
 	int nblocks, ninst, ntiles;
+	// set by a launcher whose vector and stencil operands all start on 16-byte boundaries and
+	// whose ncells is a multiple of 4: 4-cell groups at aligned indices may use vector loads
+	int vec4 = 0;
 
 	Dom() = default;
 	__host__ Dom(const phb_domain &d)
@@ -275,6 +278,100 @@ __device__ __forceinline__ bool cellAt(const int32_t *sB, int l0, int nc, int j,
 	c.g = sB[B_CELLOFF] + l;
 	c.mi = sB[B_METOFF] + l;
 	return true;
+}
+
+// Four consecutive cells of a tile taken by one thread (cells l0 + 4 t + i, i < n): the
+// coordinates are computed once per group, and a group inside one row away from the y and z
+// faces of its block has its stencil neighbours at the fixed strides 1, nx and nx*ny (only a
+// row end needs the neighbour across the x face), so that four cells' loads issue together
+// (as 16-byte vectors when aligned) instead of one neighbour search per cell and face.
+static_assert(PHB_TILE_CELLS == 4 * PHB_TILE, "a quad is four cells per thread");
+struct Quad {
+	const int32_t *B; // block record
+	int64_t g;        // flat index of the first cell
+	int l;            // block-local index of the first cell
+	int n;            // valid cells, 0..4
+	int p[3];         // coordinates of the first cell
+	int sy, sz;       // neighbour strides in y and z
+	bool fast;        // four valid cells in one row, none on a y or z face of the block: the
+	                  // neighbours are at fixed strides except across an x face at a row end
+	bool al;          // four valid cells at a 4-aligned index of every operand: vector loads
+	bool alY, alZ;    // al, and the y (z) neighbour groups aligned too
+};
+
+// K: right-hand sides per instance ([inst][K][cells] layout; their offsets must keep the
+// alignment for vector access).
+template <int D, int K = 1>
+__device__ __forceinline__ void quadAt(int vec4, const int32_t *sB, int l0, int nc, Quad &q) {
+	const int l = l0 + 4 * (int)threadIdx.x;
+	const int nx = sB[B_NX], ny = sB[B_NY];
+	q.B = sB;
+	q.l = l;
+	q.n = max(0, min(4, nc - l));
+	q.g = (int64_t)sB[B_CELLOFF] + l;
+	const int row = l / nx;
+	q.p[0] = l - row * nx;
+	q.p[1] = D > 2 ? row % ny : row;
+	q.p[2] = D > 2 ? row / ny : 0;
+	q.sy = nx;
+	q.sz = nx * ny;
+	bool fast = q.n == 4 && q.p[0] + 3 <= nx - 1 && q.p[1] >= 1 && q.p[1] <= ny - 2;
+	if (D > 2) fast = fast && q.p[2] >= 1 && q.p[2] <= sB[B_NZ] - 2;
+	q.fast = fast;
+	bool al = vec4 && q.n == 4 && (q.g & 3) == 0;
+	if (K > 1) al = al && ((sB[B_INSTOFF] | sB[B_INSTN]) & 3) == 0;
+	q.al = al;
+	q.alY = al && (nx & 3) == 0;
+	q.alZ = al && (q.sz & 3) == 0;
+}
+
+// The i-th cell of a quad (i < q.n) as a Cell.
+template <int D>
+__device__ __forceinline__ void quadCell(const Quad &q, int i, Cell &c) {
+	const int nx = q.B[B_NX], ny = q.B[B_NY];
+	c.B = q.B;
+	c.p[0] = q.p[0] + i;
+	c.p[1] = q.p[1];
+	c.p[2] = q.p[2];
+	while (c.p[0] >= nx) {
+		c.p[0] -= nx;
+		if (++c.p[1] == ny && D > 2) { c.p[1] = 0; ++c.p[2]; }
+	}
+	c.g = (int)(q.g + i);
+	c.mi = q.B[B_METOFF] + q.l + i;
+}
+
+// Four consecutive values: one 16-byte vector load (two for double) when `al`, else scalar
+// loads of the first n (zeros after).
+template <typename T>
+__device__ __forceinline__ void ld4(const T *p, int n, bool al, T (&v)[4]) {
+	if (al) {
+		if constexpr (sizeof(T) == 4) {
+			const float4 f = *reinterpret_cast<const float4 *>(p);
+			v[0] = f.x; v[1] = f.y; v[2] = f.z; v[3] = f.w;
+		} else {
+			const double2 a = reinterpret_cast<const double2 *>(p)[0], b = reinterpret_cast<const double2 *>(p)[1];
+			v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+		}
+		return;
+	}
+#pragma unroll
+	for (int i = 0; i < 4; ++i) v[i] = i < n ? p[i] : T(0);
+}
+template <typename T>
+__device__ __forceinline__ void st4(T *p, int n, bool al, const T (&v)[4]) {
+	if (al) {
+		if constexpr (sizeof(T) == 4) {
+			*reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+		} else {
+			reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+			reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+		}
+		return;
+	}
+#pragma unroll
+	for (int i = 0; i < 4; ++i)
+		if (i < n) p[i] = v[i];
 }
 
 } // namespace phb
