@@ -144,6 +144,7 @@ class AmgHierarchy:
         self.sizes: list[int] = []
         self.records = records  # host (blocks, tiles, insts) of every level
         self.level_A: list[torch.Tensor | None] = [None]  # coarse operators (level 0: the fine matrix)
+        self.level_wdinv: list[torch.Tensor] = []  # omega / diagonal per level (0 on zero rows)
         fine = domain.desc()
         N0 = int(fine.ncells)
         self.z = torch.zeros(N0, dtype=torch.float32, device=dev)
@@ -155,6 +156,7 @@ class AmgHierarchy:
                 lv.x = self.z.data_ptr()
                 wd = torch.zeros(N0, dtype=torch.float32, device=dev)
                 self._keep.append(wd)
+                self.level_wdinv.append(wd)
                 lv.wdinv = wd.data_ptr()
                 self.sizes.append(N0)
                 continue
@@ -168,6 +170,7 @@ class AmgHierarchy:
             x = torch.zeros(n, dtype=torch.float32, device=dev)
             wd = torch.zeros(n, dtype=torch.float32, device=dev)
             self._keep += [bt, tt, it, A, b, x, wd]
+            self.level_wdinv.append(wd)
             lv.wdinv = wd.data_ptr()
             self.level_A.append(A)
             d = _lib.PhbDomain()

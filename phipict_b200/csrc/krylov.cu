@@ -680,7 +680,7 @@ __device__ __forceinline__ void pcgRho(SysState &s, double rz) {
 template <int D>
 __global__ void __launch_bounds__(PHB_TILE) kPcgPrecond(Dom<double, D> dom, AmgView<D> mg, SysState *st, double *partial, Control *ctrl) {
 	__shared__ int32_t sB[PHB_BREC];
-	double acc[1] = {amgProlongTile<D>(mg, 0, blockIdx.x, sB, mg.x[0])};
+	double acc[1] = {amgFineQuads(mg) ? amgProlongQuad<D>(mg, 0, blockIdx.x, sB, mg.x[0]) : amgProlongTile<D>(mg, 0, blockIdx.x, sB, mg.x[0])};
 	if (storePartials<1>(acc, partial, &ctrl->counter)) {
 		finalizeSystems<1, 1>(dom.insts, dom.ninst, partial, st, ctrl, [&](SysState &s, int, const double *red, double) { pcgRho(s, red[0]); });
 	}
@@ -1062,10 +1062,15 @@ __device__ __forceinline__ void residualDecision(const Dom<double, 3> *, SysStat
 
 // PC: AMG-preconditioned CG (float, one right-hand side): every iteration first runs the
 // V-cycle of `mg` on r, level by level between grid barriers, and takes the direction from z.
-template <typename T, int D, int K, bool STOPSTART, bool PC = false>
-__global__ void __launch_bounds__(PHB_TILE) kCgPersistent(Dom<double, D> dom, const T *__restrict__ A, const T *__restrict__ b,
+// QUADS (kCgPersistentQuads, for a finest level of at least AMG_QUAD_MIN_CELLS cells): the
+// finest restriction and prolongation in their one-coarse-cell-per-thread and quad forms. It is
+// a kernel of its own, so that the smaller grids' kernel keeps the compiler's register choice,
+// and is held to four resident CTAs per SM (64 registers, some spills), which measured faster
+// on large grids than the 128 registers the compiler takes at two CTAs per SM.
+template <typename T, int D, int K, bool STOPSTART, bool PC, bool QUADS>
+__device__ __forceinline__ void cgPersistentBody(const Dom<double, D> &dom, const T *__restrict__ A, const T *__restrict__ b,
 		T *__restrict__ x, T *__restrict__ r, T *__restrict__ p0, T *__restrict__ p1, T *__restrict__ q, T *__restrict__ xbest,
-		SysState *st, double *partial, Control *ctrl, phb_tolerance tol, int returnBest, int maxit, AmgView<D> mg) {
+		SysState *st, double *partial, Control *ctrl, const phb_tolerance &tol, int returnBest, int maxit, const AmgView<D> &mg) {
 	static_assert(!PC || (std::is_same<T, float>::value && K == 1), "the V-cycle preconditions float single-rhs CG");
 	extern __shared__ SysState sst[];
 	__shared__ int32_t sB[PHB_BREC];
@@ -1104,8 +1109,13 @@ __global__ void __launch_bounds__(PHB_TILE) kCgPersistent(Dom<double, D> dom, co
 	for (int iter = 0; running > 0 && iter <= maxit + 1; ++iter) {
 		if constexpr (PC) {
 			const int L = mg.nlevels;
+			constexpr bool quads = QUADS;
 			for (int l = 0; l + 1 < L; ++l) {
-				for (int sub = blockIdx.x; sub < mg.lv[l + 1].ntiles * Restrict<D>::PER_TILE; sub += gridDim.x) amgRestrictSub<D>(mg, l, sub, sB);
+				if (l == 0 && quads) {
+					for (int sub = blockIdx.x; sub < mg.lv[1].ntiles * RESTRICT1_PER_TILE; sub += gridDim.x) amgRestrictCoarseCell<D>(mg, 0, sub, sB);
+				} else {
+					for (int sub = blockIdx.x; sub < mg.lv[l + 1].ntiles * Restrict<D>::PER_TILE; sub += gridDim.x) amgRestrictSub<D>(mg, l, sub, sB);
+				}
 				if (!gridBarrier(ctrl, gen)) return;
 			}
 			amgCoarseRows<D>(mg, int(blockIdx.x * NWARPS + (threadIdx.x >> 5)), int(gridDim.x * NWARPS));
@@ -1119,7 +1129,7 @@ __global__ void __launch_bounds__(PHB_TILE) kCgPersistent(Dom<double, D> dom, co
 			}
 			pp = partial + (size_t)(ph++ & 1) * half;
 			for (int tile = blockIdx.x; tile < dom.ntiles; tile += gridDim.x) {
-				double acc[1] = {amgProlongTile<D>(mg, 0, tile, sB, mg.x[0])};
+				double acc[1] = {quads ? amgProlongQuad<D>(mg, 0, tile, sB, mg.x[0]) : amgProlongTile<D>(mg, 0, tile, sB, mg.x[0])};
 				blockSumTo<1>(acc, pp + tile);
 			}
 			if (!gridBarrier(ctrl, gen)) return;
@@ -1206,6 +1216,20 @@ __global__ void __launch_bounds__(PHB_TILE) kCgPersistent(Dom<double, D> dom, co
 		__syncthreads();
 		for (int s = threadIdx.x; s < nsys; s += blockDim.x) st[s] = sst[s];
 	}
+}
+
+template <typename T, int D, int K, bool STOPSTART, bool PC = false>
+__global__ void __launch_bounds__(PHB_TILE) kCgPersistent(Dom<double, D> dom, const T *__restrict__ A, const T *__restrict__ b,
+		T *__restrict__ x, T *__restrict__ r, T *__restrict__ p0, T *__restrict__ p1, T *__restrict__ q, T *__restrict__ xbest,
+		SysState *st, double *partial, Control *ctrl, phb_tolerance tol, int returnBest, int maxit, AmgView<D> mg) {
+	cgPersistentBody<T, D, K, STOPSTART, PC, false>(dom, A, b, x, r, p0, p1, q, xbest, st, partial, ctrl, tol, returnBest, maxit, mg);
+}
+
+template <typename T, int D, int K, bool STOPSTART>
+__global__ void __launch_bounds__(PHB_TILE, 4) kCgPersistentQuads(Dom<double, D> dom, const T *__restrict__ A, const T *__restrict__ b,
+		T *__restrict__ x, T *__restrict__ r, T *__restrict__ p0, T *__restrict__ p1, T *__restrict__ q, T *__restrict__ xbest,
+		SysState *st, double *partial, Control *ctrl, phb_tolerance tol, int returnBest, int maxit, AmgView<D> mg) {
+	cgPersistentBody<T, D, K, STOPSTART, true, true>(dom, A, b, x, r, p0, p1, q, xbest, st, partial, ctrl, tol, returnBest, maxit, mg);
 }
 
 template <typename T, int D, int K>
@@ -1548,6 +1572,8 @@ static int launchPersistent(const phb_domain *dom, const phb_solve *sv, cudaStre
 		if constexpr (std::is_same<T, float>::value && K == 1) {
 			if (sv->amg) {
 				mg = makeAmgView<D>(*sv->amg, (const float *)r, sv->amg->levels[0].x);
+				if (amgFineQuads(mg))
+					return stopStart ? launch(kCgPersistentQuads<T, D, K, true>) : launch(kCgPersistentQuads<T, D, K, false>);
 				return stopStart ? launch(kCgPersistent<T, D, K, true, true>) : launch(kCgPersistent<T, D, K, false, true>);
 			}
 		}

@@ -125,6 +125,61 @@ def test_folded_levels_give_the_same_cycle(cuda, case):
     assert float((z0 - z1).abs().max() / z0.abs().max()) < 1e-5
 
 
+def _host_cycle(h, dims, r):
+    """The V-cycle in float64 on the host from the hierarchy's own operators: x0 = S b,
+    b' = P^T (b - A x0), e = cycle(b'), x1 = x0 + P e, z = x1 + S (b - A x1), and the dense
+    operator C_T (per instance) at the last level of the cycle."""
+    T = h.tail_level
+    A = [_dense(h.struct().levels[l].dom, h.level_A[l]) for l in range(T + 1)]
+    P = [_prolongation(h.records[l], h.records[l + 1], dims) for l in range(T)]
+    S = [h.level_wdinv[l].double().cpu().numpy() for l in range(T)]
+    cn = h.coarse_n
+    insts = h.records[T][2]
+    C = h.coarse_inv.view(-1, cn, cn).cpu().numpy()
+
+    def cyc(l, b):
+        if l == T:
+            x = np.zeros_like(b)
+            for i in range(insts.shape[0]):
+                off, n = int(insts[i, 0]), int(insts[i, 1])
+                x[off:off + n] = C[i, :n, :n] @ b[off:off + n]
+            return x
+        x0 = S[l] * b
+        e = cyc(l + 1, P[l].T @ (b - A[l] @ x0))
+        x1 = x0 + P[l] @ e
+        return x1 + S[l] * (b - A[l] @ x1)
+
+    return cyc(0, r)
+
+
+VCYCLE_CASES = {
+    "hartmann2d": lambda: hartmann_2d(64, 48, dtype=torch.float32),
+    "duct3d": lambda: duct_3d(16, 12, 10, 2, dtype=torch.float32),
+    "rotated2d": lambda: rotated_pair_2d(32, dtype=torch.float32),
+    "duct3d_odd": lambda: duct_3d(13, 7, 9, 2, dtype=torch.float32),
+    # above the size where the finest level switches to the one-coarse-cell-per-thread
+    # restriction and the quad prolongation
+    "hartmann2d_large": lambda: hartmann_2d(1024, 1040, dtype=torch.float32),
+    "duct3d_large": lambda: duct_3d(64, 96, 88, 2, dtype=torch.float32),
+}
+
+
+@pytest.mark.parametrize("case", list(VCYCLE_CASES))
+def test_vcycle_matches_host_emulation(cuda, case):
+    """The device cycle equals the cycle evaluated with SciPy from the same level operators,
+    float32 roundoff apart: per-cell and lane-group forms on small grids; vector, fixed-stride
+    and per-cell paths of the finest level on large ones."""
+    dom = VCYCLE_CASES[case]()
+    _pressure_system(dom, 29)
+    h = AmgHierarchy(dom)
+    h.setup(dom._P_st)
+    r = torch.randn(dom.getTotalSize(), generator=torch.Generator().manual_seed(6)).cuda()
+    z = h.vcycle(r).double().cpu().numpy()
+    torch.cuda.synchronize()
+    ref = _host_cycle(h, dom.getSpatialDims(), r.double().cpu().numpy())
+    assert np.abs(z - ref).max() <= 1e-4 * np.abs(ref).max()
+
+
 @pytest.mark.parametrize("case", ["hartmann2d", "duct3d"])
 def test_vcycle_is_symmetric(cuda, case):
     dom = CASES[case](torch.float32)
