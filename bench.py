@@ -202,28 +202,32 @@ class ClockSampler:
 
 
 def dist_setup(args):
+    """Rank, world size and local rank from the torchrun environment. With more than one rank a
+    process group is formed (NCCL on GPUs; gloo without CUDA, or when PHIPICT_B200_DIST_BACKEND
+    says so). The reference arm forms none: rank 0 alone runs it, the others leave at once."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local if world > 1 else 0)
+    if world > 1 and args.impl != "reference":
         import datetime
 
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        backend = "nccl" if args.impl != "reference" else "gloo"
+        backend = os.environ.get("PHIPICT_B200_DIST_BACKEND") or ("nccl" if torch.cuda.is_available() else "gloo")
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
-    elif torch.cuda.is_available():
-        torch.cuda.set_device(0)
     return rank, world, local
 
 
 def max_over_ranks(v: float, world: int) -> float:
+    """The largest of every rank's v (the device times of a step loop)."""
     if world == 1:
         return v
     import torch.distributed as dist
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -540,13 +544,13 @@ def serve_requests(wl, device, seed=0):
             dom.PrepareSolve()
             return dom
         reqs.append(Request(rid=k, build=build, stuart=N, e_b=(0.0, 1.0, 0.0), steps=wl["steps"], dt=dt,
-                            arrival=arrivals[k]))
+                            arrival=arrivals[k], cost_hint=float(side ** (3 if three else 2) * wl["steps"])))
     return reqs
 
 
 def run_serve(args, rank, world, local):
     import phipict_b200 as pb
-    from phipict_b200.serve import Server
+    from phipict_b200.serve import Server, gather_reports, route
 
     wl = dict(WORKLOADS["serve"])
     if args.requests:
@@ -558,17 +562,23 @@ def run_serve(args, rank, world, local):
               potential_use_preconditioner=not args.plain_fp64,
               hooks=pb.Hooks().append(pb.Hook.PRE_VELOCITY_SETUP, reset_cell_source))
     server = Server(device=device, hbm_budget=150e9, sim_kwargs=kw)
-    rep = server.run(serve_requests(wl, device, seed=rank))
-    cells = sum(r.cells for r in server.finished)
-    return dict(metric="Mcell-steps/s", value=round(rep["mcell_steps_per_s"] * world, 4), unit="Mcell-steps/s",
+    # one stream of world x requests at world x the rate; every rank routes it the same way
+    # and serves its share (weak scaling), the reports are merged over the ranks
+    stream = serve_requests(dict(wl, requests=wl["requests"] * world, rate=wl["rate"] * world), device, seed=0)
+    mine = route(stream, world)[rank]
+    server.run(mine)
+    rep = gather_reports(server.report(), world)
+    cells = rep["cells_total"]
+    return dict(metric="Mcell-steps/s", value=round(rep["mcell_steps_per_s"], 4), unit="Mcell-steps/s",
                 n_gpus=world, steps=wl["steps"], warmup=0, higher_is_better=True, scaling="weak", vs_baseline=None,
                 dtype="f64 fields, f32 Krylov + f64 refinement" if not args.plain_fp64 else "f64",
                 data="synthetic (seeded Poisson request stream)",
                 config={"workload": f"serve: {wl['requests']} requests at {wl['rate']}/s, 50% 2D side U[64,512], "
                                     f"50% 3D side U[32,128], Ha log-uniform [1,1000], {wl['steps']} steps each, "
                                     f"rtol {wl['rtol']}, admission against 150 GB", "parallelism": f"replicas x{world}"},
-                served={"p50_s": rep["p50_s"], "p99_s": rep["p99_s"], "wall_s": round(rep["wall_s"], 3),
-                        "failed": rep["failed"], "batch_steps": rep["batch_steps"], "cells_total": cells,
+                served={"requests": rep["requests"], "p50_s": rep["p50_s"], "p99_s": rep["p99_s"],
+                        "wall_s": round(rep["wall_s"], 3), "failed": rep["failed"], "batch_steps": rep["batch_steps"],
+                        "cells_total": cells,
                         "failures": [f"{r.rid}: {r.failed[:160]}" for r in server.finished if r.failed][:4],
                         "peak_held_bytes": rep["peak_held_bytes"]},
                 gpu_launches=None)

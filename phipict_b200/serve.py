@@ -39,6 +39,7 @@ class Request:
     steps: int
     dt: float
     arrival: float = 0.0           # seconds after the server starts
+    cost_hint: float | None = None  # estimated work (cells x steps) for routing; None: 1
     # filled by the server
     domain: Domain | None = None
     uxb: torch.Tensor | None = None
@@ -226,18 +227,61 @@ class Server:
 
     def report(self) -> dict:
         lat = sorted(r.latency for r in self.finished if r.latency is not None)
-
-        def pct(p):
-            if not lat:
-                return None
-            k = min(len(lat) - 1, max(0, math.ceil(p / 100 * len(lat)) - 1))
-            return lat[k]
-
         wall = self._now() if self._t0 is not None else 0.0
         return {"requests": len(self.finished), "failed": sum(1 for r in self.finished if r.failed),
-                "p50_s": pct(50), "p99_s": pct(99), "wall_s": wall,
+                "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99), "wall_s": wall,
                 "mcell_steps_per_s": self.cell_steps / wall / 1e6 if wall > 0 else None,
-                "batch_steps": self.steps_run, "peak_held_bytes": self.peak_held}
+                "batch_steps": self.steps_run, "peak_held_bytes": self.peak_held,
+                "latencies": lat, "cell_steps": self.cell_steps, "cells_total": sum(r.cells for r in self.finished)}
+
+
+def percentile(sorted_values: list[float], p: float) -> float | None:
+    """The nearest-rank p-th percentile of an ascending list (None when empty)."""
+    if not sorted_values:
+        return None
+    k = min(len(sorted_values) - 1, max(0, math.ceil(p / 100 * len(sorted_values)) - 1))
+    return sorted_values[k]
+
+
+def route(requests: list[Request], world: int) -> list[list[Request]]:
+    """Assign a request stream to `world` servers, one per GPU: in arrival order, each request
+    goes to the server with the least estimated work so far (cost_hint, or 1 per request;
+    ties to the lower rank). Deterministic, so every rank computes the same assignment from
+    the same stream without exchanging anything."""
+    load = [0.0] * world
+    out: list[list[Request]] = [[] for _ in range(world)]
+    for req in sorted(requests, key=lambda r: (r.arrival, r.rid)):
+        k = min(range(world), key=lambda i: (load[i], i))
+        out[k].append(req)
+        load[k] += req.cost_hint if req.cost_hint is not None else 1.0
+    return out
+
+
+def merge_reports(reports: list[dict]) -> dict:
+    """One report for the whole job from the servers' reports: latency percentiles over all
+    requests, cell-steps of all servers over the longest wall time."""
+    lat = sorted(x for r in reports for x in r["latencies"])
+    wall = max(r["wall_s"] for r in reports)
+    cell_steps = sum(r["cell_steps"] for r in reports)
+    return {"requests": sum(r["requests"] for r in reports), "failed": sum(r["failed"] for r in reports),
+            "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99), "wall_s": wall,
+            "mcell_steps_per_s": cell_steps / wall / 1e6 if wall > 0 else None,
+            "batch_steps": sum(r["batch_steps"] for r in reports),
+            "peak_held_bytes": max(r["peak_held_bytes"] for r in reports),
+            "latencies": lat, "cell_steps": cell_steps, "cells_total": sum(r["cells_total"] for r in reports),
+            "servers": len(reports)}
+
+
+def gather_reports(report: dict, world: int) -> dict:
+    """The merged report of all ranks' servers (every rank gets it); the report itself when
+    there is one rank. Uses the default process group."""
+    if world == 1:
+        return merge_reports([report])
+    import torch.distributed as dist
+
+    reports: list = [None] * world
+    dist.all_gather_object(reports, report)
+    return merge_reports(reports)
 
 
 def poisson_arrivals(n: int, rate: float, seed: int) -> list[float]:
@@ -247,4 +291,4 @@ def poisson_arrivals(n: int, rate: float, seed: int) -> list[float]:
     return torch.cumsum(gaps, 0).tolist()
 
 
-__all__ = ["Request", "Server", "estimate_bytes", "poisson_arrivals"]
+__all__ = ["Request", "Server", "estimate_bytes", "gather_reports", "merge_reports", "percentile", "poisson_arrivals", "route"]
