@@ -112,6 +112,32 @@ int phb_uxb_epot_rhs(const phb_domain *dom, const void *u, const double *e_b, vo
 int phb_current_lorentz(const phb_domain *dom, const void *phi, const void *uxb, const double *e_b,
                         const double *stuart, void *J, void *src, int accumulate, phb_stream stream);
 
+/* --- passive scalar transport ------------------------------------------------------ */
+/* Scalar fields are [inst][channels][cells]. Fixed-face data per fixed record r (records as
+ * in phb_domain.fixed): types[r * channels + c] (0 Dirichlet value, 1 Neumann gradient
+ * dphi/dn) and the value of channel c at face cell fc, values[offsets[r] + c] when
+ * statics[r], else values[offsets[r] + c * facecells_r + fc] (domain dtype). The scalar
+ * diffusivity is nu[0] (nu_count 1), nu[c] (nu_count = channels), or the velocity viscosity
+ * of the instance (nu_count 0, the reference's default without scalarViscosity). */
+typedef struct phb_scalar {
+	int32_t channels;
+	int32_t nu_count;
+	const double *nu;
+	const int8_t *types;
+	const void *values;
+	const int64_t *offsets;
+	const int8_t *statics;
+} phb_scalar;
+/* SetupAdvectionMatrix(forPassiveScalar=True, passiveScalarChannel=channel) (bindings.cpp:639,
+ * advection.cu:27-305): the advection-diffusion row with the scalar diffusivity of `channel`
+ * and its fixed-face types (a Neumann face adds no wall diffusion). Outputs as
+ * phb_advection_matrix. */
+int phb_scalar_matrix(const phb_domain *dom, const void *u, const phb_scalar *sc, int channel, void *C, void *Adiag,
+                      float *C_lo, phb_stream stream);
+/* SetupAdvectionScalar (advection.cu:545-698 kPISO_build_scalar_advection_RHS, CENTRAL,
+ * orthogonal): rhs [inst][channels][cells] from the block scalar phi (same layout). */
+int phb_scalar_rhs(const phb_domain *dom, const void *phi, const phb_scalar *sc, void *rhs, phb_stream stream);
+
 /* --- vectors ------------------------------------------------------------------------ */
 /* Per-instance reductions use a caller-owned scratch of phb_scratch_doubles() doubles whose
  * first word must be zero before the first call (each call leaves it zero again).

@@ -262,9 +262,13 @@ static void forEachCell(const Dom<S> &D, const std::function<void(int, const int
 	}
 }
 
-// advection.cu:27-305 PISO_build_matrix (CENTRAL, orthogonal, domain viscosity)
+// advection.cu:27-305 PISO_build_matrix (CENTRAL, orthogonal, domain viscosity). With
+// faceTypes (forPassiveScalar): the wall diffusion of a fixed face follows the scalar
+// channel's type faceTypes[fixed id] instead of the velocity type (advection.cu:254-266), and
+// nu is the channel's diffusivity.
 template <typename S>
-static void advMatrix(const Dom<S> &D, const S *u, S dt, S nu, const int *row, int *col, S *val, S *Adiag) {
+static void advMatrix(const Dom<S> &D, const S *u, S dt, S nu, const int *row, int *col, S *val, S *Adiag,
+		const int8_t *faceTypes = nullptr) {
 	forEachCell<S>(D, [&](int b, const int *p, int g) {
 		S fl[6];
 		fluxes(D, b, p, u, fl);
@@ -293,7 +297,8 @@ static void advMatrix(const Dom<S> &D, const S *u, S dt, S nu, const int *row, i
 				diag += coeff;
 				rv[f + 1] -= coeff;
 			} else {
-				const S slip = D.velType(b, f) == 0 ? S(0) : S(1);
+				const int type = faceTypes ? int(faceTypes[D.fixedId(b, f)]) : D.velType(b, f);
+				const S slip = type == 0 ? S(0) : S(1);
 				diag += (S(1) - slip) * S(2) * nu * alphaP[dim];
 			}
 		}
@@ -325,6 +330,37 @@ static void advRhs(const Dom<S> &D, const S *u, const S *src, int srcStatic, S d
 			if (src) r += srcStatic ? src[dim] : src[(size_t)dim * D.n + g];
 			rhs[(size_t)dim * D.n + g] = r;
 		}
+	});
+}
+
+// advection.cu:545-698 kPISO_build_scalar_advection_RHS (CENTRAL, orthogonal) for one channel:
+// det phi/dt, at fixed faces Dirichlet -phi_b F + phi_b nu 2 alpha, Neumann -phi_P F +
+// (dphi/dn) nu |S_f| (|S_f| = det_f |Minv_f[dim]|, discretization.cuh:618-634), over det.
+// faceTypes[fixed id]: 0 Dirichlet, 1 Neumann; faceValue(fixed id, face cell) the face data.
+template <typename S>
+static void scalarRhs(const Dom<S> &D, const S *phi, S dt, S nu, const int8_t *faceTypes, const S *faceValues,
+		const int64_t *faceOffsets, const int8_t *faceStatic, S *rhs) {
+	forEachCell<S>(D, [&](int b, const int *p, int g) {
+		const S det = D.det(D.T(b, p));
+		S r = det * phi[g] / dt;
+		for (int f = 0; f < 2 * D.dims; ++f) {
+			if (!D.atBound(b, f, p) || D.ftype(b, f) != FT_FIXED) continue;
+			const S faceNormal = (f & 1) ? S(1) : S(-1);
+			const int fid = D.fixedId(b, f);
+			const S value = faceStatic[fid] ? faceValues[faceOffsets[fid]] : faceValues[faceOffsets[fid] + D.faceCell(b, f, p)];
+			const S *tf = D.faceT(b, f, p);
+			const S flux = contraFixed(D, b, f, p, f >> 1) * faceNormal;
+			if (faceTypes[fid] == 0) {
+				r -= value * flux;
+				r += value * nu * S(2) * alphaOf(D, tf, f >> 1);
+			} else {
+				const S *mi = D.Minv(tf, f >> 1);
+				const S area = D.det(tf) * std::sqrt(dotv(mi, mi, D.dims));
+				r -= phi[g] * flux;
+				r += value * nu * area;
+			}
+		}
+		rhs[g] = r / det;
 	});
 }
 
@@ -704,6 +740,12 @@ static int bicgstab(int n, const int *row, const int *col, const S *val, const S
 extern "C" void orc_row_pointers##SUF(ORC_DOM_ARGS(S), int *row) { ORC_DOM(S); orc::rowPointers(D, row); }              \
 extern "C" void orc_adv_matrix##SUF(ORC_DOM_ARGS(S), const S *u, double dt, double nu, const int *row, int *col, S *val, S *Adiag) { \
 	ORC_DOM(S); orc::advMatrix<S>(D, u, S(dt), S(nu), row, col, val, Adiag); }                                           \
+extern "C" void orc_scalar_matrix##SUF(ORC_DOM_ARGS(S), const S *u, double dt, double nu, const int8_t *types,            \
+		const int *row, int *col, S *val, S *Adiag) {                                                                     \
+	ORC_DOM(S); orc::advMatrix<S>(D, u, S(dt), S(nu), row, col, val, Adiag, types); }                                      \
+extern "C" void orc_scalar_rhs##SUF(ORC_DOM_ARGS(S), const S *phi, double dt, double nu, const int8_t *types,            \
+		const S *values, const int64_t *offsets, const int8_t *statics, S *rhs) {                                         \
+	ORC_DOM(S); orc::scalarRhs<S>(D, phi, S(dt), S(nu), types, values, offsets, statics, rhs); }                            \
 extern "C" void orc_adv_rhs##SUF(ORC_DOM_ARGS(S), const S *u, const S *src, int srcStatic, double dt, double nu, S *rhs) { \
 	ORC_DOM(S); orc::advRhs<S>(D, u, src, srcStatic, S(dt), S(nu), rhs); }                                               \
 extern "C" void orc_laplace_matrix##SUF(ORC_DOM_ARGS(S), const S *Adiag, int epot, const int *row, int *col, S *val) { \

@@ -138,6 +138,18 @@ class OracleDomain:
             else:
                 Tf.append(np.tile(_identity(d, TS, self.S), (fc, 1)))
             to += fc
+        # passive scalar per fixed face and channel: type, values (static: one per channel)
+        C = domain.getPassiveScalarChannels() if hasattr(domain, "getPassiveScalarChannels") else 0
+        self.channels = C
+        self.scalar_faces = []
+        for k, (i, f, bd) in enumerate(fixed):
+            if C == 0 or bd.passiveScalar is None:
+                self.scalar_faces.append(None)
+                continue
+            ps = bd.passiveScalar.detach().cpu()
+            pe = ps[env if ps.shape[0] > 1 else 0].numpy().astype(self.S)  # [C] or [C, *face]
+            types = list(bd._scalar_types())
+            self.scalar_faces.append((pe.ndim == 1, pe.reshape(C, -1), types, bd.isPassiveScalarBoundaryTypeStatic()))
         self.desc = desc
         self.Tc = np.ascontiguousarray(Tc)
         self.Tf = np.ascontiguousarray(np.concatenate(Tf) if Tf else np.zeros((1, TS), dtype=self.S))
@@ -173,6 +185,45 @@ class OracleDomain:
         self._f("orc_adv_matrix")(*self._dargs(), _p(self._a(u)), ct.c_double(dt), ct.c_double(nu), _p(self.row),
                                   _p(self.col), _p(val), _p(A))
         return val, A
+
+    def _scalar_face_data(self, c):
+        """Channel c's fixed-face types, values, offsets and static flags (one environment)."""
+        nf = max(1, len(self.scalar_faces))
+        types = np.zeros(nf, dtype=np.int8)
+        offs = np.zeros(nf, dtype=np.int64)
+        stat = np.zeros(nf, dtype=np.int8)
+        vals, o = [], 0
+        for k, fd in enumerate(self.scalar_faces):
+            if fd is None:
+                stat[k] = 1
+                offs[k] = o
+                vals.append(np.zeros(1, dtype=self.S))
+                o += 1
+                continue
+            static, v, t, _ = fd
+            types[k] = t[c]
+            stat[k] = 1 if static else 0
+            offs[k] = o
+            vals.append(np.ascontiguousarray(v[c]).astype(self.S))
+            o += v.shape[1]
+        return types, np.ascontiguousarray(np.concatenate(vals) if vals else np.zeros(1, dtype=self.S)), offs, stat
+
+    def scalar_matrix(self, u, dt, nu, channel):
+        """advection.cu:27-305 with forPassiveScalar for one channel (its diffusivity nu)."""
+        types, _, _, _ = self._scalar_face_data(channel)
+        val = np.zeros(self.nnz, dtype=self.S)
+        A = self.vec()
+        self._f("orc_scalar_matrix")(*self._dargs(), _p(self._a(u)), ct.c_double(dt), ct.c_double(nu), _p(types),
+                                     _p(self.row), _p(self.col), _p(val), _p(A))
+        return val, A
+
+    def scalar_rhs(self, phi_c, dt, nu, channel):
+        """advection.cu:545-698 for one channel's field phi_c [n]."""
+        types, vals, offs, stat = self._scalar_face_data(channel)
+        rhs = self.vec()
+        self._f("orc_scalar_rhs")(*self._dargs(), _p(self._a(phi_c)), ct.c_double(dt), ct.c_double(nu), _p(types),
+                                  _p(vals), _p(offs), _p(stat), _p(rhs))
+        return rhs
 
     def advection_rhs(self, u, src, dt, nu):
         rhs = self.vec(self.dims)
@@ -276,7 +327,7 @@ class OracleSim:
     """Reference PISO (+ inductionless MHD) step of one environment on the CPU."""
 
     def __init__(self, od: OracleDomain, u0: np.ndarray, dt: float, nu: float, *, corrector_steps=2,
-                 advection_tol=None, pressure_tol=None, source=None, mhd=None, maxit=5000):
+                 advection_tol=None, pressure_tol=None, source=None, mhd=None, maxit=5000, scalar=None):
         self.od = od
         self.dt = dt
         self.nu = nu
@@ -293,13 +344,45 @@ class OracleSim:
             self.phi = od.vec()
             self.uxb = od.vec(3)
             self.Eval, self.Ecol = od.laplace_matrix(epot=True)
+        # passive scalar: dict(phi=[C][n] initial field, nu=None | [1] | [C] diffusivities)
+        self.scalar = scalar
+        if scalar is not None:
+            self.phi_s = od._a(scalar["phi"]).reshape(od.channels, od.n).copy()
         self.iterations = {}
 
     def _mean_sub(self, x):
         return x - x.mean()
 
+    def scalar_step(self):
+        """core/piso_simulation.py:3589-3775 (orthogonal): every channel advected and diffused
+        implicitly with the step-start velocity, zero initial guess. Returns the channel-0
+        matrix when the velocity step reuses it (same diffusivity as the velocity, one set of
+        face types for all channels), else None."""
+        od, C = self.od, self.od.channels
+        nus = self.scalar.get("nu")
+        static_nu = nus is None or len(nus) == 1
+        types_static = all(fd is None or fd[3] for fd in od.scalar_faces)
+        split = not (static_nu and types_static)
+        nu_of = (lambda c: self.nu) if nus is None else (lambda c: float(nus[0] if len(nus) == 1 else nus[c]))
+        mat = None if split else od.scalar_matrix(self.u, self.dt, nu_of(0), 0)
+        its = []
+        for c in range(C):
+            Cval, _ = od.scalar_matrix(self.u, self.dt, nu_of(c), c) if split else mat
+            rhs = od.scalar_rhs(self.phi_s[c], self.dt, nu_of(c), c)
+            tol = resolve_tol(self.advection_tol, rhs, od.S)
+            x = od.vec()
+            st, it, _ = od.solve(Cval, rhs, x, tol, self.maxit, bicg=True)
+            if st != 1:
+                raise RuntimeError(f"oracle scalar solve failed ({st})")
+            self.phi_s[c] = x
+            its.append(it)
+        self.iterations["scalar"] = its
+        reuse = nus is None and not split
+        return mat if reuse else None
+
     def step(self):
         od, d, n = self.od, self.od.dims, self.od.n
+        reused = self.scalar_step() if self.scalar is not None else None
         if self.mhd is not None:
             J = od.current_density(self.phi, self.uxb).reshape(3, n)
             e = np.asarray(self.mhd["e_b"], dtype=od.S)
@@ -311,8 +394,7 @@ class OracleSim:
             else:
                 base = self.src if self.src.size == d * n else np.repeat(self.src, n)
                 self.src = (F + base).astype(od.S)
-        Cval, A = od.advection_matrix(self.u, self.dt, self.nu)
-        od.col = od.col  # pattern filled by the matrix kernel
+        Cval, A = reused if reused is not None else od.advection_matrix(self.u, self.dt, self.nu)
         rhs = od.advection_rhs(self.u, self.src, self.dt, self.nu)
         tol = resolve_tol(self.advection_tol, rhs, od.S)
         its = []

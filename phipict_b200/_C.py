@@ -79,12 +79,17 @@ def SetupAdvectionMatrix(domain: Domain, timeStep, nonOrthoFlags=0, forPassiveSc
     """Implicit Euler advection-diffusion matrix C and its diagonal A (advection.cu:27-305)."""
     _check(domain)
     _no_nonortho(nonOrthoFlags)
-    if forPassiveScalar:
-        raise NotImplementedError("passive scalar advection is not implemented by phipict_b200")
     domain.setTimeStep(timeStep)
     lo = _lo(domain, "C")
-    _lib.call("phb_advection_matrix", ct.byref(domain.desc()), domain._u_block.data_ptr(), domain._C_st.data_ptr(),
-              domain.A.data_ptr(), lo.data_ptr() if lo is not None else None, _S(domain))
+    if forPassiveScalar:
+        c = int(passiveScalarChannel)
+        if not 0 <= c < domain.getPassiveScalarChannels():
+            raise RuntimeError(f"passive scalar channel {c} out of range")
+        _lib.call("phb_scalar_matrix", ct.byref(domain.desc()), domain._u_block.data_ptr(), ct.byref(domain._scalar_struct()),
+                  c, domain._C_st.data_ptr(), domain.A.data_ptr(), lo.data_ptr() if lo is not None else None, _S(domain))
+    else:
+        _lib.call("phb_advection_matrix", ct.byref(domain.desc()), domain._u_block.data_ptr(), domain._C_st.data_ptr(),
+                  domain.A.data_ptr(), lo.data_ptr() if lo is not None else None, _S(domain))
     _assembled(domain, "C", lo)
 
 
@@ -98,6 +103,16 @@ def SetupAdvectionVelocity(domain: Domain, timeStep, nonOrthoFlags=0, applyPress
     src, mode = _src(domain)
     _lib.call("phb_advection_rhs", ct.byref(domain.desc()), domain._u_block.data_ptr(), src, mode,
               domain.velocityRHS.data_ptr(), _S(domain))
+
+
+def SetupAdvectionScalar(domain: Domain, timeStep, nonOrthoFlags=0) -> None:
+    """Passive-scalar right-hand side into ``domain.scalarRHS`` [B][channels][cells]
+    (advection.cu:545-698, bindings SetupAdvectionScalar)."""
+    _check(domain)
+    _no_nonortho(nonOrthoFlags)
+    domain.setTimeStep(timeStep)
+    _lib.call("phb_scalar_rhs", ct.byref(domain.desc()), domain._phi_block.data_ptr(), ct.byref(domain._scalar_struct()),
+              domain.scalarRHS.data_ptr(), _S(domain))
 
 
 # --- pressure ---------------------------------------------------------------------------
@@ -171,6 +186,14 @@ def CopyPressureResultToBlocks(domain: Domain) -> None:
 
 def CopyPressureResultFromBlocks(domain: Domain) -> None:
     domain.pressureResult.copy_(domain._p_block.view(-1))
+
+
+def CopyScalarResultToBlocks(domain: Domain) -> None:
+    domain._phi_block.view(-1).copy_(domain.scalarResult)
+
+
+def CopyScalarResultFromBlocks(domain: Domain) -> None:
+    domain.scalarResult.copy_(domain._phi_block.view(-1))
 
 
 def CopyEpotResultToBlocks(domain: Domain) -> None:

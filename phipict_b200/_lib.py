@@ -25,7 +25,7 @@ EXPORTS = (
     "phb_cell_metrics", "phb_face_metrics",
     "phb_advection_matrix", "phb_advection_rhs", "phb_pressure_matrix", "phb_pressure_rhs",
     "phb_divergence", "phb_correct_velocity", "phb_epot_matrix", "phb_epot_rhs", "phb_uxb_epot_rhs",
-    "phb_current_lorentz",
+    "phb_current_lorentz", "phb_scalar_matrix", "phb_scalar_rhs",
     "phb_scratch_doubles", "phb_subtract_mean", "phb_rms",
     "phb_csr_row_sizes", "phb_csr_pattern", "phb_csr_gather",
     "phb_solve_work_bytes", "phb_solve_state_bytes", "phb_solve_run", "phb_solve_results",
@@ -47,6 +47,13 @@ class PhbDomain(ct.Structure):
         ("metrics", ct.c_void_p), ("face_metrics", ct.c_void_p),
         ("fvel", ct.c_void_p), ("fpot", ct.c_void_p), ("fcw", ct.c_void_p), ("fmask", ct.c_void_p),
         ("dt", ct.c_void_p), ("nu", ct.c_void_p),
+    ]
+
+
+class PhbScalar(ct.Structure):
+    _fields_ = [
+        ("channels", ct.c_int32), ("nu_count", ct.c_int32), ("nu", ct.c_void_p), ("types", ct.c_void_p),
+        ("values", ct.c_void_p), ("offsets", ct.c_void_p), ("statics", ct.c_void_p),
     ]
 
 
@@ -127,6 +134,8 @@ def load() -> ct.CDLL:
         "phb_face_metrics": [I, I, I, I, I, P, I, P, I64, P],
         "phb_advection_matrix": [DP, P, P, P, P, P],
         "phb_advection_rhs": [DP, P, P, I, P, P],
+        "phb_scalar_matrix": [DP, P, ct.POINTER(PhbScalar), I, P, P, P, P],
+        "phb_scalar_rhs": [DP, P, ct.POINTER(PhbScalar), P, P],
         "phb_pressure_matrix": [DP, P, P, P, P],
         "phb_pressure_rhs": [DP, P, P, P, P, P, I, P, P],
         "phb_divergence": [DP, P, P, P],

@@ -246,6 +246,17 @@ class DomainBatch:
     def IsInitialized(self) -> bool:
         return True
 
+    def hasPassiveScalar(self) -> bool:
+        """Passive scalars are not transported in a batch: the members' scalar fields stay as
+        they are (a batched step advances velocity, pressure and potential)."""
+        return False
+
+    def getPassiveScalarChannels(self) -> int:
+        return 0
+
+    def hasBlockViscosity(self) -> bool:
+        return False
+
     def PrepareSolve(self) -> None:
         pass
 

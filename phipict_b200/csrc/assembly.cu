@@ -36,11 +36,43 @@ __device__ __forceinline__ void faceFluxes(const Dom<S, D> &dom, const Cell &c, 
 	}
 }
 
+// Passive-scalar data of a launch (phb_scalar), passed by value.
+struct ScalarView {
+	int channels, nuCount;
+	const double *nu;
+	const int8_t *types;
+	const void *values;
+	const int64_t *offsets;
+	const int8_t *statics;
+};
+__host__ inline ScalarView scalarView(const phb_scalar *sc) {
+	if (!sc) return ScalarView{0, 0, nullptr, nullptr, nullptr, nullptr, nullptr};
+	return ScalarView{sc->channels, sc->nu_count, sc->nu, sc->types, sc->values, sc->offsets, sc->statics};
+}
+// getViscosity with forPassiveScalar (discretization.cuh:1141-1151): the scalar diffusivity of
+// channel c, or the velocity viscosity of the instance without one
+__device__ __forceinline__ double scalarNu(const ScalarView &sv, int c, double velocityNu) {
+	if (sv.nuCount <= 0) return velocityNu;
+	return sv.nu[sv.nuCount == 1 ? 0 : c];
+}
+// fixed-face scalar value of channel c at face cell fc (getFixedBoundaryData, PASSIVE_SCALAR)
+template <typename S>
+__device__ __forceinline__ S scalarFixed(const ScalarView &sv, const int32_t *FR, int fid, int c, int fc) {
+	const S *v = (const S *)sv.values + sv.offsets[fid];
+	return sv.statics[fid] ? v[c] : v[(int64_t)c * FR[F_FACECELLS] + fc];
+}
+// [inst][channels][cells] index of channel c of cell g
+__device__ __forceinline__ int64_t sidx(const int32_t *B, int64_t g, int c, int channels) {
+	return g + (int64_t)(channels - 1) * B[B_INSTOFF] + (int64_t)c * B[B_INSTN];
+}
+
 // PISO_build_matrix (piso/advection.cu:27-305): implicit Euler advection-diffusion row
-// divided by the cell determinant; Adiag = its diagonal.
-template <typename S, int D>
+// divided by the cell determinant; Adiag = its diagonal. SCALAR: the matrix of passive-scalar
+// channel `channel` (forPassiveScalar): its diffusivity, and the wall diffusion term of a fixed
+// face taken from the scalar's face type instead of the velocity's (advection.cu:254-266).
+template <typename S, int D, bool SCALAR = false>
 __global__ void __launch_bounds__(PHB_TILE) kAdvectionMatrix(Dom<S, D> dom, const S *__restrict__ u, S *__restrict__ C,
-		S *__restrict__ Adiag, float *__restrict__ Clo) {
+		S *__restrict__ Adiag, float *__restrict__ Clo, ScalarView sv = {}, int channel = 0) {
 	__shared__ int32_t sB[PHB_BREC];
 	int l0_, nc_;
 	loadTile<S, D>(dom, sB, l0_, nc_);
@@ -49,7 +81,7 @@ __global__ void __launch_bounds__(PHB_TILE) kAdvectionMatrix(Dom<S, D> dom, cons
 	if (!cellAt<D>(sB, l0_, nc_, j_, c)) return;
 	const int inst = c.B[B_INST];
 	const S dt = S(dom.dt[inst]);
-	const S nu = S(dom.nu[inst]);
+	const S nu = SCALAR ? S(scalarNu(sv, channel, dom.nu[inst])) : S(dom.nu[inst]);
 	S fl[2 * D];
 	faceFluxes<S, D>(dom, c, u, fl);
 	const S det = detAt<S, D>(dom, c.mi);
@@ -74,8 +106,10 @@ __global__ void __launch_bounds__(PHB_TILE) kAdvectionMatrix(Dom<S, D> dom, cons
 			diag += coeff;
 			rv[f + 1] -= coeff;
 		} else {
-			const int32_t *FR = dom.fix(fRec(c.B, f)[5]);
-			const S slip = FR[F_VELTYPE] == 0 ? S(0) : S(1);
+			const int fid = fRec(c.B, f)[5];
+			const int32_t *FR = dom.fix(fid);
+			const int type = SCALAR ? int(sv.types[(int64_t)fid * sv.channels + channel]) : FR[F_VELTYPE];
+			const S slip = type == 0 ? S(0) : S(1);
 			diag += (S(1) - slip) * S(2) * nu * alphaP[dim];
 		}
 	}
@@ -140,6 +174,54 @@ __global__ void __launch_bounds__(PHB_TILE) kAdvectionRhs(Dom<S, D> dom, const S
 		r /= det;
 		r += sourceAt<S, D>(c, src, srcMode, dim);
 		rhs[o] = r;
+	}
+	}
+}
+
+// kPISO_build_scalar_advection_RHS (advection.cu:545-698), CENTRAL, orthogonal:
+// det phi / dt plus, at fixed faces, Dirichlet: -phi_b F + 2 nu alpha phi_b (ghost cell);
+// Neumann: -phi_P F + nu |S_f| dphi/dn; all divided by det.
+template <typename S, int D>
+__global__ void __launch_bounds__(PHB_TILE) kScalarRhs(Dom<S, D> dom, const S *__restrict__ phi, ScalarView sv, S *__restrict__ rhs) {
+	__shared__ int32_t sB[PHB_BREC];
+	int l0_, nc_;
+	loadTile<S, D>(dom, sB, l0_, nc_);
+	for (int j_ = 0; j_ < CPT; ++j_) {
+	Cell c;
+	if (!cellAt<D>(sB, l0_, nc_, j_, c)) return;
+	const int inst = c.B[B_INST];
+	const S dt = S(dom.dt[inst]);
+	const double nuVel = dom.nu[inst];
+	const S det = detAt<S, D>(dom, c.mi);
+	for (int ch = 0; ch < sv.channels; ++ch) {
+		const int64_t o = sidx(c.B, c.g, ch, sv.channels);
+		const S phiP = phi[o];
+		const S nu = S(scalarNu(sv, ch, nuVel));
+		S r = det * phiP / dt;
+#pragma unroll
+		for (int f = 0; f < 2 * D; ++f) {
+			if (!atBound(c.B, f, c.p) || fType(c.B, f) != FT_FIXED) continue;
+			const S faceNormal = (f & 1) ? S(1) : S(-1);
+			const int fid = fRec(c.B, f)[5];
+			const int32_t *FR = dom.fix(fid);
+			const int fc = faceCell(c.B, f, c.p);
+			const S value = scalarFixed<S>(sv, FR, fid, ch, fc);
+			const S flux = contraFixed<S, D>(dom, FR, fc, f >> 1) * faceNormal;
+			if (sv.types[(int64_t)fid * sv.channels + ch] == 0) {
+				r -= value * flux;
+				r += value * nu * S(2) * alphaFixed<S, D>(dom, FR, fc, f >> 1);
+			} else {
+				// getFaceAreaOrthogonalBoundary (discretization.cuh:618-634): det_f |Minv_f[dim]|
+				const int64_t fi = FR[F_TOFF] + fc;
+				S m2 = 0;
+#pragma unroll
+				for (int j = 0; j < D; ++j) { const S v = dom.fm(Tr<D>::MINV + (f >> 1) * D + j, fi); m2 += v * v; }
+				const S area = dom.fm(Tr<D>::DET, fi) * sqrt(m2);
+				r -= phiP * flux;
+				r += value * nu * area;
+			}
+		}
+		rhs[o] = r / det;
 	}
 	}
 }
@@ -541,6 +623,27 @@ extern "C" int phb_advection_matrix(const phb_domain *dom, const void *u, void *
 	if (dom->ntiles == 0) return PHB_OK;
 	PHB_DISPATCH(dom, kAdvectionMatrix<S, D><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)u, (S *)C, (S *)Adiag, C_lo));
 	return checkLaunch("kAdvectionMatrix");
+}
+extern "C" int phb_scalar_matrix(const phb_domain *dom, const void *u, const phb_scalar *sc, int channel, void *C, void *Adiag,
+		float *C_lo, phb_stream stream) {
+	if (!dom || !u || !sc || !C || !Adiag) return setError(PHB_ERR_ARG, "phb_scalar_matrix: null argument");
+	if (sc->channels < 1 || channel < 0 || channel >= sc->channels || (sc->nu_count != 0 && sc->nu_count != 1 && sc->nu_count != sc->channels) ||
+			(sc->nu_count > 0 && !sc->nu) || (dom->nfixed > 0 && (!sc->types || !sc->values || !sc->offsets || !sc->statics)))
+		return setError(PHB_ERR_ARG, "phb_scalar_matrix: bad scalar description");
+	if (dom->ntiles == 0) return PHB_OK;
+	const ScalarView sv = scalarView(sc);
+	PHB_DISPATCH(dom, kAdvectionMatrix<S, D, true><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)u, (S *)C, (S *)Adiag, C_lo, sv, channel));
+	return checkLaunch("kAdvectionMatrix<scalar>");
+}
+extern "C" int phb_scalar_rhs(const phb_domain *dom, const void *phi, const phb_scalar *sc, void *rhs, phb_stream stream) {
+	if (!dom || !phi || !sc || !rhs) return setError(PHB_ERR_ARG, "phb_scalar_rhs: null argument");
+	if (sc->channels < 1 || (sc->nu_count != 0 && sc->nu_count != 1 && sc->nu_count != sc->channels) || (sc->nu_count > 0 && !sc->nu) ||
+			(dom->nfixed > 0 && (!sc->types || !sc->values || !sc->offsets || !sc->statics)))
+		return setError(PHB_ERR_ARG, "phb_scalar_rhs: bad scalar description");
+	if (dom->ntiles == 0) return PHB_OK;
+	const ScalarView sv = scalarView(sc);
+	PHB_DISPATCH(dom, kScalarRhs<S, D><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)phi, sv, (S *)rhs));
+	return checkLaunch("kScalarRhs");
 }
 extern "C" int phb_advection_rhs(const phb_domain *dom, const void *u, const void *src, int src_mode, void *rhs, phb_stream stream) {
 	if (!dom || !u || !rhs || (src_mode != 0 && !src) || src_mode < 0 || src_mode > 2) return setError(PHB_ERR_ARG, "phb_advection_rhs: bad argument");

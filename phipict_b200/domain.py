@@ -118,7 +118,8 @@ class FixedBoundary(Boundary):
     type = BoundaryType.FIXED
 
     def __init__(self, domain: "Domain", block: "Block", face: int, velocity: torch.Tensor | None,
-                 velocity_type: BoundaryConditionType):
+                 velocity_type: BoundaryConditionType, passiveScalar: torch.Tensor | None = None,
+                 passiveScalarType=None):
         super().__init__(domain)
         self._block = block
         self._face = face
@@ -131,6 +132,18 @@ class FixedBoundary(Boundary):
         self._potentialTypes: torch.Tensor | None = None
         self._potentialValues: torch.Tensor | None = None
         self._cw = 0.0
+        # passive scalar (domain/boundaries.cpp:100-120): given values, or static zeros when the
+        # domain carries scalars; the type defaults to the velocity type
+        self._passiveScalar: torch.Tensor | None = None
+        self._passiveScalarTypes: list[BoundaryConditionType] | None = None
+        if passiveScalar is not None:
+            self._passiveScalar = self._check_scalar(passiveScalar)
+        elif domain.hasPassiveScalar():
+            self._passiveScalar = torch.zeros(1, domain.getPassiveScalarChannels(), dtype=domain.getDtype(),
+                                              device=domain.getDevice())
+        if self._passiveScalar is not None:
+            t = passiveScalarType if passiveScalarType is not None else self._velocityType
+            self._passiveScalarTypes = [BoundaryConditionType(v) for v in (t if isinstance(t, (list, tuple)) else [t])]
 
     # --- geometry ---
     def getSpatialDims(self) -> int:
@@ -217,6 +230,72 @@ class FixedBoundary(Boundary):
     def GetFluxes(self) -> torch.Tensor:
         """Contravariant normal fluxes of the face cells, ``[B, 1, *face]``."""
         return self._domain._boundary_fluxes(self)
+
+    # --- passive scalar (domain/boundaries.cpp:372-440) ---
+    def _check_scalar(self, ps: torch.Tensor) -> torch.Tensor:
+        d, C = self.getSpatialDims(), self._domain.getPassiveScalarChannels()
+        ps = ps.to(device=self._domain.getDevice(), dtype=self._domain.getDtype())
+        if C < 1:
+            raise RuntimeError("Passive scalars are not active.")
+        if ps.dim() < 2 or ps.shape[0] < 1 or ps.shape[1] != C:
+            raise RuntimeError("Passive scalar channels must match domain.")
+        if ps.dim() not in (2, 2 + d):
+            raise RuntimeError("Passive Scalar must be static (shape NC) or varying (shape NC + face spatial shape).")
+        if ps.dim() == 2 + d and list(ps.shape[2:]) != self.face_shape():
+            raise RuntimeError(f"varying passive scalar must have the face shape {self.face_shape()}")
+        return ps.contiguous()
+
+    @property
+    def passiveScalar(self) -> torch.Tensor | None:
+        return self._passiveScalar
+
+    @property
+    def passiveScalarTypes(self) -> list[BoundaryConditionType] | None:
+        return None if self._passiveScalarTypes is None else list(self._passiveScalarTypes)
+
+    def hasPassiveScalar(self) -> bool:
+        return self._passiveScalar is not None
+
+    def getPassiveScalarChannels(self) -> int:
+        return self._domain.getPassiveScalarChannels()
+
+    def setPassiveScalar(self, passiveScalar: torch.Tensor) -> None:
+        ps = self._check_scalar(passiveScalar)
+        if self._passiveScalar is not None and ps.shape == self._passiveScalar.shape and self._domain._prepared_for(self):
+            self._passiveScalar.copy_(ps)
+        else:
+            self._passiveScalar = ps
+            self._domain._invalidate()
+        if self._passiveScalarTypes is None:
+            self._passiveScalarTypes = [self._velocityType]
+        self._domain._bump()
+
+    def CreatePassiveScalar(self, createStatic: bool = True) -> None:
+        C = self.getPassiveScalarChannels()
+        shape = [1, C] if createStatic else [1, C] + self.face_shape()
+        self.setPassiveScalar(torch.zeros(shape, dtype=self._domain.getDtype(), device=self._domain.getDevice()))
+
+    def isPassiveScalarStatic(self) -> bool:
+        return self._passiveScalar is None or self._passiveScalar.dim() == 2
+
+    def setPassiveScalarType(self, types) -> None:
+        """One type for every channel, or one per channel (Dirichlet: a value; Neumann: the
+        physical gradient along the outward normal)."""
+        if self._passiveScalar is None:
+            raise RuntimeError("FixedBoundary has not passive scalar.")
+        t = list(types) if isinstance(types, (list, tuple)) else [types]
+        if len(t) not in (1, self.getPassiveScalarChannels()):
+            raise RuntimeError("Passive scalar boundary conditions must be static or match channels.")
+        self._passiveScalarTypes = [BoundaryConditionType(v) for v in t]
+        self._domain._invalidate()
+
+    def isPassiveScalarBoundaryTypeStatic(self) -> bool:
+        return self._passiveScalarTypes is None or len(self._passiveScalarTypes) == 1
+
+    def _scalar_types(self) -> list[int]:
+        C = self.getPassiveScalarChannels()
+        t = self._passiveScalarTypes or [BoundaryConditionType.DIRICHLET]
+        return [int(t[0] if len(t) == 1 else t[c]) for c in range(C)]
 
     # --- electric potential (domain/boundaries.cpp:900-965) ---
     def setPotentialBC(self, type: PotentialBC, cw: float | None = None) -> None:
@@ -325,6 +404,9 @@ class Block:
         self.velocity = velocity.to(**opts).contiguous() if velocity is not None else torch.zeros(B, d, *spatial, **opts)
         self.pressure = pressure.to(**opts).contiguous() if pressure is not None else torch.zeros(B, 1, *spatial, **opts)
         self.epot: torch.Tensor | None = None
+        self.passiveScalar: torch.Tensor | None = None
+        if domain.hasPassiveScalar():
+            self.passiveScalar = torch.zeros(B, domain.getPassiveScalarChannels(), *spatial, **opts)
         self.velocitySource: torch.Tensor | None = None
         self.vertexCoordinates = vertexCoordinates.to(**opts).contiguous() if vertexCoordinates is not None else None
         self._boundaries: list[Boundary] = [PeriodicBoundary(domain) for _ in range(2 * d)]
@@ -406,6 +488,46 @@ class Block:
     def hasEpot(self) -> bool:
         return self.epot is not None
 
+    # --- passive scalar (domain/block.cpp:347-377) ---
+    def hasPassiveScalar(self) -> bool:
+        return self._domain.hasPassiveScalar()
+
+    def getPassiveScalarChannels(self) -> int:
+        return self._domain.getPassiveScalarChannels()
+
+    def setPassiveScalar(self, passiveScalar: torch.Tensor) -> None:
+        C = self.getPassiveScalarChannels()
+        if C < 1:
+            raise RuntimeError("Passive scalars are not active.")
+        d = self.getSpatialDims()
+        s = passiveScalar.to(dtype=self._domain.getDtype(), device=self._domain.getDevice())
+        want = [C] + list(reversed(self._sizes[:d]))
+        if s.dim() != d + 2 or list(s.shape[1:]) != want:
+            raise RuntimeError(f"passive scalar must have shape [B, {C}, *spatial], got {tuple(s.shape)}")
+        if self.passiveScalar is not None and s.shape == self.passiveScalar.shape:
+            self.passiveScalar.copy_(s)
+        else:
+            self.passiveScalar = s.contiguous()
+            self._domain._invalidate()
+
+    def CreatePassiveScalar(self) -> None:
+        C = self.getPassiveScalarChannels()
+        if C < 1:
+            raise RuntimeError("Passive scalars are not active.")
+        d = self.getSpatialDims()
+        self.setPassiveScalar(torch.zeros(self._domain.getBatchSize(), C, *reversed(self._sizes[:d]),
+                                          dtype=self._domain.getDtype(), device=self._domain.getDevice()))
+
+    @property
+    def passiveScalarViscosity(self) -> torch.Tensor | None:
+        return None
+
+    def hasPassiveScalarViscosity(self) -> bool:
+        return False
+
+    def isAllFixedBoundariesPassiveScalarTypeStatic(self) -> bool:
+        return all(b.isPassiveScalarBoundaryTypeStatic() for _, b in self.getFixedBoundaries())
+
     # --- boundaries ---
     def getBoundary(self, face: int | str) -> Boundary:
         return self._boundaries[face_index(face)]
@@ -437,18 +559,22 @@ class Block:
         self._domain._invalidate()
 
     def CloseBoundary(self, face: int | str, velocity: torch.Tensor | None = None, passiveScalar=None) -> None:
-        """A no-slip (velocity given: Dirichlet) wall or inflow (domain/block.cpp:960-964)."""
+        """A no-slip (velocity given: Dirichlet) wall or inflow (domain/block.cpp:960-964); the
+        passive scalar is Dirichlet (zero unless given)."""
         f = face_index(face)
         self._check_face(f)
         self._close_connection(f)
-        self._set_boundary(f, FixedBoundary(self._domain, self, f, velocity, BoundaryConditionType.DIRICHLET))
+        self._set_boundary(f, FixedBoundary(self._domain, self, f, velocity, BoundaryConditionType.DIRICHLET,
+                                            passiveScalar))
 
     def OpenBoundary(self, face: int | str, passiveScalar=None) -> None:
-        """A zero-gradient (Neumann) velocity face (domain/block.cpp:969-977)."""
+        """A zero-gradient (Neumann) velocity face (domain/block.cpp:969-977); the passive scalar
+        is Neumann too (zero gradient unless given)."""
         f = face_index(face)
         self._check_face(f)
         self._close_connection(f)
-        self._set_boundary(f, FixedBoundary(self._domain, self, f, None, BoundaryConditionType.NEUMANN))
+        self._set_boundary(f, FixedBoundary(self._domain, self, f, None, BoundaryConditionType.NEUMANN, passiveScalar,
+                                            BoundaryConditionType.NEUMANN))
 
     def CloseAllBoundaries(self) -> None:
         for f in range(2 * self.getSpatialDims()):
@@ -605,7 +731,12 @@ class Domain:
         self._epot_flags = (0, False)
         self._advection_scheme = AdvectionScheme.CENTRAL
         self._timestep = torch.ones(1, dtype=torch.float64)
-        self.passiveScalarChannels = passiveScalarChannels
+        if int(passiveScalarChannels) < 0:
+            raise RuntimeError("passiveScalarChannels must not be negative")
+        self._scalar_channels = int(passiveScalarChannels)
+        self.passiveScalarViscosity: torch.Tensor | None = None
+        if scalarViscosity is not None:
+            self.setPassiveScalarViscosity(scalarViscosity)
 
     # --- basic accessors ---
     def getSpatialDims(self) -> int:
@@ -639,8 +770,48 @@ class Domain:
     def IsInitialized(self) -> bool:
         return self._prepared
 
+    # --- passive scalar (domain/domain.cpp:618-636) ---
     def hasPassiveScalar(self) -> bool:
+        return self._scalar_channels > 0
+
+    def getPassiveScalarChannels(self) -> int:
+        return self._scalar_channels
+
+    def setPassiveScalarViscosity(self, scalarViscosity) -> None:
+        """The scalar diffusivity: one value for every channel, or one per channel."""
+        v = scalarViscosity if isinstance(scalarViscosity, torch.Tensor) else torch.tensor([float(scalarViscosity)])
+        v = v.detach().to("cpu", torch.float64).reshape(-1).clone()
+        if v.numel() not in (1, max(1, self._scalar_channels)):
+            raise RuntimeError("scalar viscosity must have 1 or one-per-channel entries")
+        self.passiveScalarViscosity = v
+        if getattr(self, "_prepared", False):
+            self._upload_scalar_viscosity()
+
+    def hasPassiveScalarViscosity(self) -> bool:
+        return self.passiveScalarViscosity is not None
+
+    def isPassiveScalarViscosityStatic(self) -> bool:
+        return self.passiveScalarViscosity is None or self.passiveScalarViscosity.numel() == 1
+
+    def hasPassiveScalarBlockViscosity(self) -> bool:
         return False
+
+    def isAllFixedBoundariesPassiveScalarTypeStatic(self) -> bool:
+        return all(b.isAllFixedBoundariesPassiveScalarTypeStatic() for b in self._blocks)
+
+    def CreatePassiveScalarOnBlocks(self) -> None:
+        if self.hasPassiveScalar():
+            for b in self._blocks:
+                b.CreatePassiveScalar()
+
+    def setScalarResult(self, result: torch.Tensor) -> None:
+        r = result.detach().reshape(-1)
+        if r.numel() != self.scalarResult.numel():
+            raise RuntimeError(f"scalar result must have {self.scalarResult.numel()} values")
+        self.scalarResult.copy_(r)
+
+    def CreateScalarResult(self) -> None:
+        self.scalarResult.zero_()
 
     def hasVertexCoordinates(self) -> bool:
         return all(b.hasVertexCoordinates() for b in self._blocks)
@@ -705,6 +876,8 @@ class Domain:
             else:
                 raise RuntimeError("velocity batch size does not match the domain")
         blk = Block(self, name, sizes, velocity, pressure, vertexCoordinates)
+        if passiveScalar is not None:
+            blk.setPassiveScalar(passiveScalar)
         self._blocks.append(blk)
         self._invalidate()
         return blk
@@ -732,6 +905,9 @@ class Domain:
             if b.velocitySource is not None and b.velocitySource.shape[0] == 1 and B > 1:
                 s = b.velocitySource
                 b.velocitySource = s.expand(B, *s.shape[1:]).contiguous()
+            if b.passiveScalar is not None and b.passiveScalar.shape[0] == 1 and B > 1:
+                s = b.passiveScalar
+                b.passiveScalar = s.expand(B, *s.shape[1:]).contiguous()
         self._batch = B
         self._invalidate()
 
@@ -770,6 +946,21 @@ class Domain:
             spatial = list(reversed(b._sizes[:d]))
             b.velocity = u[:, :, b.globalOffset:b.globalOffset + n].view(B, d, *spatial)
             b.pressure = p[:, b.globalOffset:b.globalOffset + n].view(B, 1, *spatial)
+        # passive scalar: one flat [B][channels][cells] buffer, blocks are views
+        C = self._scalar_channels
+        if C > 0:
+            phi = torch.zeros(B, C, N, **opts)
+            for b in self._blocks:
+                n = b.ncells()
+                spatial = list(reversed(b._sizes[:d]))
+                if b.passiveScalar is not None:
+                    phi[:, :, b.globalOffset:b.globalOffset + n] = b.passiveScalar.expand(B, C, *spatial).reshape(B, C, n)
+                b.passiveScalar = phi[:, :, b.globalOffset:b.globalOffset + n].view(B, C, *spatial)
+            self._phi_block = phi
+            self.scalarRHS = torch.zeros(B * C * N, **opts)
+            self.scalarResult = torch.zeros(B * C * N, **opts)
+        else:
+            self._phi_block = None
         # velocity sources: one per-cell buffer when any block has a per-cell source,
         # otherwise static [B, d] per block (all equal) or none
         self._rebuild_sources()
@@ -822,9 +1013,12 @@ class Domain:
         self._pack_fixed()
         # records
         self._build_records()
+        self._pack_scalar_faces()
         self._dt_dev = torch.ones(B, dtype=torch.float64, device=self._device)
         self._nu_dev = torch.zeros(B, dtype=torch.float64, device=self._device)
         self._upload_viscosity()
+        self._snu_dev = torch.zeros(max(1, self._scalar_channels), dtype=torch.float64, device=self._device)
+        self._upload_scalar_viscosity()
         self._scratch = torch.zeros(int(_lib.load().phb_scratch_doubles(ct.byref(self._desc_struct()), 3)) + 64,
                                     dtype=torch.float64, device=self._device)
         self._rms_out = torch.zeros(B, dtype=torch.float64, device=self._device)
@@ -840,6 +1034,67 @@ class Domain:
         self._attach_csr_pattern()
         if self._epot_on:
             self.SetupEpotOnDomain(*self._epot_flags)
+
+    def _upload_scalar_viscosity(self) -> None:
+        v = self.passiveScalarViscosity
+        if v is not None:
+            self._snu_dev[: v.numel()].copy_(v)
+
+    def _pack_scalar_faces(self) -> None:
+        """Fixed-face passive-scalar data per fixed record (one per environment and face):
+        values (boundary tensors become views of the packed buffer), offsets, static flags
+        and per-channel types, the layout phb_scalar describes."""
+        B, C = self._batch, self._scalar_channels
+        nf = len(self._fixed)
+        opts = dict(dtype=self._dtype, device=self._device)
+        if C == 0:
+            self._fscal = None
+            return
+        chunks, offs, stat, types = [], [0] * max(1, B * nf), [0] * max(1, B * nf), [0] * max(1, B * nf * C)
+        off = 0
+        for k, (i, f, bd) in enumerate(self._fixed):
+            ps = bd._passiveScalar
+            if ps is None:
+                ps = torch.zeros(1, C, **opts)
+                bd._passiveScalar = ps
+                bd._passiveScalarTypes = [bd._velocityType]
+            if ps.shape[0] not in (1, B):
+                raise RuntimeError("boundary passive scalar batch size must be 1 or the domain batch size")
+            static = ps.dim() == 2
+            esize = C if static else C * self._fixed_cells[k]
+            tv = bd._scalar_types()
+            for e in range(B):
+                r = e * nf + k
+                offs[r] = off + (e if ps.shape[0] == B else 0) * esize
+                stat[r] = 1 if static else 0
+                for c in range(C):
+                    types[r * C + c] = tv[c]
+            chunks.append(ps.reshape(-1))
+            off += ps.numel()
+        self._fscal = torch.cat(chunks) if chunks else torch.zeros(1, **opts)
+        self._fscal_off = torch.tensor(offs, dtype=torch.int64, device=self._device)
+        self._fscal_static = torch.tensor(stat, dtype=torch.int8, device=self._device)
+        self._fscal_types = torch.tensor(types, dtype=torch.int8, device=self._device)
+        o = 0
+        for k, (i, f, bd) in enumerate(self._fixed):
+            ps = bd._passiveScalar
+            bd._passiveScalar = self._fscal[o:o + ps.numel()].view(ps.shape)
+            o += ps.numel()
+
+    def _scalar_struct(self) -> _lib.PhbScalar:
+        """The phb_scalar description of this domain's passive scalar."""
+        if not self.hasPassiveScalar():
+            raise RuntimeError("the domain has no passive scalar")
+        s = _lib.PhbScalar()
+        s.channels = self._scalar_channels
+        v = self.passiveScalarViscosity
+        s.nu_count = 0 if v is None else int(v.numel())
+        s.nu = self._snu_dev.data_ptr()
+        s.types = self._fscal_types.data_ptr()
+        s.values = self._fscal.data_ptr()
+        s.offsets = self._fscal_off.data_ptr()
+        s.statics = self._fscal_static.data_ptr()
+        return s
 
     def _upload_viscosity(self) -> None:
         v = self.viscosity

@@ -117,6 +117,7 @@ class Simulation:
         self.normalize_pressure_result = normalize_pressure_result
         self.pressure_return_best_result = pressure_return_best_result
         self.non_orthogonal = non_orthogonal
+        self.advect_passive_scalar = bool(advect_passive_scalar)
         self.differentiable = False
         self.linear_solve_max_iterations = 5000
         self.mixed_precision = bool(mixed_precision)
@@ -297,8 +298,12 @@ class Simulation:
             if self.convergence_tol is not None:
                 last_vel = d._u_block.clone()
             self._run_hooks(Hook.PRE, local_step=step, time_step=ts)
+            matrix_for_velocity = False
+            if self.advect_passive_scalar and d.hasPassiveScalar():
+                matrix_for_velocity = self._advect_scalar(ts, step)
             self._run_hooks(Hook.PRE_VELOCITY_SETUP, local_step=step, time_step=ts)
-            backend.SetupAdvectionMatrix(d, ts, 0)
+            if not matrix_for_velocity:
+                backend.SetupAdvectionMatrix(d, ts, 0)
             backend.SetupAdvectionVelocity(d, ts, 0, False)
             self._run_hooks(Hook.POST_VELOCITY_SETUP, local_step=step, time_step=ts, no_step=0)
             self.solve("C", d.velocityRHS, d.velocityResult, use_BiCG=self.advection_use_BiCG,
@@ -343,6 +348,36 @@ class Simulation:
             if not ok:
                 return False
         return True
+
+    def _advect_scalar(self, ts, step: int) -> bool:
+        """Implicit advection-diffusion of every passive-scalar channel with the velocity of
+        the step start (core/piso_simulation.py:3589-3775, orthogonal path): one matrix for
+        all channels when their diffusivity and face types agree, else one per channel; a
+        zero initial guess; the result copied to the blocks. Returns whether the velocity
+        step reuses the scalar matrix (same diffusivity as the velocity, one set of face types
+        for all channels), as phiPICT does."""
+        d = self.domain
+        C = d.getPassiveScalarChannels()
+        B = d.getBatchSize()
+        split = not (d.isPassiveScalarViscosityStatic() and d.isAllFixedBoundariesPassiveScalarTypeStatic())
+        reuse = not (d.hasPassiveScalarViscosity() or d.hasBlockViscosity() or d.hasPassiveScalarBlockViscosity() or split)
+        rhs = d.scalarRHS.view(B, C, -1)
+        res = d.scalarResult.view(B, C, -1)
+        if not split:
+            backend.SetupAdvectionMatrix(d, ts, 0, forPassiveScalar=True, passiveScalarChannel=0)
+        backend.SetupAdvectionScalar(d, ts, 0)
+        self._run_hooks(Hook.POST_SCALAR_SETUP, local_step=step, time_step=ts, no_step=0)
+        for c in range(C):
+            if split:
+                backend.SetupAdvectionMatrix(d, ts, 0, forPassiveScalar=True, passiveScalarChannel=c)
+            # channel c of every environment as one flat [B][cells] system (launches are
+            # stream-ordered, so a per-channel matrix is consumed before the next overwrites it)
+            b = rhs[:, c].contiguous().view(-1)
+            x = torch.zeros_like(b)
+            self.solve("C", b, x, use_BiCG=self.advection_use_BiCG, tol=self.advection_tol, tag=f"scalar{c}")
+            res[:, c].copy_(x.view(B, -1))
+        backend.CopyScalarResultToBlocks(d)
+        return reuse
 
     def make_divergence_free(self, iterations: int = 1, max_iter: int = 1000) -> bool:
         """Project the block velocity onto a divergence-free field with A = 1, dt = 1

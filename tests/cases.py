@@ -12,11 +12,13 @@ import phipict_b200 as pb
 from phipict_b200.grid import make_weights_tanh, rectilinear_vertices, span
 
 
-def hartmann_2d(nx=16, ny=12, *, device="cuda", dtype=torch.float64, length=4.0, grading=1.5, nu=0.01, batch=1):
-    """Periodic x, no-slip insulating walls at y = +-1, tanh-graded in y."""
+def hartmann_2d(nx=16, ny=12, *, device="cuda", dtype=torch.float64, length=4.0, grading=1.5, nu=0.01, batch=1,
+                channels=1):
+    """Periodic x, no-slip insulating walls at y = +-1, tanh-graded in y; `channels` passive
+    scalar channels (phiPICT's default is one)."""
     xs = np.linspace(0.0, length, nx + 1)
     ys = span(-1.0, 1.0, make_weights_tanh(ny, grading))
-    dom = pb.Domain(2, torch.tensor([nu]), name="hartmann", device=device, dtype=dtype)
+    dom = pb.Domain(2, torch.tensor([nu]), name="hartmann", device=device, dtype=dtype, passiveScalarChannels=channels)
     b = dom.CreateBlock(vertexCoordinates=rectilinear_vertices(xs, ys, dtype=dtype), name="channel")
     b.CloseBoundary("-y")
     b.CloseBoundary("+y")
@@ -27,14 +29,14 @@ def hartmann_2d(nx=16, ny=12, *, device="cuda", dtype=torch.float64, length=4.0,
 
 
 def duct_3d(nx=8, ny=6, nz=5, nblocks=2, *, device="cuda", dtype=torch.float64, grading=2.0, nu=0.05,
-            seed=0, noise=1e-2, batch=1):
+            seed=0, noise=1e-2, batch=1, channels=1):
     """nblocks blocks connected along x; inflow (u=1 + seeded noise, flux-balanced by a
     varying outflow) at -x, open-potential outflow at +x, insulating walls in y and z."""
     ws = make_weights_tanh(ny, grading)
     wz = make_weights_tanh(nz, grading)
     ys = span(-1.0, 1.0, ws)
     zs = span(-1.0, 1.0, wz)
-    dom = pb.Domain(3, torch.tensor([nu]), name="duct", device=device, dtype=dtype)
+    dom = pb.Domain(3, torch.tensor([nu]), name="duct", device=device, dtype=dtype, passiveScalarChannels=channels)
     blocks = []
     for i in range(nblocks):
         xs = np.linspace(i * 1.0, (i + 1) * 1.0, nx + 1)

@@ -39,3 +39,4 @@ def test_struct_layouts_match_header():
     assert ct.sizeof(_lib.PhbSolveResult) == 32
     assert _lib.PhbSolve.tol.offset == 32
     assert _lib.PhbDomain.blocks.offset == 48
+    assert ct.sizeof(_lib.PhbScalar) == 48 and _lib.PhbScalar.nu.offset == 8

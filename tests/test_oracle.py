@@ -131,3 +131,41 @@ def test_hartmann_profile():
     exact = G / N * (1 - np.cosh(Ha * y) / math.cosh(Ha))
     err = np.abs(u - exact).max() / np.abs(exact).max()
     assert err < 5e-3, err
+
+
+def test_scalar_constant_field_is_steady_under_uniform_flow():
+    """Passive scalar (advection.cu:27-305 forPassiveScalar, :545-698): in a fully periodic
+    box a uniform, divergence-free velocity leaves a constant scalar constant, so the scalar
+    matrix applied to it reproduces its right-hand side."""
+    from phipict_b200.grid import rectilinear_vertices
+
+    dom = pb.Domain(2, torch.tensor([0.05]), name="box", device="cpu", dtype=torch.float64)
+    b = dom.CreateBlock(vertexCoordinates=rectilinear_vertices(np.linspace(0, 1, 9), np.linspace(0, 2, 7),
+                                                               dtype=torch.float64), name="box")
+    b.MakePeriodic("x")
+    b.MakePeriodic("y")
+    v = torch.zeros(b.velocity.shape, dtype=torch.float64)
+    v[:, 0], v[:, 1] = 1.0, 0.5
+    b.velocity.copy_(v)
+    od = OracleDomain(dom)
+    u = v.reshape(-1).numpy()
+    val, _ = od.scalar_matrix(u, 0.01, 0.02, 0)
+    rhs = od.scalar_rhs(np.full(od.n, 2.5), 0.01, 0.02, 0)
+    assert np.abs(od.spmv(val, np.full(od.n, 2.5)) - rhs).max() < 1e-10 * np.abs(rhs).max()
+
+
+def test_scalar_dirichlet_wall_value_enters_linearly():
+    """A Dirichlet face value enters the scalar right-hand side linearly and only at the cells
+    of that face."""
+    dom = hartmann_2d(6, 5, device="cpu")
+    wall = dom.getBlocks()[0].getBoundary("-y")
+    od0 = OracleDomain(dom)
+    phi = np.zeros(od0.n)
+    r0 = od0.scalar_rhs(phi, 0.01, 0.02, 0)
+    wall.setPassiveScalar(torch.full((1, 1), 3.0, dtype=torch.float64))
+    r1 = OracleDomain(dom).scalar_rhs(phi, 0.01, 0.02, 0)
+    changed = np.flatnonzero(np.abs(r1 - r0) > 0)
+    assert changed.size == 6 and np.all(changed < 6)  # the first row of cells (y = 0)
+    wall.setPassiveScalar(torch.full((1, 1), 6.0, dtype=torch.float64))
+    r2 = OracleDomain(dom).scalar_rhs(phi, 0.01, 0.02, 0)
+    assert np.allclose(r2 - r0, 2 * (r1 - r0), rtol=1e-12, atol=0)
