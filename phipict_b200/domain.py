@@ -1489,19 +1489,38 @@ class Domain:
 
     # --- misc ---------------------------------------------------------------------------
     def getMaxVelocity(self, withBounds: bool = True, computational: bool = False) -> torch.Tensor:
+        """Largest velocity component magnitude over all environments (block.cpp:505-535)."""
         return self.getMaxVelocityPerEnv(withBounds, computational).max()
 
     def getMaxVelocityPerEnv(self, withBounds: bool = True, computational: bool = False) -> torch.Tensor:
-        m = self._u_block.abs().amax(dim=(1, 2))
+        """Largest velocity component magnitude per environment, [B] (block.cpp:537-575):
+        cell velocities and, withBounds, the fixed faces' velocities; computational: the
+        velocities in computational space, Minv u per cell (grid/transform_vectors.cu:42-72),
+        as the CFL bound of adaptive substeps uses them."""
+        d = self._dims
+        u = self._u_block
+        if computational:
+            u = _to_computational(u, self._metrics, d)
+        m = u.abs().amax(dim=(1, 2))
         if withBounds:
-            for _, _, bd in self._fixed:
+            for k, (_, _, bd) in enumerate(self._fixed):
                 v = bd._velocity
+                if computational:
+                    fc, to = self._fixed_cells[k], self._fixed_toff[k]
+                    vv = v.reshape(v.shape[0], d, -1).expand(v.shape[0], d, fc) if v.dim() == 2 else v.reshape(v.shape[0], d, fc)
+                    v = _to_computational(vv, self._face_metrics[:, to:to + fc], d)
                 mb = v.abs().reshape(v.shape[0], -1).amax(1)
                 m = torch.maximum(m, mb.expand_as(m))
         return m
 
     def __str__(self) -> str:
         return f"Domain({self.name}, dims={self._dims}, blocks={len(self._blocks)}, batch={self._batch})"
+
+
+def _to_computational(u: torch.Tensor, metrics: torch.Tensor, d: int) -> torch.Tensor:
+    """Minv u per cell: u [B, d, n] with metrics [2d^2+1, n] (Minv rows at d^2 + i d + j)."""
+    rows = [sum(metrics[d * d + i * d + j] * u[:, j] for j in range(d)) for i in range(d)]
+    return torch.stack(rows, dim=1)
 
 
 def _identity_metrics(view: torch.Tensor, d: int) -> None:

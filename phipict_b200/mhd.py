@@ -139,6 +139,11 @@ class MHDSimulation(Simulation):
         if not torch.equal(old, self._e_b_dev):
             self._potential_stale = True
 
+    def _env_state_extras(self) -> list:
+        """Adds u x e_b of the last magnetic step, which the next substep's Lorentz force uses
+        (simulation/mhd.py:864-875)."""
+        return [*super()._env_state_extras(), lambda: self._uxb]
+
     def _accept_best(self, info: LinearSolverResultInfo) -> bool:
         # a non-converged plain solve returns its best iterate (mhd.py:430-433); a refined
         # solve has no best iterate, so it has to converge

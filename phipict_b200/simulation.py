@@ -20,9 +20,9 @@ Extensions (keyword arguments phiPICT does not have):
 """
 from __future__ import annotations
 
-import math
 from typing import Any, Literal
 
+import numpy as np
 import torch
 
 from . import _C as backend
@@ -92,14 +92,16 @@ class Simulation:
             raise NotImplementedError("phipict_b200 implements the finite-difference velocity corrector ('FD')")
         if pressure_time_step_normalized:
             raise NotImplementedError("pressure_time_step_normalized is not implemented")
-        if substeps not in (1,) and not (isinstance(substeps, int) and substeps > 0):
-            raise NotImplementedError("phipict_b200 runs fixed substeps (substeps >= 1)")
+        if substeps != "ADAPTIVE" and not (isinstance(substeps, int) and substeps > 0):
+            raise ValueError("substeps must be a positive int or 'ADAPTIVE'")
         if differentiable:
             raise NotImplementedError(
                 "the differentiable step is provided by phipict_b200.adjoint.DifferentiableStep")
         self.domain = domain
         self.time_step = float(dt)
-        self.substeps = int(substeps)
+        self.substeps = substeps if substeps == "ADAPTIVE" else int(substeps)
+        self.adaptive_CFL = float(adaptive_CFL)
+        self.adaptive_CFL_per_env = bool(adaptive_CFL_per_env)
         self.corrector_steps = int(corrector_steps)
         self.density_viscosity = density_viscosity
         self.hooks = Hooks.coerce(hooks if hooks is not None else prep_fn)
@@ -279,6 +281,8 @@ class Simulation:
         """One simulation step of ``substeps`` PISO steps (simulation/simulation.py:262-333)."""
         self._check_flux_balance()
         try:
+            if self.substeps == "ADAPTIVE":
+                return self._PISO_adaptive_step()
             return self._PISO_split_step(self.substeps)
         except LinsolveError as e:
             self.last_error = str(e)
@@ -349,6 +353,67 @@ class Simulation:
                 return False
         return True
 
+    # --- adaptive substeps (core/piso_simulation.py:4171-4340) -------------------------------
+    def _env_state_extras(self) -> list:
+        """Getters of per-environment state outside the domain, restored with it for
+        environments that sit out a substep."""
+        return []
+
+    def _PISO_adaptive_step(self, CFL_cond: float | None = None, max_substeps: int = 1000) -> bool:
+        """Advance by `time_step` in substeps that keep the computational-space CFL number
+        below `adaptive_CFL`; the substep size is re-derived from the current maximum velocity
+        before every substep. Batched domains split per environment (adaptive_CFL_per_env)."""
+        d = self.domain
+        CFL = self.adaptive_CFL if CFL_cond is None else float(CFL_cond)
+        if d.getBatchSize() > 1 and self.adaptive_CFL_per_env:
+            return self._PISO_adaptive_step_per_env(CFL, max_substeps)
+        remaining = self.time_step
+        self.adaptive_substeps = 0
+        while remaining > 0 and not np.isclose(remaining, 0):
+            max_vel = d.getMaxVelocity(True, True).detach().cpu().numpy()
+            ts, _ = _cfl_substep(remaining, max_vel, CFL)
+            remaining -= ts
+            ok = self._PISO_split_step(1, time_step=torch.tensor([float(ts)], dtype=torch.float64))
+            self.adaptive_substeps += 1
+            if not ok:
+                return False
+        return True
+
+    def _PISO_adaptive_step_per_env(self, CFL: float, max_substeps: int) -> bool:
+        """Every environment splits `time_step` by its own maximum velocity, exactly as it
+        would alone; the batch runs until the environment with the most substeps is done, and
+        an environment that is done runs the remaining substeps at its last substep size with
+        its state restored afterwards (EnvStateSnapshot). Hooks see the [B] substep sizes."""
+        from .batching import EnvStateSnapshot
+
+        d = self.domain
+        B = d.getBatchSize()
+        start = self.total_time
+        remaining = [self.time_step] * B
+        steps = [self.time_step] * B
+        self.adaptive_substeps_per_env = [0] * B
+        while True:
+            active = [r > 0 and not np.isclose(r, 0) for r in remaining]
+            if not any(active):
+                break
+            mv = d.getMaxVelocityPerEnv(True, True).detach().cpu().numpy()
+            for b in range(B):
+                if not active[b]:
+                    continue
+                steps[b], _ = _cfl_substep(remaining[b], mv[b], CFL)
+                remaining[b] -= steps[b]
+                self.adaptive_substeps_per_env[b] += 1
+            done = [b for b in range(B) if not active[b]]
+            snap = EnvStateSnapshot(d, torch.tensor(done), extra=self._env_state_extras()) if done else None
+            ok = self._PISO_split_step(1, time_step=torch.tensor([float(t) for t in steps], dtype=torch.float64))
+            if snap is not None:
+                snap.restore()
+            self.total_time = start + self.time_step - float(min(remaining))
+            if not ok:
+                return False
+        self.total_time = start + self.time_step
+        return True
+
     def _advect_scalar(self, ts, step: int) -> bool:
         """Implicit advection-diffusion of every passive-scalar channel with the velocity of
         the step start (core/piso_simulation.py:3589-3775, orthogonal path): one matrix for
@@ -403,12 +468,25 @@ class Simulation:
         return self.collect_solves(raise_on_failure=False)
 
 
-def get_max_time_step(domain: Domain, time_step_target: float, CFL_cond: float = 0.8, with_transformations: bool = True):
-    """Largest stable step for the current velocity and the substeps to reach the target."""
-    umax = float(domain.getMaxVelocity(True, False))
-    hmin = float(domain._metrics[2 * domain.getSpatialDims() ** 2].abs().min()) ** (1.0 / domain.getSpatialDims())
-    if umax <= 0:
+def _cfl_substep(time_step_target, max_vel, CFL_cond: float):
+    """The next substep size and the number of substeps the remaining time is split into
+    (core/piso_simulation.py:187-216): max step CFL / max_vel; NumPy scalars keep their dtype."""
+    if np.isclose(max_vel, 0):
+        max_time_step = time_step_target
+    else:
+        max_time_step = CFL_cond / max_vel
+    if max_time_step >= time_step_target:
         return time_step_target, 1
-    dt = CFL_cond * hmin / umax
-    n = max(1, math.ceil(time_step_target / dt))
-    return time_step_target / n, n
+    substeps = int(np.ceil(time_step_target / max_time_step))
+    return time_step_target / substeps, substeps
+
+
+def get_max_time_step(domain: Domain, time_step_target: float, CFL_cond: float = 0.8, with_transformations: bool = True):
+    """Split a time step into substeps that satisfy a CFL condition (core/piso_simulation.py:
+    149-184): returns (substep size, number of substeps)."""
+    max_vel = domain.getMaxVelocity(True, with_transformations).cpu().numpy()
+    max_time_step = CFL_cond / max_vel
+    if max_time_step >= time_step_target:
+        return time_step_target, 1
+    ss = int(np.ceil(time_step_target / max_time_step))
+    return time_step_target / ss, ss
