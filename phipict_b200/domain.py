@@ -481,9 +481,13 @@ class Block:
         self._domain._set_block_source(self, None)
 
     def setEpot(self, epot: torch.Tensor) -> None:
+        """The electric potential [B, 1, *spatial]; before SetupEpotOnDomain it is kept and
+        taken over when the potential fields are allocated."""
+        e = epot.to(dtype=self._domain.getDtype(), device=self._domain.getDevice())
         if self.epot is None:
-            raise RuntimeError("epot is not allocated; call SetupEpotOnDomain() first")
-        self.epot.copy_(epot)
+            self.epot = e.contiguous()
+            return
+        self.epot.copy_(e)
 
     def hasEpot(self) -> bool:
         return self.epot is not None
