@@ -67,6 +67,8 @@ typedef struct phb_domain {
 	const int8_t *fmask;    /* fixed-face potential BC masks */
 	const double *dt;       /* [ninst] time step */
 	const double *nu;       /* [ninst] viscosity */
+	int32_t scheme;         /* advection scheme (AdvectionScheme): 0 CENTRAL, 1 LINEAR_UPWIND */
+	int32_t pad;
 } phb_domain;
 
 const char *phb_last_error(void);
@@ -83,7 +85,11 @@ int phb_face_metrics(int dims, int dtype, int nx, int ny, int nz, const void *co
                      void *face_out, int64_t stride, phb_stream stream);
 
 /* --- assembly (one launch each, all instances) ------------------------------------- */
-/* SetupAdvectionMatrix (bindings.cpp:639, advection.cu:27-305 PISO_build_matrix).
+/* The advection kernels follow phb_domain.scheme: with LINEAR_UPWIND a face whose downwind
+ * and far-upwind cells lie in the same block is first-order upwind in the matrix and gets the
+ * linear-upwind part as an explicit correction on the right-hand side (advection.cu:125-144,
+ * :892-934); other faces stay central.
+ * SetupAdvectionMatrix (bindings.cpp:639, advection.cu:27-305 PISO_build_matrix).
  * u: block velocity [inst][dims][cells]; C: stencil [2d+1][ncells]; Adiag [ncells].
  * C_lo (optional, may be NULL): float32 copy of C for mixed-precision inner solves. */
 int phb_advection_matrix(const phb_domain *dom, const void *u, void *C, void *Adiag, float *C_lo, phb_stream stream);
@@ -134,9 +140,11 @@ typedef struct phb_scalar {
  * phb_advection_matrix. */
 int phb_scalar_matrix(const phb_domain *dom, const void *u, const phb_scalar *sc, int channel, void *C, void *Adiag,
                       float *C_lo, phb_stream stream);
-/* SetupAdvectionScalar (advection.cu:545-698 kPISO_build_scalar_advection_RHS, CENTRAL,
- * orthogonal): rhs [inst][channels][cells] from the block scalar phi (same layout). */
-int phb_scalar_rhs(const phb_domain *dom, const void *phi, const phb_scalar *sc, void *rhs, phb_stream stream);
+/* SetupAdvectionScalar (advection.cu:545-698 kPISO_build_scalar_advection_RHS, orthogonal):
+ * rhs [inst][channels][cells] from the block scalar phi (same layout); u, the block velocity,
+ * gives the face fluxes of the LINEAR_UPWIND correction (may be NULL with CENTRAL). */
+int phb_scalar_rhs(const phb_domain *dom, const void *phi, const void *u, const phb_scalar *sc, void *rhs,
+                   phb_stream stream);
 
 /* --- vectors ------------------------------------------------------------------------ */
 /* Per-instance reductions use a caller-owned scratch of phb_scratch_doubles() doubles whose

@@ -262,13 +262,46 @@ static void forEachCell(const Dom<S> &D, const std::function<void(int, const int
 	}
 }
 
+// shared_stencils.cuh:35-43 hasFarUpwindCell: downwind and far-upwind cells inside the block
+template <typename S>
+static bool farUpwind(const Dom<S> &D, int b, const int *p, int f, bool outflow) {
+	const int ax = f >> 1, sign = (f & 1) ? 1 : -1, last = D.sz(b, ax) - 1;
+	const int iD = p[ax] + sign;
+	if (iD < 0 || iD > last) return false;
+	const int iUU = outflow ? p[ax] - sign : p[ax] + 2 * sign;
+	return iUU >= 0 && iUU <= last;
+}
+// advection.cu:892-934 (velocity) and :652-688 (scalar): LINEAR_UPWIND deferred correction,
+// r -= F 0.5 psi (phi_D - phi_U) per upwinded face, psi = (phi_U - phi_UU)/(phi_D - phi_U);
+// field(g) is the lagged block field at global cell g
+template <typename S, typename F>
+static void upwindCorrection(const Dom<S> &D, int b, const int *p, const S *fl, F field, S &r) {
+	for (int f = 0; f < 2 * D.dims; ++f) {
+		const int ax = f >> 1, sign = (f & 1) ? 1 : -1;
+		const S fout = S(sign) * fl[f];
+		const bool outflow = fout >= S(0);
+		if (!farUpwind(D, b, p, f, outflow)) continue;
+		int q[3] = {p[0], p[1], p[2]};
+		const S phiP = field(D.glob(b, q));
+		q[ax] = p[ax] + sign;
+		const S phiN = field(D.glob(b, q));
+		q[ax] = outflow ? p[ax] - sign : p[ax] + 2 * sign;
+		const S phiUU = field(D.glob(b, q));
+		const S phiU = outflow ? phiP : phiN, phiD = outflow ? phiN : phiP;
+		const S dD = phiD - phiU;
+		if ((dD < 0 ? -dD : dD) < S(1e-20)) continue;
+		const S psi = (phiU - phiUU) / dD;
+		r -= fout * S(0.5) * psi * dD;
+	}
+}
+
 // advection.cu:27-305 PISO_build_matrix (CENTRAL, orthogonal, domain viscosity). With
 // faceTypes (forPassiveScalar): the wall diffusion of a fixed face follows the scalar
 // channel's type faceTypes[fixed id] instead of the velocity type (advection.cu:254-266), and
 // nu is the channel's diffusivity.
 template <typename S>
 static void advMatrix(const Dom<S> &D, const S *u, S dt, S nu, const int *row, int *col, S *val, S *Adiag,
-		const int8_t *faceTypes = nullptr) {
+		const int8_t *faceTypes = nullptr, int scheme = 0) {
 	forEachCell<S>(D, [&](int b, const int *p, int g) {
 		S fl[6];
 		fluxes(D, b, p, u, fl);
@@ -284,9 +317,15 @@ static void advMatrix(const Dom<S> &D, const S *u, S dt, S nu, const int *row, i
 			const S faceSign = (f & 1) ? S(1) : S(-1);
 			const bool ab = D.atBound(b, f, p);
 			if (!ab || !D.isEmpty(b, f)) {
-				const S half = S(0.5) * (faceSign * fl[f]);
-				diag += half;
-				rv[f + 1] += half;
+				const S fout = faceSign * fl[f];
+				if (scheme != 0 && farUpwind(D, b, p, f, fout >= S(0))) { // advection.cu:131-139
+					if (fout >= S(0)) diag += fout;
+					else rv[f + 1] += fout;
+				} else {
+					const S half = S(0.5) * fout;
+					diag += half;
+					rv[f + 1] += half;
+				}
 				int nbk, np[3];
 				neighbor(D, b, f, p, nbk, np);
 				int comp = dim;
@@ -310,9 +349,11 @@ static void advMatrix(const Dom<S> &D, const S *u, S dt, S nu, const int *row, i
 
 // advection.cu:800-954 kPISO_build_advection_RHS (CENTRAL, no pressure gradient)
 template <typename S>
-static void advRhs(const Dom<S> &D, const S *u, const S *src, int srcStatic, S dt, S nu, S *rhs) {
+static void advRhs(const Dom<S> &D, const S *u, const S *src, int srcStatic, S dt, S nu, S *rhs, int scheme = 0) {
 	forEachCell<S>(D, [&](int b, const int *p, int g) {
 		const S det = D.det(D.T(b, p));
+		S fl[6];
+		if (scheme != 0) fluxes(D, b, p, u, fl);
 		for (int dim = 0; dim < D.dims; ++dim) {
 			S r = det * u[(size_t)dim * D.n + g] / dt;
 			for (int f = 0; f < 2 * D.dims; ++f) {
@@ -326,6 +367,7 @@ static void advRhs(const Dom<S> &D, const S *u, const S *src, int srcStatic, S d
 				const S slip = D.velType(b, f) == 0 ? S(0) : S(1);
 				r += vel * (S(1) - slip) * nu * S(2) * alpha;
 			}
+			if (scheme != 0) upwindCorrection(D, b, p, fl, [&](int gg) { return u[(size_t)dim * D.n + gg]; }, r);
 			r /= det;
 			if (src) r += srcStatic ? src[dim] : src[(size_t)dim * D.n + g];
 			rhs[(size_t)dim * D.n + g] = r;
@@ -339,9 +381,11 @@ static void advRhs(const Dom<S> &D, const S *u, const S *src, int srcStatic, S d
 // faceTypes[fixed id]: 0 Dirichlet, 1 Neumann; faceValue(fixed id, face cell) the face data.
 template <typename S>
 static void scalarRhs(const Dom<S> &D, const S *phi, S dt, S nu, const int8_t *faceTypes, const S *faceValues,
-		const int64_t *faceOffsets, const int8_t *faceStatic, S *rhs) {
+		const int64_t *faceOffsets, const int8_t *faceStatic, S *rhs, const S *u = nullptr, int scheme = 0) {
 	forEachCell<S>(D, [&](int b, const int *p, int g) {
 		const S det = D.det(D.T(b, p));
+		S fl[6];
+		if (scheme != 0) fluxes(D, b, p, u, fl);
 		S r = det * phi[g] / dt;
 		for (int f = 0; f < 2 * D.dims; ++f) {
 			if (!D.atBound(b, f, p) || D.ftype(b, f) != FT_FIXED) continue;
@@ -360,6 +404,7 @@ static void scalarRhs(const Dom<S> &D, const S *phi, S dt, S nu, const int8_t *f
 				r += value * nu * area;
 			}
 		}
+		if (scheme != 0) upwindCorrection(D, b, p, fl, [&](int gg) { return phi[gg]; }, r);
 		rhs[g] = r / det;
 	});
 }
@@ -433,10 +478,12 @@ static void laplaceMatrix(const Dom<S> &D, const S *Adiag, bool epot, const int 
 // pressure.cu:350-521 PISO_build_pressure_rhs (CENTRAL): HbyA per velocity component
 template <typename S>
 static void pressureRhs(const Dom<S> &D, const int *row, const int *col, const S *Cval, const S *Adiag,
-		const S *u, const S *ustar, const S *src, int srcStatic, S dt, S nu, S *hbya) {
+		const S *u, const S *ustar, const S *src, int srcStatic, S dt, S nu, S *hbya, int scheme = 0) {
 	forEachCell<S>(D, [&](int b, const int *p, int g) {
 		const S rDiag = S(1) / Adiag[g];
 		const S det = D.det(D.T(b, p));
+		S fl[6];
+		if (scheme != 0) fluxes(D, b, p, u, fl);
 		const int rs = row[g], re = row[g + 1];
 		for (int dim = 0; dim < D.dims; ++dim) {
 			const S velOld = u[(size_t)dim * D.n + g] / dt;
@@ -458,6 +505,11 @@ static void pressureRhs(const Dom<S> &D, const int *row, const int *col, const S
 			}
 			Ssum /= det;
 			if (src) Ssum += srcStatic ? src[dim] : src[(size_t)dim * D.n + g];
+			if (scheme != 0) { // pressure.cu:474-515: the predictor's deferred correction, / det
+				S corr = 0; // minus the face terms' sum, accumulated face by face
+				upwindCorrection(D, b, p, fl, [&](int gg) { return u[(size_t)dim * D.n + gg]; }, corr);
+				Ssum -= (-corr) / det;
+			}
 			hbya[(size_t)dim * D.n + g] = rDiag * (velOld - H + Ssum);
 		}
 	});
@@ -738,21 +790,23 @@ static int bicgstab(int n, const int *row, const int *col, const S *val, const S
 
 #define ORC_INSTANTIATE(S, SUF)                                                                                          \
 extern "C" void orc_row_pointers##SUF(ORC_DOM_ARGS(S), int *row) { ORC_DOM(S); orc::rowPointers(D, row); }              \
-extern "C" void orc_adv_matrix##SUF(ORC_DOM_ARGS(S), const S *u, double dt, double nu, const int *row, int *col, S *val, S *Adiag) { \
-	ORC_DOM(S); orc::advMatrix<S>(D, u, S(dt), S(nu), row, col, val, Adiag); }                                           \
+extern "C" void orc_adv_matrix##SUF(ORC_DOM_ARGS(S), const S *u, double dt, double nu, const int *row, int *col, S *val, S *Adiag, \
+		int scheme) {                                                                                                      \
+	ORC_DOM(S); orc::advMatrix<S>(D, u, S(dt), S(nu), row, col, val, Adiag, nullptr, scheme); }                           \
 extern "C" void orc_scalar_matrix##SUF(ORC_DOM_ARGS(S), const S *u, double dt, double nu, const int8_t *types,            \
-		const int *row, int *col, S *val, S *Adiag) {                                                                     \
-	ORC_DOM(S); orc::advMatrix<S>(D, u, S(dt), S(nu), row, col, val, Adiag, types); }                                      \
+		const int *row, int *col, S *val, S *Adiag, int scheme) {                                                         \
+	ORC_DOM(S); orc::advMatrix<S>(D, u, S(dt), S(nu), row, col, val, Adiag, types, scheme); }                              \
 extern "C" void orc_scalar_rhs##SUF(ORC_DOM_ARGS(S), const S *phi, double dt, double nu, const int8_t *types,            \
-		const S *values, const int64_t *offsets, const int8_t *statics, S *rhs) {                                         \
-	ORC_DOM(S); orc::scalarRhs<S>(D, phi, S(dt), S(nu), types, values, offsets, statics, rhs); }                            \
-extern "C" void orc_adv_rhs##SUF(ORC_DOM_ARGS(S), const S *u, const S *src, int srcStatic, double dt, double nu, S *rhs) { \
-	ORC_DOM(S); orc::advRhs<S>(D, u, src, srcStatic, S(dt), S(nu), rhs); }                                               \
+		const S *values, const int64_t *offsets, const int8_t *statics, S *rhs, const S *u, int scheme) {                 \
+	ORC_DOM(S); orc::scalarRhs<S>(D, phi, S(dt), S(nu), types, values, offsets, statics, rhs, u, scheme); }                 \
+extern "C" void orc_adv_rhs##SUF(ORC_DOM_ARGS(S), const S *u, const S *src, int srcStatic, double dt, double nu, S *rhs, \
+		int scheme) {                                                                                                      \
+	ORC_DOM(S); orc::advRhs<S>(D, u, src, srcStatic, S(dt), S(nu), rhs, scheme); }                                       \
 extern "C" void orc_laplace_matrix##SUF(ORC_DOM_ARGS(S), const S *Adiag, int epot, const int *row, int *col, S *val) { \
 	ORC_DOM(S); orc::laplaceMatrix<S>(D, Adiag, epot != 0, row, col, val); }                                             \
 extern "C" void orc_pressure_rhs##SUF(ORC_DOM_ARGS(S), const int *row, const int *col, const S *Cval, const S *Adiag,   \
-		const S *u, const S *ustar, const S *src, int srcStatic, double dt, double nu, S *hbya) {                       \
-	ORC_DOM(S); orc::pressureRhs<S>(D, row, col, Cval, Adiag, u, ustar, src, srcStatic, S(dt), S(nu), hbya); }         \
+		const S *u, const S *ustar, const S *src, int srcStatic, double dt, double nu, S *hbya, int scheme) {           \
+	ORC_DOM(S); orc::pressureRhs<S>(D, row, col, Cval, Adiag, u, ustar, src, srcStatic, S(dt), S(nu), hbya, scheme); } \
 extern "C" void orc_divergence##SUF(ORC_DOM_ARGS(S), const S *field, S *div) { ORC_DOM(S); orc::divergence<S>(D, field, div); } \
 extern "C" void orc_correct_velocity##SUF(ORC_DOM_ARGS(S), const S *pr, const S *hbya, const S *Adiag, S *uout) {       \
 	ORC_DOM(S); orc::correctVelocity<S>(D, pr, hbya, Adiag, uout); }                                                     \

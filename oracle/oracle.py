@@ -150,6 +150,8 @@ class OracleDomain:
             pe = ps[env if ps.shape[0] > 1 else 0].numpy().astype(self.S)  # [C] or [C, *face]
             types = list(bd._scalar_types())
             self.scalar_faces.append((pe.ndim == 1, pe.reshape(C, -1), types, bd.isPassiveScalarBoundaryTypeStatic()))
+        # advection scheme (0 CENTRAL, 1 LINEAR_UPWIND)
+        self.scheme = int(domain.getAdvectionScheme()) if hasattr(domain, "getAdvectionScheme") else 0
         self.desc = desc
         self.Tc = np.ascontiguousarray(Tc)
         self.Tf = np.ascontiguousarray(np.concatenate(Tf) if Tf else np.zeros((1, TS), dtype=self.S))
@@ -183,7 +185,7 @@ class OracleDomain:
         val = np.zeros(self.nnz, dtype=self.S)
         A = self.vec()
         self._f("orc_adv_matrix")(*self._dargs(), _p(self._a(u)), ct.c_double(dt), ct.c_double(nu), _p(self.row),
-                                  _p(self.col), _p(val), _p(A))
+                                  _p(self.col), _p(val), _p(A), self.scheme)
         return val, A
 
     def _scalar_face_data(self, c):
@@ -214,21 +216,24 @@ class OracleDomain:
         val = np.zeros(self.nnz, dtype=self.S)
         A = self.vec()
         self._f("orc_scalar_matrix")(*self._dargs(), _p(self._a(u)), ct.c_double(dt), ct.c_double(nu), _p(types),
-                                     _p(self.row), _p(self.col), _p(val), _p(A))
+                                     _p(self.row), _p(self.col), _p(val), _p(A), self.scheme)
         return val, A
 
-    def scalar_rhs(self, phi_c, dt, nu, channel):
-        """advection.cu:545-698 for one channel's field phi_c [n]."""
+    def scalar_rhs(self, phi_c, dt, nu, channel, u=None):
+        """advection.cu:545-698 for one channel's field phi_c [n]; u (the block velocity) gives
+        the LINEAR_UPWIND fluxes."""
         types, vals, offs, stat = self._scalar_face_data(channel)
         rhs = self.vec()
+        uu = self._a(u) if u is not None else self.vec(self.dims)
         self._f("orc_scalar_rhs")(*self._dargs(), _p(self._a(phi_c)), ct.c_double(dt), ct.c_double(nu), _p(types),
-                                  _p(vals), _p(offs), _p(stat), _p(rhs))
+                                  _p(vals), _p(offs), _p(stat), _p(rhs), _p(uu), self.scheme)
         return rhs
 
     def advection_rhs(self, u, src, dt, nu):
         rhs = self.vec(self.dims)
         src_arr, static = self._src(src)
-        self._f("orc_adv_rhs")(*self._dargs(), _p(self._a(u)), _p(src_arr), static, ct.c_double(dt), ct.c_double(nu), _p(rhs))
+        self._f("orc_adv_rhs")(*self._dargs(), _p(self._a(u)), _p(src_arr), static, ct.c_double(dt), ct.c_double(nu), _p(rhs),
+                               self.scheme)
         return rhs
 
     def _src(self, src):
@@ -249,7 +254,7 @@ class OracleDomain:
         src_arr, static = self._src(src)
         self._f("orc_pressure_rhs")(*self._dargs(), _p(self.row), _p(self.col), _p(self._a(Cval)), _p(self._a(A)),
                                     _p(self._a(u)), _p(self._a(ustar)), _p(src_arr), static, ct.c_double(dt),
-                                    ct.c_double(nu), _p(h))
+                                    ct.c_double(nu), _p(h), self.scheme)
         return h
 
     def divergence(self, field):
@@ -368,7 +373,7 @@ class OracleSim:
         its = []
         for c in range(C):
             Cval, _ = od.scalar_matrix(self.u, self.dt, nu_of(c), c) if split else mat
-            rhs = od.scalar_rhs(self.phi_s[c], self.dt, nu_of(c), c)
+            rhs = od.scalar_rhs(self.phi_s[c], self.dt, nu_of(c), c, u=self.u)
             tol = resolve_tol(self.advection_tol, rhs, od.S)
             x = od.vec()
             st, it, _ = od.solve(Cval, rhs, x, tol, self.maxit, bicg=True)

@@ -111,8 +111,8 @@ def SetupAdvectionScalar(domain: Domain, timeStep, nonOrthoFlags=0) -> None:
     _check(domain)
     _no_nonortho(nonOrthoFlags)
     domain.setTimeStep(timeStep)
-    _lib.call("phb_scalar_rhs", ct.byref(domain.desc()), domain._phi_block.data_ptr(), ct.byref(domain._scalar_struct()),
-              domain.scalarRHS.data_ptr(), _S(domain))
+    _lib.call("phb_scalar_rhs", ct.byref(domain.desc()), domain._phi_block.data_ptr(), domain._u_block.data_ptr(),
+              ct.byref(domain._scalar_struct()), domain.scalarRHS.data_ptr(), _S(domain))
 
 
 # --- pressure ---------------------------------------------------------------------------

@@ -46,7 +46,7 @@ class PhbDomain(ct.Structure):
         ("blocks", ct.c_void_p), ("tiles", ct.c_void_p), ("fixed", ct.c_void_p), ("insts", ct.c_void_p),
         ("metrics", ct.c_void_p), ("face_metrics", ct.c_void_p),
         ("fvel", ct.c_void_p), ("fpot", ct.c_void_p), ("fcw", ct.c_void_p), ("fmask", ct.c_void_p),
-        ("dt", ct.c_void_p), ("nu", ct.c_void_p),
+        ("dt", ct.c_void_p), ("nu", ct.c_void_p), ("scheme", ct.c_int32), ("pad", ct.c_int32),
     ]
 
 
@@ -135,7 +135,7 @@ def load() -> ct.CDLL:
         "phb_advection_matrix": [DP, P, P, P, P, P],
         "phb_advection_rhs": [DP, P, P, I, P, P],
         "phb_scalar_matrix": [DP, P, ct.POINTER(PhbScalar), I, P, P, P, P],
-        "phb_scalar_rhs": [DP, P, ct.POINTER(PhbScalar), P, P],
+        "phb_scalar_rhs": [DP, P, P, ct.POINTER(PhbScalar), P, P],
         "phb_pressure_matrix": [DP, P, P, P, P],
         "phb_pressure_rhs": [DP, P, P, P, P, P, I, P, P],
         "phb_divergence": [DP, P, P, P],

@@ -171,6 +171,10 @@ class DomainBatch:
         s.fmask = self._fmask.data_ptr()
         s.dt = self._dt_dev.data_ptr()
         s.nu = self._nu_dev.data_ptr()
+        schemes = {int(m.getAdvectionScheme()) for m in self.members}
+        if len(schemes) != 1:
+            raise NotImplementedError("the instances of a DomainBatch must share the advection scheme")
+        s.scheme = schemes.pop()
         return s
 
     # --- state in and out -------------------------------------------------------------

@@ -36,6 +36,45 @@ __device__ __forceinline__ void faceFluxes(const Dom<S, D> &dom, const Cell &c, 
 	}
 }
 
+// hasFarUpwindCell (piso/device/shared_stencils.cuh:35-43): the downwind neighbour across face
+// f and the far-upwind cell lie inside the block, so the face can be upwinded (LINEAR_UPWIND).
+__device__ __forceinline__ bool farUpwind(const int32_t *B, const int *p, int f, bool outflow) {
+	const int ax = f >> 1;
+	const int sign = (f & 1) ? 1 : -1;
+	const int last = B[B_NX + ax] - 1;
+	const int iD = p[ax] + sign;
+	if (iD < 0 || iD > last) return false;
+	const int iUU = outflow ? p[ax] - sign : p[ax] + 2 * sign;
+	return iUU >= 0 && iUU <= last;
+}
+// r -= the linear-upwind correction F 0.5 psi (phi_D - phi_U), psi = (phi_U - phi_UU) / (phi_D - phi_U),
+// of every upwinded face of cell c for the field value(g), face by face
+// (advection.cu:892-934, :652-688)
+template <typename S, int D, typename Val>
+__device__ __forceinline__ void upwindCorrection(const Cell &c, const S *fl, Val value, S &r) {
+#pragma unroll
+	for (int f = 0; f < 2 * D; ++f) {
+		const int ax = f >> 1;
+		const int sign = (f & 1) ? 1 : -1;
+		const S fout = S(sign) * fl[f];
+		const bool outflow = fout >= S(0);
+		if (!farUpwind(c.B, c.p, f, outflow)) continue;
+		int64_t step = 1;
+		if (ax >= 1) step *= c.B[B_NX];
+		if (ax >= 2) step *= c.B[B_NY];
+		const S phiP = value(c.g);
+		const S phiN = value(c.g + sign * step);
+		const S phiUU = value(outflow ? c.g - sign * step : c.g + 2 * sign * step);
+		const S phiU = outflow ? phiP : phiN;
+		const S phiD = outflow ? phiN : phiP;
+		const S dD = phiD - phiU;
+		const S absDD = dD < S(0) ? -dD : dD;
+		if (absDD < S(1e-20)) continue;
+		const S psi = (phiU - phiUU) / dD;
+		r -= fout * S(0.5) * psi * dD;
+	}
+}
+
 // Passive-scalar data of a launch (phb_scalar), passed by value.
 struct ScalarView {
 	int channels, nuCount;
@@ -97,9 +136,16 @@ __global__ void __launch_bounds__(PHB_TILE) kAdvectionMatrix(Dom<S, D> dom, cons
 		const int dim = f >> 1;
 		const S faceSign = (f & 1) ? S(1) : S(-1);
 		if (!atBound(c.B, f, c.p) || fType(c.B, f) != FT_FIXED) {
-			const S half = S(0.5) * (faceSign * fl[f]);
-			diag += half;
-			rv[f + 1] += half;
+			const S fout = faceSign * fl[f];
+			if (dom.scheme != 0 && farUpwind(c.B, c.p, f, fout >= S(0))) {
+				// first-order upwind implicitly (advection.cu:131-139)
+				if (fout >= S(0)) diag += fout;
+				else rv[f + 1] += fout;
+			} else {
+				const S half = S(0.5) * fout;
+				diag += half;
+				rv[f + 1] += half;
+			}
 			const Nbr n = neighbor<S, D>(dom, c, f);
 			const S alphaN = alphaAt<S, D>(dom, n.mi, n.comp);
 			const S coeff = (alphaP[dim] * nu + alphaN * nu) * S(0.5);
@@ -166,11 +212,14 @@ __global__ void __launch_bounds__(PHB_TILE) kAdvectionRhs(Dom<S, D> dom, const S
 	const S dt = S(dom.dt[inst]);
 	const S nu = S(dom.nu[inst]);
 	const S det = detAt<S, D>(dom, c.mi);
+	S fl[2 * D];
+	if (dom.scheme != 0) faceFluxes<S, D>(dom, c, u, fl);
 #pragma unroll
 	for (int dim = 0; dim < D; ++dim) {
 		const int64_t o = vidx<D>(c.B, c.g, dim);
 		S r = det * u[o] / dt;
 		r += boundarySource<S, D>(dom, c, dim, nu);
+		if (dom.scheme != 0) upwindCorrection<S, D>(c, fl, [&](int64_t g) { return u[vidx<D>(c.B, g, dim)]; }, r);
 		r /= det;
 		r += sourceAt<S, D>(c, src, srcMode, dim);
 		rhs[o] = r;
@@ -182,7 +231,8 @@ __global__ void __launch_bounds__(PHB_TILE) kAdvectionRhs(Dom<S, D> dom, const S
 // det phi / dt plus, at fixed faces, Dirichlet: -phi_b F + 2 nu alpha phi_b (ghost cell);
 // Neumann: -phi_P F + nu |S_f| dphi/dn; all divided by det.
 template <typename S, int D>
-__global__ void __launch_bounds__(PHB_TILE) kScalarRhs(Dom<S, D> dom, const S *__restrict__ phi, ScalarView sv, S *__restrict__ rhs) {
+__global__ void __launch_bounds__(PHB_TILE) kScalarRhs(Dom<S, D> dom, const S *__restrict__ phi, const S *__restrict__ u,
+		ScalarView sv, S *__restrict__ rhs) {
 	__shared__ int32_t sB[PHB_BREC];
 	int l0_, nc_;
 	loadTile<S, D>(dom, sB, l0_, nc_);
@@ -193,6 +243,8 @@ __global__ void __launch_bounds__(PHB_TILE) kScalarRhs(Dom<S, D> dom, const S *_
 	const S dt = S(dom.dt[inst]);
 	const double nuVel = dom.nu[inst];
 	const S det = detAt<S, D>(dom, c.mi);
+	S fl[2 * D];
+	if (dom.scheme != 0) faceFluxes<S, D>(dom, c, u, fl);
 	for (int ch = 0; ch < sv.channels; ++ch) {
 		const int64_t o = sidx(c.B, c.g, ch, sv.channels);
 		const S phiP = phi[o];
@@ -221,6 +273,7 @@ __global__ void __launch_bounds__(PHB_TILE) kScalarRhs(Dom<S, D> dom, const S *_
 				r += value * nu * area;
 			}
 		}
+		if (dom.scheme != 0) upwindCorrection<S, D>(c, fl, [&](int64_t g) { return phi[sidx(c.B, g, ch, sv.channels)]; }, r);
 		rhs[o] = r / det;
 	}
 	}
@@ -336,6 +389,8 @@ __global__ void __launch_bounds__(PHB_TILE) kPressureRhs(Dom<S, D> dom, const S 
 		nb[f] = neighborIndex<S, D>(dom, c, f);
 		cv[f] = C[(f + 1) * N + c.g];
 	}
+	S fl[2 * D];
+	if (dom.scheme != 0) faceFluxes<S, D>(dom, c, u, fl);
 #pragma unroll
 	for (int dim = 0; dim < D; ++dim) {
 		const int64_t o = vidx<D>(c.B, c.g, dim);
@@ -347,6 +402,12 @@ __global__ void __launch_bounds__(PHB_TILE) kPressureRhs(Dom<S, D> dom, const S 
 		S Ssum = boundarySource<S, D>(dom, c, dim, nu);
 		Ssum /= det;
 		Ssum += sourceAt<S, D>(c, src, srcMode, dim);
+		if (dom.scheme != 0) {
+			// HbyA repeats the predictor's deferred correction (pressure.cu:474-515)
+			S corr = 0;
+			upwindCorrection<S, D>(c, fl, [&](int64_t g) { return u[vidx<D>(c.B, g, dim)]; }, corr);
+			Ssum += corr / det;
+		}
 		hbya[o] = rDiag * (velOld - H + Ssum);
 	}
 	}
@@ -635,14 +696,14 @@ extern "C" int phb_scalar_matrix(const phb_domain *dom, const void *u, const phb
 	PHB_DISPATCH(dom, kAdvectionMatrix<S, D, true><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)u, (S *)C, (S *)Adiag, C_lo, sv, channel));
 	return checkLaunch("kAdvectionMatrix<scalar>");
 }
-extern "C" int phb_scalar_rhs(const phb_domain *dom, const void *phi, const phb_scalar *sc, void *rhs, phb_stream stream) {
-	if (!dom || !phi || !sc || !rhs) return setError(PHB_ERR_ARG, "phb_scalar_rhs: null argument");
+extern "C" int phb_scalar_rhs(const phb_domain *dom, const void *phi, const void *u, const phb_scalar *sc, void *rhs, phb_stream stream) {
+	if (!dom || !phi || !sc || !rhs || (dom->scheme != 0 && !u)) return setError(PHB_ERR_ARG, "phb_scalar_rhs: null argument");
 	if (sc->channels < 1 || (sc->nu_count != 0 && sc->nu_count != 1 && sc->nu_count != sc->channels) || (sc->nu_count > 0 && !sc->nu) ||
 			(dom->nfixed > 0 && (!sc->types || !sc->values || !sc->offsets || !sc->statics)))
 		return setError(PHB_ERR_ARG, "phb_scalar_rhs: bad scalar description");
 	if (dom->ntiles == 0) return PHB_OK;
 	const ScalarView sv = scalarView(sc);
-	PHB_DISPATCH(dom, kScalarRhs<S, D><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)phi, sv, (S *)rhs));
+	PHB_DISPATCH(dom, kScalarRhs<S, D><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)phi, (const S *)u, sv, (S *)rhs));
 	return checkLaunch("kScalarRhs");
 }
 extern "C" int phb_advection_rhs(const phb_domain *dom, const void *u, const void *src, int src_mode, void *rhs, phb_stream stream) {

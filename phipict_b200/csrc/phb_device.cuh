@@ -46,6 +46,7 @@ struct Dom {
 	const double *dt, *nu;
 	int64_t ms, fms, ncells;
 	int nblocks, ninst, ntiles;
+	int scheme = 0; // AdvectionScheme: 0 CENTRAL, 1 LINEAR_UPWIND
 	// set by a launcher whose vector and stencil operands all start on 16-byte boundaries and
 	// whose ncells is a multiple of 4: 4-cell groups at aligned indices may use vector loads
 	int vec4 = 0;
@@ -56,7 +57,7 @@ struct Dom {
 		  met((const S *)d.metrics), fmet((const S *)d.face_metrics), fvel((const S *)d.fvel),
 		  fpot((const S *)d.fpot), fcw((const S *)d.fcw), fmask(d.fmask), dt(d.dt), nu(d.nu),
 		  ms(d.metric_stride), fms(d.face_metric_stride), ncells(d.ncells), nblocks(d.nblocks),
-		  ninst(d.ninst), ntiles(d.ntiles) {}
+		  ninst(d.ninst), ntiles(d.ntiles), scheme(d.scheme) {}
 
 	__device__ __forceinline__ const int32_t *blk(int b) const { return blocks + b * PHB_BREC; }
 	__device__ __forceinline__ const int32_t *fix(int k) const { return fixed + k * PHB_FREC; }

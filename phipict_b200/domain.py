@@ -836,9 +836,13 @@ class Domain:
             self._upload_viscosity()
 
     def setAdvectionScheme(self, scheme: AdvectionScheme) -> None:
-        if AdvectionScheme(scheme) != AdvectionScheme.CENTRAL:
-            raise NotImplementedError("phipict_b200 implements the CENTRAL advection scheme")
+        """CENTRAL (implicit central fluxes) or LINEAR_UPWIND (first-order upwind in the matrix
+        with the linear-upwind part as a lagged explicit correction, where the far-upwind cell
+        lies in the same block; domain_structs_gpu.h:65-68)."""
         self._advection_scheme = AdvectionScheme(scheme)
+        if getattr(self, "_prepared", False):
+            self._desc.scheme = int(self._advection_scheme)
+            self._version += 1
 
     def getAdvectionScheme(self) -> AdvectionScheme:
         return self._advection_scheme
@@ -1310,6 +1314,7 @@ class Domain:
         s.fmask = self._fmask.data_ptr()
         s.dt = self._dt_dev.data_ptr()
         s.nu = self._nu_dev.data_ptr()
+        s.scheme = int(self._advection_scheme)
         return s
 
     def desc(self) -> _lib.PhbDomain:
