@@ -974,12 +974,16 @@ __device__ __forceinline__ void blockSumTo(double (&v)[NV], double *dst) {
 // Visit this CTA's tiles with the block record staged in sB.
 template <int D, typename F>
 __device__ __forceinline__ void forMyTiles(const Dom<double, D> &dom, int32_t *sB, F f) {
+	int staged = -1; // the block whose record sB holds (uniform over the CTA)
 	for (int tile = blockIdx.x; tile < dom.ntiles; tile += gridDim.x) {
-		__syncthreads();
 		const int b = __ldg(dom.tiles + 2 * tile);
 		const int l0 = __ldg(dom.tiles + 2 * tile + 1);
-		if (threadIdx.x < PHB_BREC) sB[threadIdx.x] = __ldg(dom.blocks + b * PHB_BREC + threadIdx.x);
-		__syncthreads();
+		if (b != staged) {
+			__syncthreads();
+			if (threadIdx.x < PHB_BREC) sB[threadIdx.x] = __ldg(dom.blocks + b * PHB_BREC + threadIdx.x);
+			__syncthreads();
+			staged = b;
+		}
 		const int nc = sB[B_NX] * sB[B_NY] * (D > 2 ? sB[B_NZ] : 1);
 		f(tile, l0, nc);
 	}
