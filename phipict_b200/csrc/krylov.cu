@@ -48,10 +48,9 @@ struct Control {
 	int allDone;
 	int loops;
 	int maxLoops;
-	unsigned int barCount; // grid barrier of the persistent solvers: arrivals,
-	unsigned int barGen;   // generation,
+	unsigned int barCount; // grid barrier of the persistent solvers: arrival counter
 	int barErr;            // set when a barrier wait ran out (the kernel then returns)
-	int pad;
+	int pad[2];
 };
 static_assert(sizeof(Control) == 32, "Control layout");
 
@@ -547,7 +546,7 @@ __global__ void kInit(SysState *st, int nsys, phb_tolerance tol, int fromInner, 
 	}
 	if (threadIdx.x == 0) {
 		ctrl->counter = 0; ctrl->allDone = 0; ctrl->loops = 0; ctrl->maxLoops = maxLoops;
-		ctrl->barCount = 0; ctrl->barGen = 0; ctrl->barErr = 0;
+		ctrl->barCount = 0; ctrl->barErr = 0;
 	}
 }
 
@@ -921,29 +920,42 @@ __global__ void kInitOuter(SysState *st, int nsys, phb_tolerance tol, Control *c
 // scalars in shared memory and reduces the per-tile partials itself, in the same fixed order
 // as every other CTA, so all CTAs take the same decisions without broadcasting them.
 constexpr unsigned int BARRIER_SPIN_LIMIT = 1u << 24;
+constexpr unsigned int BARRIER_ERR_POLL = 1023; // spins between reads of Control::barErr
 
-__device__ __forceinline__ bool gridBarrier(Control *ctrl, unsigned int &gen) {
+// Sense-reversing arrival counter: CTA 0 adds 2^31 - (gridDim.x - 1), every other CTA adds 1,
+// so the counter's top bit flips exactly when the last CTA of a generation arrives and the
+// low bits return to where they were (no reset, no second atomic). The arrival is a release
+// and the poll an acquire at GPU scope; with the CTA barriers on both sides that orders every
+// thread's writes before the barrier against every thread's reads after it. A CTA that has
+// seen the flip does not read barErr: a CTA that gave up at this barrier had arrived at it
+// (arrival comes before the wait), so the flip proves the phase complete, and the next
+// barrier, where that CTA never arrives, ends everyone else's wait through barErr.
+__device__ __forceinline__ unsigned int barrierArrive(unsigned int *count, unsigned int add) {
+	unsigned int old;
+	asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(count), "r"(add) : "memory");
+	return old;
+}
+
+__device__ __forceinline__ unsigned int barrierPoll(const unsigned int *count) {
+	unsigned int v;
+	asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
+	return v;
+}
+
+__device__ __forceinline__ bool gridBarrier(Control *ctrl) {
 	__shared__ int sOk;
 	__syncthreads();
 	if (threadIdx.x == 0) {
-		int ok = *(volatile int *)&ctrl->barErr == 0;
-		if (ok) {
-			__threadfence();
-			const unsigned int g = gen;
-			if (atomicAdd(&ctrl->barCount, 1u) == gridDim.x - 1) {
-				atomicExch(&ctrl->barCount, 0u);
-				__threadfence();
-				atomicExch(&ctrl->barGen, g + 1);
-			} else {
-				unsigned int spins = 0;
-				while (*(volatile unsigned int *)&ctrl->barGen == g) {
-					if (++spins > BARRIER_SPIN_LIMIT || *(volatile int *)&ctrl->barErr) { atomicExch(&ctrl->barErr, 1); break; }
-					__nanosleep(32);
-				}
+		const unsigned int add = blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1) : 1u;
+		const unsigned int old = barrierArrive(&ctrl->barCount, add);
+		int ok = 1;
+		for (unsigned int spins = 1; ((barrierPoll(&ctrl->barCount) ^ old) & 0x80000000u) == 0; ++spins) {
+			if ((spins & BARRIER_ERR_POLL) == 0 && (spins > BARRIER_SPIN_LIMIT || *(volatile int *)&ctrl->barErr)) {
+				atomicExch(&ctrl->barErr, 1);
+				ok = 0;
+				break;
 			}
-			__threadfence();
-			gen = g + 1;
-			ok = *(volatile int *)&ctrl->barErr == 0;
+			__nanosleep(32);
 		}
 		sOk = ok;
 	}
@@ -1081,7 +1093,6 @@ __device__ __forceinline__ void cgPersistentBody(const Dom<double, D> &dom, cons
 	const int nsys = dom.ninst * K;
 	for (int s = threadIdx.x; s < nsys; s += blockDim.x) sst[s] = st[s];
 	__syncthreads();
-	unsigned int gen = 0;
 	const int64_t N = dom.ncells;
 	// consecutive phases write alternate halves of the partials, so that a CTA that has left
 	// a barrier cannot overwrite partials another CTA is still reducing
@@ -1102,7 +1113,7 @@ __device__ __forceinline__ void cgPersistentBody(const Dom<double, D> &dom, cons
 				[&](int, int64_t o, const Quad &q, const T (&rv)[4]) { st4(r + o, q.n, q.al, rv); });
 		blockSumTo<2 * K>(acc, pp + (size_t)tile * 2 * K);
 	});
-	if (!gridBarrier(ctrl, gen)) return;
+	if (!gridBarrier(ctrl)) return;
 	int running = reduceStates<K, 2, 1>(dom.insts, dom.ninst, pp, sst, [&](SysState &s, int in, const double *red, double bb) {
 		residualDecision<K, false, STOPSTART>(nullptr, s, normScale(dom.insts, in), red, bb, tol);
 	});
@@ -1120,23 +1131,23 @@ __device__ __forceinline__ void cgPersistentBody(const Dom<double, D> &dom, cons
 				} else {
 					for (int sub = blockIdx.x; sub < mg.lv[l + 1].ntiles * Restrict<D>::PER_TILE; sub += gridDim.x) amgRestrictSub<D>(mg, l, sub, sB);
 				}
-				if (!gridBarrier(ctrl, gen)) return;
+				if (!gridBarrier(ctrl)) return;
 			}
 			amgCoarseRows<D>(mg, int(blockIdx.x * NWARPS + (threadIdx.x >> 5)), int(gridDim.x * NWARPS));
-			if (!gridBarrier(ctrl, gen)) return;
+			if (!gridBarrier(ctrl)) return;
 			for (int l = L - 2; l >= 1; --l) {
 				for (int sub = blockIdx.x; sub < mg.lv[l].ntiles * AMG_SUBTILES; sub += gridDim.x) {
 					const int q = sub % AMG_SUBTILES;
 					amgProlongTile<D>(mg, l, sub / AMG_SUBTILES, sB, mg.x[l], q, q + 1);
 				}
-				if (!gridBarrier(ctrl, gen)) return;
+				if (!gridBarrier(ctrl)) return;
 			}
 			pp = partial + (size_t)(ph++ & 1) * half;
 			for (int tile = blockIdx.x; tile < dom.ntiles; tile += gridDim.x) {
 				double acc[1] = {quads ? amgProlongQuad<D>(mg, 0, tile, sB, mg.x[0]) : amgProlongTile<D>(mg, 0, tile, sB, mg.x[0])};
 				blockSumTo<1>(acc, pp + tile);
 			}
-			if (!gridBarrier(ctrl, gen)) return;
+			if (!gridBarrier(ctrl)) return;
 			reduceStates<1, 1>(dom.insts, dom.ninst, pp, sst, [&](SysState &s, int, const double *red, double) { pcgRho(s, red[0]); });
 		}
 		// p' = z + beta p (z = r without preconditioner), q = A p', (p', q)
@@ -1158,7 +1169,7 @@ __device__ __forceinline__ void cgPersistentBody(const Dom<double, D> &dom, cons
 			tileCgDirection<T, D, K>(dom, sB, l0, nc, A, dsrc, pIn, pOut, q, act, rs, beta, acc);
 			blockSumTo<K>(acc, pp + (size_t)tile * K);
 		});
-		if (!gridBarrier(ctrl, gen)) return;
+		if (!gridBarrier(ctrl)) return;
 		reduceStates<K, 1>(dom.insts, dom.ninst, pp, sst, [&](SysState &s, int, const double *red, double) {
 			const double alpha = s.rho / red[0];
 			s.restart = 0;
@@ -1174,7 +1185,7 @@ __device__ __forceinline__ void cgPersistentBody(const Dom<double, D> &dom, cons
 			tileCgUpdate<T, D, K>(dom, sB, l0, nc, r, pOut, q, x, xbest, sst, acc);
 			blockSumTo<K>(acc, pp + (size_t)tile * K);
 		});
-		if (!gridBarrier(ctrl, gen)) return;
+		if (!gridBarrier(ctrl)) return;
 		running = reduceStates<K, 1>(dom.insts, dom.ninst, pp, sst, [&](SysState &s, int in, const double *red, double) {
 			const double crit = sqrt(red[0]) * normScale(dom.insts, in);
 			++s.it;
@@ -1245,7 +1256,6 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgPersistent(Dom<double, D> dom, 
 	const int nsys = dom.ninst * K;
 	for (int s = threadIdx.x; s < nsys; s += blockDim.x) sst[s] = st[s];
 	__syncthreads();
-	unsigned int gen = 0;
 	const int64_t N = dom.ncells;
 	// consecutive phases write alternate halves of the partials, so that a CTA that has left
 	// a barrier cannot overwrite partials another CTA is still reducing
@@ -1267,7 +1277,7 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgPersistent(Dom<double, D> dom, 
 		});
 		blockSumTo<2 * K>(acc, pp + (size_t)tile * 2 * K);
 	});
-	if (!gridBarrier(ctrl, gen)) return;
+	if (!gridBarrier(ctrl)) return;
 	int running = reduceStates<K, 2, 1>(dom.insts, dom.ninst, pp, sst, [&](SysState &s, int in, const double *red, double bb) {
 		residualDecision<K, true, true>(nullptr, s, normScale(dom.insts, in), red, bb, tol);
 	});
@@ -1293,7 +1303,7 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgPersistent(Dom<double, D> dom, 
 			tileBicgV<T, D, K>(dom, sB, l0, nc, A, r, pIn, vIn, pOut, vOut, r0, act, rs, beta, omega, acc);
 			blockSumTo<K>(acc, pp + (size_t)tile * K);
 		});
-		if (!gridBarrier(ctrl, gen)) return;
+		if (!gridBarrier(ctrl)) return;
 		reduceStates<K, 1>(dom.insts, dom.ninst, pp, sst, [&](SysState &s, int, const double *red, double) {
 			const double alpha = s.rho / red[0];
 			s.restart = 0;
@@ -1318,7 +1328,7 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgPersistent(Dom<double, D> dom, 
 			tileBicgT<T, D, K>(dom, sB, l0, nc, A, r, vOut, t, act, alpha, acc);
 			blockSumTo<3 * K>(acc, pp + (size_t)tile * 3 * K);
 		});
-		if (!gridBarrier(ctrl, gen)) return;
+		if (!gridBarrier(ctrl)) return;
 		reduceStates<K, 3>(dom.insts, dom.ninst, pp, sst, [&](SysState &s, int in, const double *red, double) {
 			const double critS = sqrt(red[2]) * normScale(dom.insts, in);
 			s.halfCrit = critS;
@@ -1339,7 +1349,7 @@ __global__ void __launch_bounds__(PHB_TILE) kBicgPersistent(Dom<double, D> dom, 
 			tileBicgUpdate<T, D, K>(dom, sB, l0, nc, r, r0, pOut, vOut, t, x, sst, acc);
 			blockSumTo<2 * K>(acc, pp + (size_t)tile * 2 * K);
 		});
-		if (!gridBarrier(ctrl, gen)) return;
+		if (!gridBarrier(ctrl)) return;
 		running = reduceStates<K, 2>(dom.insts, dom.ninst, pp, sst, [&](SysState &s, int in, const double *red, double) {
 			if (s.halfDone) { s.done = CONVERGED; s.crit = s.halfCrit; s.usedIt = s.it; return; }
 			const double crit = sqrt(red[1]) * normScale(dom.insts, in);
