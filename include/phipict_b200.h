@@ -68,7 +68,8 @@ typedef struct phb_domain {
 	const double *dt;       /* [ninst] time step */
 	const double *nu;       /* [ninst] viscosity */
 	int32_t scheme;         /* advection scheme (AdvectionScheme): 0 CENTRAL, 1 LINEAR_UPWIND */
-	int32_t pad;
+	int32_t nonortho;       /* non-orthogonal flag bits (PHB_NON_ORTHO_*) of the matrix and
+	                           right-hand-side builders; 0 assembles the orthogonal terms only */
 } phb_domain;
 
 const char *phb_last_error(void);
@@ -145,6 +146,33 @@ int phb_scalar_matrix(const phb_domain *dom, const void *u, const phb_scalar *sc
  * gives the face fluxes of the LINEAR_UPWIND correction (may be NULL with CENTRAL). */
 int phb_scalar_rhs(const phb_domain *dom, const void *phi, const void *u, const phb_scalar *sc, void *rhs,
                    phb_stream stream);
+
+/* --- non-orthogonal grids ---------------------------------------------------------- */
+/* Flag bits of phb_domain.nonortho, the nonOrthoFlags / nonOrthoMode argument of the
+ * reference's Setup* calls (piso/non_ortho_flags.h:23-27). With CENTER_MATRIX and
+ * DIRECT_MATRIX, phb_advection_matrix, phb_scalar_matrix and phb_pressure_matrix add the
+ * cross terms det Minv[n] . Minv[t] of curvilinear grids to the diagonal and the face
+ * neighbours (advection.cu:176-240, pressure.cu:103-156; the interpolation of
+ * nonortho_laplace.cuh:52-129). DIAGONAL_MATRIX is accepted and, as in the reference, adds
+ * nothing. phb_epot_matrix ignores the flags (the potential's own flags default to 0). */
+#define PHB_NON_ORTHO_DIRECT_MATRIX 1
+#define PHB_NON_ORTHO_DIRECT_RHS 2
+#define PHB_NON_ORTHO_DIAGONAL_MATRIX 4
+#define PHB_NON_ORTHO_DIAGONAL_RHS 8
+#define PHB_NON_ORTHO_CENTER_MATRIX 16
+enum { PHB_NONORTHO_VELOCITY = 0, PHB_NONORTHO_SCALAR = 1, PHB_NONORTHO_PRESSURE = 2 };
+/* The explicit cross terms of a result field with DIRECT_RHS / DIAGONAL_RHS
+ * (nonortho_rhs.cuh:27-180, corner values of block_data.cuh:501-620), applied in place to a
+ * right-hand side built by the call named:
+ *   PHB_NONORTHO_VELOCITY: field = velocity result [inst][dims][cells]; rhs (phb_advection_rhs)
+ *     -= S / det, S weighted with the viscosity (advection.cu:936-937);
+ *   PHB_NONORTHO_SCALAR: field = scalar result [inst][channels][cells]; rhs (phb_scalar_rhs)
+ *     -= S nu_c / det per channel (advection.cu:684-689); sc as for phb_scalar_rhs;
+ *   PHB_NONORTHO_PRESSURE: field = pressure result [ncells]; rhs (the divergence of
+ *     phb_divergence) += S weighted with 1/Adiag (pressure.cu:839-860).
+ * Does nothing when dom->nonortho has neither right-hand-side bit. */
+int phb_nonortho_rhs(const phb_domain *dom, int kind, const void *field, const phb_scalar *sc, const void *Adiag,
+                     void *rhs, phb_stream stream);
 
 /* --- vectors ------------------------------------------------------------------------ */
 /* Per-instance reductions use a caller-owned scratch of phb_scratch_doubles() doubles whose

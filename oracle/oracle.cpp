@@ -1,4 +1,4 @@
-// CPU oracle for the phiPICT PISO/MHD step (orthogonal grids, CENTRAL advection).
+// CPU oracle for the phiPICT PISO/MHD step.
 //
 // TEST INFRASTRUCTURE ONLY. This file restates the reference algorithm on the CPU so
 // that the CUDA product can be checked against it; only tests/, the smoke check and
@@ -295,14 +295,298 @@ static void upwindCorrection(const Dom<S> &D, int b, const int *p, const S *fl, 
 	}
 }
 
-// advection.cu:27-305 PISO_build_matrix (CENTRAL, orthogonal, domain viscosity). With
+// ---------------------------------------------------------------------------------------
+// Non-orthogonal Laplace terms (piso/device/nonortho_laplace.cuh, nonortho_rhs.cuh,
+// block_data.cuh:477-620). Flag bits as piso/non_ortho_flags.h:23-27.
+enum { NO_DIRECT_MATRIX = 1, NO_DIRECT_RHS = 2, NO_DIAGONAL_MATRIX = 4, NO_DIAGONAL_RHS = 8, NO_CENTER_MATRIX = 16 };
+// the field a corner walk or neighbour read looks at (GridDataType of block_data.cuh)
+enum { NF_MARK = 0, NF_PRESSURE = 1, NF_VELOCITY = 2, NF_SCALAR = 3 };
+
+template <typename S>
+struct NField {
+	int kind = NF_MARK;
+	int w = 0;                 // velocity component (scalar channel: the arrays below are the channel's)
+	const S *cells = nullptr;  // [n] cell values of component w
+	const int8_t *sTypes = nullptr;
+	const S *sValues = nullptr;
+	const int64_t *sOffsets = nullptr;
+	const int8_t *sStatic = nullptr;
+};
+template <typename S>
+static S nfCell(const Dom<S> &D, const NField<S> &F, int b, const int *p) {
+	return F.cells ? F.cells[D.glob(b, p)] : S(0);
+}
+// getFixedBoundaryType (block_data.cuh:111-135): 1 for a Neumann face
+template <typename S>
+static int nfNeumann(const Dom<S> &D, const NField<S> &F, int b, int f) {
+	if (F.kind == NF_VELOCITY) return D.velType(b, f) != 0;
+	if (F.kind == NF_SCALAR) return F.sTypes[D.fixedId(b, f)] != 0;
+	return 0;
+}
+// getFixedBoundaryData (block_data.cuh:137-205); the fixed faces carry no pressure data
+template <typename S>
+static S nfFixed(const Dom<S> &D, const NField<S> &F, int b, int f, const int *p) {
+	if (F.kind == NF_MARK) return S(1);
+	if (F.kind == NF_VELOCITY) return D.fixedVel(b, f, p, F.w);
+	if (F.kind == NF_SCALAR) {
+		if (!F.sValues) return S(0); // a matrix walk reads only the face types
+		const int fid = D.fixedId(b, f);
+		return F.sStatic[fid] ? F.sValues[F.sOffsets[fid]] : F.sValues[F.sOffsets[fid] + D.faceCell(b, f, p)];
+	}
+	return S(0);
+}
+// computeConnectedDir (topology.cuh:226-236): direction dir of block b seen from the block
+// across its connected face f
+template <typename S>
+static int connDir(const Dom<S> &D, int b, int f, int dir) {
+	const int32_t *axes = D.face(b, f) + 2;
+	return axes[posMod((dir >> 1) - (f >> 1), D.dims)] ^ (dir & 1);
+}
+// one step of a walk from (b, p) across direction dir through periodic or connected faces;
+// false at a fixed face. Connected faces land one cell inside the other block
+// (computeConnectedPos with borderOffset 1, as block_data.cuh:299,397,571 call it).
+template <typename S>
+static bool stepAcross(const Dom<S> &D, int &b, int *p, int dir) {
+	const int ax = dir >> 1;
+	if (!D.atBound(b, dir, p)) { p[ax] += (dir & 1) ? 1 : -1; return true; }
+	const int t = D.ftype(b, dir);
+	if (t == FT_FIXED) return false;
+	if (t == FT_PERIODIC) { p[ax] = (dir & 1) ? 0 : D.sz(b, ax) - 1; return true; }
+	int ob, op[3];
+	connectedPos(D, b, dir, p, 1, ob, op);
+	b = ob; p[0] = op[0]; p[1] = op[1]; p[2] = op[2];
+	return true;
+}
+// getBlockDataNeighbor (block_data.cuh:276-318)
+template <typename S>
+static S neighborData(const Dom<S> &D, const NField<S> &F, int b, const int *pos, int dir) {
+	int p[3] = {pos[0], pos[1], pos[2]};
+	if (!stepAcross(D, b, p, dir)) return nfFixed(D, F, b, dir, p);
+	return nfCell(D, F, b, p);
+}
+// getBlockDataNeighborDiagonal (block_data.cuh:372-420): dir1 first unless the block's dir1
+// face is fixed; the second step keeps its direction index in the block reached
+template <typename S>
+static S diagonalData(const Dom<S> &D, const NField<S> &F, int b, const int *pos, int dir1, int dir2) {
+	const bool first1 = !D.isEmpty(b, dir1);
+	const int dirs[2] = {first1 ? dir1 : dir2, first1 ? dir2 : dir1};
+	int p[3] = {pos[0], pos[1], pos[2]};
+	for (int i = 0; i < 2; ++i)
+		if (!stepAcross(D, b, p, dirs[i])) return nfFixed(D, F, b, dirs[i], p);
+	return nfCell(D, F, b, p);
+}
+
+template <typename S>
+struct CornerValue {
+	S data;
+	int numCells; // 0: the value came from a fixed face
+	int neumann;  // the fixed face's type when numCells is 0
+};
+// getCornerValue (block_data.cuh:501-620) with includeDepth0 false and maxDepth 2: walk around
+// the corner between directions dir1 and dir2 both ways until the walks meet or a fixed face
+// ends one of them.
+template <typename S>
+static CornerValue<S> cornerWalk(const Dom<S> &D, const NField<S> &F, int b0, const int *pos, int dir1, int dir2, bool depth1) {
+	struct Walk { int d1, d2, b, p[3]; };
+	Walk w[2] = {{dir1, dir2, b0, {pos[0], pos[1], pos[2]}}, {dir2, dir1, b0, {pos[0], pos[1], pos[2]}}};
+	S data = 0;
+	int num = 1;
+	for (int depth = 1; depth <= 2; ++depth) {
+		for (int d = 0; d < 2; ++d) {
+			Walk &c = w[d];
+			const int ax = c.d1 >> 1;
+			if (D.atBound(c.b, c.d1, c.p)) {
+				const int t = D.ftype(c.b, c.d1);
+				if (t == FT_FIXED) {
+					const int neu = nfNeumann(D, F, c.b, c.d1);
+					const S v0 = nfFixed(D, F, c.b, c.d1, c.p);
+					if (D.atBound(c.b, c.d2, c.p)) return {v0, 0, neu};
+					int q[3] = {c.p[0], c.p[1], c.p[2]};
+					q[c.d2 >> 1] += (c.d2 & 1) ? 1 : -1;
+					return {(v0 + nfFixed(D, F, c.b, c.d1, q)) * S(0.5), 0, neu};
+				}
+				if (t == FT_CONNECTED) {
+					const int nd1 = connDir(D, c.b, c.d1, c.d2);
+					const int nd2 = connDir(D, c.b, c.d1, c.d1) ^ 1;
+					int ob, op[3];
+					connectedPos(D, c.b, c.d1, c.p, 1, ob, op);
+					c.b = ob; c.p[0] = op[0]; c.p[1] = op[1]; c.p[2] = op[2];
+					c.d1 = nd1; c.d2 = nd2;
+				} else { // periodic
+					c.p[ax] = (c.d1 & 1) ? 0 : D.sz(c.b, ax) - 1;
+					const int od1 = c.d1;
+					c.d1 = c.d2; c.d2 = od1 ^ 1;
+				}
+			} else {
+				c.p[ax] += (c.d1 & 1) ? 1 : -1;
+				const int od1 = c.d1;
+				c.d1 = c.d2; c.d2 = od1 ^ 1;
+			}
+			const Walk &o = w[d ^ 1];
+			if (c.b == o.b && c.p[0] == o.p[0] && c.p[1] == o.p[1] && c.p[2] == o.p[2])
+				return {data / S(num), num, 0};
+			if (depth > 1 || depth1) data += nfCell(D, F, c.b, c.p);
+			++num;
+		}
+	}
+	return {data / S(num), num, 0};
+}
+
+// det Minv[a] . Minv[c] of transform t (discretization.cuh:419-446, 447-469)
+template <typename S>
+static inline S lapCross(const Dom<S> &D, const S *t, int a, int c) {
+	return D.det(t) * dotv(D.Minv(t, a), D.Minv(t, c), D.dims);
+}
+
+// interpolateNonOrthoLaplaceComponents (nonortho_laplace.cuh:52-129) without face transforms:
+// out[f][i-1] is the cross coefficient of face f with the tangential axis (f/2 + i) % d,
+// interpolated between the cell and its neighbour with weights ra (1/A, viscosity or 1).
+// A face gets one when its cell is not at either end of the face's axis or the block's face
+// in that direction is not fixed, as the reference tests it.
+template <typename S, typename RA>
+static void nonOrthoInterp(const Dom<S> &D, int b, const int *p, RA ra, S out[6][2]) {
+	const S *tP = D.T(b, p);
+	const S raP = ra(b, p);
+	for (int f = 0; f < 2 * D.dims; ++f) {
+		const int ax = f >> 1;
+		for (int i = 0; i < 2; ++i) out[f][i] = 0;
+		if (!((0 < p[ax] && p[ax] < D.sz(b, ax) - 1) || !D.isEmpty(b, f))) continue;
+		int nb = b, np[3] = {p[0], p[1], p[2]};
+		if (D.atBound(b, f, p) && D.ftype(b, f) == FT_CONNECTED) {
+			connectedPos(D, b, f, p, 0, nb, np);
+		} else if (D.atBound(b, f, p) && D.ftype(b, f) == FT_PERIODIC) {
+			np[ax] = (f & 1) ? 0 : D.sz(b, ax) - 1;
+		} else {
+			np[ax] += (f & 1) ? 1 : -1;
+		}
+		const S *tN = D.T(nb, np);
+		const S raN = ra(nb, np);
+		for (int i = 1; i < D.dims; ++i) {
+			const int o = (ax + i) % D.dims;
+			out[f][i - 1] = (lapCross(D, tP, ax, o) * raP + lapCross(D, tN, o, ax) * raN) * S(0.5);
+		}
+	}
+}
+
+// The non-orthogonal matrix terms of free face f of one row (pressure.cu:103-156 for the
+// pressure matrix, advection.cu:176-240 for the advection matrix), added right after the
+// face's orthogonal terms as the reference does: for each tangential axis, the corner values
+// either side are interpolations of numCells cells (their centre and direct-neighbour parts go
+// to the row when CENTER_MATRIX / DIRECT_MATRIX are set) or, at a fixed gradient face, a
+// one-sided difference from the other side. sgn = +1 adds them as the pressure matrix does,
+// -1 as the advection matrix does; a[i-1] is the face's cross coefficient with tangential
+// axis (f/2 + i) % d.
+template <typename S>
+static void nonOrthoMatrixFace(const Dom<S> &D, const NField<S> &F, int b, const int *p, int f, int flags, int sgn,
+		bool pressure, const S *a, S *rv) {
+	const bool center = flags & NO_CENTER_MATRIX, direct = flags & NO_DIRECT_MATRIX;
+	if (D.dims < 2 || !(center || direct)) return;
+	const int faceSign = (f & 1) ? 1 : -1;
+	for (int i = 1; i < D.dims; ++i) {
+		const int tAxis = ((f >> 1) + i) % D.dims;
+		if (a[i - 1] == S(0)) continue;
+		for (int tUp = 0; tUp < 2; ++tUp) {
+			const int tFace = 2 * tAxis + tUp;
+			const int tSign = tUp ? 1 : -1;
+			const CornerValue<S> cv = cornerWalk(D, F, b, p, f, tFace, false);
+			if (cv.numCells < 1) {
+				if (!(pressure || cv.neumann)) continue; // a prescribed value goes to the right-hand side
+				const S coef = S(faceSign * tSign) * a[i - 1] * S(0.25);
+				if (center) rv[0] += S(sgn * 3) * coef;
+				if (direct) { rv[f + 1] += S(sgn * 3) * coef; rv[(tFace ^ 1) + 1] -= S(sgn) * coef; }
+			} else {
+				const S coef = S(faceSign * tSign) * a[i - 1] * S(1.0 / double(cv.numCells));
+				if (center) rv[0] += S(sgn) * coef;
+				if (direct) { rv[f + 1] += S(sgn) * coef; rv[tFace + 1] += S(sgn) * coef; }
+			}
+		}
+	}
+}
+
+// getNonOrthoLaplaceRHS_v2 (nonortho_rhs.cuh:27-180) without face transforms: the explicit
+// part of the cross terms at cell (b, p) for field F; ra(b, p) the weight (1/A for the
+// pressure, the viscosity for the velocity, 1 for the scalar), raFixed the weight at a fixed
+// face (viscosity or 1).
+template <typename S, typename RA>
+static S nonOrthoRhs(const Dom<S> &D, const NField<S> &F, int b, const int *p, int flags, RA ra, S raFixed) {
+	if (!(flags & (NO_DIRECT_RHS | NO_DIAGONAL_RHS)) || D.dims < 2) return S(0);
+	const bool direct = flags & NO_DIRECT_RHS, diagonal = flags & NO_DIAGONAL_RHS;
+	const S *tP = D.T(b, p);
+	const S raP = ra(b, p);
+	S Ssum = 0;
+	for (int f = 0; f < 2 * D.dims; ++f) {
+		const int ax = f >> 1;
+		const int faceSign = (f & 1) ? 1 : -1;
+		if (D.atBound(b, f, p) && D.isEmpty(b, f)) {
+			if (F.kind == NF_PRESSURE || nfNeumann(D, F, b, f)) continue;
+			const S *tf = D.faceT(b, f, p);
+			for (int i = 1; i < D.dims; ++i) {
+				const int tAxis = (ax + i) % D.dims;
+				const bool tLow = p[tAxis] == 0, tHigh = p[tAxis] == D.sz(b, tAxis) - 1;
+				int lo[3] = {p[0], p[1], p[2]}, hi[3] = {p[0], p[1], p[2]};
+				if (!tLow) lo[tAxis] -= 1;
+				if (!tHigh) hi[tAxis] += 1;
+				const S factor = (tLow || tHigh) ? S(1) : S(0.5);
+				const S tGrad = factor * (nfFixed(D, F, b, f, hi) - nfFixed(D, F, b, f, lo));
+				Ssum -= S(faceSign) * lapCross(D, tf, tAxis, ax) * tGrad * raFixed;
+			}
+			continue;
+		}
+		// resolveNeighborCell (topology.cuh:343-383): the direct neighbour with the axis mapping
+		// of a connection (getLaplaceCoefficientsSingleAxisNeighbor, discretization.cuh:565-600)
+		int nb = b, np[3] = {p[0], p[1], p[2]};
+		int map[3] = {0, 1, 2};
+		if (D.atBound(b, f, p) && D.ftype(b, f) == FT_CONNECTED) {
+			connectedPos(D, b, f, p, 0, nb, np);
+			for (int k = 0; k < D.dims; ++k) map[k] = connDir(D, b, f, 2 * k) >> 1;
+		} else if (D.atBound(b, f, p)) {
+			np[ax] = (f & 1) ? 0 : D.sz(b, ax) - 1;
+		} else {
+			np[ax] += (f & 1) ? 1 : -1;
+		}
+		const S *tN = D.T(nb, np);
+		const S raN = ra(nb, np);
+		for (int i = 1; i < D.dims; ++i) {
+			const int tAxis = (ax + i) % D.dims;
+			const S faceAlpha = (lapCross(D, tP, ax, tAxis) * raP + lapCross(D, tN, map[tAxis], map[ax]) * raN) * S(0.5);
+			S tGrad = 0;
+			for (int tUp = 0; tUp < 2; ++tUp) {
+				const int tFace = 2 * tAxis + tUp;
+				const int tSign = tUp ? 1 : -1;
+				const CornerValue<S> cv = cornerWalk(D, F, b, p, f, tFace, direct);
+				if (cv.numCells == 0 && (cv.neumann || F.kind == NF_PRESSURE)) {
+					const int tOther = tFace ^ 1;
+					if (direct) {
+						tGrad += S(tSign) * neighborData(D, F, b, p, f) * S(0.75);
+						tGrad += S(-tSign) * neighborData(D, F, b, p, tOther) * S(0.25);
+					}
+					if (diagonal) tGrad += S(-tSign) * diagonalData(D, F, b, p, f, tOther) * S(0.25);
+				} else {
+					tGrad += S(tSign) * cv.data;
+				}
+			}
+			Ssum -= S(faceSign) * faceAlpha * tGrad;
+		}
+	}
+	return Ssum;
+}
+
+// advection.cu:27-305 PISO_build_matrix (domain viscosity; non-orthogonal terms by flags). With
 // faceTypes (forPassiveScalar): the wall diffusion of a fixed face follows the scalar
 // channel's type faceTypes[fixed id] instead of the velocity type (advection.cu:254-266), and
 // nu is the channel's diffusivity.
 template <typename S>
 static void advMatrix(const Dom<S> &D, const S *u, S dt, S nu, const int *row, int *col, S *val, S *Adiag,
-		const int8_t *faceTypes = nullptr, int scheme = 0) {
+		const int8_t *faceTypes = nullptr, int scheme = 0, int flags = 0) {
+	NField<S> F;
+	F.kind = faceTypes ? NF_SCALAR : NF_VELOCITY;
+	F.sTypes = faceTypes;
+	const bool nonOrtho = D.dims > 1 && (flags & (NO_CENTER_MATRIX | NO_DIRECT_MATRIX));
 	forEachCell<S>(D, [&](int b, const int *p, int g) {
+		// the velocity matrix weights the cross coefficients with the viscosity, the scalar
+		// matrix scales them by its diffusivity afterwards (advection.cu:181-195)
+		S ia[6][2] = {};
+		if (nonOrtho) nonOrthoInterp(D, b, p, [&](int, const int *) { return faceTypes ? S(1) : nu; }, ia);
 		S fl[6];
 		fluxes(D, b, p, u, fl);
 		const S *tP = D.T(b, p);
@@ -335,6 +619,12 @@ static void advMatrix(const Dom<S> &D, const S *u, S dt, S nu, const int *row, i
 				const S coeff = (alphaP[dim] * nu + alphaN * nu) * S(0.5);
 				diag += coeff;
 				rv[f + 1] -= coeff;
+				if (nonOrtho) {
+					const S a[2] = {ia[f][0] * (faceTypes ? nu : S(1)), ia[f][1] * (faceTypes ? nu : S(1))};
+					rv[0] = diag;
+					nonOrthoMatrixFace(D, F, b, p, f, flags, -1, false, a, rv);
+					diag = rv[0];
+				}
 			} else {
 				const int type = faceTypes ? int(faceTypes[D.fixedId(b, f)]) : D.velType(b, f);
 				const S slip = type == 0 ? S(0) : S(1);
@@ -347,9 +637,11 @@ static void advMatrix(const Dom<S> &D, const S *u, S dt, S nu, const int *row, i
 	});
 }
 
-// advection.cu:800-954 kPISO_build_advection_RHS (CENTRAL, no pressure gradient)
+// advection.cu:800-954 kPISO_build_advection_RHS (no pressure gradient); with ures the
+// non-orthogonal terms of the velocity result
 template <typename S>
-static void advRhs(const Dom<S> &D, const S *u, const S *src, int srcStatic, S dt, S nu, S *rhs, int scheme = 0) {
+static void advRhs(const Dom<S> &D, const S *u, const S *src, int srcStatic, S dt, S nu, S *rhs, int scheme = 0,
+		int flags = 0, const S *ures = nullptr) {
 	forEachCell<S>(D, [&](int b, const int *p, int g) {
 		const S det = D.det(D.T(b, p));
 		S fl[6];
@@ -368,6 +660,13 @@ static void advRhs(const Dom<S> &D, const S *u, const S *src, int srcStatic, S d
 				r += vel * (S(1) - slip) * nu * S(2) * alpha;
 			}
 			if (scheme != 0) upwindCorrection(D, b, p, fl, [&](int gg) { return u[(size_t)dim * D.n + gg]; }, r);
+			if (ures) { // advection.cu:936-937: the velocity result's cross terms, viscosity-weighted
+				NField<S> F;
+				F.kind = NF_VELOCITY;
+				F.w = dim;
+				F.cells = ures + (size_t)dim * D.n;
+				r -= nonOrthoRhs(D, F, b, p, flags, [&](int, const int *) { return nu; }, nu);
+			}
 			r /= det;
 			if (src) r += srcStatic ? src[dim] : src[(size_t)dim * D.n + g];
 			rhs[(size_t)dim * D.n + g] = r;
@@ -375,13 +674,21 @@ static void advRhs(const Dom<S> &D, const S *u, const S *src, int srcStatic, S d
 	});
 }
 
-// advection.cu:545-698 kPISO_build_scalar_advection_RHS (CENTRAL, orthogonal) for one channel:
+// advection.cu:545-698 kPISO_build_scalar_advection_RHS for one channel:
 // det phi/dt, at fixed faces Dirichlet -phi_b F + phi_b nu 2 alpha, Neumann -phi_P F +
 // (dphi/dn) nu |S_f| (|S_f| = det_f |Minv_f[dim]|, discretization.cuh:618-634), over det.
 // faceTypes[fixed id]: 0 Dirichlet, 1 Neumann; faceValue(fixed id, face cell) the face data.
 template <typename S>
 static void scalarRhs(const Dom<S> &D, const S *phi, S dt, S nu, const int8_t *faceTypes, const S *faceValues,
-		const int64_t *faceOffsets, const int8_t *faceStatic, S *rhs, const S *u = nullptr, int scheme = 0) {
+		const int64_t *faceOffsets, const int8_t *faceStatic, S *rhs, const S *u = nullptr, int scheme = 0, int flags = 0,
+		const S *phires = nullptr) {
+	NField<S> F;
+	F.kind = NF_SCALAR;
+	F.cells = phires;
+	F.sTypes = faceTypes;
+	F.sValues = faceValues;
+	F.sOffsets = faceOffsets;
+	F.sStatic = faceStatic;
 	forEachCell<S>(D, [&](int b, const int *p, int g) {
 		const S det = D.det(D.T(b, p));
 		S fl[6];
@@ -405,6 +712,8 @@ static void scalarRhs(const Dom<S> &D, const S *phi, S dt, S nu, const int8_t *f
 			}
 		}
 		if (scheme != 0) upwindCorrection(D, b, p, fl, [&](int gg) { return phi[gg]; }, r);
+		// advection.cu:684-689: the scalar result's cross terms, times the diffusivity
+		if (phires) r -= nonOrthoRhs(D, F, b, p, flags, [&](int, const int *) { return S(1); }, S(1)) * nu;
 		rhs[g] = r / det;
 	});
 }
@@ -413,8 +722,12 @@ static void scalarRhs(const Dom<S> &D, const S *phi, S dt, S nu, const int8_t *f
 // With unitWeight it is PISO_build_epot_matrix (potential.cu:30-233): 1/A replaced by 1,
 // Dirichlet ghost diagonal and the thin-wall Robin terms.
 template <typename S>
-static void laplaceMatrix(const Dom<S> &D, const S *Adiag, bool epot, const int *row, int *col, S *val) {
+static void laplaceMatrix(const Dom<S> &D, const S *Adiag, bool epot, const int *row, int *col, S *val, int flags = 0) {
+	const NField<S> F; // the matrix walks only look for fixed faces (GridDataType::IS_FIXED_BOUNDARY)
+	const bool nonOrtho = !epot && D.dims > 1 && (flags & (NO_CENTER_MATRIX | NO_DIRECT_MATRIX));
 	forEachCell<S>(D, [&](int b, const int *p, int g) {
+		S ia[6][2] = {};
+		if (nonOrtho) nonOrthoInterp(D, b, p, [&](int bb, const int *pp) { return S(1) / Adiag[D.glob(bb, pp)]; }, ia);
 		const S *tP = D.T(b, p);
 		S alphaP[3];
 		for (int d = 0; d < D.dims; ++d) alphaP[d] = alphaOf(D, tP, d);
@@ -436,6 +749,7 @@ static void laplaceMatrix(const Dom<S> &D, const S *Adiag, bool epot, const int 
 				rv[0] -= coeff;
 				rv[f + 1] += coeff;
 				cols[f + 1] = gn;
+				if (nonOrtho) nonOrthoMatrixFace(D, F, b, p, f, flags, 1, true, ia[f], rv);
 			} else if (epot && D.potBC(b, f, p) == PB_DIRICHLET) {
 				rv[0] -= alphaP[dim] * raP;
 			}
@@ -512,6 +826,18 @@ static void pressureRhs(const Dom<S> &D, const int *row, const int *col, const S
 			}
 			hbya[(size_t)dim * D.n + g] = rDiag * (velOld - H + Ssum);
 		}
+	});
+}
+
+// pressure.cu:839-860 k_pressureRHSaddNonOrthoComponents: div += the pressure result's cross
+// terms weighted with 1/A
+template <typename S>
+static void pressureNonOrtho(const Dom<S> &D, const S *Adiag, const S *pr, int flags, S *div) {
+	NField<S> F;
+	F.kind = NF_PRESSURE;
+	F.cells = pr;
+	forEachCell<S>(D, [&](int b, const int *p, int g) {
+		div[g] += nonOrthoRhs(D, F, b, p, flags, [&](int bb, const int *pp) { return S(1) / Adiag[D.glob(bb, pp)]; }, S(1));
 	});
 }
 
@@ -791,19 +1117,23 @@ static int bicgstab(int n, const int *row, const int *col, const S *val, const S
 #define ORC_INSTANTIATE(S, SUF)                                                                                          \
 extern "C" void orc_row_pointers##SUF(ORC_DOM_ARGS(S), int *row) { ORC_DOM(S); orc::rowPointers(D, row); }              \
 extern "C" void orc_adv_matrix##SUF(ORC_DOM_ARGS(S), const S *u, double dt, double nu, const int *row, int *col, S *val, S *Adiag, \
-		int scheme) {                                                                                                      \
-	ORC_DOM(S); orc::advMatrix<S>(D, u, S(dt), S(nu), row, col, val, Adiag, nullptr, scheme); }                           \
+		int scheme, int flags) {                                                                                           \
+	ORC_DOM(S); orc::advMatrix<S>(D, u, S(dt), S(nu), row, col, val, Adiag, nullptr, scheme, flags); }                    \
 extern "C" void orc_scalar_matrix##SUF(ORC_DOM_ARGS(S), const S *u, double dt, double nu, const int8_t *types,            \
-		const int *row, int *col, S *val, S *Adiag, int scheme) {                                                         \
-	ORC_DOM(S); orc::advMatrix<S>(D, u, S(dt), S(nu), row, col, val, Adiag, types, scheme); }                              \
+		const int *row, int *col, S *val, S *Adiag, int scheme, int flags) {                                              \
+	ORC_DOM(S); orc::advMatrix<S>(D, u, S(dt), S(nu), row, col, val, Adiag, types, scheme, flags); }                       \
 extern "C" void orc_scalar_rhs##SUF(ORC_DOM_ARGS(S), const S *phi, double dt, double nu, const int8_t *types,            \
-		const S *values, const int64_t *offsets, const int8_t *statics, S *rhs, const S *u, int scheme) {                 \
-	ORC_DOM(S); orc::scalarRhs<S>(D, phi, S(dt), S(nu), types, values, offsets, statics, rhs, u, scheme); }                 \
+		const S *values, const int64_t *offsets, const int8_t *statics, S *rhs, const S *u, int scheme, int flags,        \
+		const S *phires) {                                                                                                 \
+	ORC_DOM(S); orc::scalarRhs<S>(D, phi, S(dt), S(nu), types, values, offsets, statics, rhs, u, scheme, flags, phires); } \
 extern "C" void orc_adv_rhs##SUF(ORC_DOM_ARGS(S), const S *u, const S *src, int srcStatic, double dt, double nu, S *rhs, \
-		int scheme) {                                                                                                      \
-	ORC_DOM(S); orc::advRhs<S>(D, u, src, srcStatic, S(dt), S(nu), rhs, scheme); }                                       \
-extern "C" void orc_laplace_matrix##SUF(ORC_DOM_ARGS(S), const S *Adiag, int epot, const int *row, int *col, S *val) { \
-	ORC_DOM(S); orc::laplaceMatrix<S>(D, Adiag, epot != 0, row, col, val); }                                             \
+		int scheme, int flags, const S *ures) {                                                                            \
+	ORC_DOM(S); orc::advRhs<S>(D, u, src, srcStatic, S(dt), S(nu), rhs, scheme, flags, ures); }                          \
+extern "C" void orc_laplace_matrix##SUF(ORC_DOM_ARGS(S), const S *Adiag, int epot, const int *row, int *col, S *val,   \
+		int flags) {                                                                                                       \
+	ORC_DOM(S); orc::laplaceMatrix<S>(D, Adiag, epot != 0, row, col, val, flags); }                                      \
+extern "C" void orc_pressure_nonortho##SUF(ORC_DOM_ARGS(S), const S *Adiag, const S *pr, int flags, S *div) {            \
+	ORC_DOM(S); orc::pressureNonOrtho<S>(D, Adiag, pr, flags, div); }                                                     \
 extern "C" void orc_pressure_rhs##SUF(ORC_DOM_ARGS(S), const int *row, const int *col, const S *Cval, const S *Adiag,   \
 		const S *u, const S *ustar, const S *src, int srcStatic, double dt, double nu, S *hbya, int scheme) {           \
 	ORC_DOM(S); orc::pressureRhs<S>(D, row, col, Cval, Adiag, u, ustar, src, srcStatic, S(dt), S(nu), hbya, scheme); } \

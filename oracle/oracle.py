@@ -181,11 +181,12 @@ class OracleDomain:
         return np.ascontiguousarray(np.asarray(x, dtype=self.S))
 
     # --- kernels (each mirrors one reference kernel, see oracle.cpp) ---
-    def advection_matrix(self, u, dt, nu):
+    def advection_matrix(self, u, dt, nu, flags=0):
+        """flags: the non-orthogonal bits (NON_ORTHO_CENTER_MATRIX, NON_ORTHO_DIRECT_MATRIX)."""
         val = np.zeros(self.nnz, dtype=self.S)
         A = self.vec()
         self._f("orc_adv_matrix")(*self._dargs(), _p(self._a(u)), ct.c_double(dt), ct.c_double(nu), _p(self.row),
-                                  _p(self.col), _p(val), _p(A), self.scheme)
+                                  _p(self.col), _p(val), _p(A), self.scheme, int(flags))
         return val, A
 
     def _scalar_face_data(self, c):
@@ -210,30 +211,32 @@ class OracleDomain:
             o += v.shape[1]
         return types, np.ascontiguousarray(np.concatenate(vals) if vals else np.zeros(1, dtype=self.S)), offs, stat
 
-    def scalar_matrix(self, u, dt, nu, channel):
+    def scalar_matrix(self, u, dt, nu, channel, flags=0):
         """advection.cu:27-305 with forPassiveScalar for one channel (its diffusivity nu)."""
         types, _, _, _ = self._scalar_face_data(channel)
         val = np.zeros(self.nnz, dtype=self.S)
         A = self.vec()
         self._f("orc_scalar_matrix")(*self._dargs(), _p(self._a(u)), ct.c_double(dt), ct.c_double(nu), _p(types),
-                                     _p(self.row), _p(self.col), _p(val), _p(A), self.scheme)
+                                     _p(self.row), _p(self.col), _p(val), _p(A), self.scheme, int(flags))
         return val, A
 
-    def scalar_rhs(self, phi_c, dt, nu, channel, u=None):
+    def scalar_rhs(self, phi_c, dt, nu, channel, u=None, flags=0, phires=None):
         """advection.cu:545-698 for one channel's field phi_c [n]; u (the block velocity) gives
-        the LINEAR_UPWIND fluxes."""
+        the LINEAR_UPWIND fluxes; phires (the channel's scalar result) the non-orthogonal terms."""
         types, vals, offs, stat = self._scalar_face_data(channel)
         rhs = self.vec()
         uu = self._a(u) if u is not None else self.vec(self.dims)
         self._f("orc_scalar_rhs")(*self._dargs(), _p(self._a(phi_c)), ct.c_double(dt), ct.c_double(nu), _p(types),
-                                  _p(vals), _p(offs), _p(stat), _p(rhs), _p(uu), self.scheme)
+                                  _p(vals), _p(offs), _p(stat), _p(rhs), _p(uu), self.scheme, int(flags),
+                                  _p(self._a(phires)) if phires is not None else None)
         return rhs
 
-    def advection_rhs(self, u, src, dt, nu):
+    def advection_rhs(self, u, src, dt, nu, flags=0, ures=None):
+        """ures: the velocity result [d][n] whose non-orthogonal terms enter (flags)."""
         rhs = self.vec(self.dims)
         src_arr, static = self._src(src)
         self._f("orc_adv_rhs")(*self._dargs(), _p(self._a(u)), _p(src_arr), static, ct.c_double(dt), ct.c_double(nu), _p(rhs),
-                               self.scheme)
+                               self.scheme, int(flags), _p(self._a(ures)) if ures is not None else None)
         return rhs
 
     def _src(self, src):
@@ -242,12 +245,18 @@ class OracleDomain:
         s = self._a(src)
         return s, 1 if s.size == self.dims else 0
 
-    def laplace_matrix(self, A=None, epot=False):
+    def laplace_matrix(self, A=None, epot=False, flags=0):
         val = np.zeros(self.nnz, dtype=self.S)
         col = np.zeros(self.nnz, dtype=np.int32)
         self._f("orc_laplace_matrix")(*self._dargs(), _p(self._a(A) if A is not None else self.vec()), 1 if epot else 0,
-                                      _p(self.row), _p(col), _p(val))
+                                      _p(self.row), _p(col), _p(val), int(flags))
         return val, col
+
+    def pressure_nonortho(self, A, p, flags, div):
+        """pressure.cu:839-860: div + the non-orthogonal terms of the pressure result p."""
+        out = self._a(div).copy()
+        self._f("orc_pressure_nonortho")(*self._dargs(), _p(self._a(A)), _p(self._a(p)), int(flags), _p(out))
+        return out
 
     def pressure_rhs(self, Cval, A, u, ustar, src, dt, nu):
         h = self.vec(self.dims)
@@ -332,8 +341,16 @@ class OracleSim:
     """Reference PISO (+ inductionless MHD) step of one environment on the CPU."""
 
     def __init__(self, od: OracleDomain, u0: np.ndarray, dt: float, nu: float, *, corrector_steps=2,
-                 advection_tol=None, pressure_tol=None, source=None, mhd=None, maxit=5000, scalar=None):
+                 advection_tol=None, pressure_tol=None, source=None, mhd=None, maxit=5000, scalar=None,
+                 nonortho_flags=0, advect_non_ortho_steps=1, pressure_non_ortho_steps=1, pressure_bicg=False):
         self.od = od
+        self.pressure_bicg = bool(pressure_bicg)
+        # core/piso_simulation.py:3225-3345,3839-3891,3978-4117: with non-orthogonal flags the
+        # right-hand sides carry the lagged cross terms of the current result, re-solved
+        # advect/pressure_non_ortho_steps times
+        self.flags = int(nonortho_flags)
+        self.advect_no_steps = int(advect_non_ortho_steps)
+        self.pressure_no_steps = int(pressure_non_ortho_steps)
         self.dt = dt
         self.nu = nu
         self.corrector_steps = corrector_steps
@@ -369,18 +386,23 @@ class OracleSim:
         types_static = all(fd is None or fd[3] for fd in od.scalar_faces)
         split = not (static_nu and types_static)
         nu_of = (lambda c: self.nu) if nus is None else (lambda c: float(nus[0] if len(nus) == 1 else nus[c]))
-        mat = None if split else od.scalar_matrix(self.u, self.dt, nu_of(0), 0)
+        fl = self.flags
+        mat = None if split else od.scalar_matrix(self.u, self.dt, nu_of(0), 0, flags=fl)
         its = []
+        res = self.phi_s.copy()  # CopyScalarResultFromBlocks
         for c in range(C):
-            Cval, _ = od.scalar_matrix(self.u, self.dt, nu_of(c), c) if split else mat
-            rhs = od.scalar_rhs(self.phi_s[c], self.dt, nu_of(c), c, u=self.u)
-            tol = resolve_tol(self.advection_tol, rhs, od.S)
-            x = od.vec()
-            st, it, _ = od.solve(Cval, rhs, x, tol, self.maxit, bicg=True)
-            if st != 1:
-                raise RuntimeError(f"oracle scalar solve failed ({st})")
-            self.phi_s[c] = x
-            its.append(it)
+            Cval, _ = od.scalar_matrix(self.u, self.dt, nu_of(c), c, flags=fl) if split else mat
+            for no_step in range(self.advect_no_steps if fl else 1):
+                rhs = od.scalar_rhs(self.phi_s[c], self.dt, nu_of(c), c, u=self.u, flags=fl,
+                                    phires=res[c] if fl else None)
+                tol = resolve_tol(self.advection_tol, rhs, od.S)
+                x = od.vec() if no_step == 0 else res[c].copy()
+                st, it, _ = od.solve(Cval, rhs, x, tol, self.maxit, bicg=True)
+                if st != 1:
+                    raise RuntimeError(f"oracle scalar solve failed ({st})")
+                res[c] = x
+                its.append(it)
+        self.phi_s = res
         self.iterations["scalar"] = its
         reuse = nus is None and not split
         return mat if reuse else None
@@ -399,31 +421,37 @@ class OracleSim:
             else:
                 base = self.src if self.src.size == d * n else np.repeat(self.src, n)
                 self.src = (F + base).astype(od.S)
-        Cval, A = reused if reused is not None else od.advection_matrix(self.u, self.dt, self.nu)
-        rhs = od.advection_rhs(self.u, self.src, self.dt, self.nu)
-        tol = resolve_tol(self.advection_tol, rhs, od.S)
+        fl = self.flags
+        Cval, A = reused if reused is not None else od.advection_matrix(self.u, self.dt, self.nu, flags=fl)
         its = []
-        for k in range(d):
-            xk = self.u_res[k * n:(k + 1) * n].copy()
-            st, it, _ = od.solve(Cval, rhs[k * n:(k + 1) * n].copy(), xk, tol, self.maxit, bicg=True)
-            if st != 1:
-                raise RuntimeError(f"oracle momentum solve failed ({st})")
-            self.u_res[k * n:(k + 1) * n] = xk
-            its.append(it)
+        if fl:
+            self.u_res = self.u.copy()  # CopyVelocityResultFromBlocks
+        for no_step in range(self.advect_no_steps if fl else 1):
+            rhs = od.advection_rhs(self.u, self.src, self.dt, self.nu, flags=fl, ures=self.u_res if fl else None)
+            tol = resolve_tol(self.advection_tol, rhs, od.S)
+            for k in range(d):
+                xk = od.vec() if (fl and no_step == 0) else self.u_res[k * n:(k + 1) * n].copy()
+                st, it, _ = od.solve(Cval, rhs[k * n:(k + 1) * n].copy(), xk, tol, self.maxit, bicg=True)
+                if st != 1:
+                    raise RuntimeError(f"oracle momentum solve failed ({st})")
+                self.u_res[k * n:(k + 1) * n] = xk
+                its.append(it)
         self.iterations["velocity"] = its
-        Pval, Pcol = od.laplace_matrix(A)
+        Pval, Pcol = od.laplace_matrix(A, flags=fl)
         for c in range(self.corrector_steps):
             h = od.pressure_rhs(Cval, A, self.u, self.u_res, self.src, self.dt, self.nu)
-            div = od.divergence(h)
-            ptol = resolve_tol(self.pressure_tol, div, od.S)
-            p = od.vec()
-            st, it, _ = od.solve(Pval, div, p, ptol, self.maxit, col=Pcol)
-            if st != 1:
-                raise RuntimeError(f"oracle pressure solve failed ({st})")
-            self.iterations[f"pressure{c}"] = it
-            p = self._mean_sub(p).astype(od.S)
-            self.p = p
-            self.u_res = od.correct_velocity(p, h, A)
+            for pstep in range(self.pressure_no_steps if fl else 1):
+                div = od.divergence(h)
+                if fl:
+                    div = od.pressure_nonortho(A, self.p, fl, div)
+                ptol = resolve_tol(self.pressure_tol, div, od.S)
+                p = od.vec() if pstep == 0 else self.p.copy()
+                st, it, _ = od.solve(Pval, div, p, ptol, self.maxit, bicg=self.pressure_bicg, col=Pcol)
+                if st != 1:
+                    raise RuntimeError(f"oracle pressure solve failed ({st})")
+                self.iterations[f"pressure{c}"] = it
+                self.p = self._mean_sub(p).astype(od.S)
+            self.u_res = od.correct_velocity(self.p, h, A)
         self.u = self.u_res.copy()
         if self.mhd is not None:
             self.potential_step()

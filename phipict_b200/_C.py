@@ -31,9 +31,26 @@ def _check(domain: Domain) -> None:
         raise RuntimeError("Domain is not initialized.")
 
 
-def _no_nonortho(flags) -> None:
-    if int(flags) != 0:
-        raise NotImplementedError("phipict_b200 assembles the orthogonal discretization (non-orthogonal flags must be 0)")
+NON_ORTHO_RHS = NON_ORTHO_DIRECT_RHS | NON_ORTHO_DIAGONAL_RHS
+
+
+def _flags(flags) -> int:
+    """The non-orthogonal flag bits of one Setup* call (piso/non_ortho_flags.h:23-27)."""
+    f = int(flags)
+    if not 0 <= f < 32:
+        raise ValueError(f"invalid non-orthogonal flags {flags}")
+    return f
+
+
+def _desc(domain: Domain, flags: int = 0) -> _lib.PhbDomain:
+    """The domain's descriptor carrying this call's non-orthogonal flags (a copy: the cached
+    descriptor keeps 0 for every caller that passes none)."""
+    d = domain.desc()
+    if not flags:
+        return d
+    c = _lib.PhbDomain.from_buffer_copy(d)
+    c.nonortho = flags
+    return c
 
 
 def _S(domain: Domain) -> int:
@@ -78,53 +95,63 @@ def SetupAdvectionMatrix(domain: Domain, timeStep, nonOrthoFlags=0, forPassiveSc
                          passiveScalarChannel: int = 0) -> None:
     """Implicit Euler advection-diffusion matrix C and its diagonal A (advection.cu:27-305)."""
     _check(domain)
-    _no_nonortho(nonOrthoFlags)
+    desc = _desc(domain, _flags(nonOrthoFlags))
     domain.setTimeStep(timeStep)
     lo = _lo(domain, "C")
     if forPassiveScalar:
         c = int(passiveScalarChannel)
         if not 0 <= c < domain.getPassiveScalarChannels():
             raise RuntimeError(f"passive scalar channel {c} out of range")
-        _lib.call("phb_scalar_matrix", ct.byref(domain.desc()), domain._u_block.data_ptr(), ct.byref(domain._scalar_struct()),
+        _lib.call("phb_scalar_matrix", ct.byref(desc), domain._u_block.data_ptr(), ct.byref(domain._scalar_struct()),
                   c, domain._C_st.data_ptr(), domain.A.data_ptr(), lo.data_ptr() if lo is not None else None, _S(domain))
     else:
-        _lib.call("phb_advection_matrix", ct.byref(domain.desc()), domain._u_block.data_ptr(), domain._C_st.data_ptr(),
+        _lib.call("phb_advection_matrix", ct.byref(desc), domain._u_block.data_ptr(), domain._C_st.data_ptr(),
                   domain.A.data_ptr(), lo.data_ptr() if lo is not None else None, _S(domain))
     _assembled(domain, "C", lo)
 
 
 def SetupAdvectionVelocity(domain: Domain, timeStep, nonOrthoFlags=0, applyPressureGradient: bool = False) -> None:
-    """Momentum right-hand side into ``domain.velocityRHS`` (advection.cu:800-954)."""
+    """Momentum right-hand side into ``domain.velocityRHS`` (advection.cu:800-954); with
+    non-orthogonal right-hand-side flags it carries the cross terms of ``velocityResult``."""
     _check(domain)
-    _no_nonortho(nonOrthoFlags)
+    flags = _flags(nonOrthoFlags)
     if applyPressureGradient:
         raise NotImplementedError("applyPressureGradient is not used by the PISO step")
     domain.setTimeStep(timeStep)
     src, mode = _src(domain)
     _lib.call("phb_advection_rhs", ct.byref(domain.desc()), domain._u_block.data_ptr(), src, mode,
               domain.velocityRHS.data_ptr(), _S(domain))
+    if flags & NON_ORTHO_RHS:
+        _lib.call("phb_nonortho_rhs", ct.byref(_desc(domain, flags)), _lib.PHB_NONORTHO_VELOCITY,
+                  domain.velocityResult.data_ptr(), None, None, domain.velocityRHS.data_ptr(), _S(domain))
 
 
 def SetupAdvectionScalar(domain: Domain, timeStep, nonOrthoFlags=0) -> None:
     """Passive-scalar right-hand side into ``domain.scalarRHS`` [B][channels][cells]
     (advection.cu:545-698, bindings SetupAdvectionScalar)."""
     _check(domain)
-    _no_nonortho(nonOrthoFlags)
+    flags = _flags(nonOrthoFlags)
     domain.setTimeStep(timeStep)
+    sc = domain._scalar_struct()
     _lib.call("phb_scalar_rhs", ct.byref(domain.desc()), domain._phi_block.data_ptr(), domain._u_block.data_ptr(),
-              ct.byref(domain._scalar_struct()), domain.scalarRHS.data_ptr(), _S(domain))
+              ct.byref(sc), domain.scalarRHS.data_ptr(), _S(domain))
+    if flags & NON_ORTHO_RHS:
+        # the cross terms of scalarResult (CopyScalarResultFromBlocks before the first pass)
+        _lib.call("phb_nonortho_rhs", ct.byref(_desc(domain, flags)), _lib.PHB_NONORTHO_SCALAR,
+                  domain.scalarResult.data_ptr(), ct.byref(sc), None, domain.scalarRHS.data_ptr(), _S(domain))
 
 
 # --- pressure ---------------------------------------------------------------------------
 def SetupPressureMatrix(domain: Domain, timeStep, nonOrthoMode=0, useFaceTransform: bool = False) -> None:
-    """Pressure Laplacian P = div(A^-1 grad) (pressure.cu:26-191)."""
+    """Pressure Laplacian P = div(A^-1 grad) (pressure.cu:26-191), with the non-orthogonal
+    matrix terms of ``nonOrthoMode``."""
     _check(domain)
-    _no_nonortho(nonOrthoMode)
+    desc = _desc(domain, _flags(nonOrthoMode))
     if useFaceTransform:
-        raise NotImplementedError("face transforms are not used by the orthogonal pressure matrix")
+        raise NotImplementedError("face transforms (an experimental option of the reference) are not implemented")
     domain.setTimeStep(timeStep)
     lo = _lo(domain, "P")
-    _lib.call("phb_pressure_matrix", ct.byref(domain.desc()), domain.A.data_ptr(), domain._P_st.data_ptr(),
+    _lib.call("phb_pressure_matrix", ct.byref(desc), domain.A.data_ptr(), domain._P_st.data_ptr(),
               lo.data_ptr() if lo is not None else None, _S(domain))
     _assembled(domain, "P", lo)
 
@@ -134,7 +161,7 @@ def SetupPressureRHS(domain: Domain, timeStep, nonOrthoMode=0, useFaceTransform:
     """HbyA into ``pressureRHS`` and its divergence into ``pressureRHSdiv``
     (pressure.cu:350-521, :756-801)."""
     _check(domain)
-    _no_nonortho(nonOrthoMode)
+    _flags(nonOrthoMode)
     if useFaceTransform or timeStepNorm:
         raise NotImplementedError("face transforms and time step normalisation are not implemented")
     domain.setTimeStep(timeStep)
@@ -147,9 +174,18 @@ def SetupPressureRHS(domain: Domain, timeStep, nonOrthoMode=0, useFaceTransform:
 
 def SetupPressureRHSdiv(domain: Domain, timeStep, nonOrthoMode=0, useFaceTransform: bool = False,
                         timeStepNorm: bool = False) -> None:
+    """div(pressureRHS) into ``pressureRHSdiv`` (pressure.cu:756-801), plus the
+    non-orthogonal terms of ``pressureResult`` weighted with 1/A (pressure.cu:839-860)."""
     _check(domain)
+    flags = _flags(nonOrthoMode)
+    if useFaceTransform or timeStepNorm:
+        raise NotImplementedError("face transforms and time step normalisation are not implemented")
     _lib.call("phb_divergence", ct.byref(domain.desc()), domain.pressureRHS.data_ptr(),
               domain.pressureRHSdiv.data_ptr(), _S(domain))
+    if flags & NON_ORTHO_RHS:
+        _lib.call("phb_nonortho_rhs", ct.byref(_desc(domain, flags)), _lib.PHB_NONORTHO_PRESSURE,
+                  domain.pressureResult.data_ptr(), None, domain.A.data_ptr(), domain.pressureRHSdiv.data_ptr(),
+                  _S(domain))
 
 
 def SetupPressureCorrection(domain: Domain, timeStep, nonOrthoMode=0, useFaceTransform: bool = False,

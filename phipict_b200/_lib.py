@@ -25,7 +25,7 @@ EXPORTS = (
     "phb_cell_metrics", "phb_face_metrics",
     "phb_advection_matrix", "phb_advection_rhs", "phb_pressure_matrix", "phb_pressure_rhs",
     "phb_divergence", "phb_correct_velocity", "phb_epot_matrix", "phb_epot_rhs", "phb_uxb_epot_rhs",
-    "phb_current_lorentz", "phb_scalar_matrix", "phb_scalar_rhs",
+    "phb_current_lorentz", "phb_scalar_matrix", "phb_scalar_rhs", "phb_nonortho_rhs",
     "phb_scratch_doubles", "phb_subtract_mean", "phb_rms",
     "phb_csr_row_sizes", "phb_csr_pattern", "phb_csr_gather",
     "phb_solve_work_bytes", "phb_solve_state_bytes", "phb_solve_run", "phb_solve_results",
@@ -38,6 +38,10 @@ EXPORTS = (
 )
 
 
+# phb_nonortho_rhs kinds
+PHB_NONORTHO_VELOCITY, PHB_NONORTHO_SCALAR, PHB_NONORTHO_PRESSURE = 0, 1, 2
+
+
 class PhbDomain(ct.Structure):
     _fields_ = [
         ("dims", ct.c_int32), ("dtype", ct.c_int32),
@@ -46,7 +50,7 @@ class PhbDomain(ct.Structure):
         ("blocks", ct.c_void_p), ("tiles", ct.c_void_p), ("fixed", ct.c_void_p), ("insts", ct.c_void_p),
         ("metrics", ct.c_void_p), ("face_metrics", ct.c_void_p),
         ("fvel", ct.c_void_p), ("fpot", ct.c_void_p), ("fcw", ct.c_void_p), ("fmask", ct.c_void_p),
-        ("dt", ct.c_void_p), ("nu", ct.c_void_p), ("scheme", ct.c_int32), ("pad", ct.c_int32),
+        ("dt", ct.c_void_p), ("nu", ct.c_void_p), ("scheme", ct.c_int32), ("nonortho", ct.c_int32),
     ]
 
 
@@ -136,6 +140,7 @@ def load() -> ct.CDLL:
         "phb_advection_rhs": [DP, P, P, I, P, P],
         "phb_scalar_matrix": [DP, P, ct.POINTER(PhbScalar), I, P, P, P, P],
         "phb_scalar_rhs": [DP, P, P, ct.POINTER(PhbScalar), P, P],
+        "phb_nonortho_rhs": [DP, I, P, ct.POINTER(PhbScalar), P, P, P],
         "phb_pressure_matrix": [DP, P, P, P, P],
         "phb_pressure_rhs": [DP, P, P, P, P, P, I, P, P],
         "phb_divergence": [DP, P, P, P],

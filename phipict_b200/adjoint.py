@@ -68,6 +68,9 @@ class AdjointMHD:
             raise NotImplementedError("the hand-written adjoint differentiates the CENTRAL advection scheme")
         if not domain.IsInitialized():
             domain.PrepareSolve()
+        if domain.getSpatialDims() > 1 and domain.hasNonOrthogonalMetrics():
+            raise NotImplementedError("the hand-written adjoint differentiates the orthogonal step; this grid has "
+                                      "non-orthogonal cross terms")
         self.d = domain
         self.dims = domain.getSpatialDims()
         self.dt = float(dt)

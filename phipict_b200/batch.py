@@ -250,6 +250,9 @@ class DomainBatch:
     def IsInitialized(self) -> bool:
         return True
 
+    def hasNonOrthogonalMetrics(self) -> bool:
+        return any(m.hasNonOrthogonalMetrics() for m in self.members)
+
     def hasPassiveScalar(self) -> bool:
         """Passive scalars are not transported in a batch: the members' scalar fields stay as
         they are (a batched step advances velocity, pressure and potential)."""

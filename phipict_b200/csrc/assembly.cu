@@ -1,4 +1,4 @@
-// Per-cell assembly kernels of the PISO/MHD step (orthogonal grids, CENTRAL advection).
+// Per-cell assembly kernels of the PISO/MHD step.
 //
 // One thread per cell, one CTA per tile of one block (phb_device.cuh). Matrices are
 // written as stencils value[slot][cell] (slot 0 diagonal, slot f+1 face f), which keeps
@@ -10,6 +10,7 @@
 // (paths relative to the phiPICT source tree).
 #include "phb_device.cuh"
 #include "phb_launch.cuh"
+#include "phb_nonortho.cuh"
 
 namespace phb {
 
@@ -75,41 +76,14 @@ __device__ __forceinline__ void upwindCorrection(const Cell &c, const S *fl, Val
 	}
 }
 
-// Passive-scalar data of a launch (phb_scalar), passed by value.
-struct ScalarView {
-	int channels, nuCount;
-	const double *nu;
-	const int8_t *types;
-	const void *values;
-	const int64_t *offsets;
-	const int8_t *statics;
-};
-__host__ inline ScalarView scalarView(const phb_scalar *sc) {
-	if (!sc) return ScalarView{0, 0, nullptr, nullptr, nullptr, nullptr, nullptr};
-	return ScalarView{sc->channels, sc->nu_count, sc->nu, sc->types, sc->values, sc->offsets, sc->statics};
-}
-// getViscosity with forPassiveScalar (discretization.cuh:1141-1151): the scalar diffusivity of
-// channel c, or the velocity viscosity of the instance without one
-__device__ __forceinline__ double scalarNu(const ScalarView &sv, int c, double velocityNu) {
-	if (sv.nuCount <= 0) return velocityNu;
-	return sv.nu[sv.nuCount == 1 ? 0 : c];
-}
-// fixed-face scalar value of channel c at face cell fc (getFixedBoundaryData, PASSIVE_SCALAR)
-template <typename S>
-__device__ __forceinline__ S scalarFixed(const ScalarView &sv, const int32_t *FR, int fid, int c, int fc) {
-	const S *v = (const S *)sv.values + sv.offsets[fid];
-	return sv.statics[fid] ? v[c] : v[(int64_t)c * FR[F_FACECELLS] + fc];
-}
-// [inst][channels][cells] index of channel c of cell g
-__device__ __forceinline__ int64_t sidx(const int32_t *B, int64_t g, int c, int channels) {
-	return g + (int64_t)(channels - 1) * B[B_INSTOFF] + (int64_t)c * B[B_INSTN];
-}
-
 // PISO_build_matrix (piso/advection.cu:27-305): implicit Euler advection-diffusion row
 // divided by the cell determinant; Adiag = its diagonal. SCALAR: the matrix of passive-scalar
 // channel `channel` (forPassiveScalar): its diffusivity, and the wall diffusion term of a fixed
 // face taken from the scalar's face type instead of the velocity's (advection.cu:254-266).
-template <typename S, int D, bool SCALAR = false>
+// NO: with the non-orthogonal cross terms of dom.nonortho (advection.cu:176-240), the
+// velocity matrix weighting them with the viscosity, the scalar matrix scaling them by its
+// diffusivity (advection.cu:181-195).
+template <typename S, int D, bool SCALAR = false, bool NO = false>
 __global__ void __launch_bounds__(PHB_TILE) kAdvectionMatrix(Dom<S, D> dom, const S *__restrict__ u, S *__restrict__ C,
 		S *__restrict__ Adiag, float *__restrict__ Clo, ScalarView sv = {}, int channel = 0) {
 	__shared__ int32_t sB[PHB_BREC];
@@ -121,6 +95,14 @@ __global__ void __launch_bounds__(PHB_TILE) kAdvectionMatrix(Dom<S, D> dom, cons
 	const int inst = c.B[B_INST];
 	const S dt = S(dom.dt[inst]);
 	const S nu = SCALAR ? S(scalarNu(sv, channel, dom.nu[inst])) : S(dom.nu[inst]);
+	BPos bp;
+	S ia[2 * D][2];
+	NField<S> F;
+	if constexpr (NO) {
+		bp = BPos{__ldg(dom.tiles + 2 * blockIdx.x), {c.p[0], c.p[1], c.p[2]}};
+		nonOrthoInterp<S, D>(dom, bp, [&](int64_t) { return SCALAR ? S(1) : nu; }, ia);
+		F = NField<S>{SCALAR ? NF_SCALAR : NF_VELOCITY, SCALAR ? channel : 0, nullptr, sv};
+	}
 	S fl[2 * D];
 	faceFluxes<S, D>(dom, c, u, fl);
 	const S det = detAt<S, D>(dom, c.mi);
@@ -151,6 +133,12 @@ __global__ void __launch_bounds__(PHB_TILE) kAdvectionMatrix(Dom<S, D> dom, cons
 			const S coeff = (alphaP[dim] * nu + alphaN * nu) * S(0.5);
 			diag += coeff;
 			rv[f + 1] -= coeff;
+			if constexpr (NO) {
+				const S a[2] = {ia[f][0] * (SCALAR ? nu : S(1)), ia[f][1] * (SCALAR ? nu : S(1))};
+				rv[0] = diag;
+				nonOrthoMatrixFace<S, D>(dom, F, bp, f, dom.nonortho, -1, false, a, rv);
+				diag = rv[0];
+			}
 		} else {
 			const int fid = fRec(c.B, f)[5];
 			const int32_t *FR = dom.fix(fid);
@@ -160,6 +148,12 @@ __global__ void __launch_bounds__(PHB_TILE) kAdvectionMatrix(Dom<S, D> dom, cons
 		}
 	}
 	rv[0] = diag;
+	if constexpr (NO) {
+		// a share that falls on a fixed face has no column (the reference drops it)
+#pragma unroll
+		for (int f = 0; f < 2 * D; ++f)
+			if (atBound(c.B, f, c.p) && fType(c.B, f) == FT_FIXED) rv[f + 1] = 0;
+	}
 	const int64_t N = dom.ncells;
 #pragma unroll
 	for (int s = 0; s < 2 * D + 1; ++s) {
@@ -282,9 +276,12 @@ __global__ void __launch_bounds__(PHB_TILE) kScalarRhs(Dom<S, D> dom, const S *_
 // PISO_build_pressure_matrix (pressure.cu:26-191) with raP = 1/A, and
 // PISO_build_epot_matrix (mhd/potential.cu:30-233) with raP = 1 plus the Dirichlet ghost
 // diagonal and the thin-wall Robin correction.
-template <typename S, int D, bool EPOT>
+// NO (pressure only): with the non-orthogonal cross terms of dom.nonortho, weighted with 1/A
+// (pressure.cu:103-156).
+template <typename S, int D, bool EPOT, bool NO = false>
 __global__ void __launch_bounds__(PHB_TILE) kLaplaceMatrix(Dom<S, D> dom, const S *__restrict__ Adiag, S *__restrict__ P,
 		float *__restrict__ Plo) {
+	static_assert(!(EPOT && NO), "the potential matrix has no non-orthogonal terms here");
 	__shared__ int32_t sB[PHB_BREC];
 	int l0_, nc_;
 	loadTile<S, D>(dom, sB, l0_, nc_);
@@ -295,6 +292,12 @@ __global__ void __launch_bounds__(PHB_TILE) kLaplaceMatrix(Dom<S, D> dom, const 
 #pragma unroll
 	for (int d = 0; d < D; ++d) alphaP[d] = alphaAt<S, D>(dom, c.mi, d);
 	const S raP = EPOT ? S(1) : S(1) / Adiag[c.g];
+	BPos bp;
+	S ia[2 * D][2];
+	if constexpr (NO) {
+		bp = BPos{__ldg(dom.tiles + 2 * blockIdx.x), {c.p[0], c.p[1], c.p[2]}};
+		nonOrthoInterp<S, D>(dom, bp, [&](int64_t g) { return S(1) / Adiag[g]; }, ia);
+	}
 	S rv[2 * D + 1];
 	bool has[2 * D + 1];
 #pragma unroll
@@ -311,6 +314,10 @@ __global__ void __launch_bounds__(PHB_TILE) kLaplaceMatrix(Dom<S, D> dom, const 
 			rv[0] -= coeff;
 			rv[f + 1] += coeff;
 			has[f + 1] = true;
+			if constexpr (NO) {
+				const NField<S> F{NF_MARK, 0, nullptr, ScalarView{}};
+				nonOrthoMatrixFace<S, D>(dom, F, bp, f, dom.nonortho, 1, true, ia[f], rv);
+			}
 		} else if (EPOT) {
 			const int32_t *FR = dom.fix(fRec(c.B, f)[5]);
 			if (potBC(dom.fmask, FR, faceCell(c.B, f, c.p)) == PB_DIRICHLET) rv[0] -= alphaP[dim] * raP;
@@ -356,6 +363,11 @@ __global__ void __launch_bounds__(PHB_TILE) kLaplaceMatrix(Dom<S, D> dom, const 
 				}
 			}
 		}
+	}
+	if constexpr (NO) {
+#pragma unroll
+		for (int f = 0; f < 2 * D; ++f)
+			if (!has[f + 1]) rv[f + 1] = 0;
 	}
 	const int64_t N = dom.ncells;
 #pragma unroll
@@ -664,6 +676,44 @@ __global__ void __launch_bounds__(PHB_TILE) kCurrentLorentz(Dom<S, D> dom, const
 	}
 }
 
+// The explicit non-orthogonal terms of a result field applied to a right-hand side
+// (nonortho_rhs.cuh:27-180): the velocity (advection.cu:936-937) and scalar
+// (advection.cu:684-689) right-hand sides lose S / det (the scalar's times its diffusivity),
+// the pressure divergence gains S weighted with 1/A (pressure.cu:839-860).
+template <typename S, int D, int KIND>
+__global__ void __launch_bounds__(PHB_TILE) kNonOrthoRhs(Dom<S, D> dom, const S *__restrict__ field, ScalarView sv,
+		const S *__restrict__ Adiag, S *__restrict__ rhs) {
+	__shared__ int32_t sB[PHB_BREC];
+	int l0_, nc_;
+	loadTile<S, D>(dom, sB, l0_, nc_);
+	const int blk = __ldg(dom.tiles + 2 * blockIdx.x);
+	for (int j_ = 0; j_ < CPT; ++j_) {
+	Cell c;
+	if (!cellAt<D>(sB, l0_, nc_, j_, c)) return;
+	const BPos bp{blk, {c.p[0], c.p[1], c.p[2]}};
+	const int inst = c.B[B_INST];
+	if constexpr (KIND == PHB_NONORTHO_PRESSURE) {
+		const NField<S> F{NF_PRESSURE, 0, field, sv};
+		rhs[c.g] += nonOrthoRhs<S, D>(dom, F, bp, dom.nonortho, [&](int64_t g) { return S(1) / Adiag[g]; }, S(1));
+	} else if constexpr (KIND == PHB_NONORTHO_VELOCITY) {
+		const S nu = S(dom.nu[inst]);
+		const S det = detAt<S, D>(dom, c.mi);
+		for (int w = 0; w < D; ++w) {
+			const NField<S> F{NF_VELOCITY, w, field, sv};
+			rhs[vidx<D>(c.B, c.g, w)] -= nonOrthoRhs<S, D>(dom, F, bp, dom.nonortho, [&](int64_t) { return nu; }, nu) / det;
+		}
+	} else {
+		const S det = detAt<S, D>(dom, c.mi);
+		for (int ch = 0; ch < sv.channels; ++ch) {
+			const S nuc = S(scalarNu(sv, ch, dom.nu[inst]));
+			const NField<S> F{NF_SCALAR, ch, field, sv};
+			rhs[sidx(c.B, c.g, ch, sv.channels)] -=
+				nonOrthoRhs<S, D>(dom, F, bp, dom.nonortho, [&](int64_t) { return S(1); }, S(1)) * nuc / det;
+		}
+	}
+	}
+}
+
 } // namespace phb
 
 using namespace phb;
@@ -682,6 +732,10 @@ using namespace phb;
 extern "C" int phb_advection_matrix(const phb_domain *dom, const void *u, void *C, void *Adiag, float *C_lo, phb_stream stream) {
 	if (!dom || !u || !C || !Adiag) return setError(PHB_ERR_ARG, "phb_advection_matrix: null argument");
 	if (dom->ntiles == 0) return PHB_OK;
+	if (dom->dims > 1 && (dom->nonortho & NO_MATRIX_BITS)) {
+		PHB_DISPATCH(dom, (kAdvectionMatrix<S, D, false, true><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)u, (S *)C, (S *)Adiag, C_lo)));
+		return checkLaunch("kAdvectionMatrix<non-orthogonal>");
+	}
 	PHB_DISPATCH(dom, kAdvectionMatrix<S, D><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)u, (S *)C, (S *)Adiag, C_lo));
 	return checkLaunch("kAdvectionMatrix");
 }
@@ -693,6 +747,11 @@ extern "C" int phb_scalar_matrix(const phb_domain *dom, const void *u, const phb
 		return setError(PHB_ERR_ARG, "phb_scalar_matrix: bad scalar description");
 	if (dom->ntiles == 0) return PHB_OK;
 	const ScalarView sv = scalarView(sc);
+	if (dom->dims > 1 && (dom->nonortho & NO_MATRIX_BITS)) {
+		PHB_DISPATCH(dom, (kAdvectionMatrix<S, D, true, true><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)u, (S *)C, (S *)Adiag, C_lo, sv,
+			channel)));
+		return checkLaunch("kAdvectionMatrix<scalar, non-orthogonal>");
+	}
 	PHB_DISPATCH(dom, kAdvectionMatrix<S, D, true><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)u, (S *)C, (S *)Adiag, C_lo, sv, channel));
 	return checkLaunch("kAdvectionMatrix<scalar>");
 }
@@ -715,6 +774,10 @@ extern "C" int phb_advection_rhs(const phb_domain *dom, const void *u, const voi
 extern "C" int phb_pressure_matrix(const phb_domain *dom, const void *Adiag, void *P, float *P_lo, phb_stream stream) {
 	if (!dom || !Adiag || !P) return setError(PHB_ERR_ARG, "phb_pressure_matrix: null argument");
 	if (dom->ntiles == 0) return PHB_OK;
+	if (dom->dims > 1 && (dom->nonortho & NO_MATRIX_BITS)) {
+		PHB_DISPATCH(dom, (kLaplaceMatrix<S, D, false, true><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)Adiag, (S *)P, P_lo)));
+		return checkLaunch("kLaplaceMatrix<non-orthogonal>");
+	}
 	PHB_DISPATCH(dom, (kLaplaceMatrix<S, D, false><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)Adiag, (S *)P, P_lo)));
 	return checkLaunch("kLaplaceMatrix");
 }
@@ -764,4 +827,25 @@ extern "C" int phb_epot_rhs(const phb_domain *dom, const void *field, void *rhs,
 	if (dom->ntiles == 0) return PHB_OK;
 	PHB_DISPATCH(dom, kEpotRhs<S, D><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)field, (S *)rhs));
 	return checkLaunch("kEpotRhs");
+}
+extern "C" int phb_nonortho_rhs(const phb_domain *dom, int kind, const void *field, const phb_scalar *sc, const void *Adiag,
+		void *rhs, phb_stream stream) {
+	if (!dom || !field || !rhs || kind < PHB_NONORTHO_VELOCITY || kind > PHB_NONORTHO_PRESSURE ||
+			(kind == PHB_NONORTHO_PRESSURE && !Adiag))
+		return setError(PHB_ERR_ARG, "phb_nonortho_rhs: bad argument");
+	if (kind == PHB_NONORTHO_SCALAR && (!sc || sc->channels < 1 || (sc->nu_count != 0 && sc->nu_count != 1 && sc->nu_count != sc->channels) ||
+			(sc->nu_count > 0 && !sc->nu) || (dom->nfixed > 0 && (!sc->types || !sc->values || !sc->offsets || !sc->statics))))
+		return setError(PHB_ERR_ARG, "phb_nonortho_rhs: bad scalar description");
+	if (dom->ntiles == 0 || dom->dims < 2 || !(dom->nonortho & NO_RHS_BITS)) return PHB_OK;
+	const ScalarView sv = scalarView(kind == PHB_NONORTHO_SCALAR ? sc : nullptr);
+	if (kind == PHB_NONORTHO_PRESSURE)
+		PHB_DISPATCH(dom, (kNonOrthoRhs<S, D, PHB_NONORTHO_PRESSURE><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)field, sv,
+			(const S *)Adiag, (S *)rhs)));
+	else if (kind == PHB_NONORTHO_VELOCITY)
+		PHB_DISPATCH(dom, (kNonOrthoRhs<S, D, PHB_NONORTHO_VELOCITY><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)field, sv,
+			(const S *)Adiag, (S *)rhs)));
+	else
+		PHB_DISPATCH(dom, (kNonOrthoRhs<S, D, PHB_NONORTHO_SCALAR><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)field, sv,
+			(const S *)Adiag, (S *)rhs)));
+	return checkLaunch("kNonOrthoRhs");
 }

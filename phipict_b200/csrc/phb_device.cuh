@@ -47,6 +47,7 @@ struct Dom {
 	int64_t ms, fms, ncells;
 	int nblocks, ninst, ntiles;
 	int scheme = 0; // AdvectionScheme: 0 CENTRAL, 1 LINEAR_UPWIND
+	int nonortho = 0; // non-orthogonal flag bits of the matrix and right-hand-side builders
 	// set by a launcher whose vector and stencil operands all start on 16-byte boundaries and
 	// whose ncells is a multiple of 4: 4-cell groups at aligned indices may use vector loads
 	int vec4 = 0;
@@ -57,7 +58,7 @@ struct Dom {
 		  met((const S *)d.metrics), fmet((const S *)d.face_metrics), fvel((const S *)d.fvel),
 		  fpot((const S *)d.fpot), fcw((const S *)d.fcw), fmask(d.fmask), dt(d.dt), nu(d.nu),
 		  ms(d.metric_stride), fms(d.face_metric_stride), ncells(d.ncells), nblocks(d.nblocks),
-		  ninst(d.ninst), ntiles(d.ntiles), scheme(d.scheme) {}
+		  ninst(d.ninst), ntiles(d.ntiles), scheme(d.scheme), nonortho(d.nonortho) {}
 
 	__device__ __forceinline__ const int32_t *blk(int b) const { return blocks + b * PHB_BREC; }
 	__device__ __forceinline__ const int32_t *fix(int k) const { return fixed + k * PHB_FREC; }
@@ -373,6 +374,36 @@ __device__ __forceinline__ void st4(T *p, int n, bool al, const T (&v)[4]) {
 #pragma unroll
 	for (int i = 0; i < 4; ++i)
 		if (i < n) p[i] = v[i];
+}
+
+// Passive-scalar data of a launch (phb_scalar), passed by value.
+struct ScalarView {
+	int channels, nuCount;
+	const double *nu;
+	const int8_t *types;
+	const void *values;
+	const int64_t *offsets;
+	const int8_t *statics;
+};
+__host__ inline ScalarView scalarView(const phb_scalar *sc) {
+	if (!sc) return ScalarView{0, 0, nullptr, nullptr, nullptr, nullptr, nullptr};
+	return ScalarView{sc->channels, sc->nu_count, sc->nu, sc->types, sc->values, sc->offsets, sc->statics};
+}
+// getViscosity with forPassiveScalar (discretization.cuh:1141-1151): the scalar diffusivity of
+// channel c, or the velocity viscosity of the instance without one
+__device__ __forceinline__ double scalarNu(const ScalarView &sv, int c, double velocityNu) {
+	if (sv.nuCount <= 0) return velocityNu;
+	return sv.nu[sv.nuCount == 1 ? 0 : c];
+}
+// fixed-face scalar value of channel c at face cell fc (getFixedBoundaryData, PASSIVE_SCALAR)
+template <typename S>
+__device__ __forceinline__ S scalarFixed(const ScalarView &sv, const int32_t *FR, int fid, int c, int fc) {
+	const S *v = (const S *)sv.values + sv.offsets[fid];
+	return sv.statics[fid] ? v[c] : v[(int64_t)c * FR[F_FACECELLS] + fc];
+}
+// [inst][channels][cells] index of channel c of cell g
+__device__ __forceinline__ int64_t sidx(const int32_t *B, int64_t g, int c, int channels) {
+	return g + (int64_t)(channels - 1) * B[B_INSTOFF] + (int64_t)c * B[B_INSTN];
 }
 
 } // namespace phb

@@ -774,6 +774,31 @@ class Domain:
     def IsInitialized(self) -> bool:
         return self._prepared
 
+    def hasNonOrthogonalMetrics(self) -> bool:
+        """Whether any cell transform has a cross term Minv[a] . Minv[b] != 0 (a != b), or a
+        fixed-face transform one above 1e-10 of |Minv[a]| |Minv[b]|. The face transforms of a
+        rectilinear block carry rounding-level cross terms (about 1e-14 relative) from their
+        vertex averages; below that bound the cross terms are zero, or change a right-hand
+        side by rounding only, and the step may leave them out. PrepareSolve() must have run."""
+        if not self._prepared:
+            raise RuntimeError("Domain is not initialized. Run domain.PrepareSolve() first.")
+        key = (self._metrics.data_ptr(), self._face_metrics.data_ptr(), self._version)
+        cached = self.__dict__.get("_cross_terms")
+        if cached is not None and cached[0] == key:
+            return cached[1]
+        d = self._dims
+        found = False
+        for m, rtol in ((self._metrics, 0.0), (self._face_metrics, 1e-10)):
+            rows = m[d * d:2 * d * d].view(d, d, -1)
+            for a in range(d):
+                for b in range(a + 1, d):
+                    cross = (rows[a] * rows[b]).sum(0).abs()
+                    bound = rtol * rows[a].norm(dim=0) * rows[b].norm(dim=0)
+                    if bool((cross > bound).any()):
+                        found = True
+        self._cross_terms = (key, found)
+        return found
+
     # --- passive scalar (domain/domain.cpp:618-636) ---
     def hasPassiveScalar(self) -> bool:
         return self._scalar_channels > 0

@@ -141,23 +141,22 @@ class Simulation:
         domain._mixed = self.mixed_precision
         if pressure_use_amg and not self._amg_dtype_ok():
             raise NotImplementedError("the multigrid V-cycle runs in float32: use a float32 domain or mixed_precision=True")
-        if non_orthogonal:
-            self._require_orthogonal()
+        if int(advect_non_ortho_steps) < 0 or int(pressure_non_ortho_steps) < 0:
+            raise ValueError("advect_non_ortho_steps and pressure_non_ortho_steps must not be negative")
+        self.advect_non_ortho_steps = int(advect_non_ortho_steps)
+        self.pressure_non_ortho_steps = int(pressure_non_ortho_steps)
 
     # --- helpers ---------------------------------------------------------------------
-    def _require_orthogonal(self) -> None:
-        """The non-orthogonal terms vanish on grids whose metric is diagonal; phipict_b200
-        assembles the orthogonal discretization only."""
-        d = self.domain.getSpatialDims()
-        M = self.domain._metrics[: d * d].view(d, d, -1)
-        off = M.clone()
-        for i in range(d):
-            off[i, i] = 0
-        scale = M.abs().amax()
-        if float(off.abs().amax()) > 1e-10 * float(scale):
-            raise NotImplementedError(
-                "non-orthogonal grid: phipict_b200 implements the orthogonal PISO step; "
-                "pass non_orthogonal=False to ignore the cross terms as phiPICT's orthogonal path does")
+    # core/piso_simulation.py:1124-1126: the flags of the non-orthogonal mode
+    NON_ORTHO_MODE = backend.NON_ORTHO_CENTER_MATRIX | backend.NON_ORTHO_DIRECT_MATRIX | backend.NON_ORTHO_DIAGONAL_RHS
+
+    def _nonortho_flags(self) -> int:
+        """The non-orthogonal flags of this step: phiPICT's mode when ``non_orthogonal`` is set
+        and the grid has cross terms (without them every non-orthogonal term is exactly zero
+        and the orthogonal step gives the same result), else 0."""
+        if not self.non_orthogonal or self.domain.getSpatialDims() < 2:
+            return 0
+        return self.NON_ORTHO_MODE if self.domain.hasNonOrthogonalMetrics() else 0
 
     def _time_step_tensor(self, time_step: float | torch.Tensor | None) -> torch.Tensor:
         if time_step is None:
@@ -302,23 +301,39 @@ class Simulation:
             if self.convergence_tol is not None:
                 last_vel = d._u_block.clone()
             self._run_hooks(Hook.PRE, local_step=step, time_step=ts)
+            flags = self._nonortho_flags()
             matrix_for_velocity = False
             if self.advect_passive_scalar and d.hasPassiveScalar():
-                matrix_for_velocity = self._advect_scalar(ts, step)
+                matrix_for_velocity = self._advect_scalar(ts, step, flags)
             self._run_hooks(Hook.PRE_VELOCITY_SETUP, local_step=step, time_step=ts)
             if not matrix_for_velocity:
-                backend.SetupAdvectionMatrix(d, ts, 0)
-            backend.SetupAdvectionVelocity(d, ts, 0, False)
-            self._run_hooks(Hook.POST_VELOCITY_SETUP, local_step=step, time_step=ts, no_step=0)
-            self.solve("C", d.velocityRHS, d.velocityResult, use_BiCG=self.advection_use_BiCG,
-                       tol=self.advection_tol, tag="velocity", nrhs=dims)
+                backend.SetupAdvectionMatrix(d, ts, flags)
+            if not flags:
+                backend.SetupAdvectionVelocity(d, ts, 0, False)
+                self._run_hooks(Hook.POST_VELOCITY_SETUP, local_step=step, time_step=ts, no_step=0)
+                self.solve("C", d.velocityRHS, d.velocityResult, use_BiCG=self.advection_use_BiCG,
+                           tol=self.advection_tol, tag="velocity", nrhs=dims)
+            else:
+                # core/piso_simulation.py:3839-3891: the right-hand side carries the cross terms
+                # of the current result, starting from the block velocity; the first solve
+                # starts from zero, later ones from the previous result
+                backend.CopyVelocityResultFromBlocks(d)
+                for no_step in range(self.advect_non_ortho_steps):
+                    backend.SetupAdvectionVelocity(d, ts, flags, False)
+                    self._run_hooks(Hook.POST_VELOCITY_SETUP, local_step=step, time_step=ts, no_step=no_step)
+                    if no_step == 0:
+                        d.velocityResult.zero_()
+                    self.solve("C", d.velocityRHS, d.velocityResult, use_BiCG=self.advection_use_BiCG,
+                               tol=self.advection_tol, tag="velocity", nrhs=dims)
             self._run_hooks(Hook.POST_PREDICTION, local_step=step, time_step=ts)
             for cstep in range(self.corrector_steps):
                 if cstep == 0:
                     # P depends on A and the metrics only, so every corrector of a step would
                     # rebuild the same values (pressure.cu:882-927 rebuilds it each time)
-                    backend.SetupPressureMatrix(d, ts, 0, False)
-                backend.SetupPressureRHS(d, ts, 0, False, False)
+                    backend.SetupPressureMatrix(d, ts, flags, False)
+                # with flags, the divergence carries the cross terms of the pressure result in
+                # place (the previous corrector's), core/piso_simulation.py:3978-4117
+                backend.SetupPressureRHS(d, ts, flags, False, False)
                 self._run_hooks(Hook.POST_PRESSURE_SETUP, local_step=step, time_step=ts)
                 guess = self._pressure_guess.get(cstep) if self.pressure_warm_start else None
                 if guess is not None:
@@ -330,6 +345,16 @@ class Simulation:
                            return_best=self.pressure_return_best_result)
                 if self.normalize_pressure_result:
                     d._subtract_mean(d.pressureResult, 1)
+                for pstep in range(1, self.pressure_non_ortho_steps if flags else 1):
+                    # the divergence of the same HbyA with the cross terms of the new result,
+                    # re-solved from it
+                    backend.SetupPressureRHSdiv(d, ts, flags, False, False)
+                    self._run_hooks(Hook.POST_PRESSURE_SETUP, local_step=step, time_step=ts)
+                    self.solve("P", d.pressureRHSdiv, d.pressureResult, use_BiCG=self.pressure_use_BiCG,
+                               tol=self._pressure_tol_for(cstep), tag=f"pressure{cstep}",
+                               return_best=self.pressure_return_best_result)
+                    if self.normalize_pressure_result:
+                        d._subtract_mean(d.pressureResult, 1)
                 if self.pressure_warm_start:
                     g = self._pressure_guess.get(cstep)
                     if g is None:
@@ -414,7 +439,7 @@ class Simulation:
         self.total_time = start + self.time_step
         return True
 
-    def _advect_scalar(self, ts, step: int) -> bool:
+    def _advect_scalar(self, ts, step: int, flags: int = 0) -> bool:
         """Implicit advection-diffusion of every passive-scalar channel with the velocity of
         the step start (core/piso_simulation.py:3589-3775, orthogonal path): one matrix for
         all channels when their diffusivity and face types agree, else one per channel; a
@@ -429,18 +454,22 @@ class Simulation:
         rhs = d.scalarRHS.view(B, C, -1)
         res = d.scalarResult.view(B, C, -1)
         if not split:
-            backend.SetupAdvectionMatrix(d, ts, 0, forPassiveScalar=True, passiveScalarChannel=0)
-        backend.SetupAdvectionScalar(d, ts, 0)
-        self._run_hooks(Hook.POST_SCALAR_SETUP, local_step=step, time_step=ts, no_step=0)
-        for c in range(C):
-            if split:
-                backend.SetupAdvectionMatrix(d, ts, 0, forPassiveScalar=True, passiveScalarChannel=c)
-            # channel c of every environment as one flat [B][cells] system (launches are
-            # stream-ordered, so a per-channel matrix is consumed before the next overwrites it)
-            b = rhs[:, c].contiguous().view(-1)
-            x = torch.zeros_like(b)
-            self.solve("C", b, x, use_BiCG=self.advection_use_BiCG, tol=self.advection_tol, tag=f"scalar{c}")
-            res[:, c].copy_(x.view(B, -1))
+            backend.SetupAdvectionMatrix(d, ts, flags, forPassiveScalar=True, passiveScalarChannel=0)
+        if flags:
+            # the cross terms start from the block scalar (core/piso_simulation.py:3272-3283)
+            backend.CopyScalarResultFromBlocks(d)
+        for no_step in range(self.advect_non_ortho_steps if flags else 1):
+            backend.SetupAdvectionScalar(d, ts, flags)
+            self._run_hooks(Hook.POST_SCALAR_SETUP, local_step=step, time_step=ts, no_step=no_step)
+            for c in range(C):
+                if split:
+                    backend.SetupAdvectionMatrix(d, ts, flags, forPassiveScalar=True, passiveScalarChannel=c)
+                # channel c of every environment as one flat [B][cells] system (launches are
+                # stream-ordered, so a per-channel matrix is consumed before the next overwrites it)
+                b = rhs[:, c].contiguous().view(-1)
+                x = torch.zeros_like(b) if no_step == 0 else res[:, c].reshape(-1).clone()
+                self.solve("C", b, x, use_BiCG=self.advection_use_BiCG, tol=self.advection_tol, tag=f"scalar{c}")
+                res[:, c].copy_(x.view(B, -1))
         backend.CopyScalarResultToBlocks(d)
         return reuse
 

@@ -32,6 +32,8 @@ def test_version_and_error_text():
     rc = lib.phb_advection_matrix(None, None, None, None, None, None)
     assert rc == -1
     assert b"null" in lib.phb_last_error()
+    rc = lib.phb_nonortho_rhs(None, 0, None, None, None, None, None)
+    assert rc == -1 and b"phb_nonortho_rhs" in lib.phb_last_error()
 
 
 def test_struct_layouts_match_header():
@@ -39,4 +41,5 @@ def test_struct_layouts_match_header():
     assert ct.sizeof(_lib.PhbSolveResult) == 32
     assert _lib.PhbSolve.tol.offset == 32
     assert _lib.PhbDomain.blocks.offset == 48
+    assert _lib.PhbDomain.nonortho.offset == 148 and ct.sizeof(_lib.PhbDomain) == 152
     assert ct.sizeof(_lib.PhbScalar) == 48 and _lib.PhbScalar.nu.offset == 8
