@@ -96,7 +96,7 @@ class Simulation:
             raise ValueError("substeps must be a positive int or 'ADAPTIVE'")
         if differentiable:
             raise NotImplementedError(
-                "the differentiable step is provided by phipict_b200.adjoint.DifferentiableStep")
+                "the differentiable rollout is provided by phipict_b200.adjoint (AdjointMHD, rollout)")
         self.domain = domain
         self.time_step = float(dt)
         self.substeps = substeps if substeps == "ADAPTIVE" else int(substeps)
