@@ -11,6 +11,7 @@
 #include "phb_device.cuh"
 #include "phb_launch.cuh"
 #include "phb_nonortho.cuh"
+#include <initializer_list>
 
 namespace phb {
 
@@ -192,32 +193,58 @@ __device__ __forceinline__ S sourceAt(const Cell &c, const S *__restrict__ src, 
 	return S(0);
 }
 
-// kPISO_build_advection_RHS (advection.cu:800-954), CENTRAL scheme, no pressure gradient
-template <typename S, int D>
-__global__ void __launch_bounds__(PHB_TILE) kAdvectionRhs(Dom<S, D> dom, const S *__restrict__ u, const S *__restrict__ src,
+// kPISO_build_advection_RHS (advection.cu:800-954), no pressure gradient. A thread takes four
+// consecutive cells (Quad): their transforms, velocities and sources load as vectors; the
+// fixed-face sources and the LINEAR_UPWIND correction are added per cell where they apply.
+template <typename S, int D, bool UPW>
+__global__ void __launch_bounds__(PHB_TILE, sizeof(S) == 8 ? 2 : 3) kAdvectionRhs(Dom<S, D> dom, const S *__restrict__ u, const S *__restrict__ src,
 		int srcMode, S *__restrict__ rhs) {
 	__shared__ int32_t sB[PHB_BREC];
-	int l0_, nc_;
-	loadTile<S, D>(dom, sB, l0_, nc_);
-	for (int j_ = 0; j_ < CPT; ++j_) {
-	Cell c;
-	if (!cellAt<D>(sB, l0_, nc_, j_, c)) return;
-	const int inst = c.B[B_INST];
+	int l0, nc;
+	loadTile<S, D>(dom, sB, l0, nc);
+	Quad q;
+	quadAt<D, D>(dom.vec4, sB, l0, nc, q);
+	if (q.n == 0) return;
+	const int inst = sB[B_INST];
 	const S dt = S(dom.dt[inst]);
 	const S nu = S(dom.nu[inst]);
-	const S det = detAt<S, D>(dom, c.mi);
-	S fl[2 * D];
-	if (dom.scheme != 0) faceFluxes<S, D>(dom, c, u, fl);
+	const int64_t mi0 = sB[B_METOFF] + q.l;
+	S det[4];
+	ld4(dom.met + Tr<D>::DET * dom.ms + mi0, q.n, metAligned(dom, q, mi0), det);
+	// cells with a fixed face, or every cell with LINEAR_UPWIND, take the per-cell terms
+	const bool perCell = UPW || !q.fast || q.p[0] == 0 || q.p[0] + 3 == sB[B_NX] - 1;
 #pragma unroll
 	for (int dim = 0; dim < D; ++dim) {
-		const int64_t o = vidx<D>(c.B, c.g, dim);
-		S r = det * u[o] / dt;
-		r += boundarySource<S, D>(dom, c, dim, nu);
-		if (dom.scheme != 0) upwindCorrection<S, D>(c, fl, [&](int64_t g) { return u[vidx<D>(c.B, g, dim)]; }, r);
-		r /= det;
-		r += sourceAt<S, D>(c, src, srcMode, dim);
-		rhs[o] = r;
-	}
+		const int64_t o = vidx<D>(q.B, q.g, dim);
+		S uv[4], r[4];
+		ld4(u + o, q.n, q.al, uv);
+#pragma unroll
+		for (int i = 0; i < 4; ++i) r[i] = det[i] * uv[i] / dt;
+		if (perCell) {
+#pragma unroll
+			for (int i = 0; i < 4; ++i) {
+				if (i >= q.n) break;
+				Cell c;
+				quadCell<D>(q, i, c);
+				r[i] += boundarySource<S, D>(dom, c, dim, nu);
+				if constexpr (UPW) {
+					S fl[2 * D];
+					faceFluxes<S, D>(dom, c, u, fl);
+					upwindCorrection<S, D>(c, fl, [&](int64_t g) { return u[vidx<D>(c.B, g, dim)]; }, r[i]);
+				}
+			}
+		}
+		S sv[4] = {0, 0, 0, 0};
+		if (srcMode == 1) {
+			const S v = src[inst * D + dim];
+#pragma unroll
+			for (int i = 0; i < 4; ++i) sv[i] = v;
+		} else if (srcMode == 2) {
+			ld4(src + o, q.n, q.al, sv);
+		}
+#pragma unroll
+		for (int i = 0; i < 4; ++i) r[i] = r[i] / det[i] + sv[i];
+		st4(rhs + o, q.n, q.al, r);
 	}
 }
 
@@ -378,50 +405,174 @@ __global__ void __launch_bounds__(PHB_TILE) kLaplaceMatrix(Dom<S, D> dom, const 
 	}
 }
 
-// PISO_build_pressure_rhs (pressure.cu:350-521): HbyA = (u/dt - H(u*) + S)/A per component
+// The cold paths of kPressureRhs: H of cell i of a quad off the fast path, resolving each
+// face ...
 template <typename S, int D>
-__global__ void __launch_bounds__(PHB_TILE) kPressureRhs(Dom<S, D> dom, const S *__restrict__ C, const S *__restrict__ Adiag,
+struct CompSums {
+	S v[D];
+};
+template <typename S, int D>
+__device__ __forceinline__ CompSums<S, D> hbyaSlowH(const Dom<S, D> &dom, const Quad &q, int i, const S *__restrict__ C,
+		const S *__restrict__ ustar) {
+	const int64_t N = dom.ncells;
+	const int64_t cs = (int64_t)q.B[B_INSTN];
+	Cell c;
+	quadCell<D>(q, i, c);
+	const int64_t comp = vidx<D>(c.B, c.g, 0) - c.g;
+	CompSums<S, D> h;
+#pragma unroll
+	for (int d = 0; d < D; ++d) h.v[d] = 0;
+	for (int f = 0; f < 2 * D; ++f) {
+		const int64_t n = neighborIndex<S, D>(dom, c, f);
+		if (n < 0 || n == c.g) continue;
+		const S cvf = C[(f + 1) * N + c.g];
+#pragma unroll
+		for (int d = 0; d < D; ++d) h.v[d] = fma(cvf, ustar[n + comp + d * cs], h.v[d]);
+	}
+	return h;
+}
+// ... and the source of cell i with its fixed faces and the deferred LINEAR_UPWIND correction
+template <typename S, int D, bool UPW>
+__device__ __forceinline__ S hbyaCellSource(const Dom<S, D> &dom, const Quad &q, int i, int dim, S nu, S det, S src, const S *__restrict__ u) {
+	Cell c;
+	quadCell<D>(q, i, c);
+	S Ssum = boundarySource<S, D>(dom, c, dim, nu);
+	Ssum /= det;
+	Ssum += src;
+	if constexpr (UPW) {
+		// HbyA repeats the predictor's deferred correction (pressure.cu:474-515)
+		S fl[2 * D];
+		faceFluxes<S, D>(dom, c, u, fl);
+		S corr = 0;
+		upwindCorrection<S, D>(c, fl, [&](int64_t g) { return u[vidx<D>(c.B, g, dim)]; }, corr);
+		Ssum += corr / det;
+	}
+	return Ssum;
+}
+
+// Out-of-line calls of the two: in 3D the inlined cold paths make the kernel large enough to
+// stall on instruction fetch (measured: HbyA on 256^3 at 0.38 of HBM out of line against 0.34
+// inline), in 2D inlining is faster (0.66 against 0.55 on 4096^2).
+template <typename S, int D>
+__device__ __noinline__ CompSums<S, D> hbyaSlowHCall(const Dom<S, D> &dom, const Quad &q, int i, const S *__restrict__ C,
+		const S *__restrict__ ustar) {
+	return hbyaSlowH<S, D>(dom, q, i, C, ustar);
+}
+template <typename S, int D, bool UPW>
+__device__ __noinline__ S hbyaCellSourceCall(const Dom<S, D> &dom, const Quad &q, int i, int dim, S nu, S det, S src,
+		const S *__restrict__ u) {
+	return hbyaCellSource<S, D, UPW>(dom, q, i, dim, nu, det, src, u);
+}
+
+// PISO_build_pressure_rhs (pressure.cu:350-521): HbyA = (u/dt - H(u*) + S)/A per component,
+// four consecutive cells per thread. H sums the stencil's face slots in face order for every
+// component at once, so that a slot's four values are loaded once and dropped.
+template <typename S, int D, bool UPW>
+__global__ void __launch_bounds__(PHB_TILE, sizeof(S) == 8 ? 2 : 3) kPressureRhs(Dom<S, D> dom, const S *__restrict__ C, const S *__restrict__ Adiag,
 		const S *__restrict__ u, const S *__restrict__ ustar, const S *__restrict__ src, int srcMode, S *__restrict__ hbya) {
 	__shared__ int32_t sB[PHB_BREC];
-	int l0_, nc_;
-	loadTile<S, D>(dom, sB, l0_, nc_);
-	for (int j_ = 0; j_ < CPT; ++j_) {
-	Cell c;
-	if (!cellAt<D>(sB, l0_, nc_, j_, c)) return;
-	const int inst = c.B[B_INST];
+	int l0, nc;
+	loadTile<S, D>(dom, sB, l0, nc);
+	Quad q;
+	quadAt<D, D>(dom.vec4, sB, l0, nc, q);
+	if (q.n == 0) return;
+	const int inst = sB[B_INST];
 	const S dt = S(dom.dt[inst]);
 	const S nu = S(dom.nu[inst]);
-	const S rDiag = S(1) / Adiag[c.g];
-	const S det = detAt<S, D>(dom, c.mi);
 	const int64_t N = dom.ncells;
-	int64_t nb[2 * D];
-	S cv[2 * D];
+	const int64_t o0 = vidx<D>(q.B, q.g, 0);
+	const int64_t cs = (int64_t)q.B[B_INSTN]; // component stride
+	S H[D][4];
 #pragma unroll
-	for (int f = 0; f < 2 * D; ++f) {
-		nb[f] = neighborIndex<S, D>(dom, c, f);
-		cv[f] = C[(f + 1) * N + c.g];
+	for (int d = 0; d < D; ++d)
+#pragma unroll
+		for (int i = 0; i < 4; ++i) H[d][i] = 0;
+	if (q.fast) {
+		int64_t gW = q.g - 1, gE = q.g + 4;
+		if (q.p[0] == 0 || q.p[0] + 3 == q.B[B_NX] - 1) {
+			Cell c;
+			c.B = q.B;
+			c.p[1] = q.p[1];
+			c.p[2] = q.p[2];
+			if (q.p[0] == 0) {
+				c.p[0] = 0;
+				c.g = (int)q.g;
+				gW = neighborIndex<S, D>(dom, c, 0);
+			}
+			if (q.p[0] + 3 == q.B[B_NX] - 1) {
+				c.p[0] = q.p[0] + 3;
+				c.g = (int)(q.g + 3);
+				gE = neighborIndex<S, D>(dom, c, 1);
+			}
+		}
+		const int64_t comp = o0 - q.g;
+#pragma unroll
+		for (int f = 0; f < 2 * D; ++f) {
+			S cv[4];
+			ld4(C + (f + 1) * N + q.g, 4, q.al, cv);
+#pragma unroll
+			for (int d = 0; d < D; ++d) {
+				if (f < 2) {
+					S own[4];
+					ld4(ustar + o0 + d * cs, 4, q.al, own);
+					if (f == 0) {
+						if (gW >= 0) H[d][0] = fma(cv[0], ustar[gW + comp + d * cs], H[d][0]);
+#pragma unroll
+						for (int i = 1; i < 4; ++i) H[d][i] = fma(cv[i], own[i - 1], H[d][i]);
+					} else {
+#pragma unroll
+						for (int i = 0; i < 3; ++i) H[d][i] = fma(cv[i], own[i + 1], H[d][i]);
+						if (gE >= 0) H[d][3] = fma(cv[3], ustar[gE + comp + d * cs], H[d][3]);
+					}
+				} else {
+					const int64_t off = f == 2 ? -(int64_t)q.sy : f == 3 ? (int64_t)q.sy : f == 4 ? -(int64_t)q.sz : (int64_t)q.sz;
+					S v[4];
+					ld4(ustar + o0 + d * cs + off, 4, f < 4 ? q.alY : q.alZ, v);
+#pragma unroll
+					for (int i = 0; i < 4; ++i) H[d][i] = fma(cv[i], v[i], H[d][i]);
+				}
+			}
+		}
+	} else {
+#pragma unroll
+		for (int i = 0; i < 4; ++i) {
+			if (i >= q.n) break;
+			const CompSums<S, D> h = D > 2 ? hbyaSlowHCall<S, D>(dom, q, i, C, ustar) : hbyaSlowH<S, D>(dom, q, i, C, ustar);
+#pragma unroll
+			for (int d = 0; d < D; ++d) H[d][i] = h.v[d];
+		}
 	}
-	S fl[2 * D];
-	if (dom.scheme != 0) faceFluxes<S, D>(dom, c, u, fl);
+	const int64_t mi0 = sB[B_METOFF] + q.l;
+	S a[4], det[4];
+	ld4(Adiag + q.g, q.n, q.al, a);
+	ld4(dom.met + Tr<D>::DET * dom.ms + mi0, q.n, metAligned(dom, q, mi0), det);
+	const bool perCell = UPW || !q.fast || q.p[0] == 0 || q.p[0] + 3 == sB[B_NX] - 1;
 #pragma unroll
 	for (int dim = 0; dim < D; ++dim) {
-		const int64_t o = vidx<D>(c.B, c.g, dim);
-		const S velOld = u[o] / dt;
-		S H = 0;
+		const int64_t o = o0 + dim * cs;
+		S uv[4], sv[4] = {0, 0, 0, 0};
+		ld4(u + o, q.n, q.al, uv);
+		if (srcMode == 1) {
+			const S v = src[inst * D + dim];
 #pragma unroll
-		for (int f = 0; f < 2 * D; ++f)
-			if (nb[f] >= 0 && nb[f] != c.g) H += cv[f] * ustar[vidx<D>(c.B, nb[f], dim)];
-		S Ssum = boundarySource<S, D>(dom, c, dim, nu);
-		Ssum /= det;
-		Ssum += sourceAt<S, D>(c, src, srcMode, dim);
-		if (dom.scheme != 0) {
-			// HbyA repeats the predictor's deferred correction (pressure.cu:474-515)
-			S corr = 0;
-			upwindCorrection<S, D>(c, fl, [&](int64_t g) { return u[vidx<D>(c.B, g, dim)]; }, corr);
-			Ssum += corr / det;
+			for (int i = 0; i < 4; ++i) sv[i] = v;
+		} else if (srcMode == 2) {
+			ld4(src + o, q.n, q.al, sv);
 		}
-		hbya[o] = rDiag * (velOld - H + Ssum);
-	}
+		S out[4];
+#pragma unroll
+		for (int i = 0; i < 4; ++i) {
+			S Ssum = 0;
+			if (perCell && i < q.n) {
+				Ssum = D > 2 ? hbyaCellSourceCall<S, D, UPW>(dom, q, i, dim, nu, det[i], sv[i], u)
+				             : hbyaCellSource<S, D, UPW>(dom, q, i, dim, nu, det[i], sv[i], u);
+			} else {
+				Ssum /= det[i];
+				Ssum += sv[i];
+			}
+			out[i] = (S(1) / a[i]) * (uv[i] / dt - H[dim][i] + Ssum);
+		}
+		st4(hbya + o, q.n, q.al, out);
 	}
 }
 
@@ -729,6 +880,20 @@ using namespace phb;
 
 #define PHB_TILES(DOM) dim3((DOM)->ntiles), dim3(PHB_TILE), 0, (cudaStream_t)stream
 
+// The device view of a launch whose quad kernels may use vector loads: every field operand
+// on a 16-byte boundary with a cell count that keeps the component rows aligned (vec4), and
+// the metric rows aligned (metal).
+template <typename S, int D>
+static Dom<S, D> quadView(const phb_domain *dom, std::initializer_list<const void *> fields) {
+	Dom<S, D> dm(*dom);
+	int ok = dom->ncells % 4 == 0;
+	for (const void *p : fields)
+		if (p && ((uintptr_t)p & 15)) ok = 0;
+	dm.vec4 = ok;
+	dm.metal = ((uintptr_t)dom->metrics & 15) == 0 && dom->metric_stride % 4 == 0;
+	return dm;
+}
+
 extern "C" int phb_advection_matrix(const phb_domain *dom, const void *u, void *C, void *Adiag, float *C_lo, phb_stream stream) {
 	if (!dom || !u || !C || !Adiag) return setError(PHB_ERR_ARG, "phb_advection_matrix: null argument");
 	if (dom->ntiles == 0) return PHB_OK;
@@ -768,7 +933,12 @@ extern "C" int phb_scalar_rhs(const phb_domain *dom, const void *phi, const void
 extern "C" int phb_advection_rhs(const phb_domain *dom, const void *u, const void *src, int src_mode, void *rhs, phb_stream stream) {
 	if (!dom || !u || !rhs || (src_mode != 0 && !src) || src_mode < 0 || src_mode > 2) return setError(PHB_ERR_ARG, "phb_advection_rhs: bad argument");
 	if (dom->ntiles == 0) return PHB_OK;
-	PHB_DISPATCH(dom, kAdvectionRhs<S, D><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)u, (const S *)src, src_mode, (S *)rhs));
+	if (dom->scheme != 0)
+		PHB_DISPATCH(dom, (kAdvectionRhs<S, D, true><<<PHB_TILES(dom)>>>(quadView<S, D>(dom, {u, src, rhs}), (const S *)u, (const S *)src,
+			src_mode, (S *)rhs)));
+	else
+		PHB_DISPATCH(dom, (kAdvectionRhs<S, D, false><<<PHB_TILES(dom)>>>(quadView<S, D>(dom, {u, src, rhs}), (const S *)u, (const S *)src,
+			src_mode, (S *)rhs)));
 	return checkLaunch("kAdvectionRhs");
 }
 extern "C" int phb_pressure_matrix(const phb_domain *dom, const void *Adiag, void *P, float *P_lo, phb_stream stream) {
@@ -792,8 +962,12 @@ extern "C" int phb_pressure_rhs(const phb_domain *dom, const void *C, const void
 	if (!dom || !C || !Adiag || !u || !ustar || !hbya || (src_mode != 0 && !src) || src_mode < 0 || src_mode > 2)
 		return setError(PHB_ERR_ARG, "phb_pressure_rhs: bad argument");
 	if (dom->ntiles == 0) return PHB_OK;
-	PHB_DISPATCH(dom, kPressureRhs<S, D><<<PHB_TILES(dom)>>>(Dom<S, D>(*dom), (const S *)C, (const S *)Adiag, (const S *)u,
-		(const S *)ustar, (const S *)src, src_mode, (S *)hbya));
+	if (dom->scheme != 0)
+		PHB_DISPATCH(dom, (kPressureRhs<S, D, true><<<PHB_TILES(dom)>>>(quadView<S, D>(dom, {C, Adiag, u, ustar, src, hbya}),
+			(const S *)C, (const S *)Adiag, (const S *)u, (const S *)ustar, (const S *)src, src_mode, (S *)hbya)));
+	else
+		PHB_DISPATCH(dom, (kPressureRhs<S, D, false><<<PHB_TILES(dom)>>>(quadView<S, D>(dom, {C, Adiag, u, ustar, src, hbya}),
+			(const S *)C, (const S *)Adiag, (const S *)u, (const S *)ustar, (const S *)src, src_mode, (S *)hbya)));
 	return checkLaunch("kPressureRhs");
 }
 extern "C" int phb_divergence(const phb_domain *dom, const void *field, void *div, phb_stream stream) {

@@ -51,6 +51,8 @@ struct Dom {
 	// set by a launcher whose vector and stencil operands all start on 16-byte boundaries and
 	// whose ncells is a multiple of 4: 4-cell groups at aligned indices may use vector loads
 	int vec4 = 0;
+	// set by a launcher when the metric rows start on 16-byte boundaries (array and stride)
+	int metal = 0;
 
 	Dom() = default;
 	__host__ Dom(const phb_domain &d)
@@ -325,6 +327,12 @@ __device__ __forceinline__ void quadAt(int vec4, const int32_t *sB, int l0, int 
 	q.al = al;
 	q.alY = al && (nx & 3) == 0;
 	q.alZ = al && (q.sz & 3) == 0;
+}
+
+// Vector loads of the quad's four cell transforms (metric index mi0 of its first cell).
+template <typename S, int D>
+__device__ __forceinline__ bool metAligned(const Dom<S, D> &dom, const Quad &q, int64_t mi0) {
+	return dom.metal && q.n == 4 && (mi0 & 3) == 0;
 }
 
 // The i-th cell of a quad (i < q.n) as a Cell.
