@@ -163,3 +163,57 @@ def test_orthogonal_step_on_a_curvilinear_grid(cuda):
         ref.step()
     torch.cuda.synchronize()
     assert rel(host(dom._u_block).reshape(-1), ref.u) < 1e-9
+
+
+def test_nonortho_mhd_steps_match_the_oracle(cuda):
+    """The MHD step on the curvilinear duct: non-orthogonal momentum and pressure, the
+    potential with its own flags at phiPICT's default 0."""
+    dom = skewed_duct_3d(6, 5, 4, 2)
+    seeded_state(dom, 9, scale=0.1)
+    dom.PrepareSolve()
+    od = OracleDomain(dom)
+    tol = pb.SolverTolerance(rtol=1e-12, atol=1e-14)
+    N, e_b = 2.0, [0.0, 1.0, 0.0]
+    ref = OracleSim(od, host(dom._u_block).reshape(-1), 0.01, float(dom.viscosity[0]), advection_tol=tol,
+                    pressure_tol=tol, mhd=dict(stuart=N, e_b=e_b, singular=True, potential_tol=tol),
+                    scalar=dict(phi=host(dom._phi_block).reshape(-1), nu=None), nonortho_flags=MODE, pressure_bicg=True)
+    sim = pb.MHDSimulation(dom, 0.01, torch.tensor(N), torch.tensor(e_b, dtype=torch.float64), advection_tol=tol,
+                           pressure_tol=tol, potential_tol=tol, pressure_use_BiCG=True)
+    for _ in range(3):
+        assert sim.single_step(), sim.last_error
+        ref.step()
+    torch.cuda.synchronize()
+    assert rel(host(dom._u_block).reshape(-1), ref.u) < 1e-8
+    assert rel(host(dom.epotResult), ref.phi) < 1e-7
+
+
+def test_nonortho_batch_equals_instances_alone(cuda):
+    """Curvilinear domains of different grids and viscosities batched into one descriptor step
+    exactly as they do alone."""
+    def members():
+        out = []
+        for k, (nx, ny, nu, shear) in enumerate(((12, 10, 0.02, 0.35), (14, 8, 0.03, 0.2))):
+            dom = skewed_channel_2d(nx, ny, nu=nu, shear=shear, channels=0)
+            seeded_state(dom, 60 + k, scale=0.2)
+            dom.PrepareSolve()
+            out.append(dom)
+        return out
+
+    tol = pb.SolverTolerance(rtol=1e-12, atol=1e-14)
+    kw = dict(advection_tol=tol, pressure_tol=tol, pressure_use_BiCG=True)
+    alone = []
+    for dom in members():
+        sim = pb.Simulation(dom, 0.01, **kw)
+        for _ in range(3):
+            assert sim.single_step(), sim.last_error
+        alone.append((dom._u_block.clone(), dom.pressureResult.clone()))
+    ms = members()
+    batch = pb.DomainBatch(ms)
+    assert batch.hasNonOrthogonalMetrics()
+    sim = pb.Simulation(batch, 0.01, **kw)
+    for _ in range(3):
+        assert sim.single_step(), sim.last_error
+    batch.scatter()
+    for k, dom in enumerate(ms):
+        assert torch.equal(dom._u_block, alone[k][0]), k
+        assert torch.equal(dom.pressureResult, alone[k][1]), k
