@@ -587,9 +587,10 @@ def run_serve(args, rank, world, local):
 SWEEP_GRIDS = [(3, 128), (3, 192), (3, 256), (2, 2048), (2, 4096)]
 
 
-def make_box(device, dims, n, Re=1000.0, seed=0):
+def make_box(device, dims, n, Re=1000.0, seed=0, shear=0.0):
     """One block of n^dims cells on [0, 2] x [-1, 1]^(dims-1): periodic in x, no-slip
-    insulating walls elsewhere, u = (1, 0, 0) plus seeded 1e-2 noise."""
+    insulating walls elsewhere, u = (1, 0, 0) plus seeded 1e-2 noise. shear > 0 shears the
+    vertices, x += shear * y (a curvilinear grid with metric cross terms everywhere)."""
     import phipict_b200 as pb
     from phipict_b200.grid import rectilinear_vertices
 
@@ -597,7 +598,10 @@ def make_box(device, dims, n, Re=1000.0, seed=0):
     dom = pb.Domain(dims, torch.tensor([1.0 / Re]), name="box", device=device, dtype=dtype)
     xs = np.linspace(0.0, 2.0, n + 1)
     ys = np.linspace(-1.0, 1.0, n + 1)
-    b = dom.CreateBlock(vertexCoordinates=rectilinear_vertices(xs, ys, *([ys] if dims == 3 else []), dtype=dtype), name="box")
+    v = rectilinear_vertices(xs, ys, *([ys] if dims == 3 else []), dtype=dtype)
+    if shear:
+        v[0, 0] = v[0, 0] + shear * v[0, 1]
+    b = dom.CreateBlock(vertexCoordinates=v, name="box")
     for f in ("-y", "+y") + (("-z", "+z") if dims == 3 else ()):
         b.CloseBoundary(f)
     b.MakePeriodic("x")
@@ -646,7 +650,7 @@ def run_sweep(args, rank, world, local):
     clocks = ClockSampler(local)
     clocks.start()
     for dims, n in grids:
-        dom = make_box(device, dims, n)
+        dom = make_box(device, dims, n, shear=args.sweep_shear)
         dom.PrepareSolve()
         tol = pb.SolverTolerance(rtol=1e-6)
         sim = pb.MHDSimulation(dom, 1e-3, torch.tensor(10.0), torch.tensor([0.0, 1.0, 0.0], dtype=torch.float64),
@@ -676,6 +680,21 @@ def run_sweep(args, rank, world, local):
                                                  None, dom._src.data_ptr(), 1, S),
         }
         abytes = assembly_bytes(dims)
+        if args.sweep_shear:
+            # the same calls with phiPICT's non-orthogonal mode (cross terms in the matrices,
+            # the explicit corner terms of the current results on the right-hand sides); their
+            # fractions use the orthogonal kernels' byte counts, so they read as the cost of the
+            # cross terms relative to the orthogonal assembly
+            mode = backend.NON_ORTHO_CENTER_MATRIX | backend.NON_ORTHO_DIRECT_MATRIX | backend.NON_ORTHO_DIAGONAL_RHS
+            kern.update({
+                "advection_matrix (non-orthogonal)": lambda: backend.SetupAdvectionMatrix(dom, ts, mode),
+                "advection_rhs (non-orthogonal)": lambda: backend.SetupAdvectionVelocity(dom, ts, mode, False),
+                "pressure_matrix (non-orthogonal)": lambda: backend.SetupPressureMatrix(dom, ts, mode, False),
+                "divergence (non-orthogonal)": lambda: backend.SetupPressureRHSdiv(dom, ts, mode),
+            })
+            for k in list(kern):
+                if k.endswith("(non-orthogonal)"):
+                    abytes[k] = abytes[k.split(" ")[0]]
 
         def timed(fn):
             ms = []
@@ -738,7 +757,8 @@ def run_sweep(args, rank, world, local):
     return dict(metric="HBM roofline fraction (kernels of the step, grids >> L2)", value=round(min(r["frac"] for r in big), 3) if big else None,
                 unit="fraction of measured HBM GB/s", n_gpus=world, steps=reps, warmup=args.warmup, higher_is_better=True,
                 scaling="weak", vs_baseline=None, dtype="f64 fields, f32 Krylov", data="synthetic (seeded)",
-                config={"workload": "roofline sweep: " + ", ".join(f"{n}^{d}" for d, n in grids) + "; L2 flushed before every launch",
+                config={"workload": "roofline sweep: " + ", ".join(f"{n}^{d}" for d, n in grids)
+                        + (f" sheared x += {args.sweep_shear} y" if args.sweep_shear else "") + "; L2 flushed before every launch",
                         "parallelism": f"replicas x{world}"},
                 clocks=clk, peak={"hbm_gbs": peak, "source": pk.get("source")}, sweep=rows, gpu_launches=None)
 
@@ -839,6 +859,8 @@ def main():
     ap.add_argument("--fd-directions", type=int, default=8, help="adjoint: random directions of the FD check")
     ap.add_argument("--fd-eps", type=float, default=3e-3, help="adjoint: central-difference step")
     ap.add_argument("--sweep-grids", default=None, help="sweep: grids as dims x n, e.g. 3x128,2x2048")
+    ap.add_argument("--sweep-shear", type=float, default=0.0,
+                    help="sweep: shear the grids (x += shear y) and also time the non-orthogonal assembly")
     ap.add_argument("--sweep-iterations", type=int, default=30, help="sweep: Krylov iterations per timed solve")
     ap.add_argument("--sweep-modes", default="persistent", help="sweep: solver launch modes (persistent, graph, host)")
     args = ap.parse_args()

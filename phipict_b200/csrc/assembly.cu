@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(PHB_TILE) kAdvectionMatrix(Dom<S, D> dom, cons
 			if constexpr (NO) {
 				const S a[2] = {ia[f][0] * (SCALAR ? nu : S(1)), ia[f][1] * (SCALAR ? nu : S(1))};
 				rv[0] = diag;
-				nonOrthoMatrixFace<S, D>(dom, F, bp, f, dom.nonortho, -1, false, a, rv);
+				nonOrthoMatrixFace<S, D>(dom, F, bp, f, dom.nonortho, -1, false, a, rv, innerCell<D>(c.B, c.p));
 				diag = rv[0];
 			}
 		} else {
@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(PHB_TILE) kLaplaceMatrix(Dom<S, D> dom, const 
 			has[f + 1] = true;
 			if constexpr (NO) {
 				const NField<S> F{NF_MARK, 0, nullptr, ScalarView{}};
-				nonOrthoMatrixFace<S, D>(dom, F, bp, f, dom.nonortho, 1, true, ia[f], rv);
+				nonOrthoMatrixFace<S, D>(dom, F, bp, f, dom.nonortho, 1, true, ia[f], rv, innerCell<D>(c.B, c.p));
 			}
 		} else if (EPOT) {
 			const int32_t *FR = dom.fix(fRec(c.B, f)[5]);
@@ -843,6 +843,32 @@ __global__ void __launch_bounds__(PHB_TILE) kNonOrthoRhs(Dom<S, D> dom, const S 
 	if (!cellAt<D>(sB, l0_, nc_, j_, c)) return;
 	const BPos bp{blk, {c.p[0], c.p[1], c.p[2]}};
 	const int inst = c.B[B_INST];
+	if (innerCell<D>(c.B, c.p)) {
+		// away from the block's faces: all components at once from the fixed strides
+		if constexpr (KIND == PHB_NONORTHO_PRESSURE) {
+			S o[1];
+			nonOrthoRhsInner<S, D, 1>(dom, field, 0, 0, c.B, c.p, dom.nonortho, [&](int64_t g) { return S(1) / Adiag[g]; }, o);
+			rhs[c.g] += o[0];
+		} else if constexpr (KIND == PHB_NONORTHO_VELOCITY) {
+			const S nu = S(dom.nu[inst]);
+			const S det = detAt<S, D>(dom, c.mi);
+			S o[D];
+			nonOrthoRhsInner<S, D, D>(dom, field, vidx<D>(c.B, 0, 0), c.B[B_INSTN], c.B, c.p, dom.nonortho,
+				[&](int64_t) { return nu; }, o);
+#pragma unroll
+			for (int w = 0; w < D; ++w) rhs[vidx<D>(c.B, c.g, w)] -= o[w] / det;
+		} else {
+			const S det = detAt<S, D>(dom, c.mi);
+			for (int ch = 0; ch < sv.channels; ++ch) {
+				S o[1];
+				nonOrthoRhsInner<S, D, 1>(dom, field, sidx(c.B, 0, ch, sv.channels), 0, c.B, c.p, dom.nonortho,
+					[&](int64_t) { return S(1); }, o);
+				const S nuc = S(scalarNu(sv, ch, dom.nu[inst]));
+				rhs[sidx(c.B, c.g, ch, sv.channels)] -= o[0] * nuc / det;
+			}
+		}
+		continue;
+	}
 	if constexpr (KIND == PHB_NONORTHO_PRESSURE) {
 		const NField<S> F{NF_PRESSURE, 0, field, sv};
 		rhs[c.g] += nonOrthoRhs<S, D>(dom, F, bp, dom.nonortho, [&](int64_t g) { return S(1) / Adiag[g]; }, S(1));

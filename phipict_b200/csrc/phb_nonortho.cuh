@@ -124,11 +124,36 @@ struct CornerValue {
 // the diagonal cell (four cells); three blocks meeting at a corner give three.
 template <typename S, int D>
 __device__ CornerValue<S> cornerWalk(const Dom<S, D> &dom, const NField<S> &F, const BPos &start, int dir1, int dir2, bool depth1) {
+	{
+		// a cell at least one cell away from every face of its block: the walks reach the two
+		// face neighbours at depth 1 and meet at the diagonal cell at depth 2 (four cells), with
+		// the data summed in the walk's order
+		const int32_t *B = dom.blk(start.b);
+		bool inner = true;
+#pragma unroll
+		for (int a = 0; a < D; ++a) inner = inner && start.p[a] >= 1 && start.p[a] <= B[B_NX + a] - 2;
+		if (inner) {
+			BPos n1 = start, n2 = start;
+			n1.p[dir1 >> 1] += (dir1 & 1) ? 1 : -1;
+			n2.p[dir2 >> 1] += (dir2 & 1) ? 1 : -1;
+			BPos dg = n1;
+			dg.p[dir2 >> 1] += (dir2 & 1) ? 1 : -1;
+			S data = 0;
+			if (depth1) {
+				data += nfCell<S, D>(dom, F, n1);
+				data += nfCell<S, D>(dom, F, n2);
+			}
+			data += nfCell<S, D>(dom, F, dg);
+			return {data / S(4), 4, false};
+		}
+	}
 	BPos w[2] = {start, start};
 	int d1[2] = {dir1, dir2}, d2[2] = {dir2, dir1};
 	S data = 0;
 	int num = 1;
+#pragma unroll
 	for (int depth = 1; depth <= 2; ++depth) {
+#pragma unroll
 		for (int d = 0; d < 2; ++d) {
 			const int32_t *B = dom.blk(w[d].b);
 			const int a = d1[d], t2 = d2[d];
@@ -235,9 +260,11 @@ __device__ __forceinline__ void nonOrthoInterp(const Dom<S, D> &dom, const BPos 
 // for the pressure) turns into a one-sided difference from the other side; a corner on a
 // fixed value face adds nothing here. sgn: +1 as the pressure matrix adds them, -1 as the
 // advection matrix does. a[i-1]: the face's cross coefficient with axis (f/2 + i) % d.
+// inner: the cell is at least one cell away from every face of its block, where every corner
+// interpolates four cells (cornerWalk's first case) and no walk is needed.
 template <typename S, int D>
 __device__ void nonOrthoMatrixFace(const Dom<S, D> &dom, const NField<S> &F, const BPos &c, int f, int flags, int sgn, bool pressure,
-		const S *a, S *rv) {
+		const S *a, S *rv, bool inner = false) {
 	const bool center = flags & NO_CENTER_MATRIX, direct = flags & NO_DIRECT_MATRIX;
 	const int faceSign = (f & 1) ? 1 : -1;
 	for (int i = 1; i < D; ++i) {
@@ -246,7 +273,7 @@ __device__ void nonOrthoMatrixFace(const Dom<S, D> &dom, const NField<S> &F, con
 		for (int tUp = 0; tUp < 2; ++tUp) {
 			const int tFace = 2 * tAxis + tUp;
 			const int tSign = tUp ? 1 : -1;
-			const CornerValue<S> cv = cornerWalk<S, D>(dom, F, c, f, tFace, false);
+			const CornerValue<S> cv = inner ? CornerValue<S>{S(0), 4, false} : cornerWalk<S, D>(dom, F, c, f, tFace, false);
 			if (cv.numCells < 1) {
 				if (!(pressure || cv.neumann)) continue;
 				const S coef = S(faceSign * tSign) * a[i - 1] * S(0.25);
@@ -256,6 +283,63 @@ __device__ void nonOrthoMatrixFace(const Dom<S, D> &dom, const NField<S> &F, con
 				const S coef = S(faceSign * tSign) * a[i - 1] * S(1.0 / double(cv.numCells));
 				if (center) rv[0] += S(sgn) * coef;
 				if (direct) { rv[f + 1] += S(sgn) * coef; rv[tFace + 1] += S(sgn) * coef; }
+			}
+		}
+	}
+}
+
+// Whether cell p of block B is at least one cell away from every face of its block.
+template <int D>
+__device__ __forceinline__ bool innerCell(const int32_t *B, const int *p) {
+	bool inner = true;
+#pragma unroll
+	for (int a = 0; a < D; ++a) inner = inner && p[a] >= 1 && p[a] <= B[B_NX + a] - 2;
+	return inner;
+}
+
+// nonOrthoRhs for an inner cell (innerCell), all NC components of a field at once: the
+// neighbours and corner cells lie in the block at fixed strides, every corner interpolates
+// four cells, and the face coefficients are computed once for all components. Component w's
+// value at cell index h is cells[h + base + w * cstride]; out[w] receives its sum in the
+// order of nonOrthoRhs (faces, tangential axes, corners).
+template <typename S, int D, int NC, typename RA>
+__device__ __forceinline__ void nonOrthoRhsInner(const Dom<S, D> &dom, const S *__restrict__ cells, int64_t base, int64_t cstride,
+		const int32_t *B, const int *p, int flags, RA ra, S (&out)[NC]) {
+	const bool direct = flags & NO_DIRECT_RHS;
+	const int64_t sy = B[B_NX], sz = (int64_t)B[B_NX] * B[B_NY];
+	auto stride = [&](int a) -> int64_t { return a == 0 ? 1 : a == 1 ? sy : sz; };
+	const int64_t g = cellIndex(B, p), mi = metricIndex(B, p);
+	const S raP = ra(g);
+#pragma unroll
+	for (int w = 0; w < NC; ++w) out[w] = 0;
+	// faces one at a time (not unrolled): every face's loads stay in flight together without
+	// holding all faces' values in registers
+#pragma unroll 1
+	for (int f = 0; f < 2 * D; ++f) {
+		const int ax = f >> 1;
+		const int faceSign = (f & 1) ? 1 : -1;
+		const int64_t sN = (f & 1) ? stride(ax) : -stride(ax);
+		const S raN = ra(g + sN);
+#pragma unroll
+		for (int i = 1; i < D; ++i) {
+			const int tAxis = (ax + i) % D;
+			const S faceAlpha = (lapCross<S, D>(dom, mi, ax, tAxis) * raP + lapCross<S, D>(dom, mi + sN, tAxis, ax) * raN) * S(0.5);
+#pragma unroll
+			for (int w = 0; w < NC; ++w) {
+				const S *cw = cells + base + w * cstride;
+				S tGrad = 0;
+#pragma unroll
+				for (int tUp = 0; tUp < 2; ++tUp) {
+					const int64_t sT = tUp ? stride(tAxis) : -stride(tAxis);
+					S data = 0;
+					if (direct) {
+						data += __ldg(cw + g + sN);
+						data += __ldg(cw + g + sT);
+					}
+					data += __ldg(cw + g + sN + sT);
+					tGrad += S(tUp ? 1 : -1) * (data / S(4));
+				}
+				out[w] -= S(faceSign) * faceAlpha * tGrad;
 			}
 		}
 	}
