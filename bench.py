@@ -148,10 +148,10 @@ def algorithmic_pcg_bytes(dims: int, levels: list[int], dense_doubles: int = 0) 
     return algorithmic_cg_bytes(dims, 4, 4) + cyc + 8.0 * dense_doubles / levels[0]
 
 
-# DRAM bytes per preconditioned CG iteration on the duct workload, from the full ncu capture
-# of one persistent launch (25.74 MB read + 0.44 MB written in a 24-iteration inner solve,
-# profiles/kCgPersistent_pcg_duct3d_full.md): the working set is L2-resident
-PCG_DRAM_BYTES_PER_ITERATION_DUCT3D = (25.74e6 + 0.44e6) / 24
+# DRAM bytes per preconditioned CG iteration on the duct workload, from a full ncu capture of
+# one persistent launch (the first inner solve of the timed step: 25.81 MB read + 0.65 MB
+# written in a 24-iteration solve): the working set is L2-resident
+PCG_DRAM_BYTES_PER_ITERATION_DUCT3D = (25.81e6 + 0.65e6) / 24
 
 
 class ClockSampler:

@@ -6,7 +6,7 @@
  *
  * Each declaration names the phiPICT binding it replaces (csrc/phipict/bindings.cpp
  * and the kernel it wraps). The Python mirror of the reference API lives in
- * phipict_b200/_C.py; INTEGRATION.md shows the ctypes binding.
+ * phipict_b200/_C.py; phipict_b200/_lib.py binds this header with ctypes.
  *
  * Data layout (all device memory):
  *   - cells of all instances are concatenated: instance i owns cells
@@ -173,6 +173,17 @@ enum { PHB_NONORTHO_VELOCITY = 0, PHB_NONORTHO_SCALAR = 1, PHB_NONORTHO_PRESSURE
  * Does nothing when dom->nonortho has neither right-hand-side bit. */
 int phb_nonortho_rhs(const phb_domain *dom, int kind, const void *field, const phb_scalar *sc, const void *Adiag,
                      void *rhs, phb_stream stream);
+
+/* --- diagnostics -------------------------------------------------------------------- */
+/* Self-test of the bounded grid-barrier wait of the persistent solvers: a cooperative launch
+ * of `ctas` CTAs takes `rounds` grid barriers with a spin limit of `spin_limit` polls
+ * (>= 1024). With absent_cta >= 0 that CTA leaves at once, so the other CTAs' waits run out
+ * and the launch ends with the barrier error flag set instead of waiting for good (the
+ * persistent solvers then leave their systems unconverged). scratch: >= 272 bytes of device
+ * memory on a 16-byte boundary. Outputs (host): bar_err (1 when a wait ran out) and
+ * rounds_done (barriers CTA 0 passed). Synchronises the stream. */
+int phb_barrier_selftest(int ctas, int rounds, int absent_cta, unsigned int spin_limit, void *scratch, int *bar_err,
+                         int *rounds_done, phb_stream stream);
 
 /* --- vectors ------------------------------------------------------------------------ */
 /* Per-instance reductions use a caller-owned scratch of phb_scratch_doubles() doubles whose

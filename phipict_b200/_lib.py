@@ -25,7 +25,7 @@ EXPORTS = (
     "phb_cell_metrics", "phb_face_metrics",
     "phb_advection_matrix", "phb_advection_rhs", "phb_pressure_matrix", "phb_pressure_rhs",
     "phb_divergence", "phb_correct_velocity", "phb_epot_matrix", "phb_epot_rhs", "phb_uxb_epot_rhs",
-    "phb_current_lorentz", "phb_scalar_matrix", "phb_scalar_rhs", "phb_nonortho_rhs",
+    "phb_current_lorentz", "phb_scalar_matrix", "phb_scalar_rhs", "phb_nonortho_rhs", "phb_barrier_selftest",
     "phb_scratch_doubles", "phb_subtract_mean", "phb_rms",
     "phb_csr_row_sizes", "phb_csr_pattern", "phb_csr_gather",
     "phb_solve_work_bytes", "phb_solve_state_bytes", "phb_solve_run", "phb_solve_results",
@@ -141,6 +141,7 @@ def load() -> ct.CDLL:
         "phb_scalar_matrix": [DP, P, ct.POINTER(PhbScalar), I, P, P, P, P],
         "phb_scalar_rhs": [DP, P, P, ct.POINTER(PhbScalar), P, P],
         "phb_nonortho_rhs": [DP, I, P, ct.POINTER(PhbScalar), P, P, P],
+        "phb_barrier_selftest": [I, I, I, ct.c_uint, P, ct.POINTER(I), ct.POINTER(I), P],
         "phb_pressure_matrix": [DP, P, P, P, P],
         "phb_pressure_rhs": [DP, P, P, P, P, P, I, P, P],
         "phb_divergence": [DP, P, P, P],

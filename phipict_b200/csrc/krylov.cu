@@ -942,7 +942,7 @@ __device__ __forceinline__ unsigned int barrierPoll(const unsigned int *count) {
 	return v;
 }
 
-__device__ __forceinline__ bool gridBarrier(Control *ctrl) {
+__device__ __forceinline__ bool gridBarrier(Control *ctrl, unsigned int spinLimit = BARRIER_SPIN_LIMIT) {
 	__shared__ int sOk;
 	__syncthreads();
 	if (threadIdx.x == 0) {
@@ -950,7 +950,7 @@ __device__ __forceinline__ bool gridBarrier(Control *ctrl) {
 		const unsigned int old = barrierArrive(&ctrl->barCount, add);
 		int ok = 1;
 		for (unsigned int spins = 1; ((barrierPoll(&ctrl->barCount) ^ old) & 0x80000000u) == 0; ++spins) {
-			if ((spins & BARRIER_ERR_POLL) == 0 && (spins > BARRIER_SPIN_LIMIT || *(volatile int *)&ctrl->barErr)) {
+			if ((spins & BARRIER_ERR_POLL) == 0 && (spins > spinLimit || *(volatile int *)&ctrl->barErr)) {
 				atomicExch(&ctrl->barErr, 1);
 				ok = 0;
 				break;
@@ -961,6 +961,19 @@ __device__ __forceinline__ bool gridBarrier(Control *ctrl) {
 	}
 	__syncthreads();
 	return sOk;
+}
+
+// The bounded wait under test: every CTA but `absent` takes `rounds` grid barriers with spin
+// limit `spinLimit`; the absent CTA leaves at once, so the others' waits run out, set barErr
+// and end the kernel. rounds_done[0] counts the barriers CTA 0 passed.
+__global__ void kBarrierProbe(Control *ctrl, int rounds, int absent, unsigned int spinLimit, int *roundsDone) {
+	if ((int)blockIdx.x == absent) return;
+	int done = 0;
+	for (int i = 0; i < rounds; ++i) {
+		if (!gridBarrier(ctrl, spinLimit)) break;
+		++done;
+	}
+	if (blockIdx.x == 0 && threadIdx.x == 0) *roundsDone = done;
 }
 
 // Block sum of NV values written to dst[0..NV) by the first threads.
@@ -2091,5 +2104,33 @@ extern "C" int phb_cg_solve_noalloc(const phb_domain *dom, int dtype, int nrhs, 
 	sv.state = (char *)scratch + solveLayout(dom, 0, dtype == PHB_F64 ? 8 : 4, nrhs).total;
 	cudaStream_t st = (cudaStream_t)stream;
 	PHB_SOLVE_DISPATCH(dom->dims, dtype, nrhs, return runCgNoAlloc<T, D, KK>(dom, &sv, out, st));
+	return PHB_OK;
+}
+
+extern "C" int phb_barrier_selftest(int ctas, int rounds, int absent_cta, unsigned int spin_limit, void *scratch, int *bar_err,
+		int *rounds_done, phb_stream stream) {
+	if (ctas < 1 || rounds < 0 || !scratch || !bar_err || !rounds_done || spin_limit < 1024)
+		return setError(PHB_ERR_ARG, "phb_barrier_selftest: bad argument");
+	if (((uintptr_t)scratch & 15) != 0) return setError(PHB_ERR_ARG, "phb_barrier_selftest: scratch must be 16-byte aligned");
+	int perSM = 0;
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kBarrierProbe, PHB_TILE, 0) != cudaSuccess || perSM < 1) perSM = 1;
+	if (ctas > perSM * numSMs()) return setError(PHB_ERR_RANGE, "phb_barrier_selftest: more CTAs than can be co-resident");
+	cudaStream_t s = (cudaStream_t)stream;
+	Control *ctrl = (Control *)scratch;
+	int *done = (int *)((char *)scratch + 256);
+	PHB_CUDA(cudaMemsetAsync(scratch, 0, 256 + sizeof(int), s));
+	cudaLaunchConfig_t cfg = {};
+	cudaLaunchAttribute attr[1];
+	attr[0].id = cudaLaunchAttributeCooperative;
+	attr[0].val.cooperative = 1;
+	cfg.gridDim = dim3(ctas);
+	cfg.blockDim = dim3(PHB_TILE);
+	cfg.stream = s;
+	cfg.attrs = attr;
+	cfg.numAttrs = 1;
+	PHB_CUDA(cudaLaunchKernelEx(&cfg, kBarrierProbe, ctrl, rounds, absent_cta, spin_limit, done));
+	PHB_CUDA(cudaMemcpyAsync(bar_err, &ctrl->barErr, sizeof(int), cudaMemcpyDeviceToHost, s));
+	PHB_CUDA(cudaMemcpyAsync(rounds_done, done, sizeof(int), cudaMemcpyDeviceToHost, s));
+	PHB_CUDA(cudaStreamSynchronize(s));
 	return PHB_OK;
 }
