@@ -871,21 +871,26 @@ __global__ void __launch_bounds__(PHB_TILE) kNonOrthoRhs(Dom<S, D> dom, const S 
 	}
 	if constexpr (KIND == PHB_NONORTHO_PRESSURE) {
 		const NField<S> F{NF_PRESSURE, 0, field, sv};
-		rhs[c.g] += nonOrthoRhs<S, D>(dom, F, bp, dom.nonortho, [&](int64_t g) { return S(1) / Adiag[g]; }, S(1));
+		S o[1];
+		nonOrthoRhs<S, D, 1>(dom, F, bp, dom.nonortho, [&](int64_t g) { return S(1) / Adiag[g]; }, S(1), o);
+		rhs[c.g] += o[0];
 	} else if constexpr (KIND == PHB_NONORTHO_VELOCITY) {
+		// one walk per corner for all components (they share the faces' velocity type)
 		const S nu = S(dom.nu[inst]);
 		const S det = detAt<S, D>(dom, c.mi);
-		for (int w = 0; w < D; ++w) {
-			const NField<S> F{NF_VELOCITY, w, field, sv};
-			rhs[vidx<D>(c.B, c.g, w)] -= nonOrthoRhs<S, D>(dom, F, bp, dom.nonortho, [&](int64_t) { return nu; }, nu) / det;
-		}
+		const NField<S> F{NF_VELOCITY, 0, field, sv};
+		S o[D];
+		nonOrthoRhs<S, D, D>(dom, F, bp, dom.nonortho, [&](int64_t) { return nu; }, nu, o);
+#pragma unroll
+		for (int w = 0; w < D; ++w) rhs[vidx<D>(c.B, c.g, w)] -= o[w] / det;
 	} else {
 		const S det = detAt<S, D>(dom, c.mi);
 		for (int ch = 0; ch < sv.channels; ++ch) {
 			const S nuc = S(scalarNu(sv, ch, dom.nu[inst]));
 			const NField<S> F{NF_SCALAR, ch, field, sv};
-			rhs[sidx(c.B, c.g, ch, sv.channels)] -=
-				nonOrthoRhs<S, D>(dom, F, bp, dom.nonortho, [&](int64_t) { return S(1); }, S(1)) * nuc / det;
+			S o[1];
+			nonOrthoRhs<S, D, 1>(dom, F, bp, dom.nonortho, [&](int64_t) { return S(1); }, S(1), o);
+			rhs[sidx(c.B, c.g, ch, sv.channels)] -= o[0] * nuc / det;
 		}
 	}
 	}

@@ -42,14 +42,23 @@ struct BPos {
 	int p[3];
 };
 
-template <typename S, int D>
-__device__ __forceinline__ S nfCell(const Dom<S, D> &dom, const NField<S> &F, const BPos &q) {
-	if (F.kind == NF_MARK || !F.cells) return S(0); // matrix walks read no cell data
+// The value of components F.w .. F.w+NC-1 at cell q (zeros for a matrix walk, which reads no
+// cell data).
+template <typename S, int D, int NC = 1>
+__device__ __forceinline__ void nfCell(const Dom<S, D> &dom, const NField<S> &F, const BPos &q, S (&v)[NC]) {
+	if (F.kind == NF_MARK || !F.cells) {
+#pragma unroll
+		for (int j = 0; j < NC; ++j) v[j] = 0;
+		return;
+	}
 	const int32_t *B = dom.blk(q.b);
 	const int64_t g = B[B_CELLOFF] + flat(B, q.p);
-	if (F.kind == NF_PRESSURE) return __ldg(F.cells + g);
-	if (F.kind == NF_VELOCITY) return __ldg(F.cells + vidx<D>(B, g, F.w));
-	return __ldg(F.cells + sidx(B, g, F.w, F.sv.channels));
+#pragma unroll
+	for (int j = 0; j < NC; ++j) {
+		if (F.kind == NF_PRESSURE) v[j] = __ldg(F.cells + g);
+		else if (F.kind == NF_VELOCITY) v[j] = __ldg(F.cells + vidx<D>(B, g, F.w + j));
+		else v[j] = __ldg(F.cells + sidx(B, g, F.w + j, F.sv.channels));
+	}
 }
 // getFixedBoundaryType (block_data.cuh:111-135): true for a Neumann face
 template <typename S, int D>
@@ -61,14 +70,17 @@ __device__ __forceinline__ bool nfNeumann(const Dom<S, D> &dom, const NField<S> 
 }
 // getFixedBoundaryData (block_data.cuh:137-205) at the face cell of p; the fixed faces carry
 // no pressure data
-template <typename S, int D>
-__device__ __forceinline__ S nfFixed(const Dom<S, D> &dom, const NField<S> &F, const int32_t *B, int f, const int *p) {
-	if (F.kind == NF_MARK) return S(1);
+template <typename S, int D, int NC = 1>
+__device__ __forceinline__ void nfFixed(const Dom<S, D> &dom, const NField<S> &F, const int32_t *B, int f, const int *p, S (&v)[NC]) {
 	const int fid = fRec(B, f)[5];
 	const int32_t *FR = dom.fix(fid);
-	if (F.kind == NF_VELOCITY) return fixedVel<S, D>(dom, FR, faceCell(B, f, p), F.w);
-	if (F.kind == NF_SCALAR) return F.sv.values ? scalarFixed<S>(F.sv, FR, fid, F.w, faceCell(B, f, p)) : S(0);
-	return S(0);
+#pragma unroll
+	for (int j = 0; j < NC; ++j) {
+		if (F.kind == NF_MARK) v[j] = S(1);
+		else if (F.kind == NF_VELOCITY) v[j] = fixedVel<S, D>(dom, FR, faceCell(B, f, p), F.w + j);
+		else if (F.kind == NF_SCALAR) v[j] = F.sv.values ? scalarFixed<S>(F.sv, FR, fid, F.w + j, faceCell(B, f, p)) : S(0);
+		else v[j] = S(0);
+	}
 }
 
 // computeConnectedDir (topology.cuh:226-236): direction dir of block B as seen from the
@@ -95,25 +107,28 @@ __device__ __forceinline__ bool stepAcross(const Dom<S, D> &dom, BPos &q, int di
 	return true;
 }
 // getBlockDataNeighbor (block_data.cuh:276-318)
-template <typename S, int D>
-__device__ S neighborData(const Dom<S, D> &dom, const NField<S> &F, BPos q, int dir) {
-	if (!stepAcross<S, D>(dom, q, dir)) return nfFixed<S, D>(dom, F, dom.blk(q.b), dir, q.p);
-	return nfCell<S, D>(dom, F, q);
+template <typename S, int D, int NC = 1>
+__device__ void neighborData(const Dom<S, D> &dom, const NField<S> &F, BPos q, int dir, S (&v)[NC]) {
+	if (!stepAcross<S, D>(dom, q, dir)) nfFixed<S, D, NC>(dom, F, dom.blk(q.b), dir, q.p, v);
+	else nfCell<S, D, NC>(dom, F, q, v);
 }
 // getBlockDataNeighborDiagonal (block_data.cuh:372-420): dir1 first unless the starting
 // block's dir1 face is fixed; the second step keeps its direction index in the block reached
-template <typename S, int D>
-__device__ S diagonalData(const Dom<S, D> &dom, const NField<S> &F, BPos q, int dir1, int dir2) {
+template <typename S, int D, int NC = 1>
+__device__ void diagonalData(const Dom<S, D> &dom, const NField<S> &F, BPos q, int dir1, int dir2, S (&v)[NC]) {
 	const bool first1 = fType(dom.blk(q.b), dir1) != FT_FIXED;
 	const int dirs[2] = {first1 ? dir1 : dir2, first1 ? dir2 : dir1};
 	for (int i = 0; i < 2; ++i)
-		if (!stepAcross<S, D>(dom, q, dirs[i])) return nfFixed<S, D>(dom, F, dom.blk(q.b), dirs[i], q.p);
-	return nfCell<S, D>(dom, F, q);
+		if (!stepAcross<S, D>(dom, q, dirs[i])) {
+			nfFixed<S, D, NC>(dom, F, dom.blk(q.b), dirs[i], q.p, v);
+			return;
+		}
+	nfCell<S, D, NC>(dom, F, q, v);
 }
 
-template <typename S>
+template <typename S, int NC = 1>
 struct CornerValue {
-	S data;
+	S data[NC];
 	int numCells; // 0: the value came from a fixed face
 	bool neumann; // that face's type
 };
@@ -121,9 +136,14 @@ struct CornerValue {
 // getCornerValue (block_data.cuh:501-620) with includeDepth0 false and maxDepth 2: two walks
 // go around the corner between dir1 and dir2 in opposite senses, one cell per depth each,
 // until they meet or a fixed face ends one of them. At depth 2 the walks normally meet at
-// the diagonal cell (four cells); three blocks meeting at a corner give three.
-template <typename S, int D>
-__device__ CornerValue<S> cornerWalk(const Dom<S, D> &dom, const NField<S> &F, const BPos &start, int dir1, int dir2, bool depth1) {
+// the diagonal cell (four cells); three blocks meeting at a corner give three. One walk gives
+// the corner values of NC components.
+template <typename S, int D, int NC = 1>
+__device__ CornerValue<S, NC> cornerWalk(const Dom<S, D> &dom, const NField<S> &F, const BPos &start, int dir1, int dir2, bool depth1) {
+	CornerValue<S, NC> out;
+	S data[NC], v[NC];
+#pragma unroll
+	for (int j = 0; j < NC; ++j) data[j] = 0;
 	{
 		// a cell at least one cell away from every face of its block: the walks reach the two
 		// face neighbours at depth 1 and meet at the diagonal cell at depth 2 (four cells), with
@@ -138,18 +158,24 @@ __device__ CornerValue<S> cornerWalk(const Dom<S, D> &dom, const NField<S> &F, c
 			n2.p[dir2 >> 1] += (dir2 & 1) ? 1 : -1;
 			BPos dg = n1;
 			dg.p[dir2 >> 1] += (dir2 & 1) ? 1 : -1;
-			S data = 0;
 			if (depth1) {
-				data += nfCell<S, D>(dom, F, n1);
-				data += nfCell<S, D>(dom, F, n2);
+				nfCell<S, D, NC>(dom, F, n1, v);
+#pragma unroll
+				for (int j = 0; j < NC; ++j) data[j] += v[j];
+				nfCell<S, D, NC>(dom, F, n2, v);
+#pragma unroll
+				for (int j = 0; j < NC; ++j) data[j] += v[j];
 			}
-			data += nfCell<S, D>(dom, F, dg);
-			return {data / S(4), 4, false};
+			nfCell<S, D, NC>(dom, F, dg, v);
+#pragma unroll
+			for (int j = 0; j < NC; ++j) out.data[j] = (data[j] + v[j]) / S(4);
+			out.numCells = 4;
+			out.neumann = false;
+			return out;
 		}
 	}
 	BPos w[2] = {start, start};
 	int d1[2] = {dir1, dir2}, d2[2] = {dir2, dir1};
-	S data = 0;
 	int num = 1;
 #pragma unroll
 	for (int depth = 1; depth <= 2; ++depth) {
@@ -161,12 +187,16 @@ __device__ CornerValue<S> cornerWalk(const Dom<S, D> &dom, const NField<S> &F, c
 			if (atBound(B, a, w[d].p)) {
 				const int t = fType(B, a);
 				if (t == FT_FIXED) {
-					const bool neu = nfNeumann<S, D>(dom, F, B, a);
-					const S v0 = nfFixed<S, D>(dom, F, B, a, w[d].p);
-					if (atBound(B, t2, w[d].p)) return {v0, 0, neu};
+					out.neumann = nfNeumann<S, D>(dom, F, B, a);
+					out.numCells = 0;
+					nfFixed<S, D, NC>(dom, F, B, a, w[d].p, out.data);
+					if (atBound(B, t2, w[d].p)) return out;
 					int q[3] = {w[d].p[0], w[d].p[1], w[d].p[2]};
 					q[t2 >> 1] += (t2 & 1) ? 1 : -1;
-					return {(v0 + nfFixed<S, D>(dom, F, B, a, q)) * S(0.5), 0, neu};
+					nfFixed<S, D, NC>(dom, F, B, a, q, v);
+#pragma unroll
+					for (int j = 0; j < NC; ++j) out.data[j] = (out.data[j] + v[j]) * S(0.5);
+					return out;
 				}
 				if (t == FT_CONNECTED) {
 					const int n1 = connDir(B, a, t2, D);
@@ -188,13 +218,26 @@ __device__ CornerValue<S> cornerWalk(const Dom<S, D> &dom, const NField<S> &F, c
 				d2[d] = a ^ 1;
 			}
 			const BPos &o = w[d ^ 1];
-			if (w[d].b == o.b && w[d].p[0] == o.p[0] && w[d].p[1] == o.p[1] && w[d].p[2] == o.p[2])
-				return {data / S(num), num, false};
-			if (depth > 1 || depth1) data += nfCell<S, D>(dom, F, w[d]);
+			if (w[d].b == o.b && w[d].p[0] == o.p[0] && w[d].p[1] == o.p[1] && w[d].p[2] == o.p[2]) {
+#pragma unroll
+				for (int j = 0; j < NC; ++j) out.data[j] = data[j] / S(num);
+				out.numCells = num;
+				out.neumann = false;
+				return out;
+			}
+			if (depth > 1 || depth1) {
+				nfCell<S, D, NC>(dom, F, w[d], v);
+#pragma unroll
+				for (int j = 0; j < NC; ++j) data[j] += v[j];
+			}
 			++num;
 		}
 	}
-	return {data / S(num), num, false};
+#pragma unroll
+	for (int j = 0; j < NC; ++j) out.data[j] = data[j] / S(num);
+	out.numCells = num;
+	out.neumann = false;
+	return out;
 }
 
 // det Minv[a] . Minv[c] at metric index mi (discretization.cuh:419-469)
@@ -346,15 +389,17 @@ __device__ __forceinline__ void nonOrthoRhsInner(const Dom<S, D> &dom, const S *
 }
 
 // getNonOrthoLaplaceRHS_v2 (nonortho_rhs.cuh:27-180) without face transforms: the explicit
-// cross terms of field F at cell c. ra(g): the weight of cell g (1/A for the pressure, the
-// viscosity for the velocity, 1 for a scalar); raFixed: the weight at a fixed face.
-template <typename S, int D, typename RA>
-__device__ S nonOrthoRhs(const Dom<S, D> &dom, const NField<S> &F, const BPos &c, int flags, RA ra, S raFixed) {
+// cross terms of components F.w .. F.w+NC-1 of field F at cell c into sum[NC]. ra(g): the
+// weight of cell g (1/A for the pressure, the viscosity for the velocity, 1 for a scalar);
+// raFixed: the weight at a fixed face. Every corner is walked once for all NC components.
+template <typename S, int D, int NC, typename RA>
+__device__ void nonOrthoRhs(const Dom<S, D> &dom, const NField<S> &F, const BPos &c, int flags, RA ra, S raFixed, S (&sum)[NC]) {
 	const bool direct = flags & NO_DIRECT_RHS, diagonal = flags & NO_DIAGONAL_RHS;
 	const int32_t *B = dom.blk(c.b);
 	const int64_t miP = metricIndex(B, c.p);
 	const S raP = ra(cellIndex(B, c.p));
-	S sum = 0;
+#pragma unroll
+	for (int j = 0; j < NC; ++j) sum[j] = 0;
 	for (int f = 0; f < 2 * D; ++f) {
 		const int ax = f >> 1;
 		const int faceSign = (f & 1) ? 1 : -1;
@@ -369,8 +414,12 @@ __device__ S nonOrthoRhs(const Dom<S, D> &dom, const NField<S> &F, const BPos &c
 				if (!tLow) lo[tAxis] -= 1;
 				if (!tHigh) hi[tAxis] += 1;
 				const S factor = (tLow || tHigh) ? S(1) : S(0.5);
-				const S tGrad = factor * (nfFixed<S, D>(dom, F, B, f, hi) - nfFixed<S, D>(dom, F, B, f, lo));
-				sum -= S(faceSign) * lapCrossFace<S, D>(dom, fi, tAxis, ax) * tGrad * raFixed;
+				S vh[NC], vl[NC];
+				nfFixed<S, D, NC>(dom, F, B, f, hi, vh);
+				nfFixed<S, D, NC>(dom, F, B, f, lo, vl);
+				const S alpha = lapCrossFace<S, D>(dom, fi, tAxis, ax);
+#pragma unroll
+				for (int j = 0; j < NC; ++j) sum[j] -= S(faceSign) * alpha * (factor * (vh[j] - vl[j])) * raFixed;
 			}
 			continue;
 		}
@@ -395,26 +444,38 @@ __device__ S nonOrthoRhs(const Dom<S, D> &dom, const NField<S> &F, const BPos &c
 		for (int i = 1; i < D; ++i) {
 			const int tAxis = (ax + i) % D;
 			const S faceAlpha = (lapCross<S, D>(dom, miP, ax, tAxis) * raP + lapCross<S, D>(dom, miN, map[tAxis], map[ax]) * raN) * S(0.5);
-			S tGrad = 0;
+			S tGrad[NC];
+#pragma unroll
+			for (int j = 0; j < NC; ++j) tGrad[j] = 0;
 			for (int tUp = 0; tUp < 2; ++tUp) {
 				const int tFace = 2 * tAxis + tUp;
 				const int tSign = tUp ? 1 : -1;
-				const CornerValue<S> cv = cornerWalk<S, D>(dom, F, c, f, tFace, direct);
+				const CornerValue<S, NC> cv = cornerWalk<S, D, NC>(dom, F, c, f, tFace, direct);
 				if (cv.numCells == 0 && (cv.neumann || F.kind == NF_PRESSURE)) {
 					const int tOther = tFace ^ 1;
+					S v[NC];
 					if (direct) {
-						tGrad += S(tSign) * neighborData<S, D>(dom, F, c, f) * S(0.75);
-						tGrad += S(-tSign) * neighborData<S, D>(dom, F, c, tOther) * S(0.25);
+						neighborData<S, D, NC>(dom, F, c, f, v);
+#pragma unroll
+						for (int j = 0; j < NC; ++j) tGrad[j] += S(tSign) * v[j] * S(0.75);
+						neighborData<S, D, NC>(dom, F, c, tOther, v);
+#pragma unroll
+						for (int j = 0; j < NC; ++j) tGrad[j] += S(-tSign) * v[j] * S(0.25);
 					}
-					if (diagonal) tGrad += S(-tSign) * diagonalData<S, D>(dom, F, c, f, tOther) * S(0.25);
+					if (diagonal) {
+						diagonalData<S, D, NC>(dom, F, c, f, tOther, v);
+#pragma unroll
+						for (int j = 0; j < NC; ++j) tGrad[j] += S(-tSign) * v[j] * S(0.25);
+					}
 				} else {
-					tGrad += S(tSign) * cv.data;
+#pragma unroll
+					for (int j = 0; j < NC; ++j) tGrad[j] += S(tSign) * cv.data[j];
 				}
 			}
-			sum -= S(faceSign) * faceAlpha * tGrad;
+#pragma unroll
+			for (int j = 0; j < NC; ++j) sum[j] -= S(faceSign) * faceAlpha * tGrad[j];
 		}
 	}
-	return sum;
 }
 
 } // namespace phb
