@@ -916,7 +916,8 @@ __global__ void kInitOuter(SysState *st, int nsys, phb_tolerance tol, Control *c
 // and meet at grid barriers instead of kernel boundaries, so an iteration costs a few
 // barrier round trips instead of kernel launches and the vectors stay in L2. Every barrier
 // wait is bounded: when it runs out it sets Control::barErr and every CTA leaves the kernel
-// (the systems then report non-finite). Each CTA keeps its own copy of the per-system
+// (phb_solve_results then reports every system non-finite; inside a refinement the unfinished
+// inner solve leaves the outer loop unconverged). Each CTA keeps its own copy of the per-system
 // scalars in shared memory and reduces the per-tile partials itself, in the same fixed order
 // as every other CTA, so all CTAs take the same decisions without broadcasting them.
 constexpr unsigned int BARRIER_SPIN_LIMIT = 1u << 24;
@@ -1807,7 +1808,9 @@ extern "C" int phb_solve_results(const phb_domain *dom, const phb_solve *s, phb_
 	const int nsys = dom->ninst * s->nrhs;
 	std::vector<SysState> h(nsys);
 	const StateLayout SL = stateLayout(dom, s->nrhs);
+	Control c{};
 	PHB_CUDA(cudaMemcpyAsync(h.data(), (char *)s->state + SL.st, nsys * sizeof(SysState), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+	PHB_CUDA(cudaMemcpyAsync(&c, (char *)s->state + SL.ctrl, sizeof(Control), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
 	PHB_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
 	for (int i = 0; i < nsys; ++i) {
 		const SysState &x = h[i];
@@ -1817,6 +1820,13 @@ extern "C" int phb_solve_results(const phb_domain *dom, const phb_solve *s, phb_
 		o.converged = x.done == CONVERGED;
 		o.finite = std::isfinite(x.crit);
 		o.status = x.done;
+		if (c.barErr) { // a persistent solve left early at a grid-barrier wait that ran out
+			o.converged = 0;
+			o.finite = 0;
+			o.status = NONFINITE;
+			o.final_residual = NAN;
+			continue;
+		}
 		o.inner_iterations = 0;
 		if (s->return_best && (x.done == MAXIT || x.done == RISING) && x.bestIt >= 0 && x.best < x.crit) {
 			o.used_iterations = x.bestIt;
