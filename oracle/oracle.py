@@ -376,8 +376,9 @@ class OracleSim:
         return x - x.mean()
 
     def scalar_step(self):
-        """core/piso_simulation.py:3589-3775 (orthogonal): every channel advected and diffused
-        implicitly with the step-start velocity, zero initial guess. Returns the channel-0
+        """core/piso_simulation.py:3225-3345, 3589-3775: every channel advected and diffused
+        implicitly with the step-start velocity, zero initial guess, re-solved with the cross
+        terms of its result when non-orthogonal flags are set. Returns the channel-0
         matrix when the velocity step reuses it (same diffusivity as the velocity, one set of
         face types for all channels), else None."""
         od, C = self.od, self.od.channels

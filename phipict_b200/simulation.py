@@ -441,9 +441,11 @@ class Simulation:
 
     def _advect_scalar(self, ts, step: int, flags: int = 0) -> bool:
         """Implicit advection-diffusion of every passive-scalar channel with the velocity of
-        the step start (core/piso_simulation.py:3589-3775, orthogonal path): one matrix for
-        all channels when their diffusivity and face types agree, else one per channel; a
-        zero initial guess; the result copied to the blocks. Returns whether the velocity
+        the step start (core/piso_simulation.py:3225-3345, 3589-3775): one matrix for all
+        channels when their diffusivity and face types agree, else one per channel; a zero
+        initial guess; with non-orthogonal flags the right-hand side carries the cross terms
+        of the current scalar result and the solve repeats advect_non_ortho_steps times from
+        the previous result; the result copied to the blocks. Returns whether the velocity
         step reuses the scalar matrix (same diffusivity as the velocity, one set of face types
         for all channels), as phiPICT does."""
         d = self.domain
