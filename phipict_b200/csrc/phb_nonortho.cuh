@@ -353,6 +353,13 @@ __device__ __forceinline__ void nonOrthoRhsInner(const Dom<S, D> &dom, const S *
 	auto stride = [&](int a) -> int64_t { return a == 0 ? 1 : a == 1 ? sy : sz; };
 	const int64_t g = cellIndex(B, p), mi = metricIndex(B, p);
 	const S raP = ra(g);
+	// the cell's cross coefficients, one per axis pair ((0,1), (0,2), (1,2)); the dot product
+	// is symmetric in its operands, so lapCross(a, b) and lapCross(b, a) agree bit for bit
+	S cP[3];
+#pragma unroll
+	for (int a = 0; a < D; ++a)
+#pragma unroll
+		for (int b = a + 1; b < D; ++b) cP[a + b - 1] = lapCross<S, D>(dom, mi, a, b);
 #pragma unroll
 	for (int w = 0; w < NC; ++w) out[w] = 0;
 	// faces one at a time (not unrolled): every face's loads stay in flight together without
@@ -363,10 +370,20 @@ __device__ __forceinline__ void nonOrthoRhsInner(const Dom<S, D> &dom, const S *
 		const int faceSign = (f & 1) ? 1 : -1;
 		const int64_t sN = (f & 1) ? stride(ax) : -stride(ax);
 		const S raN = ra(g + sN);
+		// the neighbour's inverse-transform row of the face axis and its determinant, read once
+		const int64_t mN = mi + sN;
+		S rowN[D];
+#pragma unroll
+		for (int j = 0; j < D; ++j) rowN[j] = dom.m(Tr<D>::MINV + ax * D + j, mN);
+		const S detN = dom.m(Tr<D>::DET, mN);
 #pragma unroll
 		for (int i = 1; i < D; ++i) {
 			const int tAxis = (ax + i) % D;
-			const S faceAlpha = (lapCross<S, D>(dom, mi, ax, tAxis) * raP + lapCross<S, D>(dom, mi + sN, tAxis, ax) * raN) * S(0.5);
+			S dN = 0; // as lapCross(mN, tAxis, ax)
+#pragma unroll
+			for (int j = 0; j < D; ++j) dN += dom.m(Tr<D>::MINV + tAxis * D + j, mN) * rowN[j];
+			const int lo = ax < tAxis ? ax : tAxis, hi = ax < tAxis ? tAxis : ax;
+			const S faceAlpha = (cP[lo + hi - 1] * raP + detN * dN * raN) * S(0.5);
 #pragma unroll
 			for (int w = 0; w < NC; ++w) {
 				const S *cw = cells + base + w * cstride;

@@ -217,3 +217,29 @@ def test_nonortho_batch_equals_instances_alone(cuda):
     for k, dom in enumerate(ms):
         assert torch.equal(dom._u_block, alone[k][0]), k
         assert torch.equal(dom.pressureResult, alone[k][1]), k
+
+
+def test_nonortho_assembly_float32(cuda):
+    """The float32 instantiations against the oracle in float32 (FP32 bar 1e-5)."""
+    dom = skewed_channel_2d(12, 10, dtype=torch.float32)
+    seeded_state(dom, 2, scale=0.3)
+    dom.PrepareSolve()
+    od = OracleDomain(dom, 0, np.float32)
+    dt, nu = 0.01, float(dom.viscosity[0])
+    ts = torch.tensor([dt], dtype=torch.float64)
+    u = host(dom._u_block).reshape(-1)
+    _C.SetupAdvectionMatrix(dom, ts, ALL)
+    Cval, A = od.advection_matrix(u, dt, nu, flags=ALL)
+    assert rel(host(dom.C.value), Cval) < 1e-5 and rel(host(dom.A), A) < 1e-5
+    g = torch.Generator().manual_seed(4)
+    ures = (u + 0.2 * torch.randn(u.size, generator=g, dtype=torch.float64).numpy()).astype(np.float32)
+    dom.velocityResult.copy_(torch.from_numpy(ures).to("cuda"))
+    _C.SetupAdvectionVelocity(dom, ts, ALL, False)
+    assert rel(host(dom.velocityRHS), od.advection_rhs(u, None, dt, nu, flags=ALL, ures=ures)) < 1e-5
+    _C.SetupPressureMatrix(dom, ts, ALL, False)
+    assert rel(host(dom.P.value), od.laplace_matrix(A, flags=ALL)[0]) < 1e-5
+    pres = torch.randn(od.n, generator=g, dtype=torch.float64).numpy().astype(np.float32)
+    dom.pressureResult.copy_(torch.from_numpy(pres).to("cuda"))
+    _C.SetupPressureRHS(dom, ts, ALL, False, False)
+    h = od.pressure_rhs(Cval, A, u, ures, None, dt, nu)
+    assert rel(host(dom.pressureRHSdiv), od.pressure_nonortho(A, pres, ALL, od.divergence(h))) < 1e-5
