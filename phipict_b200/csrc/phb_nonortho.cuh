@@ -269,6 +269,12 @@ __device__ __forceinline__ void nonOrthoInterp(const Dom<S, D> &dom, const BPos 
 	const int32_t *B = dom.blk(c.b);
 	const int64_t miP = metricIndex(B, c.p);
 	const S raP = ra(cellIndex(B, c.p));
+	// the cell's cross coefficients, one per axis pair (lapCross is symmetric bit for bit)
+	S cP[3];
+#pragma unroll
+	for (int a = 0; a < D; ++a)
+#pragma unroll
+		for (int b = a + 1; b < D; ++b) cP[a + b - 1] = lapCross<S, D>(dom, miP, a, b);
 #pragma unroll
 	for (int f = 0; f < 2 * D; ++f) {
 		const int ax = f >> 1;
@@ -288,10 +294,18 @@ __device__ __forceinline__ void nonOrthoInterp(const Dom<S, D> &dom, const BPos 
 		}
 		const int64_t miN = metricIndex(NB, np);
 		const S raN = ra(cellIndex(NB, np));
+		S rowN[D];
+#pragma unroll
+		for (int j = 0; j < D; ++j) rowN[j] = dom.m(Tr<D>::MINV + ax * D + j, miN);
+		const S detN = dom.m(Tr<D>::DET, miN);
 #pragma unroll
 		for (int i = 1; i < D; ++i) {
 			const int o = (ax + i) % D;
-			ia[f][i - 1] = (lapCross<S, D>(dom, miP, ax, o) * raP + lapCross<S, D>(dom, miN, o, ax) * raN) * S(0.5);
+			S dN = 0; // as lapCross(miN, o, ax)
+#pragma unroll
+			for (int j = 0; j < D; ++j) dN += dom.m(Tr<D>::MINV + o * D + j, miN) * rowN[j];
+			const int lo = ax < o ? ax : o, hi = ax < o ? o : ax;
+			ia[f][i - 1] = (cP[lo + hi - 1] * raP + detN * dN * raN) * S(0.5);
 		}
 	}
 }
