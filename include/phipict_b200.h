@@ -338,7 +338,10 @@ int phb_refine_results(const phb_domain *dom, const phb_refine *r, phb_solve_res
  * GPU into fixed slices at start-up and allow no later allocation, or plugin hosts whose
  * allocator is not reachable through a C ABI. It calls no allocator. The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) with that device
- * current, so make that first call before any stream capture. Sizes whose workspace
+ * current, so make that first call before any stream capture; later calls whose stream is
+ * not capturing look it up again, so a context reset (which may move the array) is
+ * followed. An empty domain (no cells) reports every system converged after 0 iterations.
+ * Sizes whose workspace
  * (phb_cg_noalloc_bytes) exceeds the array are rejected with PHB_ERR_RANGE. All calls share
  * the one array: calls that overlap on the GPU (two streams, two host threads) race.
  * out (optional): per-system results, read back with synchronous copies. */

@@ -188,6 +188,17 @@ def SetupPressureRHSdiv(domain: Domain, timeStep, nonOrthoMode=0, useFaceTransfo
                   _S(domain))
 
 
+def ComputeVelocityDivergence(domain: Domain) -> torch.Tensor:
+    """Flux divergence of the block velocity, [B * n] (piso/analysis.cu:27-70, bound at
+    bindings.cpp:664): the face fluxes of the velocity interpolated to the faces (fixed
+    faces take their boundary velocity), summed per cell, as for the pressure right-hand
+    side's divergence."""
+    _check(domain)
+    div = torch.zeros_like(domain.pressureResult)
+    _lib.call("phb_divergence", ct.byref(domain.desc()), domain._u_block.data_ptr(), div.data_ptr(), _S(domain))
+    return div
+
+
 def SetupPressureCorrection(domain: Domain, timeStep, nonOrthoMode=0, useFaceTransform: bool = False,
                             timeStepNorm: bool = False) -> None:
     """Matrix, HbyA and divergence of one corrector (pressure.cu:882-927)."""

@@ -1820,6 +1820,8 @@ extern "C" int phb_solve_results(const phb_domain *dom, const phb_solve *s, phb_
 		o.converged = x.done == CONVERGED;
 		o.finite = std::isfinite(x.crit);
 		o.status = x.done;
+		o.inner_iterations = 0;
+		o.pad = 0;
 		if (c.barErr) { // a persistent solve left early at a grid-barrier wait that ran out
 			o.converged = 0;
 			o.finite = 0;
@@ -1827,7 +1829,6 @@ extern "C" int phb_solve_results(const phb_domain *dom, const phb_solve *s, phb_
 			o.final_residual = NAN;
 			continue;
 		}
-		o.inner_iterations = 0;
 		if (s->return_best && (x.done == MAXIT || x.done == RISING) && x.bestIt >= 0 && x.best < x.crit) {
 			o.used_iterations = x.bestIt;
 			o.final_residual = x.best;
@@ -1993,20 +1994,28 @@ extern "C" int phb_refine_results(const phb_domain *dom, const phb_refine *r, ph
 static __device__ __align__(256) unsigned char gNoAllocScratch[PHB_NOALLOC_SCRATCH_BYTES];
 
 // Device address of the array on each device. In host code `gNoAllocScratch` names a
-// host-side stand-in, not device memory, so the address is looked up once per device, with
-// that device current, by the first call on it.
+// host-side stand-in, not device memory, so the address is looked up with the device
+// current: by the first call on a device, and again by every call whose stream is not
+// capturing (a cheap host call), so that a context that was reset and re-created, which
+// reloads the module and may move the array, is followed. A call made while its stream is
+// capturing uses the address of the last call that was not, so the first call on a device
+// must come before any capture.
 static std::mutex gNoAllocMutex;
 static void *gNoAllocPtr[64] = {nullptr};
 
-static int noAllocScratch(void **out) {
+static int noAllocScratch(cudaStream_t s, void **out) {
 	int dev;
 	PHB_CUDA(cudaGetDevice(&dev));
 	if (dev < 0 || dev >= 64) return setError(PHB_ERR_RANGE, "phb_cg_solve_noalloc: device index out of range");
+	cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+	PHB_CUDA(cudaStreamIsCapturing(s, &cap));
 	std::lock_guard<std::mutex> lock(gNoAllocMutex);
-	if (!gNoAllocPtr[dev]) {
+	if (cap == cudaStreamCaptureStatusNone) {
 		void *p = nullptr;
 		PHB_CUDA(cudaGetSymbolAddress(&p, gNoAllocScratch));
 		gNoAllocPtr[dev] = p;
+	} else if (!gNoAllocPtr[dev]) {
+		return setError(PHB_ERR_ARG, "phb_cg_solve_noalloc: the first call on a device must not be made while its stream is capturing");
 	}
 	*out = gNoAllocPtr[dev];
 	return PHB_OK;
@@ -2094,9 +2103,23 @@ extern "C" int phb_cg_solve_noalloc(const phb_domain *dom, int dtype, int nrhs, 
 			"static array (PHB_NOALLOC_SCRATCH_BYTES)", (long long)need, (long long)PHB_NOALLOC_SCRATCH_BYTES);
 		return setError(PHB_ERR_RANGE, msg);
 	}
-	if (dom->ntiles == 0) return PHB_OK;
+	if (dom->ntiles == 0) { // nothing to solve: every system reports a converged empty solve
+		if (out) {
+			for (int i = 0; i < dom->ninst * nrhs; ++i) {
+				phb_solve_result &o = out[i];
+				o.final_residual = 0.0;
+				o.used_iterations = 0;
+				o.converged = 1;
+				o.finite = 1;
+				o.status = CONVERGED;
+				o.inner_iterations = 0;
+				o.pad = 0;
+			}
+		}
+		return PHB_OK;
+	}
 	void *scratch = nullptr;
-	int rc = noAllocScratch(&scratch);
+	int rc = noAllocScratch((cudaStream_t)stream, &scratch);
 	if (rc) return rc;
 	phb_solve sv = {};
 	sv.kind = 0;

@@ -318,6 +318,40 @@ class FixedBoundary(Boundary):
     def getPotentialCw(self) -> float:
         return self._cw
 
+    # legacy flag interface over the potential BC (domain/boundaries.cpp:968-991,
+    # domain/domain_structs.h:244-249), used by files written before PotentialBC existed
+    def setEpotCw(self, cw: float) -> None:
+        if not cw >= 0.0:
+            raise RuntimeError("Epot wall conductance Cw must be non-negative.")
+        if cw > 0.0:
+            self.setPotentialBC(PotentialBC.THIN_WALL, cw)
+        elif self._potentialType == PotentialBC.THIN_WALL:
+            self.setPotentialBC(PotentialBC.INSULATING)
+
+    def setEpotDirichlet(self, dirichlet: bool) -> None:
+        if dirichlet:
+            self.setPotentialBC(PotentialBC.DIRICHLET)
+        elif self._potentialType == PotentialBC.DIRICHLET:
+            self.setPotentialBC(PotentialBC.INSULATING)
+
+    def setEpotInsulating(self, insulating: bool) -> None:
+        if not insulating:
+            self.setPotentialBC(PotentialBC.OPEN)
+        elif self._potentialType == PotentialBC.OPEN:
+            self.setPotentialBC(PotentialBC.INSULATING)
+
+    def hasEpotCw(self) -> bool:
+        return self.hasPotentialThinWall() and self._cw > 0.0
+
+    def getEpotCw(self) -> float:
+        return self._cw if self.hasPotentialThinWall() else 0.0
+
+    def hasEpotDirichlet(self) -> bool:
+        return self.hasPotentialDirichlet()
+
+    def isEpotInsulating(self) -> bool:
+        return self._potentialType != PotentialBC.OPEN
+
     def setPotentialTypes(self, types: torch.Tensor, cw: float | None = None) -> None:
         d = self.getSpatialDims()
         if types.dim() != d + 2 or types.shape[0] != 1 or types.shape[1] != 1:

@@ -27,6 +27,40 @@ def make_weights_tanh(res: int, A: float, refinement: str = "BOTH") -> list[floa
     return w.tolist()
 
 
+def make_weights_simple(res: int, grading: float, refinement: str = "BOTH") -> list[float]:
+    """OpenFOAM-style simpleGrading (grid/shapes.py:795-877): cell sizes in geometric
+    progression with last/first ratio ``grading``; "BOTH" grades each half towards its wall
+    (the first res//2 cells growing, the rest shrinking). ``res+1`` weights in [0, 1]."""
+
+    def sizes_of(n: int) -> np.ndarray:
+        if abs(grading - 1.0) < 1e-10:
+            return np.full(n, 1.0 / n)
+        q = grading ** (1.0 / (n - 1))
+        s = q ** np.arange(n, dtype=np.float64)
+        return s / s.sum()
+
+    if refinement == "START":
+        sizes = sizes_of(res)
+    elif refinement == "END":
+        sizes = sizes_of(res)[::-1]
+    elif refinement == "BOTH":
+        half = res // 2
+        sizes = np.concatenate([sizes_of(half), sizes_of(res - half)[::-1]])
+    else:
+        raise ValueError(f"Unknown refinement '{refinement}'. Use 'START', 'END', or 'BOTH'.")
+    sizes = sizes / sizes.sum()
+    return [0.0] + np.cumsum(sizes).tolist()
+
+
+def make_weights(grading_type: str, res: int, grading: float, refinement: str = "BOTH") -> list[float]:
+    """Cell weights of a grading scheme by name (grid/shapes.py:996-1036): "simple" or "tanh"."""
+    if grading_type == "simple":
+        return make_weights_simple(res, grading, refinement)
+    if grading_type == "tanh":
+        return make_weights_tanh(res, grading, refinement)
+    raise ValueError(f"Unknown grading type '{grading_type}'. Use 'simple' or 'tanh'.")
+
+
 def make_weights_uniform(res: int) -> list[float]:
     return np.linspace(0.0, 1.0, res + 1).tolist()
 

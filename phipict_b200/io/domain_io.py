@@ -255,6 +255,15 @@ def _load_fixed(blk, f: int, fd: dict, get, with_scalar: bool) -> None:
         b.setPotentialTypes(types.to(torch.int8), cw=cw)
     elif "potentialBC" in fd:
         b.setPotentialBC(PotentialBC[fd["potentialBC"]], cw=cw)
+    else:
+        # files written before PotentialBC existed hold independent flags (reference
+        # io/domain_io.py:200-207), applied through the legacy setters in the same order
+        if "epotCw" in fd:
+            b.setEpotCw(fd["epotCw"])
+        if "epotInsulating" in fd:
+            b.setEpotInsulating(fd["epotInsulating"])
+        if fd.get("epotDirichlet", False):
+            b.setEpotDirichlet(True)
 
 
 __all__ = ["FORMAT_VERSION", "load_domain", "save_domain"]

@@ -7,7 +7,8 @@ out: that branch imports the reference's core.piso_diff, which needs the extensi
 default values themselves (1e-5 float32, 1e-8 float64) are pinned from
 core/piso_diff.py:397-421 in the test.
 
-Run from the repository root:  python tests/golden/make_tolerance_golden.py [reference root]
+Run from the repository root:  python tests/golden/make_tolerance_golden.py <reference root>
+(or with the root in the PHIPICT_REFERENCE environment variable)
 """
 from __future__ import annotations
 
@@ -101,4 +102,7 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PHIPICT_REFERENCE")
+    if not root:
+        sys.exit("give the reference root as the argument or in PHIPICT_REFERENCE")
+    main(root)

@@ -152,3 +152,33 @@ def test_reads_version_1_files_and_stores_shared_tensors_once(tmp_path: Path):
         arrays = {k: npz[k] for k in npz.files if k != "save_id"}
     np.savez_compressed(tmp_path / "d.npz", **arrays)
     _assert_same(dom, load_domain(tmp_path / "d"))
+
+
+def test_reads_the_legacy_potential_flags_of_old_files(tmp_path: Path):
+    """Files written before PotentialBC existed stored epotCw / epotInsulating /
+    epotDirichlet per face (phiPICT io/domain_io.py:200-207); they map onto the potential BC
+    as the legacy setters do (domain/boundaries.cpp:968-991)."""
+    dom = duct_3d(6, 5, 4, 2, device="cpu")
+    save_domain(dom, tmp_path / "d")
+    saved = json.loads((tmp_path / "d.json").read_text())
+    flags = {(0, 2): {"epotCw": 0.3}, (0, 3): {"epotDirichlet": True}, (1, 1): {"epotInsulating": False},
+             (1, 2): {"epotCw": 0.0, "epotInsulating": True, "epotDirichlet": False}}
+    for bi, bd in enumerate(saved["blocks"]):
+        for f, fd in enumerate(bd["boundaries"]):
+            fd.pop("potentialBC", None)
+            fd.pop("potentialCw", None)
+            fd.update(flags.get((bi, f), {}))
+    del saved["format_version"], saved["save_id"]
+    (tmp_path / "d.json").write_text(json.dumps(saved))
+    with np.load(tmp_path / "d.npz") as npz:
+        arrays = {k: npz[k] for k in npz.files if k != "save_id"}
+    np.savez_compressed(tmp_path / "d.npz", **arrays)
+    got = load_domain(tmp_path / "d")
+    b0, b1 = got.getBlocks()
+    P = pb.PotentialBC
+    assert b0.getBoundary("-y").getPotentialBC() == P.THIN_WALL and b0.getBoundary("-y").getEpotCw() == 0.3
+    assert b0.getBoundary("+y").getPotentialBC() == P.DIRICHLET and b0.getBoundary("+y").hasEpotDirichlet()
+    assert b1.getBoundary("+x").getPotentialBC() == P.OPEN and not b1.getBoundary("+x").isEpotInsulating()
+    assert b1.getBoundary("-y").getPotentialBC() == P.INSULATING
+    # faces without flags keep the default
+    assert b0.getBoundary("-x").getPotentialBC() == P.INSULATING
