@@ -303,6 +303,7 @@ def run_ours(args, rank, world, local):
     clk = clocks.stop()
     ms = t0.elapsed_time(t1)
     ms = max_over_ranks(ms, world)
+    final = (dom._u_block.clone(), dom.pressureResult.clone(), dom.epotResult.clone())
     # solver statistics of the timed steps
     solve_ms = 0.0
     per_tag: dict = {}
@@ -345,8 +346,11 @@ def run_ours(args, rank, world, local):
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), world) / e_steps
     del sim_e, dom_e
+    plain = plain_fp64_leg(args, wl, device, stream, final, world) if (mixed and not args.no_fp64_leg) else None
     total_cells = cells * world
     value = total_cells * args.steps / (ms / 1e3) / 1e6
+    if plain:
+        plain["vs_plain_fp64"]["mixed_over_plain"] = round(value / plain["vs_plain_fp64"]["value"], 3)
     # roofline of the dominant kernel: the (preconditioned) Krylov iteration, float32 when
     # mixed; solve time / inner iterations (the momentum BiCGStab iterations are counted as
     # CG-sized, a slight overestimate of their bytes)
@@ -394,11 +398,47 @@ def run_ours(args, rank, world, local):
                   "bytes_per_cell": round(per_cell, 2), "peak_source": pk["source"],
                   "iterations": inner_its, "solve_ms": round(solve_ms, 3)},
         gpu_launches=int(gpu_launches),
+        **({"vs_plain_fp64": plain["vs_plain_fp64"], "err_vs_fp64": plain["err_vs_fp64"]} if plain else {}),
         solver={"inner_iterations_per_step": round(inner_its / args.steps, 1),
                 "refinement_sweeps_per_step": round(sweeps / args.steps, 2),
                 "ms_per_step_by_solve": {k: round(v, 3) for k, v in per_tag.items()},
                 "iterations_per_step_by_solve": {k: round(v, 1) for k, v in tag_its.items()}},
     )
+
+
+def plain_fp64_leg(args, wl, device, stream, final, world) -> dict:
+    """The plain FP64 single-instance path (FP64 CG / BiCGStab, no refinement, no multigrid) on
+    the same workload: the same warm-up and timed step counts from the same initial state, timed
+    with CUDA events; its fields after the same number of steps are the all-FP64 run that the
+    mixed-precision fields are compared with (relative L2 error per field)."""
+    dom, sim = build_sim(wl, device, False, False)
+    for _ in range(args.warmup):
+        if not sim.single_step():
+            raise RuntimeError("plain FP64 warm-up step failed")
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(args.steps):
+        if not sim.single_step():
+            raise RuntimeError("plain FP64 step failed")
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(a.elapsed_time(b), world) / args.steps
+    cells = dom.getTotalSize() * world
+    ref = (dom._u_block, dom.pressureResult, dom.epotResult)
+
+    def rel(x, y):
+        return float(torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y))
+
+    err = {k: rel(x, y) for k, x, y in zip(("u", "p", "phi"), final, ref)}
+    value = cells / (ms / 1e3) / 1e6
+    return {"vs_plain_fp64": {"value": round(value, 4), "unit": "Mcell-steps/s", "ms_per_step": round(ms, 3),
+                              "dtype": "f64", "path": "FP64 CG pressure/potential, FP64 BiCGStab momentum, no refinement, "
+                                                      "no multigrid, one instance",
+                              "steps": args.steps, "warmup": args.warmup},
+            "err_vs_fp64": {**{k: float(f"{v:.3e}") for k, v in err.items()},
+                            "norm": "relative L2 against the plain FP64 run after the same warm-up + timed steps"}}
 
 
 def cpu_baseline(wl, sample_steps=1, min_seconds=0.0, max_steps=8) -> dict:
@@ -865,6 +905,7 @@ def main():
     ap.add_argument("--plain-fp64", action="store_true", help="the plain float64 path (no refinement)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-amg", action="store_true", help="unpreconditioned CG for pressure and potential")
+    ap.add_argument("--no-fp64-leg", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--inner-rtol", type=float, default=None, help="inner FP32 reduction per refinement sweep")
     ap.add_argument("--no-alone", action="store_true", help="batch64: skip the one-at-a-time comparison")
     ap.add_argument("--requests", type=int, default=None, help="serve: number of requests")

@@ -126,7 +126,9 @@ class FixedBoundary(Boundary):
         d = block.getSpatialDims()
         if velocity is None:
             velocity = torch.zeros(1, d, dtype=domain.getDtype(), device=domain.getDevice())
-        self._velocity = self._check_velocity(velocity)
+        # a differentiable simulation takes the boundary velocity as an input of the graph
+        self._velocity_ag = velocity if velocity.requires_grad else None
+        self._velocity = self._check_velocity(velocity.detach())
         self._velocityType = BoundaryConditionType(velocity_type)
         self._potentialType = PotentialBC.INSULATING
         self._potentialTypes: torch.Tensor | None = None
@@ -194,6 +196,9 @@ class FixedBoundary(Boundary):
 
     def setVelocity(self, velocity: torch.Tensor) -> None:
         v = self._check_velocity(velocity)
+        # a differentiable simulation takes the boundary velocity as an input of the graph
+        self._velocity_ag = velocity if velocity.requires_grad else None
+        v = v.detach()
         if v.shape == self._velocity.shape and self._domain._prepared_for(self):
             self._velocity.copy_(v)
         else:
@@ -435,8 +440,14 @@ class Block:
         spatial = list(reversed(self._sizes[:d]))
         opts = dict(dtype=domain.getDtype(), device=domain.getDevice())
         B = domain.getBatchSize()
-        self.velocity = velocity.to(**opts).contiguous() if velocity is not None else torch.zeros(B, d, *spatial, **opts)
-        self.pressure = pressure.to(**opts).contiguous() if pressure is not None else torch.zeros(B, 1, *spatial, **opts)
+        self.velocity = velocity.detach().to(**opts).contiguous() if velocity is not None else torch.zeros(B, d, *spatial, **opts)
+        self.pressure = pressure.detach().to(**opts).contiguous() if pressure is not None else torch.zeros(B, 1, *spatial, **opts)
+        # inputs of a differentiable simulation's graph (set when a tensor that requires grad is
+        # given; the block fields above hold their values)
+        self._velocity_ag = velocity if velocity is not None and velocity.requires_grad else None
+        self._source_ag: torch.Tensor | None = None
+        self._epot_ag: torch.Tensor | None = None
+        self._pressure_ag: torch.Tensor | None = None
         self.epot: torch.Tensor | None = None
         self.passiveScalar: torch.Tensor | None = None
         if domain.hasPassiveScalar():
@@ -493,7 +504,9 @@ class Block:
         v = velocity.to(dtype=self._domain.getDtype(), device=self._domain.getDevice())
         if v.shape != self.velocity.shape:
             raise RuntimeError(f"velocity must have shape {tuple(self.velocity.shape)}, got {tuple(v.shape)}")
-        self.velocity.copy_(v)
+        self._domain._restore_block_views(self, ("velocity",))
+        self._velocity_ag = velocity if velocity.requires_grad else None
+        self.velocity.copy_(v.detach())
 
     def setPressure(self, pressure: torch.Tensor) -> None:
         self.pressure.copy_(pressure.to(dtype=self._domain.getDtype(), device=self._domain.getDevice()))
@@ -509,15 +522,20 @@ class Block:
             s = s.view(1, -1)
         if s.shape[1] != d or s.dim() not in (2, d + 2):
             raise RuntimeError(f"velocity source must be [B, {d}] or [B, {d}, *spatial], got {tuple(s.shape)}")
-        self._domain._set_block_source(self, s)
+        self._source_ag = s if s.requires_grad else None
+        self._domain._source_writes += 1
+        self._domain._set_block_source(self, s.detach())
 
     def clearVelocitySource(self) -> None:
+        self._source_ag = None
+        self._domain._source_writes += 1
         self._domain._set_block_source(self, None)
 
     def setEpot(self, epot: torch.Tensor) -> None:
         """The electric potential [B, 1, *spatial]; before SetupEpotOnDomain it is kept and
         taken over when the potential fields are allocated."""
-        e = epot.to(dtype=self._domain.getDtype(), device=self._domain.getDevice())
+        self._epot_ag = epot if epot.requires_grad else None
+        e = epot.detach().to(dtype=self._domain.getDtype(), device=self._domain.getDevice())
         if self.epot is None:
             self.epot = e.contiguous()
             return
@@ -765,6 +783,7 @@ class Domain:
         self._batch = 1
         self._prepared = False
         self._version = 0
+        self._source_writes = 0  # velocity-source assignments (a differentiable step watches them)
         self._epot_on = False
         self._epot_flags = (0, False)
         self._advection_scheme = AdvectionScheme.CENTRAL
@@ -1381,6 +1400,48 @@ class Domain:
         if not self._prepared:
             raise RuntimeError("Domain is not initialized. Run domain.PrepareSolve() first.")
         return self._desc
+
+    # --- differentiable simulations -------------------------------------------------------
+    def _block_view(self, b: "Block", field: str) -> torch.Tensor | None:
+        """The view of the flat state buffer that a block field normally is."""
+        d, B = self._dims, self._batch
+        spatial = list(reversed(b._sizes[:d]))
+        o, n = b.globalOffset, b.ncells()
+        if field == "velocity":
+            return self._u_block[:, :, o:o + n].view(B, d, *spatial)
+        if field == "pressure":
+            return self._p_block[:, o:o + n].view(B, 1, *spatial)
+        if field == "epot":
+            e = getattr(self, "_epot_block", None)
+            return None if e is None else e[:, o:o + n].view(B, 1, *spatial)
+        if field == "velocitySource":
+            return self._src[:, :, o:o + n].view(B, d, *spatial) if self._src_mode == 2 else b.velocitySource
+        raise KeyError(field)
+
+    _AG_FIELDS = (("velocity", "_velocity_ag"), ("pressure", "_pressure_ag"), ("epot", "_epot_ag"),
+                  ("velocitySource", "_source_ag"))
+
+    def _restore_block_views(self, b: "Block", fields=None) -> None:
+        """Point fields that a differentiable step replaced by graph outputs back at the flat
+        buffers (their values are equal) and forget their graph inputs."""
+        if not self._prepared:
+            return
+        for field, ag in self._AG_FIELDS:
+            if fields is not None and field not in fields:
+                continue
+            t = getattr(b, field)
+            if t is not None and t.requires_grad:
+                setattr(b, field, self._block_view(b, field))
+            setattr(b, ag, None)
+
+    def Detach(self) -> None:
+        """Drop the autograd history of every field (reference Domain::Detach): the block fields
+        become plain views of the domain's buffers again, with their current values."""
+        for b in self._blocks:
+            self._restore_block_views(b)
+            for bd in b._boundaries:
+                if isinstance(bd, FixedBoundary):
+                    bd._velocity_ag = None
 
     def UpdateDomainData(self) -> None:
         """Re-pack after structural changes (new boundaries, sizes or data shapes). Values

@@ -152,6 +152,8 @@ class MHDSimulation(Simulation):
     # --- hooks -------------------------------------------------------------------------
     def _add_lorentz_force(self, domain: Domain, **kwargs) -> None:
         """J from phi and u x e_b, F_L = N (J x e_b) added onto the velocity source."""
+        if self._diff is not None and self._diff.rec is not None:
+            self._diff.source_in()  # the source before the force, for the reverse pass
         if self._potential_stale:
             self._magnetic_step_callback(domain)
             self._potential_stale = False
@@ -203,4 +205,4 @@ class MHDSimulation(Simulation):
         return J.view(B, 3, N)[:, :, block.globalOffset:block.globalOffset + n].reshape(B, 3, *spatial)
 
     def detach(self) -> None:
-        pass
+        super().detach()

@@ -94,9 +94,6 @@ class Simulation:
             raise NotImplementedError("pressure_time_step_normalized is not implemented")
         if substeps != "ADAPTIVE" and not (isinstance(substeps, int) and substeps > 0):
             raise ValueError("substeps must be a positive int or 'ADAPTIVE'")
-        if differentiable:
-            raise NotImplementedError(
-                "the differentiable rollout is provided by phipict_b200.adjoint (AdjointMHD, rollout)")
         self.domain = domain
         self.time_step = float(dt)
         self.substeps = substeps if substeps == "ADAPTIVE" else int(substeps)
@@ -120,7 +117,10 @@ class Simulation:
         self.pressure_return_best_result = pressure_return_best_result
         self.non_orthogonal = non_orthogonal
         self.advect_passive_scalar = bool(advect_passive_scalar)
-        self.differentiable = False
+        # differentiable=True: every PISO step is one torch.autograd node whose backward is the
+        # hand-written adjoint of the step (phipict_b200.differentiable); set up at the first step
+        self.differentiable = bool(differentiable)
+        self._diff = None
         self.linear_solve_max_iterations = 5000
         self.mixed_precision = bool(mixed_precision)
         # mixed precision: each inner FP32 solve reduces the outer residual by this factor
@@ -294,7 +294,31 @@ class Simulation:
         return True
 
     def _PISO_split_step(self, iterations: int, time_step=None) -> bool:
+        if not self.differentiable:
+            return self._PISO_split_step_plain(iterations, time_step)
+        if self._diff is None:
+            from .differentiable import DiffRunner
+
+            self._diff = DiffRunner(self)
+        if self._nonortho_flags():
+            raise NotImplementedError("the differentiable step is the orthogonal step: this grid has cross terms")
+        ts = self._time_step_tensor(time_step)
+        for _ in range(int(iterations)):
+            try:
+                self._diff.step(ts)
+            except RuntimeError as e:
+                self.last_error = str(e)
+                return False
+        return True
+
+    def detach(self) -> None:
+        """Drop the autograd history the simulation keeps between steps (u x e_b of MHD)."""
+        if self._diff is not None:
+            self._diff.uxb_ag = None
+
+    def _PISO_split_step_plain(self, iterations: int, time_step=None) -> bool:
         d = self.domain
+        rec = self._diff if (self._diff is not None and self._diff.rec is not None) else None
         ts = self._time_step_tensor(time_step)
         dims = d.getSpatialDims()
         for step in range(int(iterations)):
@@ -306,6 +330,8 @@ class Simulation:
             if self.advect_passive_scalar and d.hasPassiveScalar():
                 matrix_for_velocity = self._advect_scalar(ts, step, flags)
             self._run_hooks(Hook.PRE_VELOCITY_SETUP, local_step=step, time_step=ts)
+            if rec is not None:
+                rec.source_in()
             if not matrix_for_velocity:
                 backend.SetupAdvectionMatrix(d, ts, flags)
             if not flags:
@@ -333,7 +359,11 @@ class Simulation:
                     backend.SetupPressureMatrix(d, ts, flags, False)
                 # with flags, the divergence carries the cross terms of the pressure result in
                 # place (the previous corrector's), core/piso_simulation.py:3978-4117
+                if rec is not None:
+                    rec.ustar(d.velocityResult)
                 backend.SetupPressureRHS(d, ts, flags, False, False)
+                if rec is not None:
+                    rec.hbya(d.pressureRHS)
                 self._run_hooks(Hook.POST_PRESSURE_SETUP, local_step=step, time_step=ts)
                 guess = self._pressure_guess.get(cstep) if self.pressure_warm_start else None
                 if guess is not None:
@@ -345,6 +375,8 @@ class Simulation:
                            return_best=self.pressure_return_best_result)
                 if self.normalize_pressure_result:
                     d._subtract_mean(d.pressureResult, 1)
+                if rec is not None:
+                    rec.pressure(d.pressureResult)
                 for pstep in range(1, self.pressure_non_ortho_steps if flags else 1):
                     # the divergence of the same HbyA with the cross terms of the new result,
                     # re-solved from it
@@ -391,6 +423,8 @@ class Simulation:
         d = self.domain
         CFL = self.adaptive_CFL if CFL_cond is None else float(CFL_cond)
         if d.getBatchSize() > 1 and self.adaptive_CFL_per_env:
+            if self.differentiable:
+                raise NotImplementedError("a differentiable batch takes shared substeps: set adaptive_CFL_per_env=False")
             return self._PISO_adaptive_step_per_env(CFL, max_substeps)
         remaining = self.time_step
         self.adaptive_substeps = 0

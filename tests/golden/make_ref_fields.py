@@ -85,6 +85,7 @@ def main() -> None:
     ap.add_argument("--time-duct", action="store_true")
     ap.add_argument("--skip-fixtures", action="store_true")
     ap.add_argument("--cases", default="c1_fp64,c1_fp32,c2r_fp64", help="comma list of <case>_<dtype>")
+    ap.add_argument("--grads", action="store_true", help="also the gradient cases of the differentiable step")
     a = ap.parse_args()
     import phipict as pp
 
@@ -96,6 +97,17 @@ def main() -> None:
         for name in a.cases.split(","):
             case, dtype, tight = runs[name]
             print(json.dumps(run_case(pp, case, dtype, tight, out)), flush=True)
+    if a.grads:
+        for case, make in (("g1", rc.g1_inputs), ("g2", rc.g2_inputs)):
+            inputs = make()
+            t0 = time.time()
+            g = rc.grad_run(pp, case, inputs, torch.device("cuda"))
+            data = {k: np.asarray(v) for k, v in inputs.items()}
+            data.update({k: np.asarray(v) for k, v in g.items()})
+            data["meta"] = np.array(json.dumps(dict(case=case, params=rc.G1 if case == "g1" else rc.G2,
+                                                    device=torch.cuda.get_device_name(0))))
+            np.savez_compressed(out / f"ref_{case}_grad.npz", **data)
+            print(json.dumps(dict(tag=f"{case}_grad", loss=g["loss"], wall_s=round(time.time() - t0, 2))), flush=True)
     if a.time_duct:
         print(json.dumps(time_duct(pp, 3, 1, torch.float64)), flush=True)
         print(json.dumps(time_duct(pp, 3, 1, torch.float32)), flush=True)

@@ -117,11 +117,15 @@ def build_c2r(pp, inputs: dict, dtype, device, prepare: bool = True):
     return _finish(dom, blocks, inputs, dtype, device, prepare)
 
 
+TIGHT_RTOL, TIGHT_ATOL = 1e-14, 1e-16
+
+
 def tolerances(pp, tight: bool) -> dict:
-    """Tight: every solve to rtol 1e-12 / atol 1e-14, so that the fields are fixed to far
-    below the FP64 parity bar. Otherwise the configuration's 1e-8, read as a relative
-    tolerance (floored at 8 eps ||b||/sqrt(n) by SolverTolerance)."""
-    t = pp.SolverTolerance(rtol=1e-12, atol=1e-14) if tight else pp.SolverTolerance(rtol=1e-8)
+    """Tight: every solve to rtol 1e-14 / atol 1e-16, so that the fields are fixed to far
+    below the FP64 parity bar (a pressure solved to rtol r is off by about cond(P) r, which at
+    rtol 1e-12 already reaches 1e-10 on the duct). Otherwise the configuration's 1e-8, read as
+    a relative tolerance (floored at 8 eps ||b||/sqrt(n) by SolverTolerance)."""
+    t = pp.SolverTolerance(rtol=TIGHT_RTOL, atol=TIGHT_ATOL) if tight else pp.SolverTolerance(rtol=1e-8)
     return dict(advection_tol=t, pressure_tol=t, potential_tol=t)
 
 
@@ -171,3 +175,112 @@ def rel_l2(a, b) -> float:
     a = np.asarray(a, dtype=np.float64).ravel()
     b = np.asarray(b, dtype=np.float64).ravel()
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+# --- gradient cases (the differentiable step) -------------------------------------------
+G1 = dict(nx=24, ny=16, length=2.0, re=100.0, ha=10.0, dt=1e-2, steps=5, seed=3)
+G2 = dict(nx=8, ny=6, nz=6, nblocks=2, re=100.0, ha=5.0, beta=2.0, dt=1e-2, steps=3, noise=1e-1, seed=4)
+
+
+def g1_inputs() -> dict:
+    """Seeded state of the gradient channel: u = (1, 0) + 0.3 N(0, 1), a static source."""
+    p = G1
+    xs = np.linspace(0.0, p["length"], p["nx"] + 1)
+    ys = np.linspace(-1.0, 1.0, p["ny"] + 1)
+    g = torch.Generator(device="cpu").manual_seed(p["seed"])
+    u0 = 0.3 * torch.randn(1, 2, p["ny"], p["nx"], generator=g, dtype=torch.float64)
+    u0[:, 0] += 1.0
+    w = torch.rand(1, 2, p["ny"], p["nx"], generator=g, dtype=torch.float64)
+    return {"vertices_0": vertices(xs, ys), "velocity_0": u0.numpy(), "source": np.array([[0.5, -0.2]]),
+            "loss_w": w.numpy()}
+
+
+def g2_inputs() -> dict:
+    """Seeded state of the gradient duct: an inflow profile 1 + 0.1 N(0, 1) shared by the inflow
+    and outflow faces, u = 1 + 0.1 N(0, 1) in x."""
+    p = G2
+    ys = tanh_weights(p["ny"], p["beta"])
+    zs = tanh_weights(p["nz"], p["beta"])
+    g = torch.Generator(device="cpu").manual_seed(p["seed"])
+    prof = torch.zeros(1, 3, p["nz"], p["ny"], 1, dtype=torch.float64)
+    prof[0, 0] = 1.0 + p["noise"] * torch.randn(p["nz"], p["ny"], 1, generator=g, dtype=torch.float64)
+    out = {"inflow": prof.numpy()}
+    for i in range(p["nblocks"]):
+        xs = np.linspace(float(i), float(i + 1), p["nx"] + 1)
+        out[f"vertices_{i}"] = vertices(xs, ys, zs)
+        u0 = torch.zeros(1, 3, p["nz"], p["ny"], p["nx"], dtype=torch.float64)
+        u0[0, 0] = 1.0 + p["noise"] * torch.randn(p["nz"], p["ny"], p["nx"], generator=g, dtype=torch.float64)
+        out[f"velocity_{i}"] = u0.numpy()
+    out["loss_w"] = torch.rand(1, 3, p["nz"], p["ny"], p["nx"], generator=g, dtype=torch.float64).numpy()
+    return out
+
+
+def grad_run(pp, case: str, inputs: dict, device, sim_kwargs: dict | None = None) -> dict:
+    """The differentiable rollout of a gradient case on implementation pp; returns the loss
+    and its gradients.
+
+    g1: loss = sum(w u^2) + 0.1 sum(p^2) after G1 steps, gradients with respect to the initial
+    velocity, the static velocity source and the Stuart number.
+    g2: loss = sum(w u^2) over the outlet block + sum(phi^2) after G2 steps, gradients with
+    respect to the shared inflow/outflow profile, the initial velocity of the first block and
+    the Stuart number (the source is reset before every Lorentz force, so it has none)."""
+    dtype = torch.float64
+    p = G1 if case == "g1" else G2
+    stuart = torch.tensor([p["ha"] ** 2 / p["re"]], dtype=dtype, requires_grad=True)
+    v0 = _t(inputs["velocity_0"], dtype, device).requires_grad_(True)
+    kw = dict(dt=p["dt"], substeps=1, corrector_steps=2, non_orthogonal=False, advection_use_BiCG=True,
+              pressure_use_BiCG=False, pressure_use_amg=False, potential_use_preconditioner=False,
+              e_b=torch.tensor([0.0, 1.0, 0.0], dtype=dtype), stuart_number=stuart, differentiable=True)
+    kw.update(tolerances(pp, True))
+    kw.update(sim_kwargs or {})
+    if case == "g1":
+        dom = pp.Domain(2, torch.tensor([1.0 / p["re"]], dtype=dtype), name="gchannel", device=device, dtype=dtype)
+        b = dom.CreateBlock(vertexCoordinates=_t(inputs["vertices_0"], dtype, device), name="channel")
+        b.CloseBoundary("-y")
+        b.CloseBoundary("+y")
+        b.MakePeriodic("x")
+        dom.PrepareSolve()
+        src = _t(inputs["source"], dtype, device).requires_grad_(True)
+        b.setVelocity(v0.clone())
+        b.setVelocitySource(src.clone())
+        dom.UpdateDomainData()
+        sim = pp.MHDSimulation(domain=dom, **kw)
+        for _ in range(p["steps"]):
+            sim.single_step()
+        w = _t(inputs["loss_w"], dtype, device)
+        blk = dom.getBlocks()[0]
+        loss = (w * blk.velocity ** 2).sum() + 0.1 * (blk.pressure ** 2).sum()
+        names, wrt = ["velocity_0", "source", "stuart"], [v0, src, stuart]
+    else:
+        dom = pp.Domain(3, torch.tensor([1.0 / p["re"]], dtype=dtype), name="gduct", device=device, dtype=dtype)
+        blocks = [dom.CreateBlock(vertexCoordinates=_t(inputs[f"vertices_{i}"], dtype, device), name=f"b{i}")
+                  for i in range(p["nblocks"])]
+        for i in range(p["nblocks"] - 1):
+            blocks[i].ConnectBlock("+x", blocks[i + 1], "-x", "-y", "-z")
+        prof = _t(inputs["inflow"], dtype, device).requires_grad_(True)
+        blocks[0].CloseBoundary("-x", prof.detach().clone())
+        blocks[-1].CloseBoundary("+x", prof.detach().clone())
+        blocks[-1].getBoundary("+x").setPotentialBC(pp.PotentialBC.OPEN)
+        for b in blocks:
+            for f in ("-y", "+y", "-z", "+z"):
+                b.CloseBoundary(f)
+        dom.PrepareSolve()
+        blocks[0].setVelocity(v0.clone())
+        for i in range(1, p["nblocks"]):
+            blocks[i].setVelocity(_t(inputs[f"velocity_{i}"], dtype, device))
+        blocks[0].getBoundary("-x").setVelocity(prof)
+        blocks[-1].getBoundary("+x").setVelocity(prof)
+        dom.UpdateDomainData()
+        kw.setdefault("hooks", reset_source_hook(pp, 3, dtype))
+        sim = pp.MHDSimulation(domain=dom, **kw)
+        for _ in range(p["steps"]):
+            sim.single_step()
+        w = _t(inputs["loss_w"], dtype, device)
+        loss = (w * blocks[-1].velocity ** 2).sum() + (dom.getBlocks()[-1].epot ** 2).sum()
+        names, wrt = ["inflow", "velocity_0", "stuart"], [prof, v0, stuart]
+    grads = torch.autograd.grad(loss, wrt)
+    out = {"loss": float(loss.detach())}
+    for k, g in zip(names, grads):
+        out[f"grad_{k}"] = g.detach().double().cpu().numpy()
+    dom.Detach()
+    return out

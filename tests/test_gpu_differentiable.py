@@ -1,0 +1,187 @@
+"""Simulation(differentiable=True): each PISO step one torch.autograd node whose backward is
+the hand-written adjoint of the step (phipict_b200/differentiable.py).
+
+- gradients against the reference's own differentiable backend (phiPICT core/piso_diff.py,
+  run on a B200 by tests/golden/make_ref_fields.py --grads) on a 2D MHD channel (initial
+  velocity, static velocity source, Stuart number; a loss on u and p) and on a 2-block MHD
+  duct (shared inflow/outflow profile, initial velocity, Stuart number; a loss on u and phi);
+- gradients against central finite differences of the forward (the north star's 1e-5 bar);
+- the differentiable forward gives the same fields as the ordinary step;
+- the same gradients from the checkpointed rollout (AdjointMHD) as from the simulation.
+"""
+import math
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+import phipict_b200 as pb
+
+GOLD = Path(__file__).resolve().parent / "golden"
+sys.path.insert(0, str(GOLD))
+import ref_cases as rc  # noqa: E402
+from test_ref_fixtures import load_fixture  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+REF_BAR = 1e-6  # gradients of two FP64 implementations whose solves stop at rtol 1e-14
+FD_BAR = 1e-5
+
+
+def load_grad(case: str) -> dict:
+    return load_fixture(f"{case}_grad")
+
+
+def rel(a, b) -> float:
+    a, b = np.asarray(a, dtype=np.float64).ravel(), np.asarray(b, dtype=np.float64).ravel()
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.mark.parametrize("case", ["g1", "g2"])
+def test_gradients_match_reference(cuda, case):
+    data = load_grad(case)
+    got = rc.grad_run(pb, case, data, cuda)
+    assert abs(got["loss"] - float(data["loss"])) <= 1e-10 * abs(float(data["loss"]))
+    for k in [k for k in data if k.startswith("grad_")]:
+        e = rel(got[k], data[k])
+        assert math.isfinite(e) and e < REF_BAR, f"{case} {k}: {e:.3e}"
+        assert np.abs(data[k]).max() > 0
+
+
+def _g1_loss(inputs, v0, src, stuart, device="cuda"):
+    """The g1 loss as a plain function of its inputs (no autograd)."""
+    p = rc.G1
+    dtype = torch.float64
+    dom = pb.Domain(2, torch.tensor([1.0 / p["re"]], dtype=dtype), name="g", device=device, dtype=dtype)
+    b = dom.CreateBlock(vertexCoordinates=rc._t(inputs["vertices_0"], dtype, device), name="channel")
+    b.CloseBoundary("-y")
+    b.CloseBoundary("+y")
+    b.MakePeriodic("x")
+    dom.PrepareSolve()
+    b.setVelocity(v0)
+    b.setVelocitySource(src)
+    dom.UpdateDomainData()
+    kw = dict(dt=p["dt"], substeps=1, non_orthogonal=False, e_b=torch.tensor([0.0, 1.0, 0.0], dtype=dtype),
+              stuart_number=torch.tensor(float(stuart), dtype=torch.float64))
+    kw.update(rc.tolerances(pb, True))
+    sim = pb.MHDSimulation(domain=dom, **kw)
+    for _ in range(p["steps"]):
+        assert sim.single_step()
+    w = rc._t(inputs["loss_w"], dtype, device)
+    return float((w * b.velocity ** 2).sum() + 0.1 * (b.pressure ** 2).sum())
+
+
+def test_gradients_match_finite_differences(cuda):
+    inputs = rc.g1_inputs()
+    got = rc.grad_run(pb, "g1", inputs, cuda)
+    g = torch.Generator().manual_seed(11)
+    v0 = torch.as_tensor(inputs["velocity_0"]).cuda()
+    src = torch.as_tensor(inputs["source"]).cuda()
+    N0 = rc.G1["ha"] ** 2 / rc.G1["re"]
+    h = 1e-4
+    for name in ("velocity_0", "source", "stuart"):
+        if name == "stuart":
+            dirn = torch.ones(1, dtype=torch.float64)
+        else:
+            base = v0 if name == "velocity_0" else src
+            dirn = torch.randn(base.shape, generator=g, dtype=torch.float64)
+            dirn /= dirn.abs().max()
+        args = lambda s: (v0 + s * h * dirn.cuda() if name == "velocity_0" else v0,
+                          src + s * h * dirn.cuda() if name == "source" else src,
+                          N0 + s * h * float(dirn[0]) if name == "stuart" else N0)
+        fd = (_g1_loss(inputs, *args(1)) - _g1_loss(inputs, *args(-1))) / (2 * h)
+        ad = float((torch.as_tensor(got[f"grad_{name}"]) * dirn.reshape(got[f"grad_{name}"].shape)).sum())
+        assert abs(ad - fd) <= FD_BAR * max(abs(fd), 1e-30), f"{name}: adjoint {ad:.10e} vs FD {fd:.10e}"
+
+
+def test_differentiable_forward_is_the_plain_step(cuda):
+    """The recorded forward changes nothing: same fields as the non-differentiable run."""
+    inputs = rc.g1_inputs()
+    fields = []
+    for diff in (False, True):
+        p = rc.G1
+        dtype = torch.float64
+        dom = pb.Domain(2, torch.tensor([1.0 / p["re"]], dtype=dtype), name="g", device="cuda", dtype=dtype)
+        b = dom.CreateBlock(vertexCoordinates=rc._t(inputs["vertices_0"], dtype, "cuda"), name="channel")
+        b.CloseBoundary("-y")
+        b.CloseBoundary("+y")
+        b.MakePeriodic("x")
+        dom.PrepareSolve()
+        v0 = torch.as_tensor(inputs["velocity_0"]).cuda()
+        b.setVelocity(v0.clone().requires_grad_(diff))
+        b.setVelocitySource(torch.as_tensor(inputs["source"]).cuda())
+        dom.UpdateDomainData()
+        kw = dict(dt=p["dt"], substeps=1, non_orthogonal=False, e_b=torch.tensor([0.0, 1.0, 0.0], dtype=dtype),
+                  stuart_number=torch.tensor(p["ha"] ** 2 / p["re"]), differentiable=diff)
+        kw.update(rc.tolerances(pb, True))
+        sim = pb.MHDSimulation(domain=dom, **kw)
+        for _ in range(p["steps"]):
+            assert sim.single_step()
+        fields.append((b.velocity.detach().clone(), b.pressure.detach().clone()))
+        assert b.velocity.requires_grad == diff
+        dom.Detach()
+        assert not b.velocity.requires_grad
+    for a, c in zip(*fields):
+        assert torch.equal(a, c)
+
+
+def test_rollout_and_simulation_agree(cuda):
+    """AdjointMHD's checkpointed rollout and Simulation(differentiable=True) differentiate the
+    same steps: gradients of sum(w u^2) with respect to the duct's inflow profile and the
+    Stuart number agree."""
+    from phipict_b200.adjoint import AdjointMHD, rollout
+
+    inputs = rc.g2_inputs()
+    p = rc.G2
+    dtype = torch.float64
+    w = rc._t(inputs["loss_w"], dtype, "cuda")
+
+    def build():
+        dom = pb.Domain(3, torch.tensor([1.0 / p["re"]], dtype=dtype), name="gduct", device="cuda", dtype=dtype)
+        blocks = [dom.CreateBlock(vertexCoordinates=rc._t(inputs[f"vertices_{i}"], dtype, "cuda"), name=f"b{i}")
+                  for i in range(p["nblocks"])]
+        blocks[0].ConnectBlock("+x", blocks[1], "-x", "-y", "-z")
+        prof = rc._t(inputs["inflow"], dtype, "cuda")
+        blocks[0].CloseBoundary("-x", prof.clone())
+        blocks[1].CloseBoundary("+x", prof.clone())
+        blocks[1].getBoundary("+x").setPotentialBC(pb.PotentialBC.OPEN)
+        for b in blocks:
+            for f in ("-y", "+y", "-z", "+z"):
+                b.CloseBoundary(f)
+        dom.PrepareSolve()
+        for i, b in enumerate(blocks):
+            b.setVelocity(rc._t(inputs[f"velocity_{i}"], dtype, "cuda"))
+        dom.UpdateDomainData()
+        return dom, blocks, prof
+
+    N0 = p["ha"] ** 2 / p["re"]
+    # the simulation
+    dom, blocks, prof = build()
+    prof = prof.clone().requires_grad_(True)
+    stuart = torch.tensor([N0], dtype=dtype, requires_grad=True)
+    blocks[0].getBoundary("-x").setVelocity(prof)
+    blocks[1].getBoundary("+x").setVelocity(prof)
+    kw = dict(dt=p["dt"], substeps=1, non_orthogonal=False, e_b=torch.tensor([0.0, 1.0, 0.0], dtype=dtype),
+              stuart_number=stuart, differentiable=True, hooks=rc.reset_source_hook(pb, 3, dtype))
+    kw.update(rc.tolerances(pb, True))
+    sim = pb.MHDSimulation(domain=dom, **kw)
+    for _ in range(p["steps"]):
+        assert sim.single_step()
+    loss = sum((w * b.velocity ** 2).sum() for b in blocks)
+    g_prof, g_N = torch.autograd.grad(loss, [prof, stuart])
+    dom.Detach()
+    # the rollout
+    dom, blocks, prof0 = build()
+    model = AdjointMHD(dom, p["dt"], torch.tensor([N0]), torch.tensor([0.0, 1.0, 0.0]), p["steps"],
+                       faces=[(0, "-x"), (1, "+x")], checkpoint_every=2, tol=1e-12)
+    prof_r = prof0.clone().requires_grad_(True)
+    st_r = torch.tensor([N0], dtype=dtype, requires_grad=True)
+    u = rollout(model, prof_r, st_r)
+    B, n = 1, dom.getTotalSize()
+    uu = u.view(B, 3, n)
+    loss_r = sum((w.reshape(1, 3, -1) * uu[:, :, b.globalOffset:b.globalOffset + b.ncells()] ** 2).sum() for b in blocks)
+    g_prof_r, g_N_r = torch.autograd.grad(loss_r, [prof_r, st_r])
+    assert rel(g_prof.cpu(), g_prof_r.cpu()) < REF_BAR
+    assert rel(g_N.cpu(), g_N_r.cpu()) < REF_BAR
