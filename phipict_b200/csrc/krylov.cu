@@ -228,15 +228,16 @@ struct FBicgS { // BiCGStab half step s = r - alpha v
 };
 
 // y = A f and f itself at the quad's cells for every active right-hand side (zeros for the
-// others and past q.n). On the fast path the four cells' stencil rows and neighbour groups
-// are loaded at once, slot by slot; elsewhere every cell resolves its neighbours across
-// faces. The products are summed in the same order on both paths (centre, then faces -x +x
-// -y +y -z +z, a face without neighbour skipped).
+// others and past q.n). On the fast path (a quad inside one row whose y and z neighbours are
+// in the block or absent behind a prescribed face) the four cells' stencil rows and neighbour
+// groups are loaded at once, slot by slot; elsewhere every cell resolves its neighbours
+// across faces. The products are summed in the same order on both paths (centre, then faces
+// -x +x -y +y -z +z, a face without neighbour skipped).
 template <typename T, int D, int K, typename F>
 __device__ __forceinline__ void quadApply(const Dom<double, D> &dom, const T *__restrict__ A, const Quad &q, const bool (&act)[K],
 		const F (&fld)[K], T (&y)[K][4], T (&f)[K][4]) {
 	const int64_t N = dom.ncells;
-	if (q.fast) {
+	if (q.fastW) {
 		// x neighbours of the row ends: across the block's x face when the quad touches it
 		int64_t gW = q.g - 1, gE = q.g + 4;
 		if (q.p[0] == 0 || q.p[0] + 3 == q.B[B_NX] - 1) {
@@ -289,6 +290,7 @@ __device__ __forceinline__ void quadApply(const Dom<double, D> &dom, const T *__
 		}
 #pragma unroll
 		for (int sl = 3; sl < 2 * D + 1; ++sl) {
+			if ((q.miss >> (sl - 3)) & 1) continue; // behind a prescribed face: no neighbour
 			const int64_t off = sl == 3 ? -(int64_t)q.sy : sl == 4 ? (int64_t)q.sy : sl == 5 ? -(int64_t)q.sz : (int64_t)q.sz;
 			const bool al = sl < 5 ? q.alY : q.alZ;
 			ld4(A + sl * N + q.g, 4, q.al, a);
@@ -1104,6 +1106,7 @@ __device__ __forceinline__ void cgPersistentBody(const Dom<double, D> &dom, cons
 	static_assert(!PC || (std::is_same<T, float>::value && K == 1), "the V-cycle preconditions float single-rhs CG");
 	extern __shared__ SysState sst[];
 	__shared__ int32_t sB[PHB_BREC];
+	__shared__ int32_t sBs[PC ? 4 : 1][PHB_BREC];
 	const int nsys = dom.ninst * K;
 	for (int s = threadIdx.x; s < nsys; s += blockDim.x) sst[s] = st[s];
 	__syncthreads();
@@ -1143,7 +1146,10 @@ __device__ __forceinline__ void cgPersistentBody(const Dom<double, D> &dom, cons
 				if (l == 0 && quads) {
 					for (int sub = blockIdx.x; sub < mg.lv[1].ntiles * RESTRICT1_PER_TILE; sub += gridDim.x) amgRestrictCoarseCell<D>(mg, 0, sub, sB);
 				} else {
-					for (int sub = blockIdx.x; sub < mg.lv[l + 1].ntiles * Restrict<D>::PER_TILE; sub += gridDim.x) amgRestrictSub<D>(mg, l, sub, sB);
+					// up to four of this CTA's sub-tiles per pass, their loads in flight together
+					const int nsub = mg.lv[l + 1].ntiles * Restrict<D>::PER_TILE;
+					for (int sub = blockIdx.x; sub < nsub; sub += 4 * gridDim.x)
+						amgRestrictMulti<D, 4>(mg, l, sub, gridDim.x, nsub, sBs);
 				}
 				if (!gridBarrier(ctrl)) return;
 			}
@@ -1247,8 +1253,10 @@ __device__ __forceinline__ void cgPersistentBody(const Dom<double, D> &dom, cons
 	}
 }
 
+// At least three resident CTAs per SM (at most 85 registers): a grid of one CTA per 1024-cell
+// tile then stays co-resident up to 444 tiles (the 442,368-cell duct has 432).
 template <typename T, int D, int K, bool STOPSTART, bool PC = false>
-__global__ void __launch_bounds__(PHB_TILE) kCgPersistent(Dom<double, D> dom, const T *__restrict__ A, const T *__restrict__ b,
+__global__ void __launch_bounds__(PHB_TILE, 3) kCgPersistent(Dom<double, D> dom, const T *__restrict__ A, const T *__restrict__ b,
 		T *__restrict__ x, T *__restrict__ r, T *__restrict__ p0, T *__restrict__ p1, T *__restrict__ q, T *__restrict__ xbest,
 		SysState *st, double *partial, Control *ctrl, phb_tolerance tol, int returnBest, int maxit, AmgView<D> mg) {
 	cgPersistentBody<T, D, K, STOPSTART, PC, false>(dom, A, b, x, r, p0, p1, q, xbest, st, partial, ctrl, tol, returnBest, maxit, mg);

@@ -333,6 +333,82 @@ __device__ __forceinline__ int restrictParts(int l0, int nc) {
 	return (cells + Restrict<D>::CELLS - 1) / Restrict<D>::CELLS;
 }
 
+// Restriction of up to NS sub-tiles sub0, sub0 + stride, ... (< nsub) of level l+1 at once:
+// their block records staged together into sBs, every thread's fine residuals evaluated for
+// all of them before the shuffle trees and stores, so that their loads overlap. Same
+// arithmetic and summation order as amgRestrictPart.
+template <int D, int NS>
+__device__ __forceinline__ void amgRestrictMulti(const AmgView<D> &mg, int l, int sub0, int stride, int nsub,
+		int32_t (*sBs)[PHB_BREC]) {
+	using R = Restrict<D>;
+	const Dom<float, D> &fd = mg.lv[l], &cd = mg.lv[l + 1];
+	const float *A = mg.A[l];
+	const float *wd = mg.wd[l];
+	const float *b = mg.b[l];
+	float *bc = mg.b[l + 1];
+	int bi[NS], l0[NS], part[NS];
+	__syncthreads();
+#pragma unroll
+	for (int s = 0; s < NS; ++s) {
+		const int sub = sub0 + s * stride;
+		bi[s] = -1;
+		if (sub < nsub) {
+			const int tile = sub / R::PER_TILE;
+			part[s] = sub - tile * R::PER_TILE;
+			bi[s] = __ldg(cd.tiles + 2 * tile);
+			l0[s] = __ldg(cd.tiles + 2 * tile + 1);
+			if (threadIdx.x < PHB_BREC) sBs[s][threadIdx.x] = __ldg(cd.blocks + bi[s] * PHB_BREC + threadIdx.x);
+		}
+	}
+	__syncthreads();
+	const int o = int(threadIdx.x) % R::G; // fine cell of its aggregate
+	float v[NS];
+	bool store[NS];
+#pragma unroll
+	for (int s = 0; s < NS; ++s) {
+		v[s] = 0.f;
+		store[s] = false;
+		if (bi[s] < 0) continue;
+		const int32_t *sB = sBs[s];
+		const int nc = sB[B_NX] * sB[B_NY] * (D > 2 ? sB[B_NZ] : 1);
+		if (part[s] >= restrictParts<D>(l0[s], nc)) continue;
+		const int lc = l0[s] + part[s] * R::CELLS + int(threadIdx.x) / R::G;
+		if (!(lc < nc && lc < l0[s] + PHB_TILE_CELLS)) continue;
+		store[s] = o == 0;
+		const int32_t *FB = fd.blk(bi[s]);
+		const int nx = sB[B_NX], ny = sB[B_NY];
+		const int cp[3] = {lc % nx, (lc / nx) % ny, D > 2 ? lc / (nx * ny) : 0};
+		Cell c;
+		bool fvalid = true;
+#pragma unroll
+		for (int a = 0; a < 3; ++a) {
+			const int fs = __ldg(FB + B_NX + a);
+			const int oa = (o >> a) & 1;
+			const bool co = a < D && sB[B_NX + a] < fs;
+			c.p[a] = co ? 2 * cp[a] + oa : cp[a];
+			fvalid &= co ? c.p[a] < fs : oa == 0;
+		}
+		if (fvalid) {
+			c.B = FB;
+			c.b = bi[s];
+			c.g = __ldg(FB + B_CELLOFF) + flat(FB, c.p);
+			c.mi = c.g;
+			v[s] = amgFineResidual<D>(fd, A, wd, b, c);
+		}
+	}
+#pragma unroll
+	for (int s = 0; s < NS; ++s) {
+#pragma unroll
+		for (int m = 1; m < R::G; m <<= 1) v[s] += __shfl_xor_sync(0xffffffffu, v[s], m);
+	}
+#pragma unroll
+	for (int s = 0; s < NS; ++s) {
+		if (!store[s]) continue;
+		const int lc = l0[s] + part[s] * R::CELLS + int(threadIdx.x) / R::G;
+		bc[sBs[s][B_CELLOFF] + lc] = v[s];
+	}
+}
+
 // Restriction for coarse sub-tile `sub` (part sub % PER_TILE of tile sub / PER_TILE) of level
 // l+1: b_{l+1} = P^T (b_l - A_l omega D^-1 b_l). Level vectors are read with plain loads: in
 // the persistent solver other CTAs wrote them earlier in the same launch.
@@ -398,12 +474,27 @@ __device__ __forceinline__ double amgProlongTile(const AmgView<D> &mg, int l, in
 	const int nc = stageBlock<D>(fd, bi, sB);
 	const int32_t *CB = cd.blk(bi);
 	double dot = 0;
-	for (int j = j0; j < j1; ++j) {
+	// every cell's value first, then the stores: amgProlongCell reads b, the stencil and the
+	// coarse correction, never `out`, so the loads of all cells can be in flight together
+	float z[CPT], bv[CPT];
+	int g[CPT];
+	int cnt = 0;
+#pragma unroll
+	for (int jj = 0; jj < CPT; ++jj) {
+		const int j = j0 + jj;
+		if (j >= j1) break;
 		Cell c;
 		if (!cellAt<D>(sB, l0, nc, j, c)) break;
-		const float z = amgProlongCell<D>(mg, l, sB, CB, c);
-		out[c.g] = z;
-		dot = fma(double(b[c.g]), double(z), dot);
+		z[jj] = amgProlongCell<D>(mg, l, sB, CB, c);
+		bv[jj] = b[c.g];
+		g[jj] = c.g;
+		cnt = jj + 1;
+	}
+#pragma unroll
+	for (int jj = 0; jj < CPT; ++jj) {
+		if (jj >= cnt) break;
+		out[g[jj]] = z[jj];
+		dot = fma(double(bv[jj]), double(z[jj]), dot);
 	}
 	return dot;
 }

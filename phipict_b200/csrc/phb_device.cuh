@@ -301,6 +301,9 @@ struct Quad {
 	                  // neighbours are at fixed strides except across an x face at a row end
 	bool al;          // four valid cells at a 4-aligned index of every operand: vector loads
 	bool alY, alZ;    // al, and the y (z) neighbour groups aligned too
+	bool fastW;       // as fast, but also on a y or z face of the block where that face is
+	                  // prescribed (a wall): the neighbour across it is absent
+	unsigned char miss; // fastW quads: bit 0/1/2/3 set when the -y/+y/-z/+z neighbour is absent
 };
 
 // K: right-hand sides per instance ([inst][K][cells] layout; their offsets must keep the
@@ -322,6 +325,18 @@ __device__ __forceinline__ void quadAt(int vec4, const int32_t *sB, int l0, int 
 	bool fast = q.n == 4 && q.p[0] + 3 <= nx - 1 && q.p[1] >= 1 && q.p[1] <= ny - 2;
 	if (D > 2) fast = fast && q.p[2] >= 1 && q.p[2] <= sB[B_NZ] - 2;
 	q.fast = fast;
+	// a row on a prescribed y or z face keeps the fixed strides: its neighbour across that face
+	// is absent, as a per-cell resolution finds it (neighborIndex returns -1 there)
+	bool inner = q.n == 4 && q.p[0] + 3 <= nx - 1;
+	int miss = 0;
+	if (q.p[1] == 0) { if (fType(sB, 2) == FT_FIXED) miss |= 1; else inner = false; }
+	if (q.p[1] == ny - 1) { if (fType(sB, 3) == FT_FIXED) miss |= 2; else inner = false; }
+	if (D > 2) {
+		if (q.p[2] == 0) { if (fType(sB, 4) == FT_FIXED) miss |= 4; else inner = false; }
+		if (q.p[2] == sB[B_NZ] - 1) { if (fType(sB, 5) == FT_FIXED) miss |= 8; else inner = false; }
+	}
+	q.fastW = inner;
+	q.miss = (unsigned char)miss;
 	bool al = vec4 && q.n == 4 && (q.g & 3) == 0;
 	if (K > 1) al = al && ((sB[B_INSTOFF] | sB[B_INSTN]) & 3) == 0;
 	q.al = al;
