@@ -23,14 +23,16 @@ def _selftest(lib, ctas, rounds, absent, limit, scratch):
     return err.value, done.value
 
 
-def test_barrier_passes_with_every_cta_present(cuda):
+@pytest.mark.parametrize("per_sm", [1, 3])
+def test_barrier_passes_with_every_cta_present(cuda, per_sm):
+    """One CTA per SM, and three (432 or 444 CTAs: many arrival groups, the last one short)."""
     lib = _lib.load()
     scratch = torch.zeros(512, dtype=torch.uint8, device="cuda")
-    ctas = torch.cuda.get_device_properties(0).multi_processor_count
+    ctas = per_sm * torch.cuda.get_device_properties(0).multi_processor_count - (12 if per_sm == 3 else 0)
     assert _selftest(lib, ctas, 300, -1, 1 << 20, scratch) == (0, 300)
 
 
-@pytest.mark.parametrize("absent", [0, 5])
+@pytest.mark.parametrize("absent", [0, 5, 17])
 def test_barrier_wait_runs_out_when_a_cta_is_absent(cuda, absent):
     lib = _lib.load()
     scratch = torch.zeros(512, dtype=torch.uint8, device="cuda")
