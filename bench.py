@@ -149,9 +149,9 @@ def algorithmic_pcg_bytes(dims: int, levels: list[int], dense_doubles: int = 0) 
 
 
 # DRAM bytes per preconditioned CG iteration on the duct workload, from a full ncu capture of
-# one persistent launch (the first inner solve of the timed step: 25.81 MB read + 0.65 MB
+# one persistent launch (the first inner solve of the timed step: 26.11 MB read + 0.57 MB
 # written in a 24-iteration solve): the working set is L2-resident
-PCG_DRAM_BYTES_PER_ITERATION_DUCT3D = (25.81e6 + 0.65e6) / 24
+PCG_DRAM_BYTES_PER_ITERATION_DUCT3D = (26.11e6 + 0.57e6) / 24
 
 
 class ClockSampler:
@@ -239,7 +239,7 @@ def barrier(world: int):
         dist.barrier()
 
 
-def build_sim(wl: dict, device, mixed: bool, amg: bool = True):
+def build_sim(wl: dict, device, mixed: bool, amg: bool = True, warm: bool = False):
     import phipict_b200 as pb
 
     dtype = torch.float64
@@ -259,7 +259,7 @@ def build_sim(wl: dict, device, mixed: bool, amg: bool = True):
     sim = pb.MHDSimulation(dom, wl["dt"], torch.tensor(N), torch.tensor([0.0, 1.0, 0.0], dtype=dtype),
                            non_orthogonal=False, advection_tol=tol, pressure_tol=tol, potential_tol=tol,
                            mixed_precision=mixed, hooks=hooks, pressure_use_amg=amg and mixed,
-                           potential_use_preconditioner=amg and mixed)
+                           potential_use_preconditioner=amg and mixed, pressure_warm_start=warm)
     return dom, sim
 
 
@@ -268,7 +268,7 @@ def run_ours(args, rank, world, local):
     device = torch.device("cuda", local)
     mixed = not args.plain_fp64
     amg = mixed and not args.no_amg
-    dom, sim = build_sim(wl, device, mixed, amg)
+    dom, sim = build_sim(wl, device, mixed, amg, args.pressure_warm_start)
     if args.inner_rtol:
         sim.refinement_inner_rtol = args.inner_rtol
     cells = dom.getTotalSize()
@@ -321,7 +321,7 @@ def run_ours(args, rank, world, local):
     # up the same way), every step reading its velocity from pinned host memory and writing u,
     # p and phi back there; the next step starts from the velocity it wrote
     d = dom.getSpatialDims()
-    dom_e, sim_e = build_sim(wl, device, mixed, amg)
+    dom_e, sim_e = build_sim(wl, device, mixed, amg, args.pressure_warm_start)
     if args.inner_rtol:
         sim_e.refinement_inner_rtol = args.inner_rtol
     for _ in range(args.warmup):
@@ -387,6 +387,9 @@ def run_ours(args, rank, world, local):
              "h2d_bytes_per_step": int(nu * h_out.element_size()),
              "d2h_bytes_per_step": int(h_out.numel() * h_out.element_size())},
         roofline={"bound": "hbm",
+                  "limited_by": ("grid-barrier and L2 latency: the ~60 MB working set stays in L2 (DRAM traffic "
+                                 "is ~1.5 % of the algorithmic bytes), so the fraction of HBM peak is low by "
+                                 "construction; HBM-bound fractions are measured by the roofline sweep") if amg else None,
                   "kernel": ("persistent PCG iteration (V-cycle + direction + update, kCgPersistent)" if amg
                              else "CG iteration (kCgDirection + kCgUpdate)"),
                   "achieved": round(achieved, 1) if achieved else None, "peak": pk.get("hbm_gbs"),
@@ -411,7 +414,7 @@ def plain_fp64_leg(args, wl, device, stream, final, world) -> dict:
     the same workload: the same warm-up and timed step counts from the same initial state, timed
     with CUDA events; its fields after the same number of steps are the all-FP64 run that the
     mixed-precision fields are compared with (relative L2 error per field)."""
-    dom, sim = build_sim(wl, device, False, False)
+    dom, sim = build_sim(wl, device, False, False, args.pressure_warm_start)
     for _ in range(args.warmup):
         if not sim.single_step():
             raise RuntimeError("plain FP64 warm-up step failed")
@@ -576,6 +579,21 @@ def run_batch64(args, rank, world, local):
                 gpu_launches=None)
 
 
+def batch64_record(args, rank, world, local) -> dict:
+    """A compact run of the heterogeneous batch (64 2D instances in one DomainBatch, 2 warm-up
+    and 5 timed steps) with the same instances stepped one at a time on the plain FP64 path:
+    the batched, mixed-precision path against the plain single-instance path, both timed with
+    CUDA events in this run."""
+    sub = argparse.Namespace(**vars(args))
+    sub.steps, sub.warmup, sub.plain_fp64, sub.no_alone = 5, 2, False, False
+    r = run_batch64(sub, rank, world, local)
+    alone = r["one_at_a_time"]["value"]
+    return {"workload": r["config"]["workload"], "cells": r["config"]["cells_per_gpu"], "value": r["value"],
+            "unit": "Mcell-steps/s", "ms_per_step": r["ms_per_step"], "steps": sub.steps, "warmup": sub.warmup,
+            "dtype": r["dtype"], "one_at_a_time": r["one_at_a_time"],
+            "batched_over_one_at_a_time": round(r["value"] / alone, 2) if alone else None}
+
+
 def serve_requests(wl, device, seed=0):
     """The seeded request stream: half 2D Hartmann channels with side U[64, 512], half 3D
     ducts of one block with side U[32, 128]; Ha log-uniform in [1, 1000], Re = 1000."""
@@ -601,6 +619,36 @@ def serve_requests(wl, device, seed=0):
     return reqs
 
 
+def serve_one_at_a_time(wl, device, tol, sample: int, steps: int) -> dict:
+    """The first `sample` requests of the stream run one at a time on the plain FP64 path
+    (FP64 CG/BiCGStab, no refinement, no multigrid), `steps` timed steps each after one
+    warm-up step, CUDA events around each request's steps: its Mcell-steps/s."""
+    import phipict_b200 as pb
+
+    cell_steps, ms = 0, 0.0
+    stream = torch.cuda.current_stream(device)
+    reqs = serve_requests(dict(wl, requests=max(sample, 1)), device, seed=0)[:sample]
+    for r in reqs:
+        dom = r.build()
+        sim = pb.MHDSimulation(dom, r.dt, torch.tensor([r.stuart], dtype=torch.float64),
+                               torch.tensor(r.e_b, dtype=torch.float64), non_orthogonal=False, advection_tol=tol,
+                               pressure_tol=tol, potential_tol=tol,
+                               hooks=pb.Hooks().append(pb.Hook.PRE_VELOCITY_SETUP, reset_cell_source))
+        sim.single_step()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(steps):
+            sim.single_step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms += a.elapsed_time(b)
+        cell_steps += dom.numCells() * steps
+        del sim, dom
+    return {"value": round(cell_steps / (ms / 1e3) / 1e6, 4) if ms else None, "unit": "Mcell-steps/s",
+            "sample": f"the first {sample} requests of the stream, {steps} steps each after one warm-up step, plain FP64"}
+
+
 def run_serve(args, rank, world, local):
     import phipict_b200 as pb
     from phipict_b200.serve import Server, gather_reports, route
@@ -622,6 +670,7 @@ def run_serve(args, rank, world, local):
     server.run(mine)
     rep = gather_reports(server.report(), world)
     cells = rep["cells_total"]
+    plain = serve_one_at_a_time(wl, device, tol, args.plain_sample, args.plain_steps) if args.plain_sample else None
     return dict(metric="Mcell-steps/s", value=round(rep["mcell_steps_per_s"], 4), unit="Mcell-steps/s",
                 n_gpus=world, steps=wl["steps"], warmup=0, higher_is_better=True, scaling="weak", vs_baseline=None,
                 dtype="f64 fields, f32 Krylov + f64 refinement" if not args.plain_fp64 else "f64",
@@ -631,7 +680,8 @@ def run_serve(args, rank, world, local):
                                     f"rtol {wl['rtol']}, admission against 150 GB", "parallelism": f"replicas x{world}"},
                 served={"requests": rep["requests"], "p50_s": rep["p50_s"], "p99_s": rep["p99_s"],
                         "wall_s": round(rep["wall_s"], 3), "failed": rep["failed"], "batch_steps": rep["batch_steps"],
-                        "cells_total": cells,
+                        "joins_while_running": rep.get("joins"), "batch_rebuilds": rep.get("repacks"),
+                        "cells_total": cells, "one_at_a_time_fp64": plain,
                         "failures": [f"{r.rid}: {r.failed[:160]}" for r in server.finished if r.failed][:4],
                         "peak_held_bytes": rep["peak_held_bytes"]},
                 gpu_launches=None)
@@ -906,9 +956,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-amg", action="store_true", help="unpreconditioned CG for pressure and potential")
     ap.add_argument("--no-fp64-leg", action="store_true", help="skip the plain FP64 comparison run")
+    ap.add_argument("--pressure-warm-start", action="store_true",
+                    help="start every pressure solve from the last step's pressure of the same corrector")
     ap.add_argument("--inner-rtol", type=float, default=None, help="inner FP32 reduction per refinement sweep")
     ap.add_argument("--no-alone", action="store_true", help="batch64: skip the one-at-a-time comparison")
+    ap.add_argument("--no-batch64", action="store_true", help="duct3d: skip the batched-instances sub-record")
     ap.add_argument("--requests", type=int, default=None, help="serve: number of requests")
+    ap.add_argument("--plain-sample", type=int, default=8, help="serve: requests timed one at a time on plain FP64")
+    ap.add_argument("--plain-steps", type=int, default=10, help="serve: timed steps per one-at-a-time request")
     ap.add_argument("--rollout", type=int, default=None, help="adjoint: steps of the differentiable rollout")
     ap.add_argument("--fd-directions", type=int, default=8, help="adjoint: random directions of the FD check")
     ap.add_argument("--fd-eps", type=float, default=3e-3, help="adjoint: central-difference step")
@@ -934,6 +989,8 @@ def main():
         line = run_sweep(args, rank, world, local)
     else:
         line = run_ours(args, rank, world, local)
+    if args.workload == "duct3d" and not args.no_batch64 and not args.plain_fp64:
+        line["batch64"] = batch64_record(args, rank, world, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "duct3d":
         line["cpu_baseline"] = cpu_baseline(WORKLOADS[args.workload], 1, min_seconds=10.0)
     if rank == 0:

@@ -357,8 +357,9 @@ int phb_cg_solve_noalloc(const phb_domain *dom, int dtype, int nrhs, const void 
  * (LinearSolveFunction, SparseOuterProduct, csrTranspose). Every *bar output is
  * accumulated (+=): zero it before the first contribution. ubbar has the layout of the
  * fixed-face velocity buffer (phb_domain::fvel). */
-/* CT = C^T as a stencil (the adjoint momentum solve) */
-int phb_transpose_stencil(const phb_domain *dom, const double *C, double *CT, phb_stream stream);
+/* CT = C^T as a stencil (the adjoint momentum solve, SolveLinear's transposeA); C and CT hold
+ * the domain's value type (float64 or float32) */
+int phb_transpose_stencil(const phb_domain *dom, const void *C, void *CT, phb_stream stream);
 /* Mbar[s][i] += scale * sum_k lam[i,k] x[nb_s(i),k] (ncomp 1 or dims): the adjoint of a
  * solve M x = b with respect to M is -lam (x)^T on the stencil, lam = M^-T xbar */
 int phb_adj_outer(const phb_domain *dom, int ncomp, const double *lam, const double *x, double scale, double *Mbar,

@@ -298,10 +298,18 @@ def SolveLinear(A: CSRmatrix, RHS: torch.Tensor, x: torch.Tensor, maxit, tol, co
     src = A.stencil_source() if isinstance(A, CSRmatrix) else None
     if src is None:
         raise NotImplementedError("phipict_b200 solves the stencil matrices of a Domain (C, P, Epot)")
-    if transposeA or BiCGwithPreconditioner or residualResetSteps:
-        raise NotImplementedError("transposed, preconditioned BiCGStab and residual resets are not implemented")
+    if BiCGwithPreconditioner and useBiCG:
+        raise NotImplementedError("Jacobi-preconditioned BiCGStab is not implemented")
+    if residualResetSteps:
+        raise NotImplementedError("residual resets are not implemented")
     domain, which = src
     st = domain._stencil(which)
+    if transposeA:
+        # A^T as a stencil (the adjoint solves of phiPICT's LinearSolveFunction,
+        # core/piso_diff.py:1154-1421)
+        t = torch.empty_like(st)
+        _lib.call("phb_transpose_stencil", ct.byref(domain.desc()), st.data_ptr(), t.data_ptr(), _S(domain))
+        st = t
     B, N = domain.getBatchSize(), domain.getTotalSize()
     nrhs = RHS.numel() // (B * N)
     if nrhs * B * N != RHS.numel() or x.numel() != RHS.numel():
@@ -312,6 +320,29 @@ def SolveLinear(A: CSRmatrix, RHS: torch.Tensor, x: torch.Tensor, maxit, tol, co
     solver = solver_for(domain, BICGSTAB if useBiCG else CG, domain.getDtype(), nrhs, tag="SolveLinear")
     solver.solve(st, RHS.contiguous(), x, tol, maxit, return_best=returnBestResult)
     return solver.results()
+
+
+def SparseOuterProduct(a: torch.Tensor, b: torch.Tensor, out_pattern: CSRmatrix) -> None:
+    """out.value[k] = a[row(k)] * b[col(k)] on the nonzero pattern of out_pattern, written in
+    place (solvers/linear_solve.cu:167-190, the cuSPARSE SDDMM a b^T sampled at the pattern):
+    the gradient of a solve with respect to the matrix values. For a domain matrix the values
+    go back into its stencil."""
+    n = out_pattern.getRows()
+    for name, v in (("a", a), ("b", b)):
+        if not v.is_cuda:
+            raise RuntimeError(f"{name} must be a CUDA tensor")
+        if v.dim() != 1 or v.numel() != n:
+            raise RuntimeError(f"Size of {name} must match matrix size.")
+    val = out_pattern.value
+    if a.dtype != val.dtype or b.dtype != val.dtype:
+        raise RuntimeError("Data type of a and b must match the matrix.")
+    row = out_pattern.row.long()
+    col = out_pattern.index.long()
+    rows = torch.repeat_interleave(torch.arange(n, device=a.device), row[1:] - row[:-1])
+    out = (a[rows] * b[col]).to(val.dtype)
+    if val.numel() != out.numel():
+        raise RuntimeError("SparseOuterProduct writes one matrix (batch size 1)")
+    out_pattern.value = out
 
 
 def GetKrylovSettings() -> dict:

@@ -55,11 +55,11 @@ __device__ __forceinline__ void adjContraFixed(const Dom<S, D> &dom, const int32
 // --- linear-solve pieces -------------------------------------------------------------------
 // C^T as a stencil: slot f of cell i holds C[j][f'] where j is the neighbour across f and f'
 // the face of j that leads back to i (the opposite face, or the entry face of a connection).
-template <int D>
-__global__ void __launch_bounds__(PHB_TILE) kTransposeStencil(Dom<S, D> dom, const S *__restrict__ C, S *__restrict__ CT) {
+template <int D, typename V = S>
+__global__ void __launch_bounds__(PHB_TILE) kTransposeStencil(Dom<V, D> dom, const V *__restrict__ C, V *__restrict__ CT) {
 	__shared__ int32_t sB[PHB_BREC];
 	int l0, nc;
-	loadTile<S, D>(dom, sB, l0, nc);
+	loadTile<V, D>(dom, sB, l0, nc);
 	const int64_t N = dom.ncells;
 	for (int j = 0; j < CPT; ++j) {
 		Cell c;
@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(PHB_TILE) kTransposeStencil(Dom<S, D> dom, con
 #pragma unroll
 		for (int f = 0; f < 2 * D; ++f) {
 			if (atBound(c.B, f, c.p) && fType(c.B, f) == FT_FIXED) { CT[(f + 1) * N + c.g] = 0; continue; }
-			const Nbr n = neighbor<S, D>(dom, c, f);
+			const Nbr n = neighbor<V, D>(dom, c, f);
 			int back = f ^ 1;
 			if (atBound(c.B, f, c.p) && fType(c.B, f) == FT_CONNECTED) {
 				const int code = fRec(c.B, f)[2];
@@ -515,9 +515,20 @@ using namespace phb;
 	} while (0)
 #define PHB_TL dim3(dom->ntiles), dim3(PHB_TILE), 0, s_
 
-extern "C" int phb_transpose_stencil(const phb_domain *dom, const double *C, double *CT, phb_stream stream) {
-	if (!C || !CT) return setError(PHB_ERR_ARG, "phb_transpose_stencil: null argument");
-	PHB_ADJ(dom, kTransposeStencil<D><<<PHB_TL>>>(dm, C, CT));
+// the transpose reads the topology and the stencil only: any value type of the domain
+extern "C" int phb_transpose_stencil(const phb_domain *dom, const void *C, void *CT, phb_stream stream) {
+	if (!dom || !C || !CT) return setError(PHB_ERR_ARG, "phb_transpose_stencil: null argument");
+	if (dom->ntiles == 0) return PHB_OK;
+	cudaStream_t s_ = (cudaStream_t)stream;
+	auto run = [&](auto tag) {
+		using T = decltype(tag);
+		if (dom->dims == 2) kTransposeStencil<2, T><<<dim3(dom->ntiles), dim3(PHB_TILE), 0, s_>>>(Dom<T, 2>(*dom), (const T *)C, (T *)CT);
+		else kTransposeStencil<3, T><<<dim3(dom->ntiles), dim3(PHB_TILE), 0, s_>>>(Dom<T, 3>(*dom), (const T *)C, (T *)CT);
+	};
+	if (dom->dims != 2 && dom->dims != 3) return setError(PHB_ERR_ARG, "dims");
+	if (dom->dtype == PHB_F64) run(double{});
+	else if (dom->dtype == PHB_F32) run(float{});
+	else return setError(PHB_ERR_ARG, "phb_transpose_stencil: dtype");
 	return checkLaunch("kTransposeStencil");
 }
 

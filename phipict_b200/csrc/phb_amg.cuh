@@ -499,10 +499,11 @@ __device__ __forceinline__ double amgProlongTile(const AmgView<D> &mg, int l, in
 	return dot;
 }
 
-// The same for a whole tile on quads (four consecutive cells per thread): inside a row away
-// from the block's y and z faces, the x1 values of the cell groups at the centre and at +-y,
-// +-z are formed from vector loads and the coarse corrections of their aggregates; only row
-// ends resolve the x neighbour across the block face. Same arithmetic as amgProlongCell.
+// The same for a whole tile on quads (four consecutive cells per thread): inside a row whose
+// y and z neighbours are in the block or absent behind a prescribed face (Quad::fastW), the x1
+// values of the cell groups at the centre and at +-y, +-z are formed from vector loads and the
+// coarse corrections of their aggregates; only row ends resolve the x neighbour across the
+// block face. Same arithmetic and order as amgProlongCell for every cell.
 template <int D>
 __device__ __forceinline__ double amgProlongQuad(const AmgView<D> &mg, int l, int tile, int32_t *sB, float *out) {
 	const Dom<float, D> &fd = mg.lv[l], &cd = mg.lv[l + 1];
@@ -518,7 +519,7 @@ __device__ __forceinline__ double amgProlongQuad(const AmgView<D> &mg, int l, in
 	Quad q;
 	quadAt<D, 1>(fd.vec4, sB, l0, nc, q);
 	double dot = 0;
-	if (!q.fast) {
+	if (!q.fastW) {
 #pragma unroll
 		for (int i = 0; i < 4; ++i) {
 			if (i >= q.n) break;
@@ -599,6 +600,7 @@ __device__ __forceinline__ double amgProlongQuad(const AmgView<D> &mg, int l, in
 	if (hasE) y[3] = fmaf(a[3], xe, y[3]);
 #pragma unroll
 	for (int sl = 3; sl < 2 * D + 1; ++sl) {
+		if ((q.miss >> (sl - 3)) & 1) continue; // behind a prescribed face: no neighbour
 		const bool ys = sl < 5;
 		const int dir = (sl & 1) ? -1 : 1; // slots 3, 5: the minus side
 		const int64_t off = (ys ? (int64_t)q.sy : (int64_t)q.sz) * dir;

@@ -92,6 +92,8 @@ class Server:
         self.peak_held = 0
         self.steps_run = 0
         self.cell_steps = 0
+        self.joins = 0    # admissions into a batch that was already running
+        self.repacks = 0  # batch rebuilds after a membership change
         self._t0 = None
 
     # --- admission ------------------------------------------------------------------------
@@ -127,6 +129,8 @@ class Server:
             req.cells = req.domain.numCells()
             req.admitted = now
             g = self.groups.setdefault(req.domain.getSpatialDims(), _Group(req.domain.getSpatialDims()))
+            if g.requests:  # joins a batch that is already running
+                self.joins += 1
             g.requests.append(req)
             g.dirty = True
             running += 1
@@ -147,6 +151,7 @@ class Server:
         if not g.requests:
             g.dirty = False
             return
+        self.repacks += 1
         reqs = list(g.requests)
         batch = DomainBatch([r.domain for r in reqs])
         dt = torch.tensor([r.dt for r in reqs], dtype=torch.float64)
@@ -232,6 +237,7 @@ class Server:
                 "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99), "wall_s": wall,
                 "mcell_steps_per_s": self.cell_steps / wall / 1e6 if wall > 0 else None,
                 "batch_steps": self.steps_run, "peak_held_bytes": self.peak_held,
+                "joins": self.joins, "repacks": self.repacks,
                 "latencies": lat, "cell_steps": self.cell_steps, "cells_total": sum(r.cells for r in self.finished)}
 
 
@@ -267,6 +273,7 @@ def merge_reports(reports: list[dict]) -> dict:
             "p50_s": percentile(lat, 50), "p99_s": percentile(lat, 99), "wall_s": wall,
             "mcell_steps_per_s": cell_steps / wall / 1e6 if wall > 0 else None,
             "batch_steps": sum(r["batch_steps"] for r in reports),
+            "joins": sum(r.get("joins", 0) for r in reports), "repacks": sum(r.get("repacks", 0) for r in reports),
             "peak_held_bytes": max(r["peak_held_bytes"] for r in reports),
             "latencies": lat, "cell_steps": cell_steps, "cells_total": sum(r["cells_total"] for r in reports),
             "servers": len(reports)}
