@@ -350,6 +350,46 @@ int64_t phb_cg_noalloc_bytes(const phb_domain *dom, int dtype, int nrhs);
 int phb_cg_solve_noalloc(const phb_domain *dom, int dtype, int nrhs, const void *A, const void *b, void *x,
                          const phb_tolerance *tol, int maxit, int return_best, phb_solve_result *out, phb_stream stream);
 
+/* --- AMG-preconditioned CG on CSR matrices ----------------------------------------------
+ * Replaces AMGPCGSolve (bindings.cpp:764-776, solvers/krylov/krylov.cu:1248-1612) for callers
+ * that bring an algebraic hierarchy (phiPICT's solvers/amg.py builds one with pyamg). Level l
+ * holds its operator A_l (values per environment when a_val_stride > 0), the inverse diagonal
+ * (per environment likewise), R_l (coarse x fine) and P_l (fine x coarse) with shared values;
+ * the level below the last is solved with coarse_pinv ([coarse_n]^2, or one per environment
+ * when coarse_batched). dtype: the system and the CG vectors; hdtype: the hierarchy. Environments
+ * share the pattern and are solved independently, each to its own tolerance (tolerances, or
+ * tol for all). `levels` is a host array; every other pointer is device memory. */
+typedef struct phb_csr_level {
+	const int32_t *a_row, *a_col;
+	const void *a_val;
+	int64_t a_val_stride; /* values per environment, or 0 when shared */
+	const void *dinv;     /* [n] or [nenv][n] with a_val_stride */
+	const int32_t *r_row, *r_col;
+	const void *r_val;
+	const int32_t *p_row, *p_col;
+	const void *p_val;
+	int32_t n;            /* rows of A_l */
+	int32_t pad;
+} phb_csr_level;
+typedef struct phb_csr_pcg {
+	int32_t dtype, hdtype;
+	int32_t n, nenv, nlevels, coarse_n, coarse_batched;
+	int32_t maxit, normalized, return_best, project_constant, pre_sweeps, post_sweeps, pad;
+	double tol, omega;
+	const double *tolerances;  /* host, [nenv], or NULL */
+	const int32_t *row, *col;  /* the system matrix (the finest level's operator) */
+	const void *val;
+	int64_t val_stride;
+	const phb_csr_level *levels; /* host array [nlevels] */
+	const void *coarse_pinv;
+	const void *b;
+	void *x;                   /* initial guess, overwritten with the solution */
+	void *work;                /* >= phb_csr_pcg_work_bytes() */
+} phb_csr_pcg;
+int64_t phb_csr_pcg_work_bytes(const phb_csr_pcg *a);
+/* out[nenv]: per-environment results (synchronises the stream) */
+int phb_csr_pcg_solve(const phb_csr_pcg *a, phb_solve_result *out, phb_stream stream);
+
 /* --- adjoint of the step (float64 domains) ------------------------------------------
  * Replace phiPICT's *Grad kernels (piso/advection.cu:310-544,958-1195; pressure.cu:196-345,
  * 525-750; velocity_correction.cu:301-375; mhd/potential.cu:981-1329, bound at

@@ -345,6 +345,115 @@ def SparseOuterProduct(a: torch.Tensor, b: torch.Tensor, out_pattern: CSRmatrix)
     out_pattern.value = out
 
 
+def AMGPCGSolve(aRow: torch.Tensor, aCol: torch.Tensor, aVal: torch.Tensor, levels, coarsePinv: torch.Tensor,
+                rhs: torch.Tensor, x: torch.Tensor, maxIterations: int, tolerance: float, normalized: bool = True,
+                returnBestResult: bool = False, projectConstant: bool = False, preSweeps: int = 1,
+                postSweeps: int = 1, omega: float = 2.0 / 3.0, tolerances=()) -> list[LinearSolverResultInfo]:
+    """AMG-preconditioned CG on CSR matrices, solving in place in x (bindings.cpp:764-776,
+    krylov.cu:1565-1612; the solver of krylov.cu:1400-1546): for callers that bring an algebraic
+    hierarchy, like phiPICT's solvers/amg.py. `levels` holds, per level but the coarsest,
+    (A row, A col, A val, inverse diagonal, R row, R col, R val, P row, P col, P val) with int32
+    indices; coarsePinv is the coarsest level's dense pseudo-inverse, [nc, nc] or [B, nc, nc].
+    rhs and x hold B environments of aRow.numel()-1 rows each; aVal and every level's A values
+    and inverse diagonal are one matrix or one per environment. One result per environment."""
+    def cuda_contig(name: str, t: torch.Tensor) -> None:
+        if not t.is_cuda:
+            raise RuntimeError("AMG tensors must be on the GPU")
+        if not t.is_contiguous():
+            raise RuntimeError(f"{name}: AMG tensors must be contiguous")
+
+    if not (rhs.is_contiguous() and x.is_contiguous() and rhs.numel() == x.numel()):
+        raise RuntimeError("rhs and x must be contiguous and of equal size")
+    if rhs.dtype != aVal.dtype or x.dtype != aVal.dtype:
+        raise RuntimeError("rhs, x and the matrix must have the same dtype")
+    if aVal.dtype not in (torch.float32, torch.float64):
+        raise RuntimeError("the system must be float32 or float64")
+    n = aRow.numel() - 1
+    if n <= 0 or rhs.numel() % n != 0:
+        raise RuntimeError("rhs size must be a multiple of the matrix size")
+    B = rhs.numel() // n
+    hdt = coarsePinv.dtype
+    if hdt not in (torch.float32, torch.float64):
+        raise RuntimeError("AMG hierarchy dtype must be float32 or float64")
+
+    def batched_stride(name: str, row, col, val) -> int:
+        for t in (row, col, val):
+            cuda_contig(name, t)
+        if row.dtype != torch.int32 or col.dtype != torch.int32:
+            raise RuntimeError("AMG index tensors must be int32")
+        nnz = col.numel()
+        if val.numel() != nnz and val.numel() != nnz * B:
+            raise RuntimeError(f"{name}: values must hold one matrix or one per right-hand side.")
+        return 0 if val.numel() == nnz else nnz
+
+    for t in (rhs, x):
+        cuda_contig("rhs/x", t)
+    stride = batched_stride("system matrix", aRow, aCol, aVal)
+    if len(levels) < 1:
+        raise RuntimeError("AMG hierarchy needs at least one level above the coarsest")
+    lv = (_lib.PhbCsrLevel * len(levels))()
+    keep = []
+    for i, t in enumerate(levels):
+        if len(t) != 10:
+            raise RuntimeError("each AMG level needs (A row, col, val, dinv, R row, col, val, P row, col, val)")
+        t = [v.contiguous() for v in t]
+        keep.append(t)
+        if any(t[k].dtype != hdt for k in (2, 3, 6, 9)):
+            raise RuntimeError("all hierarchy values must have the dtype of the coarse pseudo-inverse")
+        s = batched_stride("level operator", t[0], t[1], t[2])
+        nl = t[0].numel() - 1
+        cuda_contig("inverse diagonal", t[3])
+        if t[3].numel() != (nl * B if s else nl):
+            raise RuntimeError("inverse diagonal must match the level operator(s)")
+        for name, (r, c, v) in (("R", t[4:7]), ("P", t[7:10])):
+            for u in (r, c, v):
+                cuda_contig(name, u)
+            if r.dtype != torch.int32 or c.dtype != torch.int32:
+                raise RuntimeError("AMG index tensors must be int32")
+            if v.numel() != c.numel():
+                raise RuntimeError(f"{name}: values and column indices differ in size")
+        lv[i] = _lib.PhbCsrLevel(t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr(), s, t[3].data_ptr(),
+                                 t[4].data_ptr(), t[5].data_ptr(), t[6].data_ptr(), t[7].data_ptr(), t[8].data_ptr(),
+                                 t[9].data_ptr(), nl, 0)
+    for i in range(len(levels)):  # R_l maps level l to the next one, P_l back
+        nnext = keep[i + 1][0].numel() - 1 if i + 1 < len(levels) else coarsePinv.shape[-1]
+        if keep[i][4].numel() - 1 != nnext or keep[i][7].numel() - 1 != keep[i][0].numel() - 1:
+            raise RuntimeError("restriction / prolongation sizes do not chain the levels")
+    if keep[0][0].numel() - 1 != n:
+        raise RuntimeError("finest AMG level does not match the system matrix")
+    nc = int(coarsePinv.shape[-1])
+    batched = coarsePinv.dim() == 3 and B > 1
+    pinv = coarsePinv.contiguous()
+    cuda_contig("coarse pseudo-inverse", pinv)
+    if pinv.numel() != (nc * nc * B if batched else nc * nc):
+        raise RuntimeError("coarse pseudo-inverse has the wrong size")
+    tols = [float(v) for v in tolerances]
+    if tols and len(tols) != B:
+        raise RuntimeError("tolerances must hold one value per right-hand side")
+    htol = (ct.c_double * B)(*tols) if tols else None
+    dt = {torch.float32: 0, torch.float64: 1}
+    a = _lib.PhbCsrPcg()
+    a.dtype, a.hdtype, a.n, a.nenv, a.nlevels, a.coarse_n = dt[aVal.dtype], dt[hdt], n, B, len(levels), nc
+    a.coarse_batched = int(batched)
+    a.maxit, a.normalized, a.return_best = int(maxIterations), int(bool(normalized)), int(bool(returnBestResult))
+    a.project_constant, a.pre_sweeps, a.post_sweeps = int(bool(projectConstant)), int(preSweeps), int(postSweeps)
+    a.tol, a.omega = float(tolerance), float(omega)
+    a.tolerances = ct.cast(htol, ct.c_void_p) if htol is not None else None
+    a.row, a.col, a.val, a.val_stride = aRow.data_ptr(), aCol.data_ptr(), aVal.data_ptr(), stride
+    a.levels = ct.cast(lv, ct.c_void_p)
+    a.coarse_pinv, a.b, a.x = pinv.data_ptr(), rhs.data_ptr(), x.data_ptr()
+    nbytes = _lib.load().phb_csr_pcg_work_bytes(ct.byref(a))
+    if nbytes < 0:
+        raise RuntimeError(_lib.load().phb_last_error().decode(errors="replace"))
+    work = torch.empty(max(256, int(nbytes)), dtype=torch.uint8, device=rhs.device)
+    a.work = work.data_ptr()
+    out = (_lib.PhbSolveResult * B)()
+    with torch.cuda.device(rhs.device):
+        _lib.call("phb_csr_pcg_solve", ct.byref(a), out, _lib.stream_ptr(rhs.device))
+    return [LinearSolverResultInfo(o.final_residual, o.used_iterations, bool(o.converged), bool(o.finite), o.status,
+                                   o.inner_iterations) for o in out]
+
+
 def GetKrylovSettings() -> dict:
     from .solvers import SETTINGS
 

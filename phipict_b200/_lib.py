@@ -32,6 +32,7 @@ EXPORTS = (
     "phb_release_graphs", "phb_refine_work_bytes", "phb_refine_run", "phb_refine_results",
     "phb_cg_noalloc_bytes", "phb_cg_solve_noalloc",
     "phb_amg_setup", "phb_amg_vcycle", "phb_amg_work_doubles",
+    "phb_csr_pcg_work_bytes", "phb_csr_pcg_solve",
     "phb_transpose_stencil", "phb_adj_outer", "phb_adj_advection_matrix", "phb_adj_advection_rhs",
     "phb_adj_pressure_rhs", "phb_adj_divergence", "phb_adj_correct_velocity", "phb_adj_pressure_matrix",
     "phb_adj_uxb_epot_rhs", "phb_adj_lorentz",
@@ -112,6 +113,28 @@ class PhbAmg(ct.Structure):
     ]
 
 
+class PhbCsrLevel(ct.Structure):
+    _fields_ = [
+        ("a_row", ct.c_void_p), ("a_col", ct.c_void_p), ("a_val", ct.c_void_p), ("a_val_stride", ct.c_int64),
+        ("dinv", ct.c_void_p), ("r_row", ct.c_void_p), ("r_col", ct.c_void_p), ("r_val", ct.c_void_p),
+        ("p_row", ct.c_void_p), ("p_col", ct.c_void_p), ("p_val", ct.c_void_p), ("n", ct.c_int32), ("pad", ct.c_int32),
+    ]
+
+
+class PhbCsrPcg(ct.Structure):
+    _fields_ = [
+        ("dtype", ct.c_int32), ("hdtype", ct.c_int32),
+        ("n", ct.c_int32), ("nenv", ct.c_int32), ("nlevels", ct.c_int32), ("coarse_n", ct.c_int32),
+        ("coarse_batched", ct.c_int32),
+        ("maxit", ct.c_int32), ("normalized", ct.c_int32), ("return_best", ct.c_int32), ("project_constant", ct.c_int32),
+        ("pre_sweeps", ct.c_int32), ("post_sweeps", ct.c_int32), ("pad", ct.c_int32),
+        ("tol", ct.c_double), ("omega", ct.c_double), ("tolerances", ct.c_void_p),
+        ("row", ct.c_void_p), ("col", ct.c_void_p), ("val", ct.c_void_p), ("val_stride", ct.c_int64),
+        ("levels", ct.c_void_p), ("coarse_pinv", ct.c_void_p), ("b", ct.c_void_p), ("x", ct.c_void_p),
+        ("work", ct.c_void_p),
+    ]
+
+
 _lib: ct.CDLL | None = None
 
 
@@ -173,6 +196,7 @@ def load() -> ct.CDLL:
         "phb_adj_uxb_epot_rhs": [DP, P, P, P, P, P],
         "phb_adj_lorentz": [DP, P, P, P, P, P, P, P, P, P],
         "phb_amg_vcycle": [ct.POINTER(PhbAmg), P, P, P],
+        "phb_csr_pcg_solve": [ct.POINTER(PhbCsrPcg), ct.POINTER(PhbSolveResult), P],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -185,6 +209,7 @@ def load() -> ct.CDLL:
         "phb_refine_work_bytes": [DP, I, I],
         "phb_cg_noalloc_bytes": [DP, I, I],
         "phb_amg_work_doubles": [ct.POINTER(PhbAmg)],
+        "phb_csr_pcg_work_bytes": [ct.POINTER(PhbCsrPcg)],
     }.items():
         f = getattr(lib, name)
         f.argtypes = args

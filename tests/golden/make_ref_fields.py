@@ -8,7 +8,8 @@ GPU machine with the reference built by ``oracle/build_ref.py`` into ``oracle/_r
 
 It writes one ``.npz`` per case and dtype holding the inputs (vertices, initial velocity,
 inflow) and the fields u, p (per block) and phi after each recorded step, plus a JSON line per
-run (iterations, timing) to stdout. ``--time-duct`` also times the reference's plain
+run (iterations, timing) to stdout. ``--amg`` writes ``ref_amg_pcg.npz``: phiPICT's
+``_C.AMGPCGSolve`` on the cases of ``amg_cases.py``. ``--time-duct`` also times the reference's plain
 (non-AMG; pyamg is not installed) GPU step on the full 3-block 64x48x48 duct.
 """
 from __future__ import annotations
@@ -79,6 +80,26 @@ def time_duct(pp, steps: int, warmup: int, dtype) -> dict:
                 mcell_steps_per_s=round(cells / dt / 1e6, 3), steps=steps)
 
 
+def amg_fixture(out: Path) -> None:
+    """Run phiPICT's _C.AMGPCGSolve on every case of amg_cases.py: ref_amg_pcg.npz holds each
+    case's solution and result infos (residual, iterations, converged, finite)."""
+    import amg_cases as ac
+    from phipict import _C
+
+    data = {}
+    for name in ac.CASES:
+        case = ac.build(name)
+        args, kw = ac.torch_args(case, torch.device("cuda"), torch)
+        infos = _C.AMGPCGSolve(*args, **kw)
+        torch.cuda.synchronize()
+        data[f"{name}_x"] = args[6].double().cpu().numpy().reshape(case["nenv"], -1)
+        data[f"{name}_info"] = np.array([[i.finalResidual, i.usedIterations, float(i.converged),
+                                          float(i.isFiniteResidual)] for i in infos])
+        print(json.dumps(dict(tag=f"amg_{name}", infos=data[f"{name}_info"].tolist())), flush=True)
+    data["meta"] = np.array(json.dumps(dict(device=torch.cuda.get_device_name(0))))
+    np.savez_compressed(out / "ref_amg_pcg.npz", **data)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default="tests/golden")
@@ -86,6 +107,7 @@ def main() -> None:
     ap.add_argument("--skip-fixtures", action="store_true")
     ap.add_argument("--cases", default="c1_fp64,c1_fp32,c2r_fp64", help="comma list of <case>_<dtype>")
     ap.add_argument("--grads", action="store_true", help="also the gradient cases of the differentiable step")
+    ap.add_argument("--amg", action="store_true", help="also the CSR AMG-PCG cases of amg_cases.py (_C.AMGPCGSolve)")
     a = ap.parse_args()
     import phipict as pp
 
@@ -108,6 +130,8 @@ def main() -> None:
                                                     device=torch.cuda.get_device_name(0))))
             np.savez_compressed(out / f"ref_{case}_grad.npz", **data)
             print(json.dumps(dict(tag=f"{case}_grad", loss=g["loss"], wall_s=round(time.time() - t0, 2))), flush=True)
+    if a.amg:
+        amg_fixture(out)
     if a.time_duct:
         print(json.dumps(time_duct(pp, 3, 1, torch.float64)), flush=True)
         print(json.dumps(time_duct(pp, 3, 1, torch.float32)), flush=True)

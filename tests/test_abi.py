@@ -43,3 +43,14 @@ def test_struct_layouts_match_header():
     assert _lib.PhbDomain.blocks.offset == 48
     assert _lib.PhbDomain.nonortho.offset == 148 and ct.sizeof(_lib.PhbDomain) == 152
     assert ct.sizeof(_lib.PhbScalar) == 48 and _lib.PhbScalar.nu.offset == 8
+    assert ct.sizeof(_lib.PhbCsrLevel) == 96 and _lib.PhbCsrLevel.n.offset == 88
+    assert _lib.PhbCsrPcg.tol.offset == 56 and _lib.PhbCsrPcg.levels.offset == 112
+    assert ct.sizeof(_lib.PhbCsrPcg) == 152
+
+
+def test_csr_pcg_rejects_bad_arguments_without_a_gpu():
+    lib = _lib.load()
+    a = _lib.PhbCsrPcg()
+    assert lib.phb_csr_pcg_work_bytes(ct.byref(a)) == -1
+    assert b"phb_csr_pcg" in lib.phb_last_error()
+    assert lib.phb_csr_pcg_solve(ct.byref(a), None, None) == -1
