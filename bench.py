@@ -352,8 +352,10 @@ def run_ours(args, rank, world, local):
     if plain:
         plain["vs_plain_fp64"]["mixed_over_plain"] = round(value / plain["vs_plain_fp64"]["value"], 3)
     # roofline of the dominant kernel: the (preconditioned) Krylov iteration, float32 when
-    # mixed; solve time / inner iterations (the momentum BiCGStab iterations are counted as
-    # CG-sized, a slight overestimate of their bytes)
+    # mixed; solve time / inner iterations. The momentum BiCGStab iterations (about a tenth of
+    # the iterations) are charged at the PCG's bytes per cell, which undercounts them (a 3-RHS
+    # float32 BiCGStab iteration moves 2(2d+1)*4 + 18d*4 = 272 B/cell in 3D): the achieved
+    # figure is conservative
     s = 4 if mixed else 8
     hier = sim._amg_cache.get("P") if amg else None
     levels = hier.sizes if hier is not None else None
