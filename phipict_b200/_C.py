@@ -10,6 +10,7 @@ e.g. piso/advection.cu:1217,1225). Matrices live in stencil form on the domain
 from __future__ import annotations
 
 import ctypes as ct
+import math
 
 import torch
 
@@ -294,10 +295,22 @@ def SolveLinear(A: CSRmatrix, RHS: torch.Tensor, x: torch.Tensor, maxit, tol, co
                 printResidual: bool = False, returnBestResult: bool = False,
                 BiCGwithPreconditioner: bool = False) -> list[LinearSolverResultInfo]:
     """Solve ``A x = RHS`` in place (solvers/linear_solve.cu:22-162). ``A`` must be one of
-    a domain's matrices (C, P or Epot); right-hand sides per instance = RHS size / rows."""
+    a domain's matrices (C, P or Epot); right-hand sides per instance = RHS size / rows.
+
+    conv: NORM2_NORMALIZED (None: the same) or NORM2, which tests ||r||_2 < tol and is run as
+    NORM2_NORMALIZED with tol / sqrt(rows per instance). matrixRankDeficient: phiPICT hands a
+    singular (pure Neumann) system to its legacy CG, which adds a constant-mode term to A; here
+    CG runs on the system as given, which converges on the consistent (mean-free) right-hand
+    sides that phiPICT's driver passes. The ABS_* criteria, preconditioned BiCGStab and
+    residual resets are refused."""
+    from .solvers import ConvergenceCriterion
+
     src = A.stencil_source() if isinstance(A, CSRmatrix) else None
     if src is None:
         raise NotImplementedError("phipict_b200 solves the stencil matrices of a Domain (C, P, Epot)")
+    crit = ConvergenceCriterion.NORM2_NORMALIZED if conv is None else ConvergenceCriterion(int(conv))
+    if crit not in (ConvergenceCriterion.NORM2, ConvergenceCriterion.NORM2_NORMALIZED):
+        raise NotImplementedError(f"convergence criterion {crit.name} is not implemented (NORM2, NORM2_NORMALIZED)")
     if BiCGwithPreconditioner and useBiCG:
         raise NotImplementedError("Jacobi-preconditioned BiCGStab is not implemented")
     if residualResetSteps:
@@ -317,6 +330,9 @@ def SolveLinear(A: CSRmatrix, RHS: torch.Tensor, x: torch.Tensor, maxit, tol, co
     maxit = int(maxit.reshape(-1)[0]) if isinstance(maxit, torch.Tensor) else int(maxit)
     if isinstance(tol, torch.Tensor) and tol.numel() > 1 and tol.numel() != B * nrhs:
         raise RuntimeError("tolerance must have 1 or (batch * right-hand sides) entries")
+    if crit == ConvergenceCriterion.NORM2:
+        scale = 1.0 / math.sqrt(N)
+        tol = tol * scale if isinstance(tol, torch.Tensor) else float(tol) * scale
     solver = solver_for(domain, BICGSTAB if useBiCG else CG, domain.getDtype(), nrhs, tag="SolveLinear")
     solver.solve(st, RHS.contiguous(), x, tol, maxit, return_best=returnBestResult)
     return solver.results()

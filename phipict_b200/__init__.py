@@ -23,11 +23,11 @@ from .domain import (
 from .hooks import Hook, Hooks
 from .mhd import MHDSimulation
 from .simulation import Simulation
-from .solvers import LinearSolverResultInfo, LinsolveError
+from .solvers import ConvergenceCriterion, LinearSolverResultInfo, LinsolveError
 from .tolerance import SolverTolerance
 
 __all__ = [
     "AdvectionScheme", "Block", "Boundary", "BoundaryConditionType", "BoundaryType", "ConnectedBoundary",
-    "CSRmatrix", "Domain", "DomainBatch", "FixedBoundary", "Hook", "Hooks", "LinearSolverResultInfo", "LinsolveError",
+    "ConvergenceCriterion", "CSRmatrix", "Domain", "DomainBatch", "FixedBoundary", "Hook", "Hooks", "LinearSolverResultInfo", "LinsolveError",
     "MHDSimulation", "PeriodicBoundary", "PotentialBC", "Simulation", "SolverTolerance", "_C",
 ]

@@ -895,6 +895,84 @@ class Domain:
     def CreateScalarResult(self) -> None:
         self.scalarResult.zero_()
 
+    def _set_vector(self, name: str, value: torch.Tensor) -> None:
+        """Domain::set<Vector> (domain.cpp:644-760): the values of a solve vector, [B*comp*n]
+        in the domain's dtype on its device. They are copied into the domain's own buffer,
+        whose address the prepared descriptors and cached solver graphs hold."""
+        cur = getattr(self, name, None)
+        if cur is None:
+            raise RuntimeError(f"{name}: the domain is not prepared (PrepareSolve)")
+        if not isinstance(value, torch.Tensor) or value.device != cur.device or value.dtype != cur.dtype:
+            raise RuntimeError(f"{name} must be a {cur.dtype} tensor on {cur.device}")
+        if value.numel() != cur.numel():
+            raise RuntimeError(f"{name} must have {cur.numel()} values, got {value.numel()}")
+        if value.data_ptr() != cur.data_ptr():
+            cur.copy_(value.detach().reshape(-1))
+
+    def setA(self, a: torch.Tensor) -> None:
+        self._set_vector("A", a)
+
+    def setVelocityRHS(self, v: torch.Tensor) -> None:
+        self._set_vector("velocityRHS", v)
+
+    def setVelocityResult(self, v: torch.Tensor) -> None:
+        self._set_vector("velocityResult", v)
+
+    def setPressureRHS(self, v: torch.Tensor) -> None:
+        self._set_vector("pressureRHS", v)
+
+    def setPressureRHSdiv(self, v: torch.Tensor) -> None:
+        self._set_vector("pressureRHSdiv", v)
+
+    def setPressureResult(self, v: torch.Tensor) -> None:
+        self._set_vector("pressureResult", v)
+
+    def setScalarRHS(self, v: torch.Tensor) -> None:
+        self._set_vector("scalarRHS", v)
+
+    def setEpotRHS(self, v: torch.Tensor) -> None:
+        self._set_vector("epotRHS", v)
+
+    def setEpotResult(self, v: torch.Tensor) -> None:
+        self._set_vector("epotResult", v)
+
+    def GetCoordinateOrientation(self) -> int:
+        """Domain/Block::GetCoordinateOrientation (domain.cpp:265-276, block.cpp:1091-1105):
+        the sign of the cell volumes (det M) when all cells of all blocks share it, else 0; a
+        block without vertex coordinates counts as +1."""
+        signs = set()
+        for b in self._blocks:
+            if b.vertexCoordinates is None:
+                signs.add(1)
+                continue
+            met = getattr(self, "_metrics", None)
+            if met is None:
+                raise RuntimeError("GetCoordinateOrientation needs a prepared domain (PrepareSolve)")
+            det = met[-1, b.globalOffset:b.globalOffset + b.ncells()]
+            lo, hi = int(torch.sign(det).min().item()), int(torch.sign(det).max().item())
+            signs.add(lo if lo == hi else 0)
+        if not signs:
+            raise RuntimeError("Domain does not contain any blocks.")
+        return signs.pop() if len(signs) == 1 else 0
+
+    def getMaxVelocityMagnitude(self, withBounds: bool = True, computational: bool = False) -> torch.Tensor:
+        """Largest velocity magnitude |u|_2 over cells (and, withBounds, fixed faces), all
+        environments (domain.cpp:234-243, block.cpp:578-612)."""
+        d = self._dims
+        u = self._u_block
+        if computational:
+            u = _to_computational(u, self._metrics, d)
+        m = torch.linalg.vector_norm(u, 2, dim=1).max()
+        if withBounds:
+            for k, (_, _, bd) in enumerate(self._fixed):
+                v = bd._velocity
+                if computational:
+                    fc, to = self._fixed_cells[k], self._fixed_toff[k]
+                    vv = v.reshape(v.shape[0], d, -1).expand(v.shape[0], d, fc) if v.dim() == 2 else v.reshape(v.shape[0], d, fc)
+                    v = _to_computational(vv, self._face_metrics[:, to:to + fc], d)
+                m = torch.maximum(m, torch.linalg.vector_norm(v.reshape(v.shape[0], d, -1), 2, dim=1).max())
+        return m
+
     def hasVertexCoordinates(self) -> bool:
         return all(b.hasVertexCoordinates() for b in self._blocks)
 
@@ -1483,16 +1561,17 @@ class Domain:
         d, B, N = self._dims, self._batch, self._N
         opts = dict(dtype=self._dtype, device=self._device)
         self._E_st = torch.zeros(2 * d + 1, B * N, **opts)
-        self.epotRHS = torch.zeros(B * N, **opts)
-        self.epotResult = torch.zeros(B * N, **opts)
-        e = torch.zeros(B, N, **opts)
-        for b in self._blocks:
-            old = b.epot
-            spatial = list(reversed(b._sizes[:d]))
-            b.epot = e[:, b.globalOffset:b.globalOffset + b.ncells()].view(B, 1, *spatial)
-            if old is not None and old.shape == b.epot.shape:
-                b.epot.copy_(old)
-        self._epot_block = e
+        # existing vectors are kept (domain.cpp:755-775): a second call rebuilds the matrix
+        # only, and the potential of the last solve survives it
+        if getattr(self, "epotRHS", None) is None or self.epotRHS.numel() != B * N:
+            self.epotRHS = torch.zeros(B * N, **opts)
+        had_result = getattr(self, "epotResult", None) is not None and self.epotResult.numel() == B * N
+        if not had_result:
+            self.epotResult = torch.zeros(B * N, **opts)
+        all_blocks_had = all(b.epot is not None for b in self._blocks)
+        self._attach_epot_blocks(copy_old=True)
+        if not had_result and all_blocks_had:
+            self.epotResult.copy_(self._epot_block.view(-1))
         _lib.call("phb_epot_matrix", ct.byref(self._desc), self._E_st.data_ptr(), None, _lib.stream_ptr(self._device))
         self._bump_matrix("E")
         self.Epot = CSRmatrix(_domain=self, _which="E")
@@ -1502,8 +1581,26 @@ class Domain:
     def hasEpot(self) -> bool:
         return self._epot_on and self._prepared
 
+    def _attach_epot_blocks(self, copy_old: bool) -> None:
+        """A fresh potential buffer [B, n] whose slices are the blocks' epot views (with the
+        blocks' previous values when copy_old)."""
+        d, B, N = self._dims, self._batch, self._N
+        e = torch.zeros(B, N, dtype=self._dtype, device=self._device)
+        for b in self._blocks:
+            old = b.epot
+            spatial = list(reversed(b._sizes[:d]))
+            b.epot = e[:, b.globalOffset:b.globalOffset + b.ncells()].view(B, 1, *spatial)
+            if copy_old and old is not None and old.shape == b.epot.shape:
+                b.epot.copy_(old)
+        self._epot_block = e
+
     def CreateEpotOnBlocks(self) -> None:
-        self.SetupEpotOnDomain(*self._epot_flags)
+        """Domain::CreateEpotOnBlocks (domain.cpp:607-611): every block gets a new zero
+        potential field; the domain's potential vectors and matrix stay as they are."""
+        if getattr(self, "_epot_block", None) is None:
+            self.SetupEpotOnDomain(*self._epot_flags)
+            return
+        self._attach_epot_blocks(copy_old=False)
 
     # --- CSR views ----------------------------------------------------------------------
     def _attach_csr_pattern(self) -> None:

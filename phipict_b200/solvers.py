@@ -10,6 +10,7 @@ that synchronises.
 from __future__ import annotations
 
 import ctypes as ct
+import enum
 import os
 from dataclasses import dataclass
 
@@ -61,6 +62,17 @@ class LinearSolverResultInfo:
     def __str__(self) -> str:
         return (f"LinearSolverResultInfo(residual={self.finalResidual:.3e}, iterations={self.usedIterations}, "
                 f"converged={self.converged}, finite={self.isFiniteResidual})")
+
+
+class ConvergenceCriterion(enum.IntEnum):
+    """Stop criteria of SolveLinear (solvers/linear_solvers.h:27-33). The Krylov solvers here
+    test NORM2_NORMALIZED, ||r||_2 / sqrt(n) < tol; SolveLinear maps NORM2 onto it by scaling
+    the tolerance, as phiPICT's fused solvers do (linear_solve.cu:48-55)."""
+    NORM2 = 0
+    NORM2_NORMALIZED = 1
+    ABS_SUM = 2
+    ABS_MEAN = 3
+    ABS_MAX = 4
 
 
 class LinsolveError(RuntimeError):
