@@ -84,10 +84,61 @@ def adjoint_solve(sim, which: str, rhs: torch.Tensor, x: torch.Tensor, kind: int
         raise RuntimeError(f"adjoint step: {which} solve did not converge: {bad}")
 
 
-def step_backward(sim, rec: StepRecord, ubar_out, pbar_out, phibar_out, xbar_out, Sbar_out, ubbar, Nbar, mhd: bool):
+def viscosity_cotangent(d, rec: StepRecord, Cbar: torch.Tensor, rhsbar: torch.Tensor, nubar: torch.Tensor) -> None:
+    """nubar[b] += <Cbar, dC/dnu> + <rhsbar, drhs/dnu> over instance b's cells. The momentum
+    matrix and right-hand side are affine in the viscosity (the diffusion coefficients and the
+    wall terms 2 nu alpha u_b, advection.cu:27-305,800-954), so their derivatives are exactly
+    the differences of the forward kernels run with nu = 1 and nu = 0 at the step's input
+    velocity (the source, independent of nu, is left out of both)."""
+    st = _lib.stream_ptr(d.getDevice())
+    desc = ct.byref(d.desc())
+    B, n = d.getBatchSize(), d.numCells()
+    dims = d.getSpatialDims()
+    S = 2 * dims + 1
+    saved = d._nu_dev.clone()
+    C1, C0 = torch.empty_like(d._C_st), torch.empty_like(d._C_st)
+    A1, A0 = torch.empty_like(d.A), torch.empty_like(d.A)
+    r1, r0 = torch.empty_like(d.velocityRHS), torch.empty_like(d.velocityRHS)
+    d._u_block.view(-1).copy_(rec.u_in)
+    try:
+        for val, C, A, r in ((1.0, C1, A1, r1), (0.0, C0, A0, r0)):
+            d._nu_dev.fill_(val)
+            _lib.call("phb_advection_matrix", desc, d._u_block.data_ptr(), C.data_ptr(), A.data_ptr(), None, st)
+            _lib.call("phb_advection_rhs", desc, d._u_block.data_ptr(), None, 0, r.data_ptr(), st)
+    finally:
+        d._nu_dev.copy_(saved)
+    per_cell = (Cbar.view(S, n) * (C1 - C0).view(S, n)).sum(0)
+    per_cell += (rhsbar.view(B, dims, -1) * (r1 - r0).view(B, dims, -1)).sum(1).reshape(-1)
+    nubar += per_cell.view(B, -1).sum(1)
+
+
+def hbya_viscosity_cotangent(d, rec: StepRecord, k: int, C: torch.Tensor, A: torch.Tensor, hbar: torch.Tensor,
+                             nubar: torch.Tensor) -> None:
+    """nubar[b] += <hbar, dHbyA/dnu> for corrector k through HbyA's explicit boundary terms
+    (pressure.cu:350-521: the fixed faces' 2 nu alpha u_b); its dependence through C and A is
+    carried by Cbar and Abar. HbyA is affine in nu at fixed C, A and velocities, so the
+    derivative is the difference of the forward kernel run with nu = 1 and nu = 0."""
+    st = _lib.stream_ptr(d.getDevice())
+    desc = ct.byref(d.desc())
+    B, dims = d.getBatchSize(), d.getSpatialDims()
+    saved = d._nu_dev.clone()
+    h1, h0 = torch.empty_like(rec.h[k]), torch.empty_like(rec.h[k])
+    try:
+        for val, h in ((1.0, h1), (0.0, h0)):
+            d._nu_dev.fill_(val)
+            _lib.call("phb_pressure_rhs", desc, C.data_ptr(), A.data_ptr(), rec.u_in.data_ptr(), rec.ustar[k].data_ptr(),
+                      None, 0, h.data_ptr(), st)
+    finally:
+        d._nu_dev.copy_(saved)
+    nubar += (hbar.view(B, dims, -1) * (h1 - h0).view(B, dims, -1)).sum((1, 2))
+
+
+def step_backward(sim, rec: StepRecord, ubar_out, pbar_out, phibar_out, xbar_out, Sbar_out, ubbar, Nbar, mhd: bool,
+                  nubar: torch.Tensor | None = None):
     """Reverse pass of one recorded step. Takes the cotangents of the step's outputs (u', p',
     phi', uxb', S; any may be None) and returns those of (u_in, S_in, phi_in, uxb_in); the
-    fixed-face and Stuart-number cotangents are accumulated into ubbar and Nbar."""
+    fixed-face and Stuart-number cotangents are accumulated into ubbar and Nbar, and, when
+    nubar is given, the viscosity's per instance into nubar."""
     d = sim.domain
     st = _lib.stream_ptr(d.getDevice())
     desc = ct.byref(d.desc())
@@ -126,6 +177,8 @@ def step_backward(sim, rec: StepRecord, ubar_out, pbar_out, phibar_out, xbar_out
         dbar = _proj(d, lamP)
         _lib.call("phb_adj_outer", desc, 1, lamP.data_ptr(), rec.p[k].data_ptr(), -1.0, Pbar.data_ptr(), st)
         _lib.call("phb_adj_divergence", desc, dbar.data_ptr(), hbar.data_ptr(), ubbar.data_ptr(), st)
+        if nubar is not None:
+            hbya_viscosity_cotangent(d, rec, k, C, A, hbar, nubar)
         ustar_bar = _zeros(d, dn)
         _lib.call("phb_adj_pressure_rhs", desc, C.data_ptr(), A.data_ptr(), rec.ustar[k].data_ptr(), rec.h[k].data_ptr(),
                   hbar.data_ptr(), uin_bar.data_ptr(), ustar_bar.data_ptr(), Cbar.data_ptr(), Abar.data_ptr(),
@@ -140,6 +193,8 @@ def step_backward(sim, rec: StepRecord, ubar_out, pbar_out, phibar_out, xbar_out
     _lib.call("phb_adj_advection_rhs", desc, lamM.data_ptr(), uin_bar.data_ptr(), Sbar.data_ptr(), ubbar.data_ptr(), st)
     Cbar.view(S, n)[0] += Abar
     _lib.call("phb_adj_advection_matrix", desc, Cbar.data_ptr(), uin_bar.data_ptr(), st)
+    if nubar is not None:
+        viscosity_cotangent(d, rec, Cbar, lamM, nubar)
     if Sbar_out is not None:
         Sbar += Sbar_out.detach().reshape(-1).to(torch.float64)
     phi_bar = x_bar = None
@@ -155,11 +210,12 @@ class _DiffStep(torch.autograd.Function):
     """One PISO step as one autograd node (forward: the CUDA step; backward: its adjoint)."""
 
     @staticmethod
-    def forward(ctx, runner, u_in, S_in, fvel, stuart, phi_in, uxb_in):
+    def forward(ctx, runner, u_in, S_in, fvel, stuart, phi_in, uxb_in, nu):
         outs, rec = runner.forward_step()
         ctx.runner, ctx.rec = runner, rec
         ctx.shapes = (u_in.shape, S_in.shape, fvel.shape, stuart.shape, phi_in.shape, uxb_in.shape)
         ctx.stuart_device = stuart.device
+        ctx.nu_shape, ctx.nu_device = nu.shape, nu.device
         return outs
 
     @staticmethod
@@ -169,12 +225,18 @@ class _DiffStep(torch.autograd.Function):
         d = sim.domain
         ubbar = torch.zeros_like(d._fvel, dtype=torch.float64)
         Nbar = torch.zeros(d.getBatchSize(), dtype=torch.float64, device=d.getDevice())
+        nubar = torch.zeros(d.getBatchSize(), dtype=torch.float64, device=d.getDevice()) \
+            if ctx.needs_input_grad[7] else None
         state = runner.save_state()
         try:
             uin_bar, S_bar, phi_bar, x_bar = step_backward(sim, rec, ubar, pbar, phibar if runner.mhd else None,
-                                                          xbar if runner.mhd else None, Sbar, ubbar, Nbar, runner.mhd)
+                                                          xbar if runner.mhd else None, Sbar, ubbar, Nbar, runner.mhd,
+                                                          nubar)
         finally:
             runner.restore_state(state)
+        g_nu = None
+        if nubar is not None:
+            g_nu = (nubar.sum() if ctx.nu_shape.numel() == 1 else nubar).reshape(ctx.nu_shape).to(ctx.nu_device)
         su, sS, sf, sN, sp, sx = ctx.shapes
         g_u = uin_bar.view(su)
         g_S = S_bar.view(sS) if S_bar is not None else None
@@ -184,7 +246,7 @@ class _DiffStep(torch.autograd.Function):
             g_N = (Nbar.sum().reshape(sN) if sN.numel() == 1 else Nbar.reshape(sN)).to(ctx.stuart_device)
         g_p = phi_bar.view(sp) if phi_bar is not None else None
         g_x = x_bar.view(sx) if x_bar is not None else None
-        return None, g_u, g_S, g_f, g_N, g_p, g_x
+        return None, g_u, g_S, g_f, g_N, g_p, g_x, g_nu
 
 
 class DiffRunner:
@@ -305,8 +367,9 @@ class DiffRunner:
             stuart = torch.zeros(1, dtype=torch.float64)
             phi_in = torch.zeros(1, dtype=torch.float64, device=d.getDevice())
             uxb_in = torch.zeros(1, dtype=torch.float64, device=d.getDevice())
+        nu = d._viscosity_ag if d._viscosity_ag is not None else d.viscosity
         self._ts = ts
-        u, p, phi, uxb, S = _DiffStep.apply(self, u_in, S_in, fvel, stuart, phi_in, uxb_in)
+        u, p, phi, uxb, S = _DiffStep.apply(self, u_in, S_in, fvel, stuart, phi_in, uxb_in, nu)
         # the block fields become views of the graph outputs (the flat buffers keep the values)
         for b in d.getBlocks():
             o, n = b.globalOffset, b.ncells()

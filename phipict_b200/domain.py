@@ -779,6 +779,8 @@ class Domain:
         _lib.dtype_code(dtype)
         v = viscosity if isinstance(viscosity, torch.Tensor) else torch.tensor([float(viscosity)])
         self.viscosity = v.detach().to("cpu", torch.float64).reshape(-1).clone()
+        # the autograd input of a differentiable simulation (phiPICT's tracked VISCOSITY)
+        self._viscosity_ag = v if v.requires_grad else None
         self._blocks: list[Block] = []
         self._batch = 1
         self._prepared = False
@@ -988,6 +990,7 @@ class Domain:
     def setViscosity(self, viscosity) -> None:
         v = viscosity if isinstance(viscosity, torch.Tensor) else torch.tensor([float(viscosity)])
         self.viscosity = v.detach().to("cpu", torch.float64).reshape(-1).clone()
+        self._viscosity_ag = v if v.requires_grad else None
         if self._prepared:
             self._upload_viscosity()
 
@@ -1520,6 +1523,7 @@ class Domain:
             for bd in b._boundaries:
                 if isinstance(bd, FixedBoundary):
                     bd._velocity_ag = None
+        self._viscosity_ag = None
 
     def UpdateDomainData(self) -> None:
         """Re-pack after structural changes (new boundaries, sizes or data shapes). Values

@@ -107,6 +107,8 @@ def main() -> None:
     ap.add_argument("--skip-fixtures", action="store_true")
     ap.add_argument("--cases", default="c1_fp64,c1_fp32,c2r_fp64", help="comma list of <case>_<dtype>")
     ap.add_argument("--grads", action="store_true", help="also the gradient cases of the differentiable step")
+    ap.add_argument("--viscosity-grad", action="store_true",
+                    help="gradient cases: also the gradient with respect to the viscosity")
     ap.add_argument("--amg", action="store_true", help="also the CSR AMG-PCG cases of amg_cases.py (_C.AMGPCGSolve)")
     a = ap.parse_args()
     import phipict as pp
@@ -123,7 +125,7 @@ def main() -> None:
         for case, make in (("g1", rc.g1_inputs), ("g2", rc.g2_inputs)):
             inputs = make()
             t0 = time.time()
-            g = rc.grad_run(pp, case, inputs, torch.device("cuda"))
+            g = rc.grad_run(pp, case, inputs, torch.device("cuda"), viscosity=a.viscosity_grad)
             data = {k: np.asarray(v) for k, v in inputs.items()}
             data.update({k: np.asarray(v) for k, v in g.items()})
             data["meta"] = np.array(json.dumps(dict(case=case, params=rc.G1 if case == "g1" else rc.G2,

@@ -215,7 +215,7 @@ def g2_inputs() -> dict:
     return out
 
 
-def grad_run(pp, case: str, inputs: dict, device, sim_kwargs: dict | None = None) -> dict:
+def grad_run(pp, case: str, inputs: dict, device, sim_kwargs: dict | None = None, viscosity: bool = False) -> dict:
     """The differentiable rollout of a gradient case on implementation pp; returns the loss
     and its gradients.
 
@@ -223,9 +223,12 @@ def grad_run(pp, case: str, inputs: dict, device, sim_kwargs: dict | None = None
     velocity, the static velocity source and the Stuart number.
     g2: loss = sum(w u^2) over the outlet block + sum(phi^2) after G2 steps, gradients with
     respect to the shared inflow/outflow profile, the initial velocity of the first block and
-    the Stuart number (the source is reset before every Lorentz force, so it has none)."""
+    the Stuart number (the source is reset before every Lorentz force, so it has none).
+    viscosity: also the gradient with respect to the domain's viscosity (a tensor with
+    requires_grad handed to the Domain constructor)."""
     dtype = torch.float64
     p = G1 if case == "g1" else G2
+    nu = torch.tensor([1.0 / p["re"]], dtype=dtype, requires_grad=viscosity)
     stuart = torch.tensor([p["ha"] ** 2 / p["re"]], dtype=dtype, requires_grad=True)
     v0 = _t(inputs["velocity_0"], dtype, device).requires_grad_(True)
     kw = dict(dt=p["dt"], substeps=1, corrector_steps=2, non_orthogonal=False, advection_use_BiCG=True,
@@ -234,7 +237,7 @@ def grad_run(pp, case: str, inputs: dict, device, sim_kwargs: dict | None = None
     kw.update(tolerances(pp, True))
     kw.update(sim_kwargs or {})
     if case == "g1":
-        dom = pp.Domain(2, torch.tensor([1.0 / p["re"]], dtype=dtype), name="gchannel", device=device, dtype=dtype)
+        dom = pp.Domain(2, nu, name="gchannel", device=device, dtype=dtype)
         b = dom.CreateBlock(vertexCoordinates=_t(inputs["vertices_0"], dtype, device), name="channel")
         b.CloseBoundary("-y")
         b.CloseBoundary("+y")
@@ -252,7 +255,7 @@ def grad_run(pp, case: str, inputs: dict, device, sim_kwargs: dict | None = None
         loss = (w * blk.velocity ** 2).sum() + 0.1 * (blk.pressure ** 2).sum()
         names, wrt = ["velocity_0", "source", "stuart"], [v0, src, stuart]
     else:
-        dom = pp.Domain(3, torch.tensor([1.0 / p["re"]], dtype=dtype), name="gduct", device=device, dtype=dtype)
+        dom = pp.Domain(3, nu, name="gduct", device=device, dtype=dtype)
         blocks = [dom.CreateBlock(vertexCoordinates=_t(inputs[f"vertices_{i}"], dtype, device), name=f"b{i}")
                   for i in range(p["nblocks"])]
         for i in range(p["nblocks"] - 1):
@@ -278,9 +281,12 @@ def grad_run(pp, case: str, inputs: dict, device, sim_kwargs: dict | None = None
         w = _t(inputs["loss_w"], dtype, device)
         loss = (w * blocks[-1].velocity ** 2).sum() + (dom.getBlocks()[-1].epot ** 2).sum()
         names, wrt = ["inflow", "velocity_0", "stuart"], [prof, v0, stuart]
-    grads = torch.autograd.grad(loss, wrt)
+    if viscosity:
+        names, wrt = names + ["viscosity"], wrt + [nu]
+    grads = torch.autograd.grad(loss, wrt, allow_unused=True)
     out = {"loss": float(loss.detach())}
     for k, g in zip(names, grads):
-        out[f"grad_{k}"] = g.detach().double().cpu().numpy()
+        if g is not None:
+            out[f"grad_{k}"] = g.detach().double().cpu().numpy()
     dom.Detach()
     return out

@@ -42,7 +42,7 @@ def rel(a, b) -> float:
 @pytest.mark.parametrize("case", ["g1", "g2"])
 def test_gradients_match_reference(cuda, case):
     data = load_grad(case)
-    got = rc.grad_run(pb, case, data, cuda)
+    got = rc.grad_run(pb, case, data, cuda, viscosity="grad_viscosity" in data)
     assert abs(got["loss"] - float(data["loss"])) <= 1e-10 * abs(float(data["loss"]))
     for k in [k for k in data if k.startswith("grad_")]:
         e = rel(got[k], data[k])
@@ -50,11 +50,12 @@ def test_gradients_match_reference(cuda, case):
         assert np.abs(data[k]).max() > 0
 
 
-def _g1_loss(inputs, v0, src, stuart, device="cuda"):
+def _g1_loss(inputs, v0, src, stuart, nu=None, device="cuda"):
     """The g1 loss as a plain function of its inputs (no autograd)."""
     p = rc.G1
     dtype = torch.float64
-    dom = pb.Domain(2, torch.tensor([1.0 / p["re"]], dtype=dtype), name="g", device=device, dtype=dtype)
+    nu = 1.0 / p["re"] if nu is None else nu
+    dom = pb.Domain(2, torch.tensor([nu], dtype=dtype), name="g", device=device, dtype=dtype)
     b = dom.CreateBlock(vertexCoordinates=rc._t(inputs["vertices_0"], dtype, device), name="channel")
     b.CloseBoundary("-y")
     b.CloseBoundary("+y")
@@ -75,7 +76,7 @@ def _g1_loss(inputs, v0, src, stuart, device="cuda"):
 
 def test_gradients_match_finite_differences(cuda):
     inputs = rc.g1_inputs()
-    got = rc.grad_run(pb, "g1", inputs, cuda)
+    got = rc.grad_run(pb, "g1", inputs, cuda, viscosity=True)
     g = torch.Generator().manual_seed(11)
     v0 = torch.as_tensor(inputs["velocity_0"]).cuda()
     src = torch.as_tensor(inputs["source"]).cuda()
@@ -94,6 +95,11 @@ def test_gradients_match_finite_differences(cuda):
         fd = (_g1_loss(inputs, *args(1)) - _g1_loss(inputs, *args(-1))) / (2 * h)
         ad = float((torch.as_tensor(got[f"grad_{name}"]) * dirn.reshape(got[f"grad_{name}"].shape)).sum())
         assert abs(ad - fd) <= FD_BAR * max(abs(fd), 1e-30), f"{name}: adjoint {ad:.10e} vs FD {fd:.10e}"
+    # the viscosity, with a step of 1e-3 of its value
+    nu0, hn = 1.0 / rc.G1["re"], 1e-3 / rc.G1["re"]
+    fd = (_g1_loss(inputs, v0, src, N0, nu0 + hn) - _g1_loss(inputs, v0, src, N0, nu0 - hn)) / (2 * hn)
+    ad = float(got["grad_viscosity"].sum())
+    assert abs(ad - fd) <= FD_BAR * max(abs(fd), 1e-30), f"viscosity: adjoint {ad:.10e} vs FD {fd:.10e}"
 
 
 def test_differentiable_forward_is_the_plain_step(cuda):
