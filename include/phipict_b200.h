@@ -409,6 +409,11 @@ int phb_adj_advection_matrix(const phb_domain *dom, const double *Cbar, double *
 /* phb_advection_rhs (per-cell source): rhsbar -> ubar, srcbar (may be NULL), ubbar (may be NULL) */
 int phb_adj_advection_rhs(const phb_domain *dom, const double *rhsbar, double *ubar, double *srcbar, double *ubbar,
                           phb_stream stream);
+/* phb_scalar_rhs (CENTRAL): rhsbar [inst][channels][cells] -> phibar (same layout), valuesbar (the
+ * layout of sc->values; may be NULL), ubbar (fixed-face velocities; may be NULL); phi = the forward
+ * scalar field */
+int phb_adj_scalar_rhs(const phb_domain *dom, const phb_scalar *sc, const double *phi, const double *rhsbar,
+                       double *phibar, double *valuesbar, double *ubbar, phb_stream stream);
 /* phb_pressure_rhs: hbar -> ubar, ustarbar, Cbar (off-diagonal slots), Abar, srcbar, ubbar; h = the forward HbyA */
 int phb_adj_pressure_rhs(const phb_domain *dom, const double *C, const double *Adiag, const double *ustar, const double *h,
                          const double *hbar, double *ubar, double *ustarbar, double *Cbar, double *Abar, double *srcbar,

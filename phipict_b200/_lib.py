@@ -33,7 +33,7 @@ EXPORTS = (
     "phb_cg_noalloc_bytes", "phb_cg_solve_noalloc",
     "phb_amg_setup", "phb_amg_vcycle", "phb_amg_work_doubles",
     "phb_csr_pcg_work_bytes", "phb_csr_pcg_solve",
-    "phb_transpose_stencil", "phb_adj_outer", "phb_adj_advection_matrix", "phb_adj_advection_rhs",
+    "phb_transpose_stencil", "phb_adj_outer", "phb_adj_advection_matrix", "phb_adj_advection_rhs", "phb_adj_scalar_rhs",
     "phb_adj_pressure_rhs", "phb_adj_divergence", "phb_adj_correct_velocity", "phb_adj_pressure_matrix",
     "phb_adj_uxb_epot_rhs", "phb_adj_lorentz",
 )
@@ -189,6 +189,7 @@ def load() -> ct.CDLL:
         "phb_adj_outer": [DP, I, P, P, ct.c_double, P, P],
         "phb_adj_advection_matrix": [DP, P, P, P],
         "phb_adj_advection_rhs": [DP, P, P, P, P, P],
+        "phb_adj_scalar_rhs": [DP, ct.POINTER(PhbScalar), P, P, P, P, P, P],
         "phb_adj_pressure_rhs": [DP, P, P, P, P, P, P, P, P, P, P, P, P],
         "phb_adj_divergence": [DP, P, P, P, P],
         "phb_adj_correct_velocity": [DP, P, P, P, P, P, P, P],

@@ -191,6 +191,60 @@ __global__ void __launch_bounds__(PHB_TILE) kAdjAdvectionRhs(Dom<S, D> dom, cons
 	}
 }
 
+// kScalarRhs (CENTRAL): rhs_c = (det phi_c/dt + sum over fixed faces of the face terms)/det;
+// Dirichlet faces: -v flux + v nu 2 alpha; Neumann-type faces: -phi flux + v nu area
+// (advection.cu:545-698). rhsbar -> phibar, the fixed-face scalar values (valuesbar, the
+// layout of phb_scalar::values) and the fixed-face velocities through the flux (ubbar).
+template <int D>
+__global__ void __launch_bounds__(PHB_TILE) kAdjScalarRhs(Dom<S, D> dom, ScalarView sv, const S *__restrict__ phi,
+		const S *__restrict__ rhsbar, S *__restrict__ phibar, S *__restrict__ valuesbar, S *__restrict__ ubbar) {
+	__shared__ int32_t sB[PHB_BREC];
+	int l0, nc;
+	loadTile<S, D>(dom, sB, l0, nc);
+	for (int j = 0; j < CPT; ++j) {
+		Cell c;
+		if (!cellAt<D>(sB, l0, nc, j, c)) break;
+		const int inst = c.B[B_INST];
+		const S dt = dom.dt[inst];
+		const double nuVel = dom.nu[inst];
+		const S det = detAt<S, D>(dom, c.mi);
+		for (int ch = 0; ch < sv.channels; ++ch) {
+			const int64_t o = sidx(c.B, c.g, ch, sv.channels);
+			const S rb = rhsbar[o] / det; // cotangent of r (rhs = r / det)
+			if (rb == 0.0) continue;
+			const S nu = S(scalarNu(sv, ch, nuVel));
+			S pb = rb * det / dt;
+#pragma unroll
+			for (int f = 0; f < 2 * D; ++f) {
+				if (!atBound(c.B, f, c.p) || fType(c.B, f) != FT_FIXED) continue;
+				const S faceNormal = (f & 1) ? S(1) : S(-1);
+				const int fid = fRec(c.B, f)[5];
+				const int32_t *FR = dom.fix(fid);
+				const int fc = faceCell(c.B, f, c.p);
+				const int64_t vo = sv.offsets[fid] + (sv.statics[fid] ? ch : (int64_t)ch * FR[F_FACECELLS] + fc);
+				const S value = ((const S *)sv.values)[vo];
+				const S flux = contraFixed<S, D>(dom, FR, fc, f >> 1) * faceNormal;
+				S fluxBar;
+				if (sv.types[(int64_t)fid * sv.channels + ch] == 0) {
+					if (valuesbar) aadd(valuesbar + vo, rb * (-flux + nu * S(2) * alphaFixed<S, D>(dom, FR, fc, f >> 1)));
+					fluxBar = -rb * value;
+				} else {
+					const int64_t fi = FR[F_TOFF] + fc;
+					S m2 = 0;
+#pragma unroll
+					for (int k = 0; k < D; ++k) { const S v = dom.fm(Tr<D>::MINV + (f >> 1) * D + k, fi); m2 += v * v; }
+					const S area = dom.fm(Tr<D>::DET, fi) * sqrt(m2);
+					if (valuesbar) aadd(valuesbar + vo, rb * nu * area);
+					pb -= rb * flux;
+					fluxBar = -rb * phi[o];
+				}
+				adjContraFixed<D>(dom, FR, fc, f >> 1, fluxBar * faceNormal, ubbar);
+			}
+			phibar[o] += pb;
+		}
+	}
+}
+
 // kPressureRhs: h_d = (u_d/dt - sum_f C_f ustar_{j,d} + B_d/det + S_d) / A
 template <int D>
 __global__ void __launch_bounds__(PHB_TILE) kAdjPressureRhs(Dom<S, D> dom, const S *__restrict__ C, const S *__restrict__ Adiag,
@@ -553,6 +607,18 @@ extern "C" int phb_adj_advection_rhs(const phb_domain *dom, const double *rhsbar
 	if (!rhsbar || !ubar) return setError(PHB_ERR_ARG, "phb_adj_advection_rhs: null argument");
 	PHB_ADJ(dom, kAdjAdvectionRhs<D><<<PHB_TL>>>(dm, rhsbar, ubar, srcbar, ubbar));
 	return checkLaunch("kAdjAdvectionRhs");
+}
+
+extern "C" int phb_adj_scalar_rhs(const phb_domain *dom, const phb_scalar *sc, const double *phi, const double *rhsbar,
+		double *phibar, double *valuesbar, double *ubbar, phb_stream stream) {
+	if (!sc || !phi || !rhsbar || !phibar) return setError(PHB_ERR_ARG, "phb_adj_scalar_rhs: null argument");
+	if (sc->channels < 1 || (sc->nu_count != 0 && sc->nu_count != 1 && sc->nu_count != sc->channels) || (sc->nu_count > 0 && !sc->nu) ||
+			(dom && dom->nfixed > 0 && (!sc->types || !sc->values || !sc->offsets || !sc->statics)))
+		return setError(PHB_ERR_ARG, "phb_adj_scalar_rhs: bad scalar description");
+	if (dom && dom->scheme != 0) return setError(PHB_ERR_ARG, "phb_adj_scalar_rhs: the adjoint covers the CENTRAL scheme");
+	const ScalarView sv = scalarView(sc);
+	PHB_ADJ(dom, kAdjScalarRhs<D><<<PHB_TL>>>(dm, sv, phi, rhsbar, phibar, valuesbar, ubbar));
+	return checkLaunch("kAdjScalarRhs");
 }
 
 extern "C" int phb_adj_pressure_rhs(const phb_domain *dom, const double *C, const double *Adiag, const double *ustar, const double *h,

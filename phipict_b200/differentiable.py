@@ -43,9 +43,14 @@ class StepRecord:
     phi_in: torch.Tensor | None = None
     uxb_in: torch.Tensor | None = None
     source_reset: bool = False            # a hook assigned the source during the step
+    # the momentum solve reused the passive scalar's matrix (its face types at fixed faces),
+    # as phiPICT does when the scalar's diffusivity is the viscosity
+    velocity_uses_scalar_matrix: bool = False
     ustar: list = field(default_factory=list)
     h: list = field(default_factory=list)
     p: list = field(default_factory=list)
+    phis_in: torch.Tensor | None = None   # passive scalar before and after the step's scalar stage
+    phis_out: torch.Tensor | None = None
 
 
 def _zeros(d, n):
@@ -100,10 +105,15 @@ def viscosity_cotangent(d, rec: StepRecord, Cbar: torch.Tensor, rhsbar: torch.Te
     A1, A0 = torch.empty_like(d.A), torch.empty_like(d.A)
     r1, r0 = torch.empty_like(d.velocityRHS), torch.empty_like(d.velocityRHS)
     d._u_block.view(-1).copy_(rec.u_in)
+    sc = d._scalar_struct() if rec.velocity_uses_scalar_matrix else None
     try:
         for val, C, A, r in ((1.0, C1, A1, r1), (0.0, C0, A0, r0)):
             d._nu_dev.fill_(val)
-            _lib.call("phb_advection_matrix", desc, d._u_block.data_ptr(), C.data_ptr(), A.data_ptr(), None, st)
+            if sc is not None:
+                _lib.call("phb_scalar_matrix", desc, d._u_block.data_ptr(), ct.byref(sc), 0, C.data_ptr(), A.data_ptr(),
+                          None, st)
+            else:
+                _lib.call("phb_advection_matrix", desc, d._u_block.data_ptr(), C.data_ptr(), A.data_ptr(), None, st)
             _lib.call("phb_advection_rhs", desc, d._u_block.data_ptr(), None, 0, r.data_ptr(), st)
     finally:
         d._nu_dev.copy_(saved)
@@ -147,7 +157,7 @@ def step_backward(sim, rec: StepRecord, ubar_out, pbar_out, phibar_out, xbar_out
     ts = rec.ts
     # the matrices of this step, rebuilt from its input velocity
     d._u_block.view(-1).copy_(rec.u_in)
-    backend.SetupAdvectionMatrix(d, ts, 0)
+    backend.SetupAdvectionMatrix(d, ts, 0, forPassiveScalar=rec.velocity_uses_scalar_matrix, passiveScalarChannel=0)
     backend.SetupPressureMatrix(d, ts, 0, False)
     C, A = d._C_st, d.A
     ubar = _zeros(d, dn) if ubar_out is None else ubar_out.detach().reshape(-1).to(torch.float64).clone()
@@ -206,20 +216,90 @@ def step_backward(sim, rec: StepRecord, ubar_out, pbar_out, phibar_out, xbar_out
     return uin_bar, S_in_bar, phi_bar, x_bar
 
 
+def scalar_backward(sim, rec: StepRecord, phisbar: torch.Tensor, uin_bar: torch.Tensor, ubbar: torch.Tensor,
+                    nubar: torch.Tensor | None):
+    """Reverse pass of the step's passive-scalar stage (every channel c solved from zero with
+    its advection-diffusion matrix C_c(u_in) and right-hand side r(phi_in, boundary values,
+    boundary velocities); advection.cu:27-305,545-698, core/piso_simulation.py:3589-3775):
+    lambda_c = C_c^-T phibar_c, then C_c's cotangent -lambda_c phi_c^T -> u_in, and the
+    right-hand side's cotangent lambda -> phi_in, the boundary scalar values and velocities.
+    The scalar's diffusivity is the velocity's when the domain sets none; then the viscosity's
+    cotangent gets the stage's share. Returns (phi_in bar, boundary values bar)."""
+    d = sim.domain
+    st = _lib.stream_ptr(d.getDevice())
+    desc = ct.byref(d.desc())
+    B, n = d.getBatchSize(), d.numCells()
+    Cn = d.getPassiveScalarChannels()
+    dims = d.getSpatialDims()
+    S = 2 * dims + 1
+    sc = d._scalar_struct()
+    d._u_block.view(-1).copy_(rec.u_in)
+    phis_out = rec.phis_out.view(B, Cn, -1)
+    gout = phisbar.detach().reshape(B, Cn, -1).to(torch.float64)
+    rhsbar = torch.zeros(B, Cn, n // B, dtype=torch.float64, device=d.getDevice())
+    split = not (d.isPassiveScalarViscosityStatic() and d.isAllFixedBoundariesPassiveScalarTypeStatic())
+    nu_shared = sc.nu_count == 0
+    for c in range(Cn):
+        if c == 0 or split:
+            backend.SetupAdvectionMatrix(d, rec.ts, 0, forPassiveScalar=True, passiveScalarChannel=c)
+            CT = torch.empty_like(d._C_st)
+            _lib.call("phb_transpose_stencil", desc, d._C_st.data_ptr(), CT.data_ptr(), st)
+            Cs = d._C_st.clone()
+        g = gout[:, c].contiguous().view(-1)
+        if not bool(g.any()):
+            continue
+        lam = _zeros(d, n)
+        adjoint_solve(sim, "C", g, lam, BICGSTAB, 1, sim.advection_tol, A=CT)
+        rhsbar[:, c] = lam.view(B, -1)
+        Cbar = _zeros(d, S * n)
+        x = phis_out[:, c].contiguous().view(-1)
+        _lib.call("phb_adj_outer", desc, 1, lam.data_ptr(), x.data_ptr(), -1.0, Cbar.data_ptr(), st)
+        _lib.call("phb_adj_advection_matrix", desc, Cbar.data_ptr(), uin_bar.data_ptr(), st)
+        if nubar is not None and nu_shared:
+            saved = d._nu_dev.clone()
+            C1, C0 = torch.empty_like(Cs), torch.empty_like(Cs)
+            A1, A0 = torch.empty_like(d.A), torch.empty_like(d.A)
+            try:
+                for val, Cv, Av in ((1.0, C1, A1), (0.0, C0, A0)):
+                    d._nu_dev.fill_(val)
+                    _lib.call("phb_scalar_matrix", desc, d._u_block.data_ptr(), ct.byref(sc), c, Cv.data_ptr(),
+                              Av.data_ptr(), None, st)
+            finally:
+                d._nu_dev.copy_(saved)
+            nubar += (Cbar.view(S, n) * (C1 - C0).view(S, n)).sum(0).view(B, -1).sum(1)
+    phis_in = rec.phis_in
+    phis_in_bar = torch.zeros_like(phis_in)
+    fscal_bar = torch.zeros_like(d._fscal, dtype=torch.float64)
+    _lib.call("phb_adj_scalar_rhs", desc, ct.byref(sc), phis_in.data_ptr(), rhsbar.data_ptr(), phis_in_bar.data_ptr(),
+              fscal_bar.data_ptr(), ubbar.data_ptr(), st)
+    if nubar is not None and nu_shared:
+        saved = d._nu_dev.clone()
+        r1, r0 = torch.empty_like(rhsbar), torch.empty_like(rhsbar)
+        try:
+            for val, r in ((1.0, r1), (0.0, r0)):
+                d._nu_dev.fill_(val)
+                _lib.call("phb_scalar_rhs", desc, phis_in.data_ptr(), d._u_block.data_ptr(), ct.byref(sc), r.data_ptr(), st)
+        finally:
+            d._nu_dev.copy_(saved)
+        nubar += (rhsbar * (r1 - r0)).sum((1, 2))
+    return phis_in_bar, fscal_bar
+
+
 class _DiffStep(torch.autograd.Function):
     """One PISO step as one autograd node (forward: the CUDA step; backward: its adjoint)."""
 
     @staticmethod
-    def forward(ctx, runner, u_in, S_in, fvel, stuart, phi_in, uxb_in, nu):
+    def forward(ctx, runner, u_in, S_in, fvel, stuart, phi_in, uxb_in, nu, phis_in, fscal):
         outs, rec = runner.forward_step()
         ctx.runner, ctx.rec = runner, rec
         ctx.shapes = (u_in.shape, S_in.shape, fvel.shape, stuart.shape, phi_in.shape, uxb_in.shape)
         ctx.stuart_device = stuart.device
         ctx.nu_shape, ctx.nu_device = nu.shape, nu.device
+        ctx.scalar_shapes = (phis_in.shape, fscal.shape)
         return outs
 
     @staticmethod
-    def backward(ctx, ubar, pbar, phibar, xbar, Sbar):
+    def backward(ctx, ubar, pbar, phibar, xbar, Sbar, phisbar):
         runner, rec = ctx.runner, ctx.rec
         sim = runner.sim
         d = sim.domain
@@ -228,10 +308,15 @@ class _DiffStep(torch.autograd.Function):
         nubar = torch.zeros(d.getBatchSize(), dtype=torch.float64, device=d.getDevice()) \
             if ctx.needs_input_grad[7] else None
         state = runner.save_state()
+        g_phis = g_fscal = None
         try:
             uin_bar, S_bar, phi_bar, x_bar = step_backward(sim, rec, ubar, pbar, phibar if runner.mhd else None,
                                                           xbar if runner.mhd else None, Sbar, ubbar, Nbar, runner.mhd,
                                                           nubar)
+            if runner.scalar and phisbar is not None:
+                g_phis, g_fscal = scalar_backward(sim, rec, phisbar, uin_bar, ubbar, nubar)
+                g_phis = g_phis.view(ctx.scalar_shapes[0])
+                g_fscal = g_fscal.view(ctx.scalar_shapes[1])
         finally:
             runner.restore_state(state)
         g_nu = None
@@ -246,7 +331,7 @@ class _DiffStep(torch.autograd.Function):
             g_N = (Nbar.sum().reshape(sN) if sN.numel() == 1 else Nbar.reshape(sN)).to(ctx.stuart_device)
         g_p = phi_bar.view(sp) if phi_bar is not None else None
         g_x = x_bar.view(sx) if x_bar is not None else None
-        return None, g_u, g_S, g_f, g_N, g_p, g_x, g_nu
+        return None, g_u, g_S, g_f, g_N, g_p, g_x, g_nu, g_phis, g_fscal
 
 
 class DiffRunner:
@@ -263,6 +348,7 @@ class DiffRunner:
             raise NotImplementedError("the hand-written adjoint differentiates the orthogonal step; this grid has "
                                       "non-orthogonal cross terms (use non_orthogonal=False only if they vanish)")
         self.mhd = hasattr(sim, "_stuart_number")
+        self.scalar = bool(sim.advect_passive_scalar and d.hasPassiveScalar())
         self.rec: StepRecord | None = None
         self.uxb_ag: torch.Tensor | None = None
 
@@ -270,6 +356,8 @@ class DiffRunner:
     def begin(self, ts):
         d = self.sim.domain
         self.rec = StepRecord(ts=ts.clone(), u_in=d._u_block.reshape(-1).clone(), src_writes=d._source_writes)
+        if self.scalar:
+            self.rec.phis_in = d._phi_block.reshape(-1).clone()
 
     def source_in(self):
         """Just before the Lorentz force is added (MHD) or the momentum is set up."""
@@ -303,6 +391,8 @@ class DiffRunner:
             keep += [d.epotResult, d._epot_block, self.sim._uxb]
         if d._src is not None:
             keep.append(d._src)
+        if self.scalar:
+            keep += [d._phi_block, d.scalarResult, d.scalarRHS]
         return [(t, t.clone()) for t in keep]
 
     @staticmethod
@@ -351,6 +441,19 @@ class DiffRunner:
             f[off:off + bd._velocity.numel()] = v.expand(bd._velocity.shape).reshape(-1)
         return f
 
+    def _gather_fscal(self) -> torch.Tensor:
+        d = self.sim.domain
+        f = d._fscal.detach()
+        fixed = [bd for b in d.getBlocks() for bd in b.getBoundaries() if getattr(bd, "_scalar_ag", None) is not None]
+        if not fixed:
+            return f
+        f = f.clone()
+        for bd in fixed:
+            off = (bd._passiveScalar.data_ptr() - d._fscal.data_ptr()) // d._fscal.element_size()
+            v = bd._scalar_ag.to(torch.float64)
+            f[off:off + bd._passiveScalar.numel()] = v.expand(bd._passiveScalar.shape).reshape(-1)
+        return f
+
     def step(self, ts) -> None:
         """One recorded step wrapped as a graph node; the block fields become its outputs."""
         sim, d = self.sim, self.sim.domain
@@ -368,8 +471,15 @@ class DiffRunner:
             phi_in = torch.zeros(1, dtype=torch.float64, device=d.getDevice())
             uxb_in = torch.zeros(1, dtype=torch.float64, device=d.getDevice())
         nu = d._viscosity_ag if d._viscosity_ag is not None else d.viscosity
+        if self.scalar:
+            Cn = d.getPassiveScalarChannels()
+            phis_in = self._gather_blocks("_scalar_ag", "passiveScalar", Cn)
+            fscal = self._gather_fscal()
+        else:
+            phis_in = torch.zeros(1, dtype=torch.float64, device=d.getDevice())
+            fscal = torch.zeros(1, dtype=torch.float64, device=d.getDevice())
         self._ts = ts
-        u, p, phi, uxb, S = _DiffStep.apply(self, u_in, S_in, fvel, stuart, phi_in, uxb_in, nu)
+        u, p, phi, uxb, S, phis = _DiffStep.apply(self, u_in, S_in, fvel, stuart, phi_in, uxb_in, nu, phis_in, fscal)
         # the block fields become views of the graph outputs (the flat buffers keep the values)
         for b in d.getBlocks():
             o, n = b.globalOffset, b.ncells()
@@ -383,10 +493,14 @@ class DiffRunner:
             if self.mhd:
                 b.epot = phi[:, o:o + n].view(B, 1, *spatial)
                 b._epot_ag = b.epot
+            if self.scalar:
+                b.passiveScalar = phis[:, :, o:o + n].view(B, phis.shape[1], *spatial)
+                b._scalar_ag = b.passiveScalar
         self.uxb_ag = uxb if self.mhd else None
 
     def forward_step(self):
-        """The ordinary step with recording; returns the outputs (u, p, phi, uxb, S) and the record."""
+        """The ordinary step with recording; returns the outputs (u, p, phi, uxb, S, passive scalar)
+        and the record."""
         sim, d = self.sim, self.sim.domain
         B, dims, N = d.getBatchSize(), d.getSpatialDims(), d.getTotalSize()
         self.begin(self._ts)
@@ -398,10 +512,14 @@ class DiffRunner:
             raise RuntimeError(f"differentiable step failed: {sim.last_error}")
         if rec.S_in is None:  # no Lorentz hook ran (plain PISO): the source as the step used it
             rec.S_in = d._src.reshape(-1).clone()
+        if self.scalar:
+            rec.phis_out = d._phi_block.reshape(-1).clone()
+        zero = torch.zeros(1, dtype=torch.float64, device=d.getDevice())
         outs = (d._u_block.view(B, dims, N).clone(), d.pressureResult.view(B, N).clone(),
-                d.epotResult.view(B, N).clone() if self.mhd else torch.zeros(1, dtype=torch.float64, device=d.getDevice()),
-                sim._uxb.clone() if self.mhd else torch.zeros(1, dtype=torch.float64, device=d.getDevice()),
-                d._src.view(B, dims, N).clone())
+                d.epotResult.view(B, N).clone() if self.mhd else zero,
+                sim._uxb.clone() if self.mhd else zero.clone(),
+                d._src.view(B, dims, N).clone(),
+                d._phi_block.view(B, -1, N).clone() if self.scalar else zero.clone())
         return outs, rec
 
 

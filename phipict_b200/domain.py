@@ -138,6 +138,7 @@ class FixedBoundary(Boundary):
         # domain carries scalars; the type defaults to the velocity type
         self._passiveScalar: torch.Tensor | None = None
         self._passiveScalarTypes: list[BoundaryConditionType] | None = None
+        self._scalar_ag = passiveScalar if passiveScalar is not None and passiveScalar.requires_grad else None
         if passiveScalar is not None:
             self._passiveScalar = self._check_scalar(passiveScalar)
         elif domain.hasPassiveScalar():
@@ -248,7 +249,7 @@ class FixedBoundary(Boundary):
             raise RuntimeError("Passive Scalar must be static (shape NC) or varying (shape NC + face spatial shape).")
         if ps.dim() == 2 + d and list(ps.shape[2:]) != self.face_shape():
             raise RuntimeError(f"varying passive scalar must have the face shape {self.face_shape()}")
-        return ps.contiguous()
+        return ps.detach().contiguous()
 
     @property
     def passiveScalar(self) -> torch.Tensor | None:
@@ -265,6 +266,8 @@ class FixedBoundary(Boundary):
         return self._domain.getPassiveScalarChannels()
 
     def setPassiveScalar(self, passiveScalar: torch.Tensor) -> None:
+        # a differentiable simulation takes the boundary scalar as an input of the graph
+        self._scalar_ag = passiveScalar if passiveScalar.requires_grad else None
         ps = self._check_scalar(passiveScalar)
         if self._passiveScalar is not None and ps.shape == self._passiveScalar.shape and self._domain._prepared_for(self):
             self._passiveScalar.copy_(ps)
@@ -448,6 +451,7 @@ class Block:
         self._source_ag: torch.Tensor | None = None
         self._epot_ag: torch.Tensor | None = None
         self._pressure_ag: torch.Tensor | None = None
+        self._scalar_ag: torch.Tensor | None = None
         self.epot: torch.Tensor | None = None
         self.passiveScalar: torch.Tensor | None = None
         if domain.hasPassiveScalar():
@@ -560,6 +564,10 @@ class Block:
         want = [C] + list(reversed(self._sizes[:d]))
         if s.dim() != d + 2 or list(s.shape[1:]) != want:
             raise RuntimeError(f"passive scalar must have shape [B, {C}, *spatial], got {tuple(s.shape)}")
+        if self._domain._prepared:
+            self._domain._restore_block_views(self, ("passiveScalar",))
+        self._scalar_ag = passiveScalar if passiveScalar.requires_grad else None
+        s = s.detach()
         if self.passiveScalar is not None and s.shape == self.passiveScalar.shape:
             self.passiveScalar.copy_(s)
         else:
@@ -1497,10 +1505,13 @@ class Domain:
             return None if e is None else e[:, o:o + n].view(B, 1, *spatial)
         if field == "velocitySource":
             return self._src[:, :, o:o + n].view(B, d, *spatial) if self._src_mode == 2 else b.velocitySource
+        if field == "passiveScalar":
+            ph = getattr(self, "_phi_block", None)
+            return None if ph is None else ph[:, :, o:o + n].view(B, ph.shape[1], *spatial)
         raise KeyError(field)
 
     _AG_FIELDS = (("velocity", "_velocity_ag"), ("pressure", "_pressure_ag"), ("epot", "_epot_ag"),
-                  ("velocitySource", "_source_ag"))
+                  ("velocitySource", "_source_ag"), ("passiveScalar", "_scalar_ag"))
 
     def _restore_block_views(self, b: "Block", fields=None) -> None:
         """Point fields that a differentiable step replaced by graph outputs back at the flat
@@ -1523,6 +1534,7 @@ class Domain:
             for bd in b._boundaries:
                 if isinstance(bd, FixedBoundary):
                     bd._velocity_ag = None
+                    bd._scalar_ag = None
         self._viscosity_ag = None
 
     def UpdateDomainData(self) -> None:

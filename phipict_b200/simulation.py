@@ -329,6 +329,8 @@ class Simulation:
             matrix_for_velocity = False
             if self.advect_passive_scalar and d.hasPassiveScalar():
                 matrix_for_velocity = self._advect_scalar(ts, step, flags)
+                if rec is not None:
+                    rec.rec.velocity_uses_scalar_matrix = matrix_for_velocity
             self._run_hooks(Hook.PRE_VELOCITY_SETUP, local_step=step, time_step=ts)
             if rec is not None:
                 rec.source_in()

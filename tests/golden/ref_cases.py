@@ -182,6 +182,70 @@ G1 = dict(nx=24, ny=16, length=2.0, re=100.0, ha=10.0, dt=1e-2, steps=5, seed=3)
 G2 = dict(nx=8, ny=6, nz=6, nblocks=2, re=100.0, ha=5.0, beta=2.0, dt=1e-2, steps=3, noise=1e-1, seed=4)
 
 
+G3 = dict(nx=24, ny=16, length=2.0, re=50.0, dt=1e-2, steps=4, seed=5)
+
+
+def g3_inputs() -> dict:
+    """Seeded state of the passive-scalar gradient channel: u = (1, 0) + 0.2 N(0, 1), a scalar
+    field U(0, 1), a Dirichlet scalar 1 on the -y wall and a Neumann scalar flux 0.5 on the +y
+    wall."""
+    p = G3
+    xs = np.linspace(0.0, p["length"], p["nx"] + 1)
+    ys = np.linspace(-1.0, 1.0, p["ny"] + 1)
+    g = torch.Generator(device="cpu").manual_seed(p["seed"])
+    u0 = 0.2 * torch.randn(1, 2, p["ny"], p["nx"], generator=g, dtype=torch.float64)
+    u0[:, 0] += 1.0
+    s0 = torch.rand(1, 1, p["ny"], p["nx"], generator=g, dtype=torch.float64)
+    w = torch.rand(1, 1, p["ny"], p["nx"], generator=g, dtype=torch.float64)
+    wu = torch.rand(1, 2, p["ny"], p["nx"], generator=g, dtype=torch.float64)
+    return {"vertices_0": vertices(xs, ys), "velocity_0": u0.numpy(), "scalar_0": s0.numpy(),
+            "wall_lo": np.array([[1.0]]), "wall_hi": np.array([[0.5]]), "loss_w": w.numpy(), "loss_wu": wu.numpy()}
+
+
+def g3_grad_run(pp, inputs: dict, device, sim_kwargs: dict | None = None) -> dict:
+    """g3: the plain PISO step (no MHD) with one passive-scalar channel. loss = sum(w s^2) +
+    0.1 sum(wu u^2) after G3 steps; gradients with respect to the initial scalar and
+    velocity, the two wall scalar values and the viscosity (the scalar's diffusivity is the
+    viscosity: the domain sets none)."""
+    dtype = torch.float64
+    p = G3
+    nu = torch.tensor([1.0 / p["re"]], dtype=dtype, requires_grad=True)
+    dom = pp.Domain(2, nu, name="gscalar", device=device, dtype=dtype)
+    b = dom.CreateBlock(vertexCoordinates=_t(inputs["vertices_0"], dtype, device), name="channel")
+    b.CloseBoundary("-y")
+    b.CloseBoundary("+y")
+    b.MakePeriodic("x")
+    lo = _t(inputs["wall_lo"], dtype, device).requires_grad_(True)
+    hi = _t(inputs["wall_hi"], dtype, device).requires_grad_(True)
+    b.getBoundary("-y").setPassiveScalar(lo)
+    b.getBoundary("+y").setPassiveScalar(hi)
+    b.getBoundary("+y").setPassiveScalarType(pp.BoundaryConditionType.NEUMANN)
+    dom.PrepareSolve()
+    v0 = _t(inputs["velocity_0"], dtype, device).requires_grad_(True)
+    s0 = _t(inputs["scalar_0"], dtype, device).requires_grad_(True)
+    b.setVelocity(v0.clone())
+    b.setPassiveScalar(s0.clone())
+    dom.UpdateDomainData()
+    kw = dict(dt=p["dt"], substeps=1, corrector_steps=2, non_orthogonal=False, advection_use_BiCG=True,
+              pressure_use_BiCG=False, pressure_use_amg=False, differentiable=True)
+    kw.update({k: v for k, v in tolerances(pp, True).items() if k != "potential_tol"})
+    kw.update(sim_kwargs or {})
+    sim = pp.Simulation(domain=dom, **kw)
+    for _ in range(p["steps"]):
+        sim.single_step()
+    blk = dom.getBlocks()[0]
+    loss = (_t(inputs["loss_w"], dtype, device) * blk.passiveScalar ** 2).sum() \
+        + 0.1 * (_t(inputs["loss_wu"], dtype, device) * blk.velocity ** 2).sum()
+    names, wrt = ["scalar_0", "velocity_0", "wall_lo", "wall_hi", "viscosity"], [s0, v0, lo, hi, nu]
+    grads = torch.autograd.grad(loss, wrt, allow_unused=True)
+    out = {"loss": float(loss.detach())}
+    for k, g in zip(names, grads):
+        if g is not None:
+            out[f"grad_{k}"] = g.detach().double().cpu().numpy()
+    dom.Detach()
+    return out
+
+
 def g1_inputs() -> dict:
     """Seeded state of the gradient channel: u = (1, 0) + 0.3 N(0, 1), a static source."""
     p = G1

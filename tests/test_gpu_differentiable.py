@@ -191,3 +191,80 @@ def test_rollout_and_simulation_agree(cuda):
     g_prof_r, g_N_r = torch.autograd.grad(loss_r, [prof_r, st_r])
     assert rel(g_prof.cpu(), g_prof_r.cpu()) < REF_BAR
     assert rel(g_N.cpu(), g_N_r.cpu()) < REF_BAR
+
+
+def _g3_loss(inputs, s0, v0, lo, hi, nu, device="cuda"):
+    """The g3 loss as a plain function of its inputs (no autograd)."""
+    p = rc.G3
+    dtype = torch.float64
+    dom = pb.Domain(2, torch.tensor([nu], dtype=dtype), name="g3", device=device, dtype=dtype)
+    b = dom.CreateBlock(vertexCoordinates=rc._t(inputs["vertices_0"], dtype, device), name="channel")
+    b.CloseBoundary("-y")
+    b.CloseBoundary("+y")
+    b.MakePeriodic("x")
+    b.getBoundary("-y").setPassiveScalar(torch.tensor([[lo]], dtype=dtype, device=device))
+    b.getBoundary("+y").setPassiveScalar(torch.tensor([[hi]], dtype=dtype, device=device))
+    b.getBoundary("+y").setPassiveScalarType(pb.BoundaryConditionType.NEUMANN)
+    dom.PrepareSolve()
+    b.setVelocity(v0)
+    b.setPassiveScalar(s0)
+    dom.UpdateDomainData()
+    kw = dict(dt=p["dt"], substeps=1, corrector_steps=2, non_orthogonal=False, advection_use_BiCG=True,
+              pressure_use_BiCG=False, pressure_use_amg=False)
+    kw.update({k: v for k, v in rc.tolerances(pb, True).items() if k != "potential_tol"})
+    sim = pb.Simulation(domain=dom, **kw)
+    for _ in range(p["steps"]):
+        assert sim.single_step()
+    return float((rc._t(inputs["loss_w"], dtype, device) * b.passiveScalar ** 2).sum()
+                 + 0.1 * (rc._t(inputs["loss_wu"], dtype, device) * b.velocity ** 2).sum())
+
+
+# phiPICT's gradient of a Neumann-type passive-scalar face still follows an older forward
+# formulation (piso/advection.cu:768-773 marks it as to be updated): it omits the face area of
+# the diffusive term and sends the advective part to the boundary value. Its gradients with
+# respect to that face's value and to the viscosity (which that term also carries) therefore
+# disagree with its own forward; here both are held to central differences instead.
+REFERENCE_NEUMANN_SCALAR_DEFECT = ("grad_wall_hi", "grad_viscosity")
+
+
+def test_scalar_gradients_match_reference(cuda):
+    """The passive-scalar stage of the differentiable step against phiPICT's own gradients."""
+    data = load_grad("g3")
+    got = rc.g3_grad_run(pb, data, cuda)
+    assert abs(got["loss"] - float(data["loss"])) <= 1e-10 * abs(float(data["loss"]))
+    keys = [k for k in data if k.startswith("grad_") and k not in REFERENCE_NEUMANN_SCALAR_DEFECT]
+    assert {"grad_scalar_0", "grad_velocity_0", "grad_wall_lo"} <= set(keys)
+    errs = {k: rel(got[k], data[k]) for k in keys}
+    assert all(math.isfinite(e) and e < REF_BAR for e in errs.values()), errs
+    # the defect itself: on this grid phiPICT's Neumann value gradient is the face-cell sum
+    # without the face area dx = 1/12
+    dx = rc.G3["length"] / rc.G3["nx"]
+    assert abs(float(got["grad_wall_hi"].sum()) - dx * float(data["grad_wall_hi"].sum())) \
+        <= 1e-8 * abs(float(got["grad_wall_hi"].sum()))
+
+
+def test_scalar_gradients_match_finite_differences(cuda):
+    inputs = rc.g3_inputs()
+    got = rc.g3_grad_run(pb, inputs, cuda)
+    g = torch.Generator().manual_seed(13)
+    s0 = torch.as_tensor(inputs["scalar_0"]).cuda()
+    v0 = torch.as_tensor(inputs["velocity_0"]).cuda()
+    base = dict(s0=s0, v0=v0, lo=1.0, hi=0.5, nu=1.0 / rc.G3["re"])
+    cases = []
+    for name, key in (("scalar_0", "s0"), ("velocity_0", "v0")):
+        dirn = torch.randn(base[key].shape, generator=g, dtype=torch.float64)
+        dirn /= dirn.abs().max()
+        cases.append((name, key, dirn.cuda(), 1e-4))
+    cases += [("wall_lo", "lo", 1.0, 1e-4), ("wall_hi", "hi", 1.0, 1e-4), ("viscosity", "nu", 1.0, 1e-3 / rc.G3["re"])]
+    bad = []
+    for name, key, dirn, h in cases:
+        def at(sgn):
+            kw = dict(base)
+            kw[key] = base[key] + sgn * h * dirn
+            return _g3_loss(inputs, kw["s0"], kw["v0"], kw["lo"], kw["hi"], kw["nu"])
+        fd = (at(1) - at(-1)) / (2 * h)
+        grad = torch.as_tensor(got[f"grad_{name}"])
+        ad = float((grad * dirn.cpu().reshape(grad.shape)).sum()) if isinstance(dirn, torch.Tensor) else float(grad.sum())
+        if not abs(ad - fd) <= FD_BAR * max(abs(fd), 1e-30):
+            bad.append(f"{name}: adjoint {ad:.10e} vs FD {fd:.10e}")
+    assert not bad, bad
