@@ -1255,10 +1255,19 @@ __device__ __forceinline__ void cgPersistentBody(const Dom<double, D> &dom, cons
 	}
 }
 
-// At least three resident CTAs per SM (at most 85 registers): a grid of one CTA per 1024-cell
-// tile then stays co-resident up to 444 tiles (the 442,368-cell duct has 432).
+// Resident CTAs per SM that the register budget must allow. The preconditioned solve keeps
+// at least three (at most 85 registers): a grid of one CTA per 1024-cell tile then stays
+// co-resident up to 444 tiles (the 442,368-cell duct has 432). The plain float32 CG is bound
+// by HBM on large grids and is faster with more warps in flight: four CTAs in 3D (64
+// registers), five in 2D (48), which it fits without spilling. Several right-hand sides and
+// float64 need more registers per thread.
+template <typename T, int D, int K, bool PC>
+constexpr int cgMinBlocks() {
+	return PC ? 3 : (std::is_same<T, float>::value && K == 1) ? (D == 2 ? 5 : 4) : (K == 1 ? 3 : 2);
+}
+
 template <typename T, int D, int K, bool STOPSTART, bool PC = false>
-__global__ void __launch_bounds__(PHB_TILE, 3) kCgPersistent(Dom<double, D> dom, const T *__restrict__ A, const T *__restrict__ b,
+__global__ void __launch_bounds__(PHB_TILE, (cgMinBlocks<T, D, K, PC>())) kCgPersistent(Dom<double, D> dom, const T *__restrict__ A, const T *__restrict__ b,
 		T *__restrict__ x, T *__restrict__ r, T *__restrict__ p0, T *__restrict__ p1, T *__restrict__ q, T *__restrict__ xbest,
 		SysState *st, double *partial, Control *ctrl, phb_tolerance tol, int returnBest, int maxit, AmgView<D> mg) {
 	cgPersistentBody<T, D, K, STOPSTART, PC, false>(dom, A, b, x, r, p0, p1, q, xbest, st, partial, ctrl, tol, returnBest, maxit, mg);
