@@ -404,18 +404,23 @@ int phb_transpose_stencil(const phb_domain *dom, const void *C, void *CT, phb_st
  * solve M x = b with respect to M is -lam (x)^T on the stencil, lam = M^-T xbar */
 int phb_adj_outer(const phb_domain *dom, int ncomp, const double *lam, const double *x, double scale, double *Mbar,
                   phb_stream stream);
-/* phb_advection_matrix: Cbar (slot 0 including the adjoint of Adiag) -> ubar */
-int phb_adj_advection_matrix(const phb_domain *dom, const double *Cbar, double *ubar, phb_stream stream);
-/* phb_advection_rhs (per-cell source): rhsbar -> ubar, srcbar (may be NULL), ubbar (may be NULL) */
-int phb_adj_advection_rhs(const phb_domain *dom, const double *rhsbar, double *ubar, double *srcbar, double *ubbar,
-                          phb_stream stream);
-/* phb_scalar_rhs (CENTRAL): rhsbar [inst][channels][cells] -> phibar (same layout), valuesbar (the
- * layout of sc->values; may be NULL), ubbar (fixed-face velocities; may be NULL); phi = the forward
- * scalar field */
-int phb_adj_scalar_rhs(const phb_domain *dom, const phb_scalar *sc, const double *phi, const double *rhsbar,
-                       double *phibar, double *valuesbar, double *ubbar, phb_stream stream);
-/* phb_pressure_rhs: hbar -> ubar, ustarbar, Cbar (off-diagonal slots), Abar, srcbar, ubbar; h = the forward HbyA */
-int phb_adj_pressure_rhs(const phb_domain *dom, const double *C, const double *Adiag, const double *ustar, const double *h,
+/* phb_advection_matrix: Cbar (slot 0 including the adjoint of Adiag) -> ubar; u = the forward velocity
+ * (needed with LINEAR_UPWIND, whose upwinded faces follow the sign of its fluxes; may be NULL for CENTRAL) */
+int phb_adj_advection_matrix(const phb_domain *dom, const double *Cbar, const double *u, double *ubar, phb_stream stream);
+/* phb_advection_rhs (per-cell source): rhsbar -> ubar, srcbar (may be NULL), ubbar (may be NULL); u = the
+ * forward velocity (LINEAR_UPWIND's deferred correction; may be NULL for CENTRAL) */
+int phb_adj_advection_rhs(const phb_domain *dom, const double *rhsbar, const double *u, double *ubar, double *srcbar,
+                          double *ubbar, phb_stream stream);
+/* phb_scalar_rhs: rhsbar [inst][channels][cells] -> phibar (same layout), valuesbar (the layout of
+ * sc->values; may be NULL), ubbar (fixed-face velocities; may be NULL); phi = the forward scalar field;
+ * with LINEAR_UPWIND also ubar through the fluxes of u, the forward velocity (both required then) */
+int phb_adj_scalar_rhs(const phb_domain *dom, const phb_scalar *sc, const double *phi, const double *u,
+                       const double *rhsbar, double *phibar, double *valuesbar, double *ubar, double *ubbar,
+                       phb_stream stream);
+/* phb_pressure_rhs: hbar -> ubar, ustarbar, Cbar (off-diagonal slots), Abar, srcbar, ubbar; h = the forward HbyA;
+ * u = the forward velocity (LINEAR_UPWIND's deferred correction; may be NULL for CENTRAL) */
+int phb_adj_pressure_rhs(const phb_domain *dom, const double *C, const double *Adiag, const double *u, const double *ustar,
+                         const double *h,
                          const double *hbar, double *ubar, double *ustarbar, double *Cbar, double *Abar, double *srcbar,
                          double *ubbar, phb_stream stream);
 /* phb_divergence: dbar -> fbar (the field) and ubbar (fixed faces) */

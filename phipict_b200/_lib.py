@@ -187,10 +187,10 @@ def load() -> ct.CDLL:
         "phb_amg_setup": [ct.POINTER(PhbAmg), P],
         "phb_transpose_stencil": [DP, P, P, P],
         "phb_adj_outer": [DP, I, P, P, ct.c_double, P, P],
-        "phb_adj_advection_matrix": [DP, P, P, P],
-        "phb_adj_advection_rhs": [DP, P, P, P, P, P],
-        "phb_adj_scalar_rhs": [DP, ct.POINTER(PhbScalar), P, P, P, P, P, P],
-        "phb_adj_pressure_rhs": [DP, P, P, P, P, P, P, P, P, P, P, P, P],
+        "phb_adj_advection_matrix": [DP, P, P, P, P],
+        "phb_adj_advection_rhs": [DP, P, P, P, P, P, P],
+        "phb_adj_scalar_rhs": [DP, ct.POINTER(PhbScalar), P, P, P, P, P, P, P, P],
+        "phb_adj_pressure_rhs": [DP, P, P, P, P, P, P, P, P, P, P, P, P, P],
         "phb_adj_divergence": [DP, P, P, P, P],
         "phb_adj_correct_velocity": [DP, P, P, P, P, P, P, P],
         "phb_adj_pressure_matrix": [DP, P, P, P, P],

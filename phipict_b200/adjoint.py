@@ -234,9 +234,9 @@ class AdjointMHD:
             _lib.call("phb_adj_outer", desc, 1, lamP.data_ptr(), rec.p[k].data_ptr(), -1.0, Pbar.data_ptr(), st)
             _lib.call("phb_adj_divergence", desc, dbar.data_ptr(), hbar.data_ptr(), ubbar.data_ptr(), st)
             ustar_bar = self._zeros(dn)
-            _lib.call("phb_adj_pressure_rhs", desc, C.data_ptr(), A.data_ptr(), rec.ustar[k].data_ptr(), rec.h[k].data_ptr(),
-                      hbar.data_ptr(), uin_bar.data_ptr(), ustar_bar.data_ptr(), Cbar.data_ptr(), Abar.data_ptr(),
-                      Sbar.data_ptr(), ubbar.data_ptr(), st)
+            _lib.call("phb_adj_pressure_rhs", desc, C.data_ptr(), A.data_ptr(), d._u_block.data_ptr(),
+                      rec.ustar[k].data_ptr(), rec.h[k].data_ptr(), hbar.data_ptr(), uin_bar.data_ptr(),
+                      ustar_bar.data_ptr(), Cbar.data_ptr(), Abar.data_ptr(), Sbar.data_ptr(), ubbar.data_ptr(), st)
             ubar = ustar_bar
         _lib.call("phb_adj_pressure_matrix", desc, A.data_ptr(), Pbar.data_ptr(), Abar.data_ptr(), st)
         # momentum solve on C^T
@@ -245,9 +245,10 @@ class AdjointMHD:
         lamM = self._zeros(dn)
         self._solve("C", ubar, lamM, BICGSTAB, self.dims, A=CT)
         _lib.call("phb_adj_outer", desc, self.dims, lamM.data_ptr(), rec.ustar[0].data_ptr(), -1.0, Cbar.data_ptr(), st)
-        _lib.call("phb_adj_advection_rhs", desc, lamM.data_ptr(), uin_bar.data_ptr(), Sbar.data_ptr(), ubbar.data_ptr(), st)
+        _lib.call("phb_adj_advection_rhs", desc, lamM.data_ptr(), d._u_block.data_ptr(), uin_bar.data_ptr(),
+                  Sbar.data_ptr(), ubbar.data_ptr(), st)
         Cbar.view(S, n)[0] += Abar
-        _lib.call("phb_adj_advection_matrix", desc, Cbar.data_ptr(), uin_bar.data_ptr(), st)
+        _lib.call("phb_adj_advection_matrix", desc, Cbar.data_ptr(), d._u_block.data_ptr(), uin_bar.data_ptr(), st)
         # Lorentz source
         phi_bar, x_bar = self._zeros(n), self._zeros(3 * n)
         _lib.call("phb_adj_lorentz", desc, rec.phi_in.data_ptr(), rec.uxb_in.data_ptr(), self.e_b.data_ptr(),

@@ -12,6 +12,7 @@
 // contribution. The kernels run in FP64.
 #include "phb_device.cuh"
 #include "phb_launch.cuh"
+#include "phb_upwind.cuh"
 
 namespace phb {
 
@@ -50,6 +51,58 @@ __device__ __forceinline__ void adjContraFixed(const Dom<S, D> &dom, const int32
 	const S det = dom.fm(Tr<D>::DET, fi);
 #pragma unroll
 	for (int j = 0; j < D; ++j) aadd(fixedVelBar<D>(FR, fc, j, ubbar), det * dom.fm(Tr<D>::MINV + c * D + j, fi) * vbar);
+}
+
+// faceFluxes adjoint: flBar[f] (cotangent of the face flux fl[f] of cell c) -> the field
+// (ubar) and, on fixed faces, the boundary velocity (ubbar)
+template <int D>
+__device__ __forceinline__ void adjFaceFluxes(const Dom<S, D> &dom, const Cell &c, const S (&flBar)[2 * D], S *ubar, S *ubbar) {
+#pragma unroll
+	for (int f = 0; f < 2 * D; ++f) {
+		if (flBar[f] == 0.0) continue;
+		const int dim = f >> 1;
+		if (atBound(c.B, f, c.p) && fType(c.B, f) == FT_FIXED) {
+			adjContraFixed<D>(dom, dom.fix(fRec(c.B, f)[5]), faceCell(c.B, f, c.p), dim, flBar[f], ubbar);
+		} else {
+			adjContra<D>(dom, c.B, c.g, c.mi, dim, S(0.5) * flBar[f], ubar);
+			const Nbr n = neighbor<S, D>(dom, c, f);
+			adjContra<D>(dom, n.B, n.g, n.mi, n.comp, n.flip ? -S(0.5) * flBar[f] : S(0.5) * flBar[f], ubar);
+		}
+	}
+}
+
+// upwindCorrection adjoint for one field value(g) at cell c with the fluxes fl: rb is the
+// cotangent of r; the field's cotangent goes to vbar(g), the fluxes' to flBar. As phiPICT's
+// adjoint of the deferred correction (piso/advection.cu:1049-1063), the correction is taken
+// as its linear form -F/2 (phi_U - phi_UU) with the upwind branch and the skip of a vanishing
+// phi_D - phi_U frozen.
+template <int D, typename Val, typename VBar>
+__device__ __forceinline__ void adjUpwindCorrection(const Cell &c, const S (&fl)[2 * D], Val value, VBar vbar, S rb,
+		S (&flBar)[2 * D]) {
+	if (rb == 0.0) return;
+#pragma unroll
+	for (int f = 0; f < 2 * D; ++f) {
+		const int ax = f >> 1;
+		const int sign = (f & 1) ? 1 : -1;
+		const S fout = S(sign) * fl[f];
+		const bool outflow = fout >= S(0);
+		if (!farUpwind(c.B, c.p, f, outflow)) continue;
+		int64_t step = 1;
+		if (ax >= 1) step *= c.B[B_NX];
+		if (ax >= 2) step *= c.B[B_NY];
+		const int64_t gN = c.g + sign * step;
+		const int64_t gUU = outflow ? c.g - sign * step : c.g + 2 * sign * step;
+		const int64_t gU = outflow ? c.g : gN;
+		const S phiP = value(c.g), phiN = value(gN), phiUU = value(gUU);
+		const S phiU = outflow ? phiP : phiN;
+		const S phiD = outflow ? phiN : phiP;
+		const S dD = phiD - phiU;
+		if ((dD < S(0) ? -dD : dD) < S(1e-20)) continue;
+		// r -= fout/2 (phi_U - phi_UU)
+		vbar(gU, -S(0.5) * fout * rb);
+		vbar(gUU, S(0.5) * fout * rb);
+		flBar[f] += S(sign) * (-S(0.5) * (phiU - phiUU) * rb);
+	}
 }
 
 // --- linear-solve pieces -------------------------------------------------------------------
@@ -115,8 +168,11 @@ __global__ void __launch_bounds__(PHB_TILE) kAdjOuter(Dom<S, D> dom, const S *__
 // --- assembly adjoints ---------------------------------------------------------------------
 // kAdvectionMatrix: Cbar (with the adjoint of Adiag already added to slot 0) -> ubar via the
 // face fluxes F_f = (contra_P + contra_N)/2 (C depends on u only through them)
+// With LINEAR_UPWIND an upwinded face puts all of s F on the diagonal (outflow) or on the
+// face slot (inflow); the branch, taken from the fluxes of u, is frozen (advection.cu:380-400).
 template <int D>
-__global__ void __launch_bounds__(PHB_TILE) kAdjAdvectionMatrix(Dom<S, D> dom, const S *__restrict__ Cbar, S *__restrict__ ubar) {
+__global__ void __launch_bounds__(PHB_TILE) kAdjAdvectionMatrix(Dom<S, D> dom, const S *__restrict__ Cbar, const S *__restrict__ u,
+		S *__restrict__ ubar) {
 	__shared__ int32_t sB[PHB_BREC];
 	int l0, nc;
 	loadTile<S, D>(dom, sB, l0, nc);
@@ -126,12 +182,18 @@ __global__ void __launch_bounds__(PHB_TILE) kAdjAdvectionMatrix(Dom<S, D> dom, c
 		if (!cellAt<D>(sB, l0, nc, j, c)) break;
 		const S det = detAt<S, D>(dom, c.mi);
 		const S d0 = Cbar[c.g];
+		S fl[2 * D];
+		if (dom.scheme != 0) faceFluxes<S, D>(dom, c, u, fl);
 #pragma unroll
 		for (int f = 0; f < 2 * D; ++f) {
 			if (atBound(c.B, f, c.p) && fType(c.B, f) == FT_FIXED) continue;
 			const S faceSign = (f & 1) ? S(1) : S(-1);
-			// diag += 0.5 s F / det, off_f += 0.5 s F / det
-			const S Fbar = S(0.5) * faceSign * (d0 + Cbar[(f + 1) * N + c.g]) / det;
+			// CENTRAL: diag += 0.5 s F / det, off_f += 0.5 s F / det
+			S Fbar = S(0.5) * faceSign * (d0 + Cbar[(f + 1) * N + c.g]) / det;
+			if (dom.scheme != 0) {
+				const S fout = faceSign * fl[f];
+				if (farUpwind(c.B, c.p, f, fout >= S(0))) Fbar = faceSign * (fout >= S(0) ? d0 : Cbar[(f + 1) * N + c.g]) / det;
+			}
 			// F = (velC + velN)/2
 			adjContra<D>(dom, c.B, c.g, c.mi, f >> 1, S(0.5) * Fbar, ubar);
 			const Nbr n = neighbor<S, D>(dom, c, f);
@@ -165,10 +227,27 @@ __device__ __forceinline__ void adjBoundarySource(const Dom<S, D> &dom, const Ce
 	}
 }
 
+// The deferred LINEAR_UPWIND correction of every velocity component at cell c (advection
+// and HbyA right-hand sides): Bbar[d] is the cotangent of the component's correction sum
+// (before the division by det) -> ubar through the values and the fluxes of u.
+template <int D>
+__device__ __forceinline__ void adjUpwindTerms(const Dom<S, D> &dom, const Cell &c, const S *u, const S (&Bbar)[D], S *ubar,
+		S *ubbar) {
+	S fl[2 * D], flBar[2 * D];
+	faceFluxes<S, D>(dom, c, u, fl);
+#pragma unroll
+	for (int f = 0; f < 2 * D; ++f) flBar[f] = 0;
+#pragma unroll
+	for (int d = 0; d < D; ++d)
+		adjUpwindCorrection<D>(c, fl, [&](int64_t g) { return u[vidx<D>(c.B, g, d)]; },
+				[&](int64_t g, S v) { aadd(ubar + vidx<D>(c.B, g, d), v); }, Bbar[d], flBar);
+	adjFaceFluxes<D>(dom, c, flBar, ubar, ubbar);
+}
+
 // kAdvectionRhs: rhs_d = u_d/dt + B_d/det + S_d
 template <int D>
-__global__ void __launch_bounds__(PHB_TILE) kAdjAdvectionRhs(Dom<S, D> dom, const S *__restrict__ rhsbar, S *__restrict__ ubar,
-		S *__restrict__ srcbar, S *__restrict__ ubbar) {
+__global__ void __launch_bounds__(PHB_TILE) kAdjAdvectionRhs(Dom<S, D> dom, const S *__restrict__ rhsbar, const S *__restrict__ u,
+		S *__restrict__ ubar, S *__restrict__ srcbar, S *__restrict__ ubbar) {
 	__shared__ int32_t sB[PHB_BREC];
 	int l0, nc;
 	loadTile<S, D>(dom, sB, l0, nc);
@@ -183,11 +262,12 @@ __global__ void __launch_bounds__(PHB_TILE) kAdjAdvectionRhs(Dom<S, D> dom, cons
 		for (int d = 0; d < D; ++d) {
 			const int64_t o = vidx<D>(c.B, c.g, d);
 			const S r = rhsbar[o];
-			ubar[o] += r / dt;
+			aadd(ubar + o, r / dt); // atomically: the upwind terms of other cells add here too
 			if (srcbar) srcbar[o] += r;
 			Bbar[d] = r / det;
 		}
 		adjBoundarySource<D>(dom, c, Bbar, nu, ubbar);
+		if (dom.scheme != 0) adjUpwindTerms<D>(dom, c, u, Bbar, ubar, ubbar);
 	}
 }
 
@@ -197,7 +277,8 @@ __global__ void __launch_bounds__(PHB_TILE) kAdjAdvectionRhs(Dom<S, D> dom, cons
 // layout of phb_scalar::values) and the fixed-face velocities through the flux (ubbar).
 template <int D>
 __global__ void __launch_bounds__(PHB_TILE) kAdjScalarRhs(Dom<S, D> dom, ScalarView sv, const S *__restrict__ phi,
-		const S *__restrict__ rhsbar, S *__restrict__ phibar, S *__restrict__ valuesbar, S *__restrict__ ubbar) {
+		const S *__restrict__ u, const S *__restrict__ rhsbar, S *__restrict__ phibar, S *__restrict__ valuesbar,
+		S *__restrict__ ubar, S *__restrict__ ubbar) {
 	__shared__ int32_t sB[PHB_BREC];
 	int l0, nc;
 	loadTile<S, D>(dom, sB, l0, nc);
@@ -208,10 +289,17 @@ __global__ void __launch_bounds__(PHB_TILE) kAdjScalarRhs(Dom<S, D> dom, ScalarV
 		const S dt = dom.dt[inst];
 		const double nuVel = dom.nu[inst];
 		const S det = detAt<S, D>(dom, c.mi);
+		S fl[2 * D], flBar[2 * D];
+#pragma unroll
+		for (int f = 0; f < 2 * D; ++f) flBar[f] = 0;
+		if (dom.scheme != 0) faceFluxes<S, D>(dom, c, u, fl);
 		for (int ch = 0; ch < sv.channels; ++ch) {
 			const int64_t o = sidx(c.B, c.g, ch, sv.channels);
 			const S rb = rhsbar[o] / det; // cotangent of r (rhs = r / det)
 			if (rb == 0.0) continue;
+			if (dom.scheme != 0) // the deferred LINEAR_UPWIND correction of the channel
+				adjUpwindCorrection<D>(c, fl, [&](int64_t g) { return phi[sidx(c.B, g, ch, sv.channels)]; },
+						[&](int64_t g, S v) { aadd(phibar + sidx(c.B, g, ch, sv.channels), v); }, rb, flBar);
 			const S nu = S(scalarNu(sv, ch, nuVel));
 			S pb = rb * det / dt;
 #pragma unroll
@@ -240,16 +328,17 @@ __global__ void __launch_bounds__(PHB_TILE) kAdjScalarRhs(Dom<S, D> dom, ScalarV
 				}
 				adjContraFixed<D>(dom, FR, fc, f >> 1, fluxBar * faceNormal, ubbar);
 			}
-			phibar[o] += pb;
+			aadd(phibar + o, pb);
 		}
+		if (dom.scheme != 0) adjFaceFluxes<D>(dom, c, flBar, ubar, ubbar);
 	}
 }
 
 // kPressureRhs: h_d = (u_d/dt - sum_f C_f ustar_{j,d} + B_d/det + S_d) / A
 template <int D>
 __global__ void __launch_bounds__(PHB_TILE) kAdjPressureRhs(Dom<S, D> dom, const S *__restrict__ C, const S *__restrict__ Adiag,
-		const S *__restrict__ ustar, const S *__restrict__ h, const S *__restrict__ hbar, S *__restrict__ ubar, S *__restrict__ ustarbar,
-		S *__restrict__ Cbar, S *__restrict__ Abar, S *__restrict__ srcbar, S *__restrict__ ubbar) {
+		const S *__restrict__ u, const S *__restrict__ ustar, const S *__restrict__ h, const S *__restrict__ hbar, S *__restrict__ ubar,
+		S *__restrict__ ustarbar, S *__restrict__ Cbar, S *__restrict__ Abar, S *__restrict__ srcbar, S *__restrict__ ubbar) {
 	__shared__ int32_t sB[PHB_BREC];
 	int l0, nc;
 	loadTile<S, D>(dom, sB, l0, nc);
@@ -267,7 +356,7 @@ __global__ void __launch_bounds__(PHB_TILE) kAdjPressureRhs(Dom<S, D> dom, const
 			const int64_t o = vidx<D>(c.B, c.g, d);
 			qbar[d] = hbar[o] * rD;
 			aAcc -= hbar[o] * h[o] * rD;
-			ubar[o] += qbar[d] / dt;
+			aadd(ubar + o, qbar[d] / dt); // atomically: the upwind terms of other cells add here too
 			if (srcbar) srcbar[o] += qbar[d];
 			Bbar[d] = qbar[d] / det;
 		}
@@ -287,6 +376,8 @@ __global__ void __launch_bounds__(PHB_TILE) kAdjPressureRhs(Dom<S, D> dom, const
 			Cbar[(f + 1) * N + c.g] += s;
 		}
 		adjBoundarySource<D>(dom, c, Bbar, nu, ubbar);
+		// HbyA repeats the predictor's deferred correction of u (pressure.cu:474-515)
+		if (dom.scheme != 0) adjUpwindTerms<D>(dom, c, u, Bbar, ubar, ubbar);
 	}
 }
 
@@ -596,37 +687,38 @@ extern "C" int phb_adj_outer(const phb_domain *dom, int ncomp, const double *lam
 	return checkLaunch("kAdjOuter");
 }
 
-extern "C" int phb_adj_advection_matrix(const phb_domain *dom, const double *Cbar, double *ubar, phb_stream stream) {
-	if (!Cbar || !ubar) return setError(PHB_ERR_ARG, "phb_adj_advection_matrix: null argument");
-	PHB_ADJ(dom, kAdjAdvectionMatrix<D><<<PHB_TL>>>(dm, Cbar, ubar));
+extern "C" int phb_adj_advection_matrix(const phb_domain *dom, const double *Cbar, const double *u, double *ubar, phb_stream stream) {
+	if (!Cbar || !ubar || (dom && dom->scheme != 0 && !u)) return setError(PHB_ERR_ARG, "phb_adj_advection_matrix: null argument");
+	PHB_ADJ(dom, kAdjAdvectionMatrix<D><<<PHB_TL>>>(dm, Cbar, u, ubar));
 	return checkLaunch("kAdjAdvectionMatrix");
 }
 
-extern "C" int phb_adj_advection_rhs(const phb_domain *dom, const double *rhsbar, double *ubar, double *srcbar, double *ubbar,
-		phb_stream stream) {
-	if (!rhsbar || !ubar) return setError(PHB_ERR_ARG, "phb_adj_advection_rhs: null argument");
-	PHB_ADJ(dom, kAdjAdvectionRhs<D><<<PHB_TL>>>(dm, rhsbar, ubar, srcbar, ubbar));
+extern "C" int phb_adj_advection_rhs(const phb_domain *dom, const double *rhsbar, const double *u, double *ubar, double *srcbar,
+		double *ubbar, phb_stream stream) {
+	if (!rhsbar || !ubar || (dom && dom->scheme != 0 && !u)) return setError(PHB_ERR_ARG, "phb_adj_advection_rhs: null argument");
+	PHB_ADJ(dom, kAdjAdvectionRhs<D><<<PHB_TL>>>(dm, rhsbar, u, ubar, srcbar, ubbar));
 	return checkLaunch("kAdjAdvectionRhs");
 }
 
-extern "C" int phb_adj_scalar_rhs(const phb_domain *dom, const phb_scalar *sc, const double *phi, const double *rhsbar,
-		double *phibar, double *valuesbar, double *ubbar, phb_stream stream) {
-	if (!sc || !phi || !rhsbar || !phibar) return setError(PHB_ERR_ARG, "phb_adj_scalar_rhs: null argument");
+extern "C" int phb_adj_scalar_rhs(const phb_domain *dom, const phb_scalar *sc, const double *phi, const double *u,
+		const double *rhsbar, double *phibar, double *valuesbar, double *ubar, double *ubbar, phb_stream stream) {
+	if (!sc || !phi || !rhsbar || !phibar || (dom && dom->scheme != 0 && (!u || !ubar)))
+		return setError(PHB_ERR_ARG, "phb_adj_scalar_rhs: null argument");
 	if (sc->channels < 1 || (sc->nu_count != 0 && sc->nu_count != 1 && sc->nu_count != sc->channels) || (sc->nu_count > 0 && !sc->nu) ||
 			(dom && dom->nfixed > 0 && (!sc->types || !sc->values || !sc->offsets || !sc->statics)))
 		return setError(PHB_ERR_ARG, "phb_adj_scalar_rhs: bad scalar description");
-	if (dom && dom->scheme != 0) return setError(PHB_ERR_ARG, "phb_adj_scalar_rhs: the adjoint covers the CENTRAL scheme");
 	const ScalarView sv = scalarView(sc);
-	PHB_ADJ(dom, kAdjScalarRhs<D><<<PHB_TL>>>(dm, sv, phi, rhsbar, phibar, valuesbar, ubbar));
+	PHB_ADJ(dom, kAdjScalarRhs<D><<<PHB_TL>>>(dm, sv, phi, u, rhsbar, phibar, valuesbar, ubar, ubbar));
 	return checkLaunch("kAdjScalarRhs");
 }
 
-extern "C" int phb_adj_pressure_rhs(const phb_domain *dom, const double *C, const double *Adiag, const double *ustar, const double *h,
+extern "C" int phb_adj_pressure_rhs(const phb_domain *dom, const double *C, const double *Adiag, const double *u, const double *ustar,
+		const double *h,
 		const double *hbar, double *ubar, double *ustarbar, double *Cbar, double *Abar, double *srcbar, double *ubbar,
 		phb_stream stream) {
-	if (!C || !Adiag || !ustar || !h || !hbar || !ubar || !ustarbar || !Cbar || !Abar)
+	if (!C || !Adiag || !ustar || !h || !hbar || !ubar || !ustarbar || !Cbar || !Abar || (dom && dom->scheme != 0 && !u))
 		return setError(PHB_ERR_ARG, "phb_adj_pressure_rhs: null argument");
-	PHB_ADJ(dom, kAdjPressureRhs<D><<<PHB_TL>>>(dm, C, Adiag, ustar, h, hbar, ubar, ustarbar, Cbar, Abar, srcbar, ubbar));
+	PHB_ADJ(dom, kAdjPressureRhs<D><<<PHB_TL>>>(dm, C, Adiag, u, ustar, h, hbar, ubar, ustarbar, Cbar, Abar, srcbar, ubbar));
 	return checkLaunch("kAdjPressureRhs");
 }
 

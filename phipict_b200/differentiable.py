@@ -190,9 +190,9 @@ def step_backward(sim, rec: StepRecord, ubar_out, pbar_out, phibar_out, xbar_out
         if nubar is not None:
             hbya_viscosity_cotangent(d, rec, k, C, A, hbar, nubar)
         ustar_bar = _zeros(d, dn)
-        _lib.call("phb_adj_pressure_rhs", desc, C.data_ptr(), A.data_ptr(), rec.ustar[k].data_ptr(), rec.h[k].data_ptr(),
-                  hbar.data_ptr(), uin_bar.data_ptr(), ustar_bar.data_ptr(), Cbar.data_ptr(), Abar.data_ptr(),
-                  Sbar.data_ptr(), ubbar.data_ptr(), st)
+        _lib.call("phb_adj_pressure_rhs", desc, C.data_ptr(), A.data_ptr(), d._u_block.data_ptr(), rec.ustar[k].data_ptr(),
+                  rec.h[k].data_ptr(), hbar.data_ptr(), uin_bar.data_ptr(), ustar_bar.data_ptr(),
+                  Cbar.data_ptr(), Abar.data_ptr(), Sbar.data_ptr(), ubbar.data_ptr(), st)
         ubar = ustar_bar
     _lib.call("phb_adj_pressure_matrix", desc, A.data_ptr(), Pbar.data_ptr(), Abar.data_ptr(), st)
     CT = torch.empty_like(C)
@@ -200,9 +200,10 @@ def step_backward(sim, rec: StepRecord, ubar_out, pbar_out, phibar_out, xbar_out
     lamM = _zeros(d, dn)
     adjoint_solve(sim, "C", ubar, lamM, BICGSTAB, dims, sim.advection_tol, A=CT)
     _lib.call("phb_adj_outer", desc, dims, lamM.data_ptr(), rec.ustar[0].data_ptr(), -1.0, Cbar.data_ptr(), st)
-    _lib.call("phb_adj_advection_rhs", desc, lamM.data_ptr(), uin_bar.data_ptr(), Sbar.data_ptr(), ubbar.data_ptr(), st)
+    _lib.call("phb_adj_advection_rhs", desc, lamM.data_ptr(), d._u_block.data_ptr(), uin_bar.data_ptr(), Sbar.data_ptr(),
+              ubbar.data_ptr(), st)
     Cbar.view(S, n)[0] += Abar
-    _lib.call("phb_adj_advection_matrix", desc, Cbar.data_ptr(), uin_bar.data_ptr(), st)
+    _lib.call("phb_adj_advection_matrix", desc, Cbar.data_ptr(), d._u_block.data_ptr(), uin_bar.data_ptr(), st)
     if nubar is not None:
         viscosity_cotangent(d, rec, Cbar, lamM, nubar)
     if Sbar_out is not None:
@@ -254,7 +255,7 @@ def scalar_backward(sim, rec: StepRecord, phisbar: torch.Tensor, uin_bar: torch.
         Cbar = _zeros(d, S * n)
         x = phis_out[:, c].contiguous().view(-1)
         _lib.call("phb_adj_outer", desc, 1, lam.data_ptr(), x.data_ptr(), -1.0, Cbar.data_ptr(), st)
-        _lib.call("phb_adj_advection_matrix", desc, Cbar.data_ptr(), uin_bar.data_ptr(), st)
+        _lib.call("phb_adj_advection_matrix", desc, Cbar.data_ptr(), d._u_block.data_ptr(), uin_bar.data_ptr(), st)
         if nubar is not None and nu_shared:
             saved = d._nu_dev.clone()
             C1, C0 = torch.empty_like(Cs), torch.empty_like(Cs)
@@ -270,8 +271,8 @@ def scalar_backward(sim, rec: StepRecord, phisbar: torch.Tensor, uin_bar: torch.
     phis_in = rec.phis_in
     phis_in_bar = torch.zeros_like(phis_in)
     fscal_bar = torch.zeros_like(d._fscal, dtype=torch.float64)
-    _lib.call("phb_adj_scalar_rhs", desc, ct.byref(sc), phis_in.data_ptr(), rhsbar.data_ptr(), phis_in_bar.data_ptr(),
-              fscal_bar.data_ptr(), ubbar.data_ptr(), st)
+    _lib.call("phb_adj_scalar_rhs", desc, ct.byref(sc), phis_in.data_ptr(), d._u_block.data_ptr(), rhsbar.data_ptr(),
+              phis_in_bar.data_ptr(), fscal_bar.data_ptr(), uin_bar.data_ptr(), ubbar.data_ptr(), st)
     if nubar is not None and nu_shared:
         saved = d._nu_dev.clone()
         r1, r0 = torch.empty_like(rhsbar), torch.empty_like(rhsbar)
@@ -342,8 +343,6 @@ class DiffRunner:
         d = sim.domain
         if d.getDtype() != torch.float64:
             raise TypeError("a differentiable simulation runs on a float64 domain")
-        if int(d.getAdvectionScheme()) != 0:
-            raise NotImplementedError("the hand-written adjoint differentiates the CENTRAL advection scheme")
         if d.getSpatialDims() > 1 and d.hasNonOrthogonalMetrics() and sim.non_orthogonal:
             raise NotImplementedError("the hand-written adjoint differentiates the orthogonal step; this grid has "
                                       "non-orthogonal cross terms (use non_orthogonal=False only if they vanish)")

@@ -132,14 +132,20 @@ def main() -> None:
                                                     device=torch.cuda.get_device_name(0))))
             np.savez_compressed(out / f"ref_{case}_grad.npz", **data)
             print(json.dumps(dict(tag=f"{case}_grad", loss=g["loss"], wall_s=round(time.time() - t0, 2))), flush=True)
-        inputs = rc.g3_inputs()
-        g = rc.g3_grad_run(pp, inputs, torch.device("cuda"))
-        data = {k: np.asarray(v) for k, v in inputs.items()}
-        data.update({k: np.asarray(v) for k, v in g.items()})
-        data["meta"] = np.array(json.dumps(dict(case="g3", params=rc.G3, device=torch.cuda.get_device_name(0))))
-        np.savez_compressed(out / "ref_g3_grad.npz", **data)
-        print(json.dumps(dict(tag="g3_grad", loss=g["loss"], grads=sorted(k for k in g if k.startswith("grad_")))),
-              flush=True)
+        runs = [("g3", lambda: rc.g3_grad_run(pp, rc.g3_inputs(), torch.device("cuda")), rc.g3_inputs, rc.G3),
+                ("g1u", lambda: rc.grad_run(pp, "g1", rc.g1_inputs(), torch.device("cuda"), viscosity=True, upwind=True),
+                 rc.g1_inputs, rc.G1),
+                ("g3u", lambda: rc.g3_grad_run(pp, rc.g3_inputs(), torch.device("cuda"), upwind=True), rc.g3_inputs,
+                 rc.G3)]
+        for tag, run, make, params in runs:
+            g = run()
+            data = {k: np.asarray(v) for k, v in make().items()}
+            data.update({k: np.asarray(v) for k, v in g.items()})
+            data["meta"] = np.array(json.dumps(dict(case=tag, params=params, upwind=tag.endswith("u"),
+                                                    device=torch.cuda.get_device_name(0))))
+            np.savez_compressed(out / f"ref_{tag}_grad.npz", **data)
+            print(json.dumps(dict(tag=f"{tag}_grad", loss=g["loss"], grads=sorted(k for k in g if k.startswith("grad_")))),
+                  flush=True)
     if a.amg:
         amg_fixture(out)
     if a.time_duct:

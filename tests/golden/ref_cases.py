@@ -202,7 +202,7 @@ def g3_inputs() -> dict:
             "wall_lo": np.array([[1.0]]), "wall_hi": np.array([[0.5]]), "loss_w": w.numpy(), "loss_wu": wu.numpy()}
 
 
-def g3_grad_run(pp, inputs: dict, device, sim_kwargs: dict | None = None) -> dict:
+def g3_grad_run(pp, inputs: dict, device, sim_kwargs: dict | None = None, upwind: bool = False) -> dict:
     """g3: the plain PISO step (no MHD) with one passive-scalar channel. loss = sum(w s^2) +
     0.1 sum(wu u^2) after G3 steps; gradients with respect to the initial scalar and
     velocity, the two wall scalar values and the viscosity (the scalar's diffusivity is the
@@ -211,6 +211,8 @@ def g3_grad_run(pp, inputs: dict, device, sim_kwargs: dict | None = None) -> dic
     p = G3
     nu = torch.tensor([1.0 / p["re"]], dtype=dtype, requires_grad=True)
     dom = pp.Domain(2, nu, name="gscalar", device=device, dtype=dtype)
+    if upwind:
+        dom.setAdvectionScheme(pp.AdvectionScheme.LINEAR_UPWIND)
     b = dom.CreateBlock(vertexCoordinates=_t(inputs["vertices_0"], dtype, device), name="channel")
     b.CloseBoundary("-y")
     b.CloseBoundary("+y")
@@ -279,7 +281,8 @@ def g2_inputs() -> dict:
     return out
 
 
-def grad_run(pp, case: str, inputs: dict, device, sim_kwargs: dict | None = None, viscosity: bool = False) -> dict:
+def grad_run(pp, case: str, inputs: dict, device, sim_kwargs: dict | None = None, viscosity: bool = False,
+             upwind: bool = False) -> dict:
     """The differentiable rollout of a gradient case on implementation pp; returns the loss
     and its gradients.
 
@@ -289,7 +292,8 @@ def grad_run(pp, case: str, inputs: dict, device, sim_kwargs: dict | None = None
     respect to the shared inflow/outflow profile, the initial velocity of the first block and
     the Stuart number (the source is reset before every Lorentz force, so it has none).
     viscosity: also the gradient with respect to the domain's viscosity (a tensor with
-    requires_grad handed to the Domain constructor)."""
+    requires_grad handed to the Domain constructor). upwind: the LINEAR_UPWIND advection
+    scheme instead of CENTRAL."""
     dtype = torch.float64
     p = G1 if case == "g1" else G2
     nu = torch.tensor([1.0 / p["re"]], dtype=dtype, requires_grad=viscosity)
@@ -302,6 +306,8 @@ def grad_run(pp, case: str, inputs: dict, device, sim_kwargs: dict | None = None
     kw.update(sim_kwargs or {})
     if case == "g1":
         dom = pp.Domain(2, nu, name="gchannel", device=device, dtype=dtype)
+        if upwind:
+            dom.setAdvectionScheme(pp.AdvectionScheme.LINEAR_UPWIND)
         b = dom.CreateBlock(vertexCoordinates=_t(inputs["vertices_0"], dtype, device), name="channel")
         b.CloseBoundary("-y")
         b.CloseBoundary("+y")
@@ -320,6 +326,8 @@ def grad_run(pp, case: str, inputs: dict, device, sim_kwargs: dict | None = None
         names, wrt = ["velocity_0", "source", "stuart"], [v0, src, stuart]
     else:
         dom = pp.Domain(3, nu, name="gduct", device=device, dtype=dtype)
+        if upwind:
+            dom.setAdvectionScheme(pp.AdvectionScheme.LINEAR_UPWIND)
         blocks = [dom.CreateBlock(vertexCoordinates=_t(inputs[f"vertices_{i}"], dtype, device), name=f"b{i}")
                   for i in range(p["nblocks"])]
         for i in range(p["nblocks"] - 1):
