@@ -239,7 +239,7 @@ def barrier(world: int):
         dist.barrier()
 
 
-def build_sim(wl: dict, device, mixed: bool, amg: bool = True, warm: bool = False):
+def build_sim(wl: dict, device, mixed: bool, amg: bool = True, warm: bool = False, autotune: bool = False):
     import phipict_b200 as pb
 
     dtype = torch.float64
@@ -259,7 +259,8 @@ def build_sim(wl: dict, device, mixed: bool, amg: bool = True, warm: bool = Fals
     sim = pb.MHDSimulation(dom, wl["dt"], torch.tensor(N), torch.tensor([0.0, 1.0, 0.0], dtype=dtype),
                            non_orthogonal=False, advection_tol=tol, pressure_tol=tol, potential_tol=tol,
                            mixed_precision=mixed, hooks=hooks, pressure_use_amg=amg and mixed,
-                           potential_use_preconditioner=amg and mixed, pressure_warm_start=warm)
+                           potential_use_preconditioner=amg and mixed, pressure_warm_start=warm,
+                           autotune_solvers=autotune)
     return dom, sim
 
 
@@ -268,12 +269,12 @@ def run_ours(args, rank, world, local):
     device = torch.device("cuda", local)
     mixed = not args.plain_fp64
     amg = mixed and not args.no_amg
-    dom, sim = build_sim(wl, device, mixed, amg, args.pressure_warm_start)
+    dom, sim = build_sim(wl, device, mixed, amg, args.pressure_warm_start, args.autotune)
     if args.inner_rtol:
         sim.refinement_inner_rtol = args.inner_rtol
     cells = dom.getTotalSize()
     stream = torch.cuda.current_stream(device)
-    for _ in range(args.warmup):
+    for _ in range(tuned_warmup(args, sim)):
         if not sim.single_step():
             raise RuntimeError("warm-up step failed")
     torch.cuda.synchronize()
@@ -321,10 +322,10 @@ def run_ours(args, rank, world, local):
     # up the same way), every step reading its velocity from pinned host memory and writing u,
     # p and phi back there; the next step starts from the velocity it wrote
     d = dom.getSpatialDims()
-    dom_e, sim_e = build_sim(wl, device, mixed, amg, args.pressure_warm_start)
+    dom_e, sim_e = build_sim(wl, device, mixed, amg, args.pressure_warm_start, args.autotune)
     if args.inner_rtol:
         sim_e.refinement_inner_rtol = args.inner_rtol
-    for _ in range(args.warmup):
+    for _ in range(tuned_warmup(args, sim_e)):
         if not sim_e.single_step():
             raise RuntimeError("warm-up step failed")
     nu = dom_e._u_block.numel()
@@ -403,6 +404,7 @@ def run_ours(args, rank, world, local):
                   "bytes_per_cell": round(per_cell, 2), "peak_source": pk["source"],
                   "iterations": inner_its, "solve_ms": round(solve_ms, 3)},
         gpu_launches=int(gpu_launches),
+        **({"solver_tuning": sim.solver_tuner.report()} if sim.solver_tuner is not None else {}),
         **({"vs_plain_fp64": plain["vs_plain_fp64"], "err_vs_fp64": plain["err_vs_fp64"]} if plain else {}),
         solver={"inner_iterations_per_step": round(inner_its / args.steps, 1),
                 "refinement_sweeps_per_step": round(sweeps / args.steps, 2),
@@ -517,6 +519,12 @@ def reset_cell_source(domain, **kw):
         domain._src.zero_()
 
 
+def tuned_warmup(args, sim) -> int:
+    """Warm-up steps: with --autotune at least enough for every solve's tuning trials."""
+    t = sim.solver_tuner
+    return args.warmup if t is None else max(args.warmup, t.trials * len(t.CANDIDATES) + 1)
+
+
 def run_batch64(args, rank, world, local):
     import phipict_b200 as pb
 
@@ -531,10 +539,11 @@ def run_batch64(args, rank, world, local):
                            advection_tol=tol, pressure_tol=tol, potential_tol=tol, mixed_precision=not args.plain_fp64,
                            pressure_use_amg=not args.plain_fp64 and not args.no_amg,
                            potential_use_preconditioner=not args.plain_fp64 and not args.no_amg,
-                           hooks=pb.Hooks().append(pb.Hook.PRE_VELOCITY_SETUP, reset_cell_source))
+                           hooks=pb.Hooks().append(pb.Hook.PRE_VELOCITY_SETUP, reset_cell_source),
+                           autotune_solvers=args.autotune)
     sim.time_step = torch.tensor([dt for _, _, dt in inst], dtype=torch.float64)
     stream = torch.cuda.current_stream(device)
-    for _ in range(args.warmup):
+    for _ in range(tuned_warmup(args, sim)):
         if not sim.single_step():
             raise RuntimeError(f"warm-up step failed: {sim.last_error}")
     clocks = ClockSampler(local)
@@ -568,13 +577,15 @@ def run_batch64(args, rank, world, local):
             alone_ms += a.elapsed_time(b)
     value = cells * world * args.steps / (ms / 1e3) / 1e6
     return dict(metric="Mcell-steps/s", value=round(value, 4), unit="Mcell-steps/s", n_gpus=world, steps=args.steps,
-                warmup=args.warmup, ms_per_step=round(ms / args.steps, 4), higher_is_better=True, scaling="weak",
-                vs_baseline=None, dtype="f64 fields, f32 Krylov + f64 refinement" if not args.plain_fp64 else "f64",
+                warmup=tuned_warmup(args, sim), ms_per_step=round(ms / args.steps, 4), higher_is_better=True,
+                scaling="weak", vs_baseline=None,
+                dtype="f64 fields, f32 Krylov + f64 refinement" if not args.plain_fp64 else "f64",
                 data="synthetic (seeded instance mix)",
                 config={"workload": f"batch64: {len(inst)} 2D Hartmann/cavity instances, sides in {wl['sides']}, "
                                     f"Ha log-uniform [1,1000], Re U(100,2000), one DomainBatch, rtol {wl['rtol']}",
                         "cells_per_gpu": cells, "parallelism": f"replicas x{world}"},
                 clocks=clk,
+                **({"solver_tuning": sim.solver_tuner.report()} if sim.solver_tuner is not None else {}),
                 one_at_a_time={"ms_per_step": round(alone_ms, 3) if alone_ms else None,
                                "value": round(cells / (alone_ms / 1e3) / 1e6, 4) if alone_ms else None,
                                "path": "plain FP64, each instance alone"},
@@ -963,6 +974,8 @@ def main():
     ap.add_argument("--inner-rtol", type=float, default=None, help="inner FP32 reduction per refinement sweep")
     ap.add_argument("--no-alone", action="store_true", help="batch64: skip the one-at-a-time comparison")
     ap.add_argument("--no-batch64", action="store_true", help="duct3d: skip the batched-instances sub-record")
+    ap.add_argument("--autotune", action="store_true",
+                    help="tune the persistent Krylov kernels' CTAs per SM per solve during the warm-up")
     ap.add_argument("--requests", type=int, default=None, help="serve: number of requests")
     ap.add_argument("--plain-sample", type=int, default=8, help="serve: requests timed one at a time on plain FP64")
     ap.add_argument("--plain-steps", type=int, default=10, help="serve: timed steps per one-at-a-time request")

@@ -282,6 +282,9 @@ typedef struct phb_solve {
 	void *state;          /* >= phb_solve_state_bytes() bytes */
 	const phb_amg *amg;   /* optional (CG, float32, nrhs 1): precondition with one V-cycle of
 	                         this hierarchy (set up for A); its level-0 x holds z */
+	int32_t ctas_per_sm;  /* persistent kernels (use_graph 2, 3): resident CTAs per SM to launch, at
+	                         most what fits; 0: as many as fit (the grid never exceeds the tile count) */
+	int32_t pad;
 } phb_solve;
 
 /* per-system result, mirrors LinearSolverResultInfo (bindings.cpp:727-732) */
@@ -314,7 +317,7 @@ typedef struct phb_refine {
 	int32_t inner_maxit;
 	int32_t use_graph;    /* 2: graph outer loop, persistent inner solves; 3: host outer loop, persistent inner
 	                         solves (profilers see every launch); 1: nested graph loops; 0: host loops */
-	int32_t pad;
+	int32_t ctas_per_sm;  /* the inner persistent solves' phb_solve::ctas_per_sm */
 	double inner_rtol;
 	phb_tolerance tol;    /* outer tolerance, on the float64 residual */
 	const double *A64;

@@ -77,7 +77,7 @@ class PhbSolve(ct.Structure):
         ("tol", PhbTolerance),
         ("A", ct.c_void_p), ("b", ct.c_void_p), ("x", ct.c_void_p),
         ("work", ct.c_void_p), ("state", ct.c_void_p),
-        ("amg", ct.c_void_p),
+        ("amg", ct.c_void_p), ("ctas_per_sm", ct.c_int32), ("pad", ct.c_int32),
     ]
 
 
@@ -91,7 +91,7 @@ class PhbSolveResult(ct.Structure):
 class PhbRefine(ct.Structure):
     _fields_ = [
         ("kind", ct.c_int32), ("nrhs", ct.c_int32), ("max_outer", ct.c_int32), ("inner_maxit", ct.c_int32),
-        ("use_graph", ct.c_int32), ("pad", ct.c_int32), ("inner_rtol", ct.c_double),
+        ("use_graph", ct.c_int32), ("ctas_per_sm", ct.c_int32), ("inner_rtol", ct.c_double),
         ("tol", PhbTolerance),
         ("A64", ct.c_void_p), ("A32", ct.c_void_p), ("b", ct.c_void_p), ("x", ct.c_void_p),
         ("work", ct.c_void_p), ("state", ct.c_void_p),

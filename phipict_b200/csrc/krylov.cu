@@ -1605,6 +1605,7 @@ static int launchPersistent(const phb_domain *dom, const phb_solve *sv, cudaStre
 		if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 		int perSM = 0;
 		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, PHB_TILE, smem) != cudaSuccess || perSM < 1) perSM = 1;
+		if (sv->ctas_per_sm > 0) perSM = std::min(perSM, sv->ctas_per_sm); // a tuned, smaller grid
 		return std::max(1, std::min(dom->ntiles, perSM * numSMs()));
 	};
 	if (sv->kind == 0) {
@@ -1900,6 +1901,7 @@ static int emitRefine(const phb_domain *dom, const phb_refine *rf, cudaStream_t 
 	in.work = rf->work;
 	in.state = rf->state;
 	in.amg = rf->amg;
+	in.ctas_per_sm = rf->ctas_per_sm;
 	// 1: nested graph loops; 2: graph outer loop, persistent inner solves; 3: host outer loop,
 	// persistent inner solves (every launch visible to a kernel profiler); 0: host loops
 	const bool graph = rf->use_graph == 1 || rf->use_graph == 2;

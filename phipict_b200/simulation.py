@@ -28,7 +28,7 @@ import torch
 from . import _C as backend
 from .domain import Domain, FixedBoundary
 from .hooks import Hook, Hooks
-from .solvers import BICGSTAB, CG, LinearSolverResultInfo, LinsolveError, refiner_for, solver_for
+from .solvers import BICGSTAB, CG, LinearSolverResultInfo, LinsolveError, SolverTuner, refiner_for, solver_for
 from .tolerance import SolverTolerance, coerce_tolerance
 
 _UNSUPPORTED_TRUE = ("scipy_solve_advection", "scipy_solve_pressure", "differentiable_unsupported")
@@ -83,6 +83,7 @@ class Simulation:
         hooks: Hooks | dict | None = None,
         mixed_precision: bool = False,
         check_solves: bool = True,
+        autotune_solvers: bool = False,
     ) -> None:
         if hooks is not None and prep_fn is not None:
             raise ValueError("Pass hooks or its former name prep_fn, not both.")
@@ -125,11 +126,14 @@ class Simulation:
         self.mixed_precision = bool(mixed_precision)
         # mixed precision: each inner FP32 solve reduces the outer residual by this factor
         self.refinement_inner_rtol = 1e-4
+        # grid of the persistent Krylov kernels tuned per solve by measurement (SolverTuner)
+        self.solver_tuner = SolverTuner() if autotune_solvers else None
         self.check_solves = check_solves
         self.total_step = 0
         self.total_time = 0.0
         self._pressure_guess: dict[int, torch.Tensor] = {}
         self._pending: list[tuple[str, Any]] = []
+        self._tuning: list = []  # (index in _pending, tag, (candidate, start event, end event))
         self._last_report: list[tuple[str, list[LinearSolverResultInfo]]] = []
         self._flux_checked_version = -1
         self._solve_events: list | None = None  # (start, end) CUDA events per solve when a list
@@ -192,19 +196,28 @@ class Simulation:
     def _solve_launch(self, which, rhs, x, kind, tol, tag, nrhs, return_best, maxit) -> None:
         d = self.domain
         pc = kind == CG and nrhs == 1 and self._amg_wanted(which)
+        tune = None
+        ctas = 0
+        if self.solver_tuner is not None:
+            ctas = self.solver_tuner.pick(tag)
+            tune = (ctas, torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            tune[1].record()
         if self.mixed_precision:
             lo = backend._lo(d, which)
             amg = self._amg_for(which, lo) if pc else None
             r = refiner_for(d, kind, nrhs, tag=tag)
             r.inner_rtol = self.refinement_inner_rtol
-            r.solve(d._stencil(which), lo, rhs, x, tol, maxit, amg=amg)
-            self._pending.append((tag, r))
+            r.solve(d._stencil(which), lo, rhs, x, tol, maxit, amg=amg, ctas_per_sm=ctas)
+            solver = r
         else:
             A = d._stencil(which)
             amg = self._amg_for(which, A) if pc else None
-            s = solver_for(d, kind, d.getDtype(), nrhs, tag=tag)
-            s.solve(A, rhs, x, tol, maxit, return_best=return_best, amg=amg)
-            self._pending.append((tag, s))
+            solver = solver_for(d, kind, d.getDtype(), nrhs, tag=tag)
+            solver.solve(A, rhs, x, tol, maxit, return_best=return_best, amg=amg, ctas_per_sm=ctas)
+        if tune is not None:
+            tune[2].record()
+            self._tuning.append((len(self._pending), tag, tune))
+        self._pending.append((tag, solver))
 
     # --- multigrid preconditioner ------------------------------------------------------
     def _amg_dtype_ok(self) -> bool:
@@ -250,6 +263,11 @@ class Simulation:
             good = all(i.converged or (tag.startswith("epot") and self._accept_best(i)) for i in infos)
             if not good:
                 ok = False
+        for k, tag, (ctas, e0, e1) in self._tuning:
+            infos = report[k][1]
+            its = max((i.innerIterations or i.usedIterations for i in infos), default=0)
+            self.solver_tuner.record(tag, ctas, e0.elapsed_time(e1), its)
+        self._tuning.clear()
         self._pending.clear()
         self._last_report = report
         if not ok and raise_on_failure:

@@ -105,7 +105,7 @@ class StencilSolver:
         self._keep = None
 
     def solve(self, A: torch.Tensor, b: torch.Tensor, x: torch.Tensor, tol, maxit: int,
-              return_best: bool = False, use_graph: bool | None = None, amg=None) -> None:
+              return_best: bool = False, use_graph: bool | None = None, amg=None, ctas_per_sm: int = 0) -> None:
         """Launch the solve of ``A x = b`` (x: initial guess, overwritten). Asynchronous.
         ``amg``: an :class:`~phipict_b200.amg.AmgHierarchy` set up for ``A`` (float32 CG
         with one right-hand side) preconditions every iteration with one V-cycle."""
@@ -127,6 +127,7 @@ class StencilSolver:
         s.A, s.b, s.x = A.data_ptr(), b.data_ptr(), x.data_ptr()
         s.work, s.state = self.work.data_ptr(), self.state.data_ptr()
         s.amg = amg.address() if amg is not None else None
+        s.ctas_per_sm = int(ctas_per_sm)
         self._amg = amg
         _lib.call("phb_solve_run", ct.byref(d.desc()), ct.byref(s), _lib.stream_ptr(d.getDevice()))
 
@@ -160,7 +161,7 @@ class RefinedSolver:
         self.outer_used = 0
 
     def solve(self, A64: torch.Tensor, A32: torch.Tensor, b: torch.Tensor, x: torch.Tensor, tol, maxit: int,
-              fetch: bool = False, amg=None) -> list[LinearSolverResultInfo] | None:
+              fetch: bool = False, amg=None, ctas_per_sm: int = 0) -> list[LinearSolverResultInfo] | None:
         """Launch the refined solve; ``amg`` (a hierarchy set up for ``A32``) preconditions
         the inner CG."""
         d = self.domain
@@ -176,6 +177,7 @@ class RefinedSolver:
         r.A64, r.A32, r.b, r.x = A64.data_ptr(), A32.data_ptr(), b.data_ptr(), x.data_ptr()
         r.work, r.state = self.work.data_ptr(), self.state.data_ptr()
         r.amg = amg.address() if amg is not None else None
+        r.ctas_per_sm = int(ctas_per_sm)
         self._amg = amg
         if not fetch:
             _lib.call("phb_refine_run", ct.byref(d.desc()), ct.byref(r), None, None, _lib.stream_ptr(d.getDevice()))
@@ -198,6 +200,46 @@ class RefinedSolver:
         self.outer_used = used.value
         return [LinearSolverResultInfo(o.final_residual, o.used_iterations, bool(o.converged), bool(o.finite), o.status,
                                        o.inner_iterations) for o in out]
+
+
+class SolverTuner:
+    """Per-solve tuning of the persistent Krylov kernels' grid (resident CTAs per SM), by
+    measurement: the first ``trials`` x len(CANDIDATES) solves of each tag (``velocity``,
+    ``pressure0``, ``epot``, ...) cycle through the candidates, each timed with CUDA events and
+    divided by its iterations (the slowest system's; inner iterations under refinement); from
+    then on the tag runs with the candidate of the lowest median time per iteration. 0 is the
+    occupancy maximum (one CTA per tile where the grid allows), smaller values launch fewer,
+    fuller CTAs. A choice changes the launch only, never the arithmetic: the results of every
+    candidate are the same bits."""
+
+    CANDIDATES = (0, 2, 1)
+
+    def __init__(self, trials: int = 3):
+        self.trials = int(trials)
+        self.samples: dict[str, dict[int, list[float]]] = {}
+        self.choice: dict[str, int] = {}
+
+    def pick(self, tag: str) -> int:
+        if tag in self.choice:
+            return self.choice[tag]
+        n = sum(len(v) for v in self.samples.get(tag, {}).values())
+        return self.CANDIDATES[n % len(self.CANDIDATES)]
+
+    def record(self, tag: str, candidate: int, ms: float, iterations: int) -> None:
+        if tag in self.choice or iterations <= 0:
+            return
+        per = self.samples.setdefault(tag, {})
+        per.setdefault(candidate, []).append(ms / iterations)
+        if all(len(per.get(c, [])) >= self.trials for c in self.CANDIDATES):
+            med = {c: sorted(v)[len(v) // 2] for c, v in per.items()}
+            self.choice[tag] = min(med, key=med.get)
+
+    def report(self) -> dict:
+        out = {}
+        for tag, per in self.samples.items():
+            out[tag] = {"ctas_per_sm": self.choice.get(tag),
+                        "us_per_iteration": {str(c): round(1e3 * sorted(v)[len(v) // 2], 3) for c, v in per.items()}}
+        return out
 
 
 def solver_for(domain, kind: int, dtype: torch.dtype, nrhs: int, tag: str = "") -> StencilSolver:
