@@ -64,8 +64,6 @@ class AdjointMHD:
         refinement to the same tolerance; the adjoint kernels stay FP64."""
         if domain.getDtype() != torch.float64:
             raise TypeError("the adjoint step runs in float64")
-        if int(domain.getAdvectionScheme()) != 0:
-            raise NotImplementedError("the hand-written adjoint differentiates the CENTRAL advection scheme")
         if not domain.IsInitialized():
             domain.PrepareSolve()
         if domain.getSpatialDims() > 1 and domain.hasNonOrthogonalMetrics():

@@ -53,14 +53,16 @@ def _channel2d(nx=8, ny=6):
     return dom
 
 
-@pytest.mark.parametrize("case", ["channel2d", "duct3d"])
+@pytest.mark.parametrize("case", ["channel2d", "duct3d", "duct3d_upwind"])
 def test_rollout_gradient_matches_finite_differences(cuda, case):
     dom = _channel2d() if case == "channel2d" else duct_3d(6, 5, 4, 2)
+    if case.endswith("upwind"):
+        dom.setAdvectionScheme(pb.AdvectionScheme.LINEAR_UPWIND)
     seeded_state(dom, 11, scale=0.1)
     dom.PrepareSolve()
     blocks = dom.getBlocks()
     faces = [(blocks[0], "-x"), (blocks[-1], "+x")]
-    e_b = torch.tensor([0.0, 1.0, 0.0], dtype=torch.float64) if case == "duct3d" else torch.tensor([0.0, 1.0, 0.0], dtype=torch.float64)
+    e_b = torch.tensor([0.0, 1.0, 0.0], dtype=torch.float64)
     model = AdjointMHD(dom, 0.01, torch.tensor([2.0]), e_b, steps=3, faces=faces, checkpoint_every=2)
     initial = model._state()
     p0 = model.faces[0]._velocity.detach().clone()
