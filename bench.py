@@ -952,7 +952,7 @@ def run_adjoint(args, rank, world, local):
                 config={"workload": f"adjoint: 2 blocks {wl['nx']}x{wl['ny']}x{wl['nz']} ({cells} cells), Ha {wl['Ha']}, "
                                     f"Re {wl['Re']}, {wl['rollout']} steps, checkpoints every {wl['every']}, rtol {wl['rtol']}",
                         "parallelism": f"replicas x{world}"},
-                adjoint={"forward_s": round(fwd, 3), "backward_s": round(bwd, 3), "loss": float(L),
+                adjoint={"forward_s": round(fwd, 3), "backward_s": round(bwd, 3), "loss": float(L.detach()),
                          "grad_N": float(N.grad.reshape(-1)[0]), "grad_profile_norm": float(prof.grad.norm()),
                          "fd_checks": checks, "max_rel_err": max(c["rel_err"] for c in checks)},
                 gpu_launches=None)
