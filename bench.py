@@ -6,7 +6,10 @@ Workload (default ``duct3d``): the 3D MHD rectangular duct of 3 connected blocks
 and an open-potential outflow. Fields are float64; every solve runs float32 Krylov
 iterations inside float64 iterative refinement to a relative residual of 1e-10.
 Synthetic inputs (seeded), no dataset. A step is one PISO step (momentum predictor,
-2 pressure correctors) plus the potential step and the Lorentz force.
+2 pressure correctors) plus the potential step and the Lorentz force. The pressure and
+potential solves start from guesses extrapolated from the last two steps
+(``extrapolate_guesses``; ``--no-extrapolate`` for phiPICT's zero pressure guess and previous
+potential); the plain FP64 comparison leg keeps phiPICT's defaults.
 
 ``--impl reference`` times the CPU oracle (the restatement of phiPICT's step; phiPICT has no
 CPU path) on the same workload with all host threads, on rank 0.
@@ -239,7 +242,8 @@ def barrier(world: int):
         dist.barrier()
 
 
-def build_sim(wl: dict, device, mixed: bool, amg: bool = True, warm: bool = False, autotune: bool = False):
+def build_sim(wl: dict, device, mixed: bool, amg: bool = True, warm: bool = False, autotune: bool = False,
+              extrapolate: bool = False):
     import phipict_b200 as pb
 
     dtype = torch.float64
@@ -260,7 +264,7 @@ def build_sim(wl: dict, device, mixed: bool, amg: bool = True, warm: bool = Fals
                            non_orthogonal=False, advection_tol=tol, pressure_tol=tol, potential_tol=tol,
                            mixed_precision=mixed, hooks=hooks, pressure_use_amg=amg and mixed,
                            potential_use_preconditioner=amg and mixed, pressure_warm_start=warm,
-                           autotune_solvers=autotune)
+                           autotune_solvers=autotune, extrapolate_guesses=extrapolate)
     return dom, sim
 
 
@@ -269,7 +273,7 @@ def run_ours(args, rank, world, local):
     device = torch.device("cuda", local)
     mixed = not args.plain_fp64
     amg = mixed and not args.no_amg
-    dom, sim = build_sim(wl, device, mixed, amg, args.pressure_warm_start, args.autotune)
+    dom, sim = build_sim(wl, device, mixed, amg, args.pressure_warm_start, args.autotune, args.extrapolate and mixed)
     if args.inner_rtol:
         sim.refinement_inner_rtol = args.inner_rtol
     cells = dom.getTotalSize()
@@ -322,7 +326,8 @@ def run_ours(args, rank, world, local):
     # up the same way), every step reading its velocity from pinned host memory and writing u,
     # p and phi back there; the next step starts from the velocity it wrote
     d = dom.getSpatialDims()
-    dom_e, sim_e = build_sim(wl, device, mixed, amg, args.pressure_warm_start, args.autotune)
+    dom_e, sim_e = build_sim(wl, device, mixed, amg, args.pressure_warm_start, args.autotune,
+                             args.extrapolate and mixed)
     if args.inner_rtol:
         sim_e.refinement_inner_rtol = args.inner_rtol
     for _ in range(tuned_warmup(args, sim_e)):
@@ -347,7 +352,8 @@ def run_ours(args, rank, world, local):
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), world) / e_steps
     del sim_e, dom_e
-    plain = plain_fp64_leg(args, wl, device, stream, final, world) if (mixed and not args.no_fp64_leg) else None
+    plain = (plain_fp64_leg(args, wl, device, stream, final, world, tuned_warmup(args, sim))
+             if (mixed and not args.no_fp64_leg) else None)
     total_cells = cells * world
     value = total_cells * args.steps / (ms / 1e3) / 1e6
     if plain:
@@ -383,6 +389,9 @@ def run_ours(args, rank, world, local):
                             f"rtol 1e-10, {'mixed precision' if mixed else 'plain fp64'}"
                             f"{', multigrid-preconditioned pressure and potential CG' if amg else ''}",
                 "amg_levels": levels,
+                "initial_guesses": ("extrapolated from the last two steps" if args.extrapolate and mixed else
+                                    "previous step's pressure" if args.pressure_warm_start else
+                                    "zero pressure, previous step's potential"),
                 "cells_per_gpu": cells, "l2": "working set ~60 MB f32 fits L2; HBM claims on the roofline sweep",
                 "parallelism": f"replicas x{world}"},
         clocks=clk,
@@ -413,13 +422,14 @@ def run_ours(args, rank, world, local):
     )
 
 
-def plain_fp64_leg(args, wl, device, stream, final, world) -> dict:
+def plain_fp64_leg(args, wl, device, stream, final, world, warmup: int) -> dict:
     """The plain FP64 single-instance path (FP64 CG / BiCGStab, no refinement, no multigrid) on
     the same workload: the same warm-up and timed step counts from the same initial state, timed
     with CUDA events; its fields after the same number of steps are the all-FP64 run that the
-    mixed-precision fields are compared with (relative L2 error per field)."""
-    dom, sim = build_sim(wl, device, False, False, args.pressure_warm_start)
-    for _ in range(args.warmup):
+    mixed-precision fields are compared with (relative L2 error per field). Its initial guesses
+    are phiPICT's defaults (zero pressure, the previous potential)."""
+    dom, sim = build_sim(wl, device, False, False)
+    for _ in range(warmup):
         if not sim.single_step():
             raise RuntimeError("plain FP64 warm-up step failed")
     torch.cuda.synchronize()
@@ -443,7 +453,7 @@ def plain_fp64_leg(args, wl, device, stream, final, world) -> dict:
     return {"vs_plain_fp64": {"value": round(value, 4), "unit": "Mcell-steps/s", "ms_per_step": round(ms, 3),
                               "dtype": "f64", "path": "FP64 CG pressure/potential, FP64 BiCGStab momentum, no refinement, "
                                                       "no multigrid, one instance",
-                              "steps": args.steps, "warmup": args.warmup},
+                              "steps": args.steps, "warmup": warmup},
             "err_vs_fp64": {**{k: float(f"{v:.3e}") for k, v in err.items()},
                             "norm": "relative L2 against the plain FP64 run after the same warm-up + timed steps"}}
 
@@ -974,6 +984,9 @@ def main():
     ap.add_argument("--inner-rtol", type=float, default=None, help="inner FP32 reduction per refinement sweep")
     ap.add_argument("--no-alone", action="store_true", help="batch64: skip the one-at-a-time comparison")
     ap.add_argument("--no-batch64", action="store_true", help="duct3d: skip the batched-instances sub-record")
+    ap.add_argument("--no-extrapolate", dest="extrapolate", action="store_false",
+                    help="duct3d: zero pressure guesses and the previous potential (phiPICT's defaults) instead of "
+                         "guesses extrapolated from the last two steps")
     ap.add_argument("--autotune", action="store_true",
                     help="tune the persistent Krylov kernels' CTAs per SM per solve during the warm-up")
     ap.add_argument("--requests", type=int, default=None, help="serve: number of requests")

@@ -179,8 +179,15 @@ class MHDSimulation(Simulation):
             domain._subtract_mean(domain.epotRHS, 1)
         if not self._potential_reuse_result:
             domain.epotResult.zero_()
-        elif self._potential_rank_deficient:
-            domain._subtract_mean(domain.epotResult, 1)
+        else:
+            if self.extrapolate_guesses:
+                prev = getattr(self, "_epot_prev", None)
+                cur = domain.epotResult.clone()
+                if prev is not None and prev.shape == cur.shape:
+                    domain.epotResult.mul_(2.0).sub_(prev)
+                self._epot_prev = cur
+            if self._potential_rank_deficient:
+                domain._subtract_mean(domain.epotResult, 1)
         self.solve("E", domain.epotRHS, domain.epotResult, use_BiCG=self._potential_use_BiCG, tol=self.potential_tol,
                    tag="epot", return_best=self._potential_return_best_result,
                    max_iter=self._potential_solve_max_iter if max_iter is None else max_iter)

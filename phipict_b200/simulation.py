@@ -84,6 +84,7 @@ class Simulation:
         mixed_precision: bool = False,
         check_solves: bool = True,
         autotune_solvers: bool = False,
+        extrapolate_guesses: bool = False,
     ) -> None:
         if hooks is not None and prep_fn is not None:
             raise ValueError("Pass hooks or its former name prep_fn, not both.")
@@ -128,6 +129,10 @@ class Simulation:
         self.refinement_inner_rtol = 1e-4
         # grid of the persistent Krylov kernels tuned per solve by measurement (SolverTuner)
         self.solver_tuner = SolverTuner() if autotune_solvers else None
+        # initial guesses of the pressure (per corrector) and potential solves extrapolated
+        # linearly from the last two steps' results, 2 x_n - x_(n-1) (implies the warm start)
+        self.extrapolate_guesses = bool(extrapolate_guesses)
+        self._pressure_prev: dict[int, torch.Tensor] = {}
         self.check_solves = check_solves
         self.total_step = 0
         self.total_time = 0.0
@@ -385,9 +390,13 @@ class Simulation:
                 if rec is not None:
                     rec.hbya(d.pressureRHS)
                 self._run_hooks(Hook.POST_PRESSURE_SETUP, local_step=step, time_step=ts)
-                guess = self._pressure_guess.get(cstep) if self.pressure_warm_start else None
+                warm = self.pressure_warm_start or self.extrapolate_guesses
+                guess = self._pressure_guess.get(cstep) if warm else None
                 if guess is not None:
                     d.pressureResult.copy_(guess)
+                    prev = self._pressure_prev.get(cstep) if self.extrapolate_guesses else None
+                    if prev is not None and prev.shape == d.pressureResult.shape:
+                        d.pressureResult.mul_(2.0).sub_(prev)
                 else:
                     d.pressureResult.zero_()
                 self.solve("P", d.pressureRHSdiv, d.pressureResult, use_BiCG=self.pressure_use_BiCG,
@@ -407,11 +416,17 @@ class Simulation:
                                return_best=self.pressure_return_best_result)
                     if self.normalize_pressure_result:
                         d._subtract_mean(d.pressureResult, 1)
-                if self.pressure_warm_start:
+                if warm:
                     g = self._pressure_guess.get(cstep)
                     if g is None:
                         self._pressure_guess[cstep] = d.pressureResult.clone()
                     else:
+                        if self.extrapolate_guesses:
+                            prev = self._pressure_prev.get(cstep)
+                            if prev is None:
+                                self._pressure_prev[cstep] = g.clone()
+                            else:
+                                prev.copy_(g)
                         g.copy_(d.pressureResult)
                 self._run_hooks(Hook.POST_PRESSURE_RESULT, local_step=step, time_step=ts)
                 backend.CopyPressureResultToBlocks(d)
