@@ -7,9 +7,10 @@ and an open-potential outflow. Fields are float64; every solve runs float32 Kryl
 iterations inside float64 iterative refinement to a relative residual of 1e-10.
 Synthetic inputs (seeded), no dataset. A step is one PISO step (momentum predictor,
 2 pressure correctors) plus the potential step and the Lorentz force. The pressure and
-potential solves start from guesses extrapolated from the last two steps
-(``extrapolate_guesses``; ``--no-extrapolate`` for phiPICT's zero pressure guess and previous
-potential); the plain FP64 comparison leg keeps phiPICT's defaults.
+potential solves start from a degree-4 polynomial extrapolation of their last five results
+(``extrapolate_guesses``; ``--extrapolate-order`` another degree or ``adaptive``;
+``--no-extrapolate`` for phiPICT's zero pressure guess and previous potential); the plain
+FP64 comparison leg keeps phiPICT's defaults.
 
 ``--impl reference`` times the CPU oracle (the restatement of phiPICT's step; phiPICT has no
 CPU path) on the same workload with all host threads, on rank 0.
@@ -242,8 +243,19 @@ def barrier(world: int):
         dist.barrier()
 
 
+def extrapolate_order(v: str):
+    return "adaptive" if v == "adaptive" else int(v)
+
+
+def guess_label(order) -> str:
+    if order == "adaptive":
+        return ("extrapolated from the last results, the degree (<= 4) that predicted the previous "
+                "result best")
+    return f"degree-{order} polynomial extrapolation from the last {order + 1} results"
+
+
 def build_sim(wl: dict, device, mixed: bool, amg: bool = True, warm: bool = False, autotune: bool = False,
-              extrapolate: bool = False):
+              extrapolate: int | str = 0):
     import phipict_b200 as pb
 
     dtype = torch.float64
@@ -273,7 +285,8 @@ def run_ours(args, rank, world, local):
     device = torch.device("cuda", local)
     mixed = not args.plain_fp64
     amg = mixed and not args.no_amg
-    dom, sim = build_sim(wl, device, mixed, amg, args.pressure_warm_start, args.autotune, args.extrapolate and mixed)
+    dom, sim = build_sim(wl, device, mixed, amg, args.pressure_warm_start, args.autotune,
+                         args.extrapolate_order if args.extrapolate and mixed else 0)
     if args.inner_rtol:
         sim.refinement_inner_rtol = args.inner_rtol
     cells = dom.getTotalSize()
@@ -327,7 +340,7 @@ def run_ours(args, rank, world, local):
     # p and phi back there; the next step starts from the velocity it wrote
     d = dom.getSpatialDims()
     dom_e, sim_e = build_sim(wl, device, mixed, amg, args.pressure_warm_start, args.autotune,
-                             args.extrapolate and mixed)
+                             args.extrapolate_order if args.extrapolate and mixed else 0)
     if args.inner_rtol:
         sim_e.refinement_inner_rtol = args.inner_rtol
     for _ in range(tuned_warmup(args, sim_e)):
@@ -389,7 +402,7 @@ def run_ours(args, rank, world, local):
                             f"rtol 1e-10, {'mixed precision' if mixed else 'plain fp64'}"
                             f"{', multigrid-preconditioned pressure and potential CG' if amg else ''}",
                 "amg_levels": levels,
-                "initial_guesses": ("extrapolated from the last two steps" if args.extrapolate and mixed else
+                "initial_guesses": (guess_label(args.extrapolate_order) if args.extrapolate and mixed else
                                     "previous step's pressure" if args.pressure_warm_start else
                                     "zero pressure, previous step's potential"),
                 "cells_per_gpu": cells, "l2": "working set ~60 MB f32 fits L2; HBM claims on the roofline sweep",
@@ -984,9 +997,12 @@ def main():
     ap.add_argument("--inner-rtol", type=float, default=None, help="inner FP32 reduction per refinement sweep")
     ap.add_argument("--no-alone", action="store_true", help="batch64: skip the one-at-a-time comparison")
     ap.add_argument("--no-batch64", action="store_true", help="duct3d: skip the batched-instances sub-record")
+    ap.add_argument("--extrapolate-order", type=extrapolate_order, default=4,
+                    help="duct3d: degree m of the polynomial extrapolation of the pressure and potential "
+                         "guesses from the last m+1 results, or 'adaptive'")
     ap.add_argument("--no-extrapolate", dest="extrapolate", action="store_false",
                     help="duct3d: zero pressure guesses and the previous potential (phiPICT's defaults) instead of "
-                         "guesses extrapolated from the last two steps")
+                         "guesses extrapolated from the last steps")
     ap.add_argument("--autotune", action="store_true",
                     help="tune the persistent Krylov kernels' CTAs per SM per solve during the warm-up")
     ap.add_argument("--requests", type=int, default=None, help="serve: number of requests")

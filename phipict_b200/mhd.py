@@ -16,7 +16,7 @@ import torch
 from . import _C as backend
 from .domain import Domain
 from .hooks import Hook, Hooks
-from .simulation import Simulation
+from .simulation import GuessExtrapolator, Simulation
 from .solvers import LinearSolverResultInfo
 from .tolerance import SolverTolerance, coerce_tolerance
 
@@ -180,17 +180,20 @@ class MHDSimulation(Simulation):
         if not self._potential_reuse_result:
             domain.epotResult.zero_()
         else:
+            ex = None
             if self.extrapolate_guesses:
-                prev = getattr(self, "_epot_prev", None)
-                cur = domain.epotResult.clone()
-                if prev is not None and prev.shape == cur.shape:
-                    domain.epotResult.mul_(2.0).sub_(prev)
-                self._epot_prev = cur
+                ex = self.__dict__.get("_epot_extrap")
+                if ex is None:
+                    ex = self._epot_extrap = GuessExtrapolator(self.extrapolate_guesses, self._extrapolate_adaptive)
+                    ex.update(domain.epotResult)  # the current potential is the first result
+                ex.guess(domain.epotResult)
             if self._potential_rank_deficient:
                 domain._subtract_mean(domain.epotResult, 1)
         self.solve("E", domain.epotRHS, domain.epotResult, use_BiCG=self._potential_use_BiCG, tol=self.potential_tol,
                    tag="epot", return_best=self._potential_return_best_result,
                    max_iter=self._potential_solve_max_iter if max_iter is None else max_iter)
+        if self._potential_reuse_result and self.extrapolate_guesses:
+            self._epot_extrap.update(domain.epotResult)
         if self._potential_normalize and self._potential_rank_deficient:
             domain._subtract_mean(domain.epotResult, 1)
         backend.CopyEpotResultToBlocks(domain)

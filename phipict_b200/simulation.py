@@ -17,8 +17,13 @@ Extensions (keyword arguments phiPICT does not have):
   ``check_solves``: read the solver outcomes at the end of every step (default True).
       With False the step never synchronises; failures surface through
       :meth:`solve_report`.
+  ``autotune_solvers``: measure and pick the CTAs per SM of each solve (SolverTuner).
+  ``extrapolate_guesses``: start the pressure and potential solves from a polynomial
+      extrapolation of their last results: an order m >= 1 (True: 1), or "adaptive".
 """
 from __future__ import annotations
+
+import math
 
 from typing import Any, Literal
 
@@ -32,6 +37,92 @@ from .solvers import BICGSTAB, CG, LinearSolverResultInfo, LinsolveError, Solver
 from .tolerance import SolverTolerance, coerce_tolerance
 
 _UNSUPPORTED_TRUE = ("scipy_solve_advection", "scipy_solve_pressure", "differentiable_unsupported")
+
+
+def extrapolate_into(x: torch.Tensor, hist: list, order: int) -> None:
+    """x holds the last result x_n; hist the ones before it (x_(n-1), x_(n-2), ..., newest
+    first). Overwrite x with the polynomial extrapolation of the highest order m <= `order`
+    that the history allows: sum over k = 0..m of (-1)^k binom(m+1, k+1) x_(n-k) (m = 1:
+    2 x_n - x_(n-1); m = 2: 3 x_n - 3 x_(n-1) + x_(n-2))."""
+    hist = [h for h in hist if h.shape == x.shape]
+    m = min(order, len(hist))
+    if m < 1:
+        return
+    x.mul_(float(math.comb(m + 1, 1)))
+    for k in range(1, m + 1):
+        x.add_(hist[k - 1], alpha=float((-1) ** k * math.comb(m + 1, k + 1)))
+
+
+def push_history(hist: list, x: torch.Tensor, order: int) -> None:
+    """Prepend a copy of x (the result before the newest), keeping `order` entries."""
+    if len(hist) < order:
+        hist.insert(0, x.clone())
+        return
+    buf = hist.pop()
+    buf.copy_(x)
+    hist.insert(0, buf)
+
+
+class GuessExtrapolator:
+    """Initial guesses of one recurring solve (the pressure of one corrector, the potential)
+    from its results of the last steps. Fixed order m: the polynomial extrapolation of degree
+    m (extrapolate_into). Adaptive: after each solve, the extrapolations of every degree up to
+    `max_order` are compared with the new result on the device, and the next solve uses the
+    degree that predicted it best (the error norms come back through pinned memory after an
+    event and are read at the next guess, so the choice adds no wait on the GPU)."""
+
+    def __init__(self, max_order: int, adaptive: bool):
+        self.max_order = int(max_order)
+        self.adaptive = bool(adaptive)
+        self.order = 1 if adaptive else self.max_order
+        self.hist: list[torch.Tensor] = []
+        self.last: torch.Tensor | None = None
+        self._errs = None  # (host norms, event or None) of the last comparison
+
+    def guess(self, x: torch.Tensor) -> bool:
+        """Write the guess into x; False when there is no previous result yet."""
+        if self.last is None or self.last.shape != x.shape:
+            return False
+        if self._errs is not None:
+            host, ev = self._errs
+            if ev is not None:
+                ev.synchronize()
+            self.order = int(torch.argmin(host).item())
+            self._errs = None
+        x.copy_(self.last)
+        extrapolate_into(x, self.hist, self.order)
+        return True
+
+    def _compare(self, result: torch.Tensor) -> None:
+        # guesses of every degree from the backward differences of (last, hist...):
+        # degree m = sum over j <= m of the j-th backward difference at the last result
+        vals = [self.last] + [h for h in self.hist if h.shape == result.shape][: self.max_order]
+        g = torch.empty((len(vals),) + tuple(result.shape), dtype=result.dtype, device=result.device)
+        g[0].copy_(self.last)
+        row = vals
+        for m in range(1, len(vals)):
+            row = [row[i] - row[i + 1] for i in range(len(row) - 1)]
+            torch.add(g[m - 1], row[0], out=g[m])
+        errs = torch.linalg.vector_norm((g - result).reshape(len(vals), -1), dim=1)
+        if result.is_cuda:
+            host = torch.empty(errs.shape, dtype=errs.dtype, pin_memory=True)
+            host.copy_(errs, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record()
+            self._errs = (host, ev)
+        else:
+            self._errs = (errs, None)
+
+    def update(self, result: torch.Tensor) -> None:
+        """Record the result of the solve."""
+        if self.last is not None and self.last.shape == result.shape:
+            if self.adaptive:
+                self._compare(result)
+            push_history(self.hist, self.last, self.max_order)
+            self.last.copy_(result)
+        else:
+            self.hist.clear()
+            self.last = result.clone()
 
 
 class Simulation:
@@ -84,7 +175,7 @@ class Simulation:
         mixed_precision: bool = False,
         check_solves: bool = True,
         autotune_solvers: bool = False,
-        extrapolate_guesses: bool = False,
+        extrapolate_guesses: bool | int | str = False,
     ) -> None:
         if hooks is not None and prep_fn is not None:
             raise ValueError("Pass hooks or its former name prep_fn, not both.")
@@ -129,10 +220,13 @@ class Simulation:
         self.refinement_inner_rtol = 1e-4
         # grid of the persistent Krylov kernels tuned per solve by measurement (SolverTuner)
         self.solver_tuner = SolverTuner() if autotune_solvers else None
-        # initial guesses of the pressure (per corrector) and potential solves extrapolated
-        # linearly from the last two steps' results, 2 x_n - x_(n-1) (implies the warm start)
-        self.extrapolate_guesses = bool(extrapolate_guesses)
-        self._pressure_prev: dict[int, torch.Tensor] = {}
+        # initial guesses of the pressure (per corrector) and potential solves extrapolated from
+        # the last steps' results (GuessExtrapolator): an order m >= 1 (True: 1), or "adaptive"
+        # (the degree up to 4 that predicted the last result best)
+        adaptive = extrapolate_guesses == "adaptive"
+        self.extrapolate_guesses = 4 if adaptive else int(extrapolate_guesses)
+        self._extrapolate_adaptive = adaptive
+        self._pressure_extrap: dict[int, GuessExtrapolator] = {}
         self.check_solves = check_solves
         self.total_step = 0
         self.total_time = 0.0
@@ -390,13 +484,16 @@ class Simulation:
                 if rec is not None:
                     rec.hbya(d.pressureRHS)
                 self._run_hooks(Hook.POST_PRESSURE_SETUP, local_step=step, time_step=ts)
-                warm = self.pressure_warm_start or self.extrapolate_guesses
-                guess = self._pressure_guess.get(cstep) if warm else None
-                if guess is not None:
+                ex = None
+                if self.extrapolate_guesses:
+                    ex = self._pressure_extrap.setdefault(
+                        cstep, GuessExtrapolator(self.extrapolate_guesses, self._extrapolate_adaptive))
+                guess = self._pressure_guess.get(cstep) if self.pressure_warm_start else None
+                if ex is not None:
+                    if not ex.guess(d.pressureResult):
+                        d.pressureResult.zero_()
+                elif guess is not None:
                     d.pressureResult.copy_(guess)
-                    prev = self._pressure_prev.get(cstep) if self.extrapolate_guesses else None
-                    if prev is not None and prev.shape == d.pressureResult.shape:
-                        d.pressureResult.mul_(2.0).sub_(prev)
                 else:
                     d.pressureResult.zero_()
                 self.solve("P", d.pressureRHSdiv, d.pressureResult, use_BiCG=self.pressure_use_BiCG,
@@ -416,17 +513,13 @@ class Simulation:
                                return_best=self.pressure_return_best_result)
                     if self.normalize_pressure_result:
                         d._subtract_mean(d.pressureResult, 1)
-                if warm:
+                if ex is not None:
+                    ex.update(d.pressureResult)
+                if self.pressure_warm_start:
                     g = self._pressure_guess.get(cstep)
                     if g is None:
                         self._pressure_guess[cstep] = d.pressureResult.clone()
                     else:
-                        if self.extrapolate_guesses:
-                            prev = self._pressure_prev.get(cstep)
-                            if prev is None:
-                                self._pressure_prev[cstep] = g.clone()
-                            else:
-                                prev.copy_(g)
                         g.copy_(d.pressureResult)
                 self._run_hooks(Hook.POST_PRESSURE_RESULT, local_step=step, time_step=ts)
                 backend.CopyPressureResultToBlocks(d)
