@@ -7,8 +7,9 @@ and an open-potential outflow. Fields are float64; every solve runs float32 Kryl
 iterations inside float64 iterative refinement to a relative residual of 1e-10.
 Synthetic inputs (seeded), no dataset. A step is one PISO step (momentum predictor,
 2 pressure correctors) plus the potential step and the Lorentz force. The pressure and
-potential solves start from a degree-4 polynomial extrapolation of their last five results
-(``extrapolate_guesses``; ``--extrapolate-order`` another degree or ``adaptive``;
+potential solves start from a polynomial extrapolation of their last results, of the degree
+(at most 4) that predicted each solve's previous result best (``extrapolate_guesses``;
+``--extrapolate-order`` for a fixed degree;
 ``--no-extrapolate`` for phiPICT's zero pressure guess and previous potential); the plain
 FP64 comparison leg keeps phiPICT's defaults.
 
@@ -997,7 +998,7 @@ def main():
     ap.add_argument("--inner-rtol", type=float, default=None, help="inner FP32 reduction per refinement sweep")
     ap.add_argument("--no-alone", action="store_true", help="batch64: skip the one-at-a-time comparison")
     ap.add_argument("--no-batch64", action="store_true", help="duct3d: skip the batched-instances sub-record")
-    ap.add_argument("--extrapolate-order", type=extrapolate_order, default=4,
+    ap.add_argument("--extrapolate-order", type=extrapolate_order, default="adaptive",
                     help="duct3d: degree m of the polynomial extrapolation of the pressure and potential "
                          "guesses from the last m+1 results, or 'adaptive'")
     ap.add_argument("--no-extrapolate", dest="extrapolate", action="store_false",

@@ -53,10 +53,16 @@ def extrapolate_into(x: torch.Tensor, hist: list, order: int) -> None:
         x.add_(hist[k - 1], alpha=float((-1) ** k * math.comb(m + 1, k + 1)))
 
 
-def push_history(hist: list, x: torch.Tensor, order: int) -> None:
-    """Prepend a copy of x (the result before the newest), keeping `order` entries."""
+def push_history(hist: list, x: torch.Tensor, order: int, spare: list | None = None) -> None:
+    """Prepend a copy of x (the result before the newest), keeping `order` entries; new
+    entries come from `spare` (buffers allocated up front) while it has any."""
     if len(hist) < order:
-        hist.insert(0, x.clone())
+        if spare:
+            buf = spare.pop()
+            buf.copy_(x)
+            hist.insert(0, buf)
+        else:
+            hist.insert(0, x.clone())
         return
     buf = hist.pop()
     buf.copy_(x)
@@ -77,6 +83,7 @@ class GuessExtrapolator:
         self.order = 1 if adaptive else self.max_order
         self.hist: list[torch.Tensor] = []
         self.last: torch.Tensor | None = None
+        self._spare: list[torch.Tensor] = []  # history buffers not in use yet
         self._errs = None  # (host norms, event or None) of the last comparison
 
     def guess(self, x: torch.Tensor) -> bool:
@@ -118,11 +125,13 @@ class GuessExtrapolator:
         if self.last is not None and self.last.shape == result.shape:
             if self.adaptive:
                 self._compare(result)
-            push_history(self.hist, self.last, self.max_order)
+            push_history(self.hist, self.last, self.max_order, self._spare)
             self.last.copy_(result)
         else:
+            # every buffer is allocated with the first result, none in later steps
             self.hist.clear()
             self.last = result.clone()
+            self._spare = [torch.empty_like(result) for _ in range(self.max_order)]
 
 
 class Simulation:

@@ -79,12 +79,3 @@ def test_linear_upwind_steps_match_the_oracle(cuda, case):
     torch.cuda.synchronize()
     assert rel(host(dom._u_block).reshape(-1), ref.u) < 1e-9
     assert rel(host(dom._phi_block).reshape(-1), ref.phi_s.reshape(-1)) < 1e-9
-
-
-def test_adjoint_refuses_linear_upwind(cuda):
-    from phipict_b200.adjoint import AdjointMHD
-
-    dom, _ = _setup("duct3d")
-    with pytest.raises(NotImplementedError):
-        AdjointMHD(dom, 0.01, torch.tensor([1.0]), torch.tensor([0.0, 1.0, 0.0], dtype=torch.float64), steps=1,
-                   faces=[(dom.getBlocks()[0], "-x")])
