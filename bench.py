@@ -245,10 +245,13 @@ def barrier(world: int):
 
 
 def extrapolate_order(v: str):
-    return "adaptive" if v == "adaptive" else int(v)
+    return v if v == "adaptive" or v.startswith("projection") else int(v)
 
 
 def guess_label(order) -> str:
+    if isinstance(order, str) and order.startswith("projection"):
+        n = int(order.split(":", 1)[1]) if ":" in order else 8
+        return f"Galerkin projection onto the span of the last {n} results"
     if order == "adaptive":
         return ("extrapolated from the last results, the degree (<= 4) that predicted the previous "
                 "result best")
@@ -1000,7 +1003,8 @@ def main():
     ap.add_argument("--no-batch64", action="store_true", help="duct3d: skip the batched-instances sub-record")
     ap.add_argument("--extrapolate-order", type=extrapolate_order, default="adaptive",
                     help="duct3d: degree m of the polynomial extrapolation of the pressure and potential "
-                         "guesses from the last m+1 results, or 'adaptive'")
+                         "guesses from the last m+1 results, 'adaptive', or 'projection[:L]' (Galerkin "
+                         "projection onto the last L results)")
     ap.add_argument("--no-extrapolate", dest="extrapolate", action="store_false",
                     help="duct3d: zero pressure guesses and the previous potential (phiPICT's defaults) instead of "
                          "guesses extrapolated from the last steps")

@@ -306,6 +306,19 @@ int phb_solve_results(const phb_domain *dom, const phb_solve *s, phb_solve_resul
 /* drops cached solver graphs (ReleaseKrylovWorkspaces, bindings.cpp:775) */
 int phb_release_graphs(void);
 
+/* Projected initial guesses (no phiPICT counterpart: phiPICT starts the pressure from zero
+ * or its warm start and the potential from its previous result,
+ * core/piso_simulation.py:2135 _pressure_initial_guess, simulation/mhd.py:801
+ * _epot_initial_guess). phb_stencil_apply: Y[v] = A X[v] for nvec float64 vectors of
+ * ncells values, stride >= ncells values apart (a multiple of 4; A, X and Y 32-byte aligned),
+ * A a float64 stencil matrix of the domain.
+ * phb_projection_solve: alpha = G^-1 c for the m x m (m <= 16, row-major) Gram matrix of a
+ * guess basis, Jacobi-scaled with the diagonal raised by reg; rows whose pivot vanishes, or
+ * all rows when the result is not finite, get coefficient 0. Both are stream-ordered. */
+int phb_stencil_apply(const phb_domain *dom, const double *A, const double *X, double *Y, int32_t nvec, int64_t stride,
+                      phb_stream stream);
+int phb_projection_solve(const double *G, const double *c, int32_t m, double reg, double *alpha, phb_stream stream);
+
 /* Mixed precision: FP64 outer iterative refinement around FP32 inner Krylov solves.
  * A64/A32: the system in float64 and its float32 copy; b/x float64. The outer loop stops
  * when ||b - A64 x||/sqrt(n) < tol for every system or after max_outer sweeps; inner

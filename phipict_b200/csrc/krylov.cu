@@ -1757,6 +1757,81 @@ static int emitSolve(const phb_domain *dom, const phb_solve *sv, cudaStream_t s,
 	return rc;
 }
 
+// Y[v] = A X[v], v < nvec, for float64 vectors of one component (stride values apart): the
+// products of the basis of a projected initial guess with the system matrix. The centre and
+// face terms are summed in the order of the solvers' own products.
+template <int D>
+__global__ void __launch_bounds__(PHB_TILE) kStencilApply(Dom<double, D> dom, const double *__restrict__ A,
+		const double *__restrict__ X, double *__restrict__ Y, int nvec, int64_t stride) {
+	__shared__ int32_t sB[PHB_BREC];
+	int l0_, nc_;
+	loadTile<double, D>(dom, sB, l0_, nc_);
+	Quad q;
+	quadAt<D, 1>(dom.vec4, sB, l0_, nc_, q);
+	bool act[1] = {true};
+	for (int v = 0; v < nvec; ++v) {
+		FX<double> fx[1];
+		fx[0].x = X + v * stride;
+		double y[1][4], f[1][4];
+		quadApply<double, D, 1>(dom, A, q, act, fx, y, f);
+		st4(Y + v * stride + vk<1>(q.B, q.g, 0), q.n, q.al, y[0]);
+	}
+}
+
+// The coefficients of a Galerkin projection, one CTA: G (m x m, row-major, the Gram matrix
+// D A D^T of the basis rows) alpha = c. Jacobi-scaled (s_i = |G_ii|^-1/2), the diagonal
+// raised by reg relative to the scaled unit diagonal, Gaussian elimination with partial
+// pivoting; a basis row whose pivot falls below 1e-14 of the largest gets coefficient 0, and
+// so does every row when a value is not finite (the guess is then the zero vector's
+// projection: alpha = 0).
+constexpr int PROJ_MAX = 16;
+__global__ void kProjectionSolve(const double *__restrict__ G, const double *__restrict__ c, int m, double reg,
+		double *__restrict__ alpha) {
+	__shared__ double M[PROJ_MAX][PROJ_MAX + 1];
+	__shared__ double sc[PROJ_MAX];
+	const int t = threadIdx.x;
+	if (t < m) {
+		const double d = fabs(G[t * m + t]);
+		sc[t] = d > 0 && isfinite(d) ? rsqrt(d) : 0.0;
+	}
+	__syncthreads();
+	for (int e = t; e < m * (m + 1); e += blockDim.x) {
+		const int i = e / (m + 1), j = e - i * (m + 1);
+		double v = j < m ? G[i * m + j] * sc[i] * sc[j] : c[i] * sc[i];
+		if (j == i) v += (G[i * m + i] < 0 ? -reg : reg);
+		M[i][j] = v;
+	}
+	__syncthreads();
+	if (t == 0) {
+		bool ok = true;
+		double big = 0;
+		for (int i = 0; i < m; ++i) big = fmax(big, fabs(M[i][i]));
+		bool skip[PROJ_MAX];
+		for (int i = 0; i < m; ++i) skip[i] = false;
+		for (int k = 0; k < m && ok; ++k) {
+			int p = k;
+			for (int i = k + 1; i < m; ++i) if (fabs(M[i][k]) > fabs(M[p][k])) p = i;
+			if (p != k) {
+				for (int j = 0; j <= m; ++j) { const double tmp = M[k][j]; M[k][j] = M[p][j]; M[p][j] = tmp; }
+			}
+			if (!(fabs(M[k][k]) > 1e-14 * big)) { skip[k] = true; continue; }
+			for (int i = k + 1; i < m; ++i) {
+				const double f = M[i][k] / M[k][k];
+				for (int j = k; j <= m; ++j) M[i][j] -= f * M[k][j];
+			}
+		}
+		double x[PROJ_MAX];
+		for (int k = m - 1; k >= 0; --k) {
+			if (skip[k]) { x[k] = 0; continue; }
+			double v = M[k][m];
+			for (int j = k + 1; j < m; ++j) v -= M[k][j] * x[j];
+			x[k] = v / M[k][k];
+			if (!isfinite(x[k])) ok = false;
+		}
+		for (int i = 0; i < m; ++i) alpha[i] = ok ? x[i] * sc[i] : 0.0;
+	}
+}
+
 #define PHB_SOLVE_DISPATCH(DIMS, VEC, K, ...)                                                   \
 	do {                                                                                        \
 		if ((DIMS) == 2 && (VEC) == PHB_F64 && (K) == 1) { using T = double; constexpr int D = 2, KK = 1; __VA_ARGS__; } \
@@ -1855,6 +1930,30 @@ extern "C" int phb_solve_results(const phb_domain *dom, const phb_solve *s, phb_
 		}
 	}
 	return PHB_OK;
+}
+
+extern "C" int phb_stencil_apply(const phb_domain *dom, const double *A, const double *X, double *Y, int32_t nvec,
+		int64_t stride, phb_stream stream) {
+	if (!dom || !A || !X || !Y) return setError(PHB_ERR_ARG, "phb_stencil_apply: null argument");
+	// the quad loads of a row take 16-byte vector loads at cells that are multiples of four
+	if (nvec < 1 || stride < dom->ncells || (stride & 3) != 0)
+		return setError(PHB_ERR_ARG, "phb_stencil_apply: nvec < 1, stride < ncells or stride not a multiple of 4");
+	if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(Y)) & 31)
+		return setError(PHB_ERR_ARG, "phb_stencil_apply: A, X and Y must be 32-byte aligned");
+	if (dom->dims != 2 && dom->dims != 3) return setError(PHB_ERR_ARG, "phb_stencil_apply: dims");
+	if (dom->ntiles == 0) return PHB_OK;
+	cudaStream_t s = (cudaStream_t)stream;
+	if (dom->dims == 2) kStencilApply<2><<<dom->ntiles, PHB_TILE, 0, s>>>(Dom<double, 2>(*dom), A, X, Y, nvec, stride);
+	else kStencilApply<3><<<dom->ntiles, PHB_TILE, 0, s>>>(Dom<double, 3>(*dom), A, X, Y, nvec, stride);
+	return checkLaunch("kStencilApply");
+}
+
+extern "C" int phb_projection_solve(const double *G, const double *c, int32_t m, double reg, double *alpha,
+		phb_stream stream) {
+	if (!G || !c || !alpha) return setError(PHB_ERR_ARG, "phb_projection_solve: null argument");
+	if (m < 1 || m > PROJ_MAX) return setError(PHB_ERR_RANGE, "phb_projection_solve: m outside 1..16");
+	kProjectionSolve<<<1, 256, 0, (cudaStream_t)stream>>>(G, c, m, reg, alpha);
+	return checkLaunch("kProjectionSolve");
 }
 
 extern "C" int phb_release_graphs(void) {

@@ -16,7 +16,7 @@ import torch
 from . import _C as backend
 from .domain import Domain
 from .hooks import Hook, Hooks
-from .simulation import GuessExtrapolator, Simulation
+from .simulation import Simulation
 from .solvers import LinearSolverResultInfo
 from .tolerance import SolverTolerance, coerce_tolerance
 
@@ -184,9 +184,9 @@ class MHDSimulation(Simulation):
             if self.extrapolate_guesses:
                 ex = self.__dict__.get("_epot_extrap")
                 if ex is None:
-                    ex = self._epot_extrap = GuessExtrapolator(self.extrapolate_guesses, self._extrapolate_adaptive)
+                    ex = self._epot_extrap = self._new_guess()
                     ex.update(domain.epotResult)  # the current potential is the first result
-                ex.guess(domain.epotResult)
+                ex.guess(domain.epotResult, domain._stencil("E"), domain.epotRHS, domain)
             if self._potential_rank_deficient:
                 domain._subtract_mean(domain.epotResult, 1)
         self.solve("E", domain.epotRHS, domain.epotResult, use_BiCG=self._potential_use_BiCG, tol=self.potential_tol,

@@ -86,8 +86,9 @@ class GuessExtrapolator:
         self._spare: list[torch.Tensor] = []  # history buffers not in use yet
         self._errs = None  # (host norms, event or None) of the last comparison
 
-    def guess(self, x: torch.Tensor) -> bool:
-        """Write the guess into x; False when there is no previous result yet."""
+    def guess(self, x: torch.Tensor, A=None, b=None, domain=None) -> bool:
+        """Write the guess into x (the system's A and b are not needed); False when there is
+        no previous result yet."""
         if self.last is None or self.last.shape != x.shape:
             return False
         if self._errs is not None:
@@ -132,6 +133,80 @@ class GuessExtrapolator:
             self.hist.clear()
             self.last = result.clone()
             self._spare = [torch.empty_like(result) for _ in range(self.max_order)]
+
+
+class ProjectedGuess:
+    """Initial guesses of one recurring solve as the Galerkin projection of its solution onto
+    the span of its last `size` results (P. F. Fischer, "Projection techniques for iterative
+    solution of Ax = b with successive right-hand sides", Comput. Methods Appl. Mech. Engrg.
+    163, 1998): x0 = V alpha with (V^T A V) alpha = V^T b, for a symmetric definite A the
+    A-norm-best guess in that span, so never worse in that norm than a polynomial
+    extrapolation of the same results. The basis rows are the backward differences of the
+    results (x_n, x_n - x_(n-1), ...: the same span, far better conditioned than the results
+    themselves) in one float64 (size, cells) buffer; A V is taken with the current matrix
+    (phb_stencil_apply) and the size x size system solved on the device
+    (phb_projection_solve), so a guess adds no host synchronisation. `apply` and `solve`
+    replace those two calls (A, V, Y, m) -> Y[:m] = A V[:m] and (G, c) -> alpha."""
+
+    REG = 1e-13
+
+    def __init__(self, size: int, apply=None, solve=None):
+        if not 1 <= int(size) <= 16:
+            raise ValueError("a projected guess takes 1 to 16 basis vectors")
+        self.size = int(size)
+        self.n = 0
+        self.D: torch.Tensor | None = None
+        self._Dn = self._Y = self._alpha = None
+        self._apply, self._solve = apply, solve
+
+    def guess(self, x: torch.Tensor, A=None, b=None, domain=None) -> bool:
+        """Write the guess into x for the system A x = b; False before the first result."""
+        if self.n == 0 or self.D.shape[1] != x.numel():
+            return False
+        m = self.n
+        V, Y = self.D[:m], self._Y[:m]
+        if self._apply is not None:
+            self._apply(A, V, Y, m)
+        else:
+            import ctypes as ct
+
+            from . import _lib
+
+            if A.dtype != torch.float64:
+                raise ValueError("projected guesses need a float64 matrix")
+            _lib.call("phb_stencil_apply", ct.byref(domain.desc()), A.data_ptr(), V.data_ptr(), Y.data_ptr(), m,
+                      V.stride(0), _lib.stream_ptr(x.device))
+        G = torch.mm(V, Y.t())
+        c = torch.mv(V, b.reshape(-1))
+        if self._solve is not None:
+            alpha = self._solve(G, c)
+        else:
+            from . import _lib
+
+            alpha = self._alpha[:m]
+            _lib.call("phb_projection_solve", G.data_ptr(), c.data_ptr(), m, self.REG, alpha.data_ptr(),
+                      _lib.stream_ptr(x.device))
+        torch.mv(V.t(), alpha, out=x.view(-1))
+        return True
+
+    def update(self, result: torch.Tensor) -> None:
+        """Record the result of the solve: the new rows are D'_0 = x and
+        D'_j = x - (D_0 + ... + D_(j-1)), the oldest row dropped when the basis is full."""
+        v = result.reshape(-1)
+        if self.D is None or self.D.shape[1] != v.numel():
+            # rows a multiple of four values apart (the stencil product's vector loads)
+            n, stride = v.numel(), (v.numel() + 3) // 4 * 4
+            self.D, self._Dn, self._Y = (torch.empty(self.size, stride, dtype=torch.float64, device=v.device)[:, :n]
+                                         for _ in range(3))
+            self._alpha = torch.empty(self.size, dtype=torch.float64, device=v.device)
+            self.n = 0
+        k = min(self.n + 1, self.size)
+        if k > 1:
+            torch.cumsum(self.D[: k - 1], 0, out=self._Y[: k - 1])
+            torch.sub(v.unsqueeze(0), self._Y[: k - 1], out=self._Dn[1:k])
+        self._Dn[0].copy_(v)
+        self.D, self._Dn = self._Dn, self.D
+        self.n = k
 
 
 class Simulation:
@@ -232,10 +307,18 @@ class Simulation:
         # initial guesses of the pressure (per corrector) and potential solves extrapolated from
         # the last steps' results (GuessExtrapolator): an order m >= 1 (True: 1), or "adaptive"
         # (the degree up to 4 that predicted the last result best)
-        adaptive = extrapolate_guesses == "adaptive"
-        self.extrapolate_guesses = 4 if adaptive else int(extrapolate_guesses)
+        mode = extrapolate_guesses
+        adaptive = mode == "adaptive"
+        self._guess_projection = 0
+        if isinstance(mode, str) and mode.startswith("projection"):
+            self._guess_projection = int(mode.split(":", 1)[1]) if ":" in mode else 8
+            ProjectedGuess(self._guess_projection)  # checks the size
+            if domain.getDtype() != torch.float64:
+                raise ValueError("extrapolate_guesses='projection' needs a float64 domain")
+            mode = 1
+        self.extrapolate_guesses = 4 if adaptive else int(mode)
         self._extrapolate_adaptive = adaptive
-        self._pressure_extrap: dict[int, GuessExtrapolator] = {}
+        self._pressure_extrap: dict[int, GuessExtrapolator | ProjectedGuess] = {}
         self.check_solves = check_solves
         self.total_step = 0
         self.total_time = 0.0
@@ -285,6 +368,12 @@ class Simulation:
         if self.pressure_tol_intermediate is None or cstep == self.corrector_steps - 1:
             return self.pressure_tol
         return self.pressure_tol_intermediate
+
+    def _new_guess(self) -> GuessExtrapolator | ProjectedGuess:
+        """The initial-guess state of one recurring solve (extrapolate_guesses)."""
+        if self._guess_projection:
+            return ProjectedGuess(self._guess_projection)
+        return GuessExtrapolator(self.extrapolate_guesses, self._extrapolate_adaptive)
 
     def solve(self, which: str, rhs: torch.Tensor, x: torch.Tensor, *, use_BiCG: bool, tol, tag: str,
               nrhs: int = 1, return_best: bool = False, max_iter: int | None = None) -> None:
@@ -495,11 +584,12 @@ class Simulation:
                 self._run_hooks(Hook.POST_PRESSURE_SETUP, local_step=step, time_step=ts)
                 ex = None
                 if self.extrapolate_guesses:
-                    ex = self._pressure_extrap.setdefault(
-                        cstep, GuessExtrapolator(self.extrapolate_guesses, self._extrapolate_adaptive))
+                    ex = self._pressure_extrap.get(cstep)
+                    if ex is None:
+                        ex = self._pressure_extrap[cstep] = self._new_guess()
                 guess = self._pressure_guess.get(cstep) if self.pressure_warm_start else None
                 if ex is not None:
-                    if not ex.guess(d.pressureResult):
+                    if not ex.guess(d.pressureResult, d._stencil("P"), d.pressureRHSdiv, d):
                         d.pressureResult.zero_()
                 elif guess is not None:
                     d.pressureResult.copy_(guess)

@@ -1,7 +1,9 @@
-"""Extrapolated initial guesses (Simulation(extrapolate_guesses=True)): the pressure of every
-corrector and the potential start from 2 x_n - x_(n-1) of the last two steps. A guess changes
-only where the Krylov iteration starts, so the fields agree with the default run's to the
-solver tolerance, and the solves take fewer iterations."""
+"""Initial guesses of the pressure of every corrector and of the potential
+(Simulation(extrapolate_guesses=...)): polynomial extrapolations of the last results (a fixed
+degree, or the degree that predicted the last result best) and the Galerkin projection onto
+the span of the last results. A guess changes only where the Krylov iteration starts, so the
+fields agree with the default run's to the solver tolerance, and the solves take fewer
+iterations."""
 import pytest
 import torch
 
@@ -9,7 +11,7 @@ import phipict_b200 as pb
 from cases import duct_3d, seeded_state
 
 
-def _run(extrapolate: bool, steps: int = 8):
+def _run(extrapolate, steps: int = 8):
     dom = duct_3d(16, 12, 12, 2)
     seeded_state(dom, 31, scale=0.2)
     dom.PrepareSolve()
@@ -26,12 +28,71 @@ def _run(extrapolate: bool, steps: int = 8):
 
 
 @pytest.mark.gpu
-def test_extrapolated_guesses_keep_the_fields(cuda):
+@pytest.mark.parametrize("mode", [True, "adaptive", "projection:6"])
+def test_extrapolated_guesses_keep_the_fields(cuda, mode):
     d0, its0 = _run(False)
-    d1, its1 = _run(True)
+    d1, its1 = _run(mode)
     for a, b in ((d0._u_block, d1._u_block), (d0.pressureResult, d1.pressureResult), (d0.epotResult, d1.epotResult)):
         assert float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(a)) < 1e-8
     assert its1 < its0, (its0, its1)
+
+
+@pytest.mark.gpu
+def test_stencil_apply_matches_the_csr_product(cuda):
+    """phb_stencil_apply (the products of a projected guess's basis) against torch's CSR
+    product of the same pressure and potential matrices, on several vectors at a stride."""
+    import ctypes as ct
+
+    from phipict_b200 import _lib
+
+    dom, _ = _run(False, steps=1)
+    N = dom.getTotalSize()
+    g = torch.Generator(device="cuda").manual_seed(5)
+    X = torch.randn(3, N + 40, dtype=torch.float64, device="cuda", generator=g)
+    for which, M in (("P", dom.P), ("E", dom.Epot)):
+        Y = torch.full_like(X, float("nan"))
+        _lib.call("phb_stencil_apply", ct.byref(dom.desc()), dom._stencil(which).data_ptr(), X.data_ptr(),
+                  Y.data_ptr(), 3, X.stride(0), _lib.stream_ptr(X.device))
+        A = torch.sparse_csr_tensor(M.row.to(torch.int64), M.index.to(torch.int64), M.value, size=(N, N))
+        for v in range(3):
+            ref = torch.mv(A, X[v, :N].contiguous())
+            assert float(torch.linalg.vector_norm(Y[v, :N] - ref) / torch.linalg.vector_norm(ref)) < 1e-14, which
+        assert torch.isnan(Y[:, N:]).all()  # nothing past the cells of a row is written
+
+
+@pytest.mark.gpu
+def test_projection_solve_matches_a_dense_solve(cuda):
+    """phb_projection_solve against torch.linalg.solve on symmetric definite systems of both
+    signs, and the coefficient 0 of a row that is linearly dependent on the others."""
+    from phipict_b200 import _lib
+
+    g = torch.Generator().manual_seed(2)
+    for m in (1, 5, 16):
+        for sign in (1.0, -1.0):
+            B = torch.randn(m, m, dtype=torch.float64, generator=g)
+            G = sign * (B @ B.T + m * torch.eye(m, dtype=torch.float64))
+            c = torch.randn(m, dtype=torch.float64, generator=g)
+            Gd, cd = G.cuda(), c.cuda()
+            a = torch.empty(m, dtype=torch.float64, device="cuda")
+            _lib.call("phb_projection_solve", Gd.data_ptr(), cd.data_ptr(), m, 0.0, a.data_ptr(), _lib.stream_ptr(a.device))
+            ref = torch.linalg.solve(G, c)
+            assert float(torch.linalg.vector_norm(a.cpu() - ref) / torch.linalg.vector_norm(ref)) < 1e-10, (m, sign)
+    # a basis whose last row repeats the first: the Gram matrix is singular, the guess stays finite
+    V = torch.randn(4, 50, dtype=torch.float64, generator=g)
+    V[3] = V[0]
+    S = torch.randn(50, 50, dtype=torch.float64, generator=g)
+    A = S @ S.T + 50 * torch.eye(50, dtype=torch.float64)
+    xs = torch.randn(50, dtype=torch.float64, generator=g)
+    b = A @ xs
+    G, c = (V @ A @ V.T).contiguous().cuda(), (V @ b).cuda()
+    a = torch.empty(4, dtype=torch.float64, device="cuda")
+    _lib.call("phb_projection_solve", G.data_ptr(), c.data_ptr(), 4, 1e-13, a.data_ptr(), _lib.stream_ptr(a.device))
+    x0 = a.cpu() @ V
+    assert torch.isfinite(a).all()
+    Q, _ = torch.linalg.qr(V[:3].T)
+    best = Q @ torch.linalg.solve(Q.T @ A @ Q, Q.T @ b)
+    e = lambda y: float((y - xs) @ A @ (y - xs))  # noqa: E731
+    assert e(x0) <= e(best) * (1 + 1e-6), (e(x0), e(best))
 
 
 def test_extrapolation_reproduces_polynomials():
@@ -82,3 +143,49 @@ def test_adaptive_order_follows_the_sequence():
         ex.update(torch.tensor([1.0 + 0.01 * (-1) ** t, 0.0], dtype=torch.float64))
     ex.guess(x)
     assert ex.order == 0, ex.order
+
+
+def test_projected_guess_is_the_galerkin_projection():
+    """The projection basis (backward differences of the last results) spans the last `size`
+    results, and the guess is the A-norm-best combination of them: exact when the new
+    solution lies in their span, never worse in the A-norm than the degree-(size-1)
+    polynomial extrapolation of the same results."""
+    from phipict_b200.simulation import ProjectedGuess, extrapolate_into
+
+    g = torch.Generator().manual_seed(7)
+    n = 60
+    S = torch.randn(n, n, dtype=torch.float64, generator=g)
+    A = S @ S.T + n * torch.eye(n, dtype=torch.float64)
+
+    def apply(M, V, Y, m):
+        Y.copy_(V @ M.T)
+
+    ex = ProjectedGuess(4, apply=apply, solve=lambda G, c: torch.linalg.solve(G, c))
+    base = torch.randn(3, n, dtype=torch.float64, generator=g)
+    sols = [torch.cos(torch.tensor(0.3 * t)) * base[0] + 0.1 * t * base[1] + 0.01 * t * t * base[2]
+            for t in range(8)]
+    x = torch.zeros(n, dtype=torch.float64)
+    assert not ex.guess(x, A, A @ sols[0])
+    for t, v in enumerate(sols):
+        if t >= 3:  # three results span the three-dimensional solution space
+            assert ex.guess(x, A, A @ v)
+            assert float(torch.linalg.vector_norm(x - v) / torch.linalg.vector_norm(v)) < 1e-9, t
+        ex.update(v)
+    # the rows span the last four results
+    V = ex.D[: ex.n]
+    R = torch.stack(sols[-4:])
+    coef = torch.linalg.lstsq(V.T, R.T).solution
+    assert float(torch.linalg.vector_norm(V.T @ coef - R.T)) < 1e-10
+    # against the cubic extrapolation on a sequence outside any small span
+    ex = ProjectedGuess(4, apply=apply, solve=lambda G, c: torch.linalg.solve(G, c))
+    hist = []
+    seq = [torch.sin(torch.arange(n, dtype=torch.float64) * (0.1 + 0.02 * t)) for t in range(7)]
+    for v in seq[:6]:
+        ex.update(v)
+    b = A @ seq[6]
+    ex.guess(x, A, b)
+    p = seq[5].clone()
+    hist = [seq[4], seq[3], seq[2]]
+    extrapolate_into(p, hist, 3)
+    e = lambda y: float((y - seq[6]) @ A @ (y - seq[6]))  # noqa: E731
+    assert e(x) <= e(p) * (1 + 1e-9), (e(x), e(p))
