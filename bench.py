@@ -7,9 +7,10 @@ and an open-potential outflow. Fields are float64; every solve runs float32 Kryl
 iterations inside float64 iterative refinement to a relative residual of 1e-10.
 Synthetic inputs (seeded), no dataset. A step is one PISO step (momentum predictor,
 2 pressure correctors) plus the potential step and the Lorentz force. The pressure and
-potential solves start from a polynomial extrapolation of their last results, of the degree
-(at most 4) that predicted each solve's previous result best (``extrapolate_guesses``;
-``--extrapolate-order`` for a fixed degree;
+potential solves start from the Galerkin projection of their solution onto the span of
+their last 12 results, taken with the current matrix (``extrapolate_guesses``;
+``--extrapolate-order`` for a polynomial extrapolation of fixed degree, ``adaptive`` or
+another projection size;
 ``--no-extrapolate`` for phiPICT's zero pressure guess and previous potential); the plain
 FP64 comparison leg keeps phiPICT's defaults.
 
@@ -250,7 +251,7 @@ def extrapolate_order(v: str):
 
 def guess_label(order) -> str:
     if isinstance(order, str) and order.startswith("projection"):
-        n = int(order.split(":", 1)[1]) if ":" in order else 8
+        n = int(order.split(":", 1)[1]) if ":" in order else 12
         return f"Galerkin projection onto the span of the last {n} results"
     if order == "adaptive":
         return ("extrapolated from the last results, the degree (<= 4) that predicted the previous "
@@ -1001,7 +1002,7 @@ def main():
     ap.add_argument("--inner-rtol", type=float, default=None, help="inner FP32 reduction per refinement sweep")
     ap.add_argument("--no-alone", action="store_true", help="batch64: skip the one-at-a-time comparison")
     ap.add_argument("--no-batch64", action="store_true", help="duct3d: skip the batched-instances sub-record")
-    ap.add_argument("--extrapolate-order", type=extrapolate_order, default="adaptive",
+    ap.add_argument("--extrapolate-order", type=extrapolate_order, default="projection:12",
                     help="duct3d: degree m of the polynomial extrapolation of the pressure and potential "
                          "guesses from the last m+1 results, 'adaptive', or 'projection[:L]' (Galerkin "
                          "projection onto the last L results)")

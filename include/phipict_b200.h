@@ -317,6 +317,11 @@ int phb_release_graphs(void);
  * all rows when the result is not finite, get coefficient 0. Both are stream-ordered. */
 int phb_stencil_apply(const phb_domain *dom, const double *A, const double *X, double *Y, int32_t nvec, int64_t stride,
                       phb_stream stream);
+/* G = V Y^T (m x m, row-major) and c = V b for m <= 16 float64 rows of n values, stride
+ * values apart (V and Y alike), b contiguous: the Gram matrix and right-hand side of a
+ * projected guess, with Y = A V from phb_stencil_apply */
+int phb_projection_gram(const double *V, const double *Y, const double *b, int32_t m, int64_t n, int64_t stride,
+                        double *G, double *c, phb_stream stream);
 int phb_projection_solve(const double *G, const double *c, int32_t m, double reg, double *alpha, phb_stream stream);
 
 /* Mixed precision: FP64 outer iterative refinement around FP32 inner Krylov solves.

@@ -30,7 +30,7 @@ EXPORTS = (
     "phb_csr_row_sizes", "phb_csr_pattern", "phb_csr_gather",
     "phb_solve_work_bytes", "phb_solve_state_bytes", "phb_solve_run", "phb_solve_results",
     "phb_release_graphs", "phb_refine_work_bytes", "phb_refine_run", "phb_refine_results",
-    "phb_cg_noalloc_bytes", "phb_cg_solve_noalloc", "phb_stencil_apply", "phb_projection_solve",
+    "phb_cg_noalloc_bytes", "phb_cg_solve_noalloc", "phb_stencil_apply", "phb_projection_gram", "phb_projection_solve",
     "phb_amg_setup", "phb_amg_vcycle", "phb_amg_work_doubles",
     "phb_csr_pcg_work_bytes", "phb_csr_pcg_solve",
     "phb_transpose_stencil", "phb_adj_outer", "phb_adj_advection_matrix", "phb_adj_advection_rhs", "phb_adj_scalar_rhs",
@@ -187,6 +187,7 @@ def load() -> ct.CDLL:
         "phb_amg_setup": [ct.POINTER(PhbAmg), P],
         "phb_transpose_stencil": [DP, P, P, P],
         "phb_stencil_apply": [DP, P, P, P, ct.c_int32, I64, P],
+        "phb_projection_gram": [P, P, P, ct.c_int32, I64, I64, P, P, P],
         "phb_projection_solve": [P, P, ct.c_int32, ct.c_double, P, P],
         "phb_adj_outer": [DP, I, P, P, ct.c_double, P, P],
         "phb_adj_advection_matrix": [DP, P, P, P, P],

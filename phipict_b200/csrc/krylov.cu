@@ -1832,6 +1832,50 @@ __global__ void kProjectionSolve(const double *__restrict__ G, const double *__r
 	}
 }
 
+// G[i][j] = sum_c V[i][c] Y[j][c] and g[i] = sum_c V[i][c] b[c] (i, j < m): each CTA stages
+// chunks of GRAM_CHUNK cells of the m rows of V, the m rows of Y and b in shared memory (rows
+// padded by one value against bank conflicts), each thread accumulates (i, j) pairs over its
+// CTA's chunks and adds them atomically into G and g, which the caller zeroes.
+constexpr int GRAM_CHUNK = 128;
+__global__ void __launch_bounds__(256) kProjectionGram(const double *__restrict__ V, const double *__restrict__ Y,
+		const double *__restrict__ b, int m, int64_t n, int64_t stride, double *__restrict__ G, double *__restrict__ g) {
+	__shared__ double sv[PROJ_MAX][GRAM_CHUNK + 1];
+	__shared__ double sy[PROJ_MAX + 1][GRAM_CHUNK + 1];
+	const int npair = m * m + m;
+	constexpr int PAIRS = (PROJ_MAX * PROJ_MAX + PROJ_MAX + 255) / 256;
+	double acc[PAIRS];
+#pragma unroll
+	for (int q = 0; q < PAIRS; ++q) acc[q] = 0;
+	for (int64_t base = (int64_t)blockIdx.x * GRAM_CHUNK; base < n; base += (int64_t)gridDim.x * GRAM_CHUNK) {
+		const int64_t rest = n - base;
+		const int len = rest < GRAM_CHUNK ? (int)rest : GRAM_CHUNK;
+		for (int e = threadIdx.x; e < (2 * m + 1) * GRAM_CHUNK; e += blockDim.x) {
+			const int r = e / GRAM_CHUNK, k = e - r * GRAM_CHUNK;
+			double v = 0;
+			if (k < len) v = r < m ? V[r * stride + base + k] : (r < 2 * m ? Y[(r - m) * stride + base + k] : b[base + k]);
+			if (r < m) sv[r][k] = v;
+			else sy[r - m][k] = v;
+		}
+		__syncthreads();
+#pragma unroll
+		for (int q = 0; q < PAIRS; ++q) {
+			const int p = threadIdx.x + q * 256;
+			if (p < npair) {
+				const int i = p < m * m ? p / m : p - m * m, j = p < m * m ? p - (p / m) * m : m;
+				double a = acc[q];
+				for (int k = 0; k < len; ++k) a = fma(sv[i][k], sy[j][k], a);
+				acc[q] = a;
+			}
+		}
+		__syncthreads();
+	}
+#pragma unroll
+	for (int q = 0; q < PAIRS; ++q) {
+		const int p = threadIdx.x + q * 256;
+		if (p < npair) atomicAdd(p < m * m ? G + p : g + (p - m * m), acc[q]);
+	}
+}
+
 #define PHB_SOLVE_DISPATCH(DIMS, VEC, K, ...)                                                   \
 	do {                                                                                        \
 		if ((DIMS) == 2 && (VEC) == PHB_F64 && (K) == 1) { using T = double; constexpr int D = 2, KK = 1; __VA_ARGS__; } \
@@ -1946,6 +1990,24 @@ extern "C" int phb_stencil_apply(const phb_domain *dom, const double *A, const d
 	if (dom->dims == 2) kStencilApply<2><<<dom->ntiles, PHB_TILE, 0, s>>>(Dom<double, 2>(*dom), A, X, Y, nvec, stride);
 	else kStencilApply<3><<<dom->ntiles, PHB_TILE, 0, s>>>(Dom<double, 3>(*dom), A, X, Y, nvec, stride);
 	return checkLaunch("kStencilApply");
+}
+
+extern "C" int phb_projection_gram(const double *V, const double *Y, const double *b, int32_t m, int64_t n, int64_t stride,
+		double *G, double *c, phb_stream stream) {
+	if (!V || !Y || !b || !G || !c) return setError(PHB_ERR_ARG, "phb_projection_gram: null argument");
+	if (m < 1 || m > PROJ_MAX) return setError(PHB_ERR_RANGE, "phb_projection_gram: m outside 1..16");
+	if (n < 0 || stride < n) return setError(PHB_ERR_ARG, "phb_projection_gram: n < 0 or stride < n");
+	cudaStream_t s = (cudaStream_t)stream;
+	PHB_CUDA(cudaMemsetAsync(G, 0, sizeof(double) * m * m, s));
+	PHB_CUDA(cudaMemsetAsync(c, 0, sizeof(double) * m, s));
+	if (n == 0) return PHB_OK;
+	int dev = 0, sms = 0;
+	PHB_CUDA(cudaGetDevice(&dev));
+	PHB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+	const int64_t chunks = (n + GRAM_CHUNK - 1) / GRAM_CHUNK;
+	const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(chunks, (int64_t)sms * 4));
+	kProjectionGram<<<grid, 256, 0, s>>>(V, Y, b, m, n, stride, G, c);
+	return checkLaunch("kProjectionGram");
 }
 
 extern "C" int phb_projection_solve(const double *G, const double *c, int32_t m, double reg, double *alpha,

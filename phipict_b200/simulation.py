@@ -19,7 +19,8 @@ Extensions (keyword arguments phiPICT does not have):
       :meth:`solve_report`.
   ``autotune_solvers``: measure and pick the CTAs per SM of each solve (SolverTuner).
   ``extrapolate_guesses``: start the pressure and potential solves from a polynomial
-      extrapolation of their last results: an order m >= 1 (True: 1), or "adaptive".
+      extrapolation of their last results (a degree m >= 1, True: 1, or "adaptive") or from
+      the Galerkin projection onto the span of the last L results ("projection[:L]", 12).
 """
 from __future__ import annotations
 
@@ -144,9 +145,10 @@ class ProjectedGuess:
     extrapolation of the same results. The basis rows are the backward differences of the
     results (x_n, x_n - x_(n-1), ...: the same span, far better conditioned than the results
     themselves) in one float64 (size, cells) buffer; A V is taken with the current matrix
-    (phb_stencil_apply) and the size x size system solved on the device
-    (phb_projection_solve), so a guess adds no host synchronisation. `apply` and `solve`
-    replace those two calls (A, V, Y, m) -> Y[:m] = A V[:m] and (G, c) -> alpha."""
+    (phb_stencil_apply), G = V (A V)^T and c = V b in one pass (phb_projection_gram) and the
+    size x size system solved on the device (phb_projection_solve), so a guess adds no host
+    synchronisation. `apply` and `solve` replace those calls: (A, V, Y, m) -> Y[:m] = A V[:m]
+    and (G, c) -> alpha."""
 
     REG = 1e-13
 
@@ -176,16 +178,18 @@ class ProjectedGuess:
                 raise ValueError("projected guesses need a float64 matrix")
             _lib.call("phb_stencil_apply", ct.byref(domain.desc()), A.data_ptr(), V.data_ptr(), Y.data_ptr(), m,
                       V.stride(0), _lib.stream_ptr(x.device))
-        G = torch.mm(V, Y.t())
-        c = torch.mv(V, b.reshape(-1))
         if self._solve is not None:
-            alpha = self._solve(G, c)
+            alpha = self._solve(torch.mm(V, Y.t()), torch.mv(V, b.reshape(-1)))
         else:
             from . import _lib
 
-            alpha = self._alpha[:m]
-            _lib.call("phb_projection_solve", G.data_ptr(), c.data_ptr(), m, self.REG, alpha.data_ptr(),
-                      _lib.stream_ptr(x.device))
+            if not b.is_contiguous():
+                raise ValueError("projected guesses need a contiguous right-hand side")
+            st = _lib.stream_ptr(x.device)
+            G, c, alpha = self._gram[: m * m], self._gram[m * m: m * m + m], self._alpha[:m]
+            _lib.call("phb_projection_gram", V.data_ptr(), Y.data_ptr(), b.data_ptr(), m, V.shape[1], V.stride(0),
+                      G.data_ptr(), c.data_ptr(), st)
+            _lib.call("phb_projection_solve", G.data_ptr(), c.data_ptr(), m, self.REG, alpha.data_ptr(), st)
         torch.mv(V.t(), alpha, out=x.view(-1))
         return True
 
@@ -199,6 +203,7 @@ class ProjectedGuess:
             self.D, self._Dn, self._Y = (torch.empty(self.size, stride, dtype=torch.float64, device=v.device)[:, :n]
                                          for _ in range(3))
             self._alpha = torch.empty(self.size, dtype=torch.float64, device=v.device)
+            self._gram = torch.empty(self.size * self.size + self.size, dtype=torch.float64, device=v.device)
             self.n = 0
         k = min(self.n + 1, self.size)
         if k > 1:
@@ -304,14 +309,15 @@ class Simulation:
         self.refinement_inner_rtol = 1e-4
         # grid of the persistent Krylov kernels tuned per solve by measurement (SolverTuner)
         self.solver_tuner = SolverTuner() if autotune_solvers else None
-        # initial guesses of the pressure (per corrector) and potential solves extrapolated from
-        # the last steps' results (GuessExtrapolator): an order m >= 1 (True: 1), or "adaptive"
-        # (the degree up to 4 that predicted the last result best)
+        # initial guesses of the pressure (per corrector) and potential solves from the last
+        # steps' results: a polynomial extrapolation of degree m >= 1 (True: 1) or "adaptive"
+        # (the degree up to 4 that predicted the last result best), GuessExtrapolator; or
+        # "projection[:L]", the Galerkin projection onto the last L (12) results, ProjectedGuess
         mode = extrapolate_guesses
         adaptive = mode == "adaptive"
         self._guess_projection = 0
         if isinstance(mode, str) and mode.startswith("projection"):
-            self._guess_projection = int(mode.split(":", 1)[1]) if ":" in mode else 8
+            self._guess_projection = int(mode.split(":", 1)[1]) if ":" in mode else 12
             ProjectedGuess(self._guess_projection)  # checks the size
             if domain.getDtype() != torch.float64:
                 raise ValueError("extrapolate_guesses='projection' needs a float64 domain")

@@ -61,6 +61,26 @@ def test_stencil_apply_matches_the_csr_product(cuda):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("m,n", [(1, 1000), (12, 442368 // 7), (16, 130)])
+def test_projection_gram_matches_torch(cuda, m, n):
+    """phb_projection_gram (G = V Y^T, c = V b over padded rows) against torch's products."""
+    from phipict_b200 import _lib
+
+    g = torch.Generator(device="cuda").manual_seed(m)
+    stride = (n + 3) // 4 * 4 + 4
+    V = torch.randn(m, stride, dtype=torch.float64, device="cuda", generator=g)
+    Y = torch.randn(m, stride, dtype=torch.float64, device="cuda", generator=g)
+    b = torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
+    G = torch.full((m, m), float("nan"), dtype=torch.float64, device="cuda")
+    c = torch.full((m,), float("nan"), dtype=torch.float64, device="cuda")
+    _lib.call("phb_projection_gram", V.data_ptr(), Y.data_ptr(), b.data_ptr(), m, n, stride, G.data_ptr(), c.data_ptr(),
+              _lib.stream_ptr(V.device))
+    Gr, cr = V[:, :n] @ Y[:, :n].T, V[:, :n] @ b
+    assert float((G - Gr).abs().max()) < 1e-12 * n ** 0.5 * 10, float((G - Gr).abs().max())
+    assert float((c - cr).abs().max()) < 1e-12 * n ** 0.5 * 10
+
+
+@pytest.mark.gpu
 def test_projection_solve_matches_a_dense_solve(cuda):
     """phb_projection_solve against torch.linalg.solve on symmetric definite systems of both
     signs, and the coefficient 0 of a row that is linearly dependent on the others."""
