@@ -262,6 +262,11 @@ typedef struct phb_amg {
 int64_t phb_amg_work_doubles(const phb_amg *amg);
 /* Galerkin products of levels 1.., dense coarsest operators and their inverses. */
 int phb_amg_setup(const phb_amg *amg, phb_stream stream);
+/* Only the finest level follows a new level-0 matrix (its smoother omega / diagonal); the coarse
+ * operators and dense inverses of the last phb_amg_setup are kept (galerkin_refresh with
+ * coarse=False, solvers/amg.py:749, between the full refreshes of coarse_refresh_interval,
+ * core/piso_simulation.py:2268-2297). */
+int phb_amg_refresh_fine(const phb_amg *amg, phb_stream stream);
 /* z = one V-cycle applied to r (both [ncells] of level 0, float32). */
 int phb_amg_vcycle(const phb_amg *amg, const float *r, float *z, phb_stream stream);
 

@@ -31,7 +31,7 @@ EXPORTS = (
     "phb_solve_work_bytes", "phb_solve_state_bytes", "phb_solve_run", "phb_solve_results",
     "phb_release_graphs", "phb_refine_work_bytes", "phb_refine_run", "phb_refine_results",
     "phb_cg_noalloc_bytes", "phb_cg_solve_noalloc", "phb_stencil_apply", "phb_projection_gram", "phb_projection_solve",
-    "phb_amg_setup", "phb_amg_vcycle", "phb_amg_work_doubles",
+    "phb_amg_setup", "phb_amg_refresh_fine", "phb_amg_vcycle", "phb_amg_work_doubles",
     "phb_csr_pcg_work_bytes", "phb_csr_pcg_solve",
     "phb_transpose_stencil", "phb_adj_outer", "phb_adj_advection_matrix", "phb_adj_advection_rhs", "phb_adj_scalar_rhs",
     "phb_adj_pressure_rhs", "phb_adj_divergence", "phb_adj_correct_velocity", "phb_adj_pressure_matrix",
@@ -185,6 +185,7 @@ def load() -> ct.CDLL:
         "phb_refine_results": [DP, ct.POINTER(PhbRefine), ct.POINTER(PhbSolveResult), ct.POINTER(ct.c_int), P],
         "phb_cg_solve_noalloc": [DP, I, I, P, P, P, ct.POINTER(PhbTolerance), I, I, ct.POINTER(PhbSolveResult), P],
         "phb_amg_setup": [ct.POINTER(PhbAmg), P],
+        "phb_amg_refresh_fine": [ct.POINTER(PhbAmg), P],
         "phb_transpose_stencil": [DP, P, P, P],
         "phb_stencil_apply": [DP, P, P, P, ct.c_int32, I64, P],
         "phb_projection_gram": [P, P, P, ct.c_int32, I64, I64, P, P, P],

@@ -102,6 +102,9 @@ class AmgHierarchy:
         self.options = opts
         self.domain = domain
         self.version = None  # the matrix version the operators were set up from
+        # setups since the last full one, the coarse operators marked stale, the baseline
+        # iterations of the solves after the last full setup, full setups so far
+        self.refreshes, self.stale, self.baseline_iterations, self.full_setups = 0, False, None, 0
         dev = domain.getDevice()
         dims = domain.getSpatialDims()
         blocks, insts = domain._blocks_host.numpy(), domain._insts_host.numpy()
@@ -204,18 +207,38 @@ class AmgHierarchy:
     def address(self) -> int:
         return ct.addressof(self._struct)
 
-    def setup(self, A32: torch.Tensor, version=None) -> None:
+    def setup(self, A32: torch.Tensor, version=None, coarse: bool = True) -> None:
         """Coarse operators of the float32 fine stencil ``A32`` [2d+1][ncells] (on the
-        domain's current stream; the hierarchy keeps a reference to ``A32``)."""
+        domain's current stream; the hierarchy keeps a reference to ``A32``). With
+        ``coarse=False`` only the finest level follows ``A32`` (its smoother); the coarse
+        operators of the last full setup are kept (phiPICT's galerkin_refresh(..., coarse=False),
+        solvers/amg.py:749)."""
         if A32.dtype != torch.float32 or not A32.is_contiguous():
             raise TypeError("the multigrid hierarchy is built from a contiguous float32 stencil")
         if A32.numel() != (2 * self.domain.getSpatialDims() + 1) * self.sizes[0]:
             raise ValueError("stencil size does not match the domain")
+        coarse = coarse or self._A0 is not A32 or self.version is None
         self._A0 = A32
         self.level_A[0] = A32
         self._struct.levels[0].A = A32.data_ptr()
-        _lib.call("phb_amg_setup", ct.byref(self._struct), _lib.stream_ptr(self.domain.getDevice()))
+        name = "phb_amg_setup" if coarse else "phb_amg_refresh_fine"
+        _lib.call(name, ct.byref(self._struct), _lib.stream_ptr(self.domain.getDevice()))
         self.version = version
+        if coarse:
+            self.refreshes, self.stale, self.baseline_iterations = 0, False, None
+            self.full_setups += 1
+        self.refreshes += 1
+
+    def note_iterations(self, iterations: int) -> None:
+        """Iterations of a solve with this hierarchy (core/piso_simulation.py:2376-2392): the
+        solves after a full setup set the baseline, and a later solve needing more than twice
+        the baseline plus 5 marks the coarse operators stale, so that the next change of the
+        matrix sets the whole hierarchy up again."""
+        if self.baseline_iterations is None or self.refreshes <= 1:
+            b = self.baseline_iterations
+            self.baseline_iterations = iterations if b is None else max(b, iterations)
+        elif iterations > 2 * self.baseline_iterations + 5:
+            self.stale = True
 
     def vcycle(self, r: torch.Tensor, z: torch.Tensor | None = None) -> torch.Tensor:
         """z = one V-cycle applied to the float32 residual r."""
@@ -231,17 +254,24 @@ class AmgHierarchy:
         return f"AmgHierarchy(levels={self.sizes}, coarse_n={self.coarse_n}, options={self.options})"
 
 
-def hierarchy_for(domain, which: str, A32: torch.Tensor, version, cache: dict, options: dict | None = None) -> AmgHierarchy:
+def hierarchy_for(domain, which: str, A32: torch.Tensor, version, cache: dict, options: dict | None = None,
+                  coarse_refresh_interval: int = 1) -> AmgHierarchy:
     """The cached hierarchy of matrix ``which`` of ``domain``, rebuilt for a new grid and
     set up again when the matrix version changed (phiPICT's fingerprint refresh,
-    core/piso_simulation.py:2222-2300)."""
+    core/piso_simulation.py:2222-2300). ``options["coarse_refresh_interval"]`` (else the
+    argument) n > 1: the whole hierarchy is set up on every n-th change of the matrix and
+    when its coarse operators were marked stale; in between only the finest level follows
+    (core/piso_simulation.py:1042-1046,2268-2297)."""
+    options = dict(options or {})
+    interval = int(options.pop("coarse_refresh_interval", coarse_refresh_interval))
     h = cache.get(which)
     # PrepareSolve re-creates the domain's records, which level 0 points at
     if h is None or h.domain is not domain or h._fine_blocks is not domain._blocks_dev:
-        h = AmgHierarchy(domain, **(options or {}))
+        h = AmgHierarchy(domain, **options)
         cache[which] = h
     if h.version != version or h._A0 is not A32:
-        h.setup(A32, version)
+        coarse = interval <= 1 or h.refreshes % interval == 0 or h.stale
+        h.setup(A32, version, coarse=coarse)
     return h
 
 

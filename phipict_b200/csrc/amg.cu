@@ -454,6 +454,16 @@ extern "C" int phb_amg_setup(const phb_amg *amg, phb_stream stream) {
 	return amg->levels[0].dom.dims == 2 ? setup<2>(amg, s) : setup<3>(amg, s);
 }
 
+extern "C" int phb_amg_refresh_fine(const phb_amg *amg, phb_stream stream) {
+	const int rc = phbCheckAmg(amg);
+	if (rc) return rc;
+	const phb_amg_level &v = amg->levels[0];
+	const int64_t n = v.dom.ncells;
+	if (n == 0) return PHB_OK;
+	kWdinv<<<(int)std::min<int64_t>((n + 255) / 256, 148 * 8), 256, 0, (cudaStream_t)stream>>>(n, v.A, v.wdinv, amg->omega);
+	return checkLaunch("kWdinv");
+}
+
 extern "C" int phb_amg_vcycle(const phb_amg *amg, const float *r, float *z, phb_stream stream) {
 	const int rc = phbCheckAmg(amg);
 	if (rc) return rc;

@@ -451,7 +451,10 @@ class Simulation:
         if self._amg_cache.get(("unavailable", which)) is d._blocks_dev:
             return None
         try:
-            return hierarchy_for(d, which, A32, d._matrix_version(which), self._amg_cache, self._amg_options(which))
+            # the pressure matrix changes every step: phiPICT's default coarse_refresh_interval
+            # of 4 for it (core/piso_simulation.py:2268)
+            return hierarchy_for(d, which, A32, d._matrix_version(which), self._amg_cache, self._amg_options(which),
+                                 coarse_refresh_interval=4 if which == "P" else 1)
         except ValueError:
             self._amg_cache[("unavailable", which)] = d._blocks_dev
             return None
@@ -466,6 +469,11 @@ class Simulation:
             good = all(i.converged or (tag.startswith("epot") and self._accept_best(i)) for i in infos)
             if not good:
                 ok = False
+        h = self._amg_cache.get("P")
+        if h is not None:
+            for tag, infos in report:
+                if tag.startswith("pressure") and infos:
+                    h.note_iterations(max(i.innerIterations or i.usedIterations for i in infos))
         for k, tag, (ctas, e0, e1) in self._tuning:
             infos = report[k][1]
             its = max((i.innerIterations or i.usedIterations for i in infos), default=0)
