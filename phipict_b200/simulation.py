@@ -176,6 +176,8 @@ class ProjectedGuess:
 
             if A.dtype != torch.float64:
                 raise ValueError("projected guesses need a float64 matrix")
+            if x.numel() != int(domain.desc().ncells) or b.numel() != x.numel():
+                raise ValueError("projected guesses need one value per cell in x and b")
             _lib.call("phb_stencil_apply", ct.byref(domain.desc()), A.data_ptr(), V.data_ptr(), Y.data_ptr(), m,
                       V.stride(0), _lib.stream_ptr(x.device))
         if self._solve is not None:
