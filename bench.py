@@ -407,6 +407,8 @@ def run_ours(args, rank, world, local):
                             f"rtol 1e-10, {'mixed precision' if mixed else 'plain fp64'}"
                             f"{', multigrid-preconditioned pressure and potential CG' if amg else ''}",
                 "amg_levels": levels,
+                "amg_refresh": ("full pressure multigrid setup on every 4th matrix change, the finest level "
+                                "in between (coarse_refresh_interval 4)") if amg else None,
                 "initial_guesses": (guess_label(args.extrapolate_order) if args.extrapolate and mixed else
                                     "previous step's pressure" if args.pressure_warm_start else
                                     "zero pressure, previous step's potential"),
